@@ -1,0 +1,305 @@
+"""ctypes binding of libapcloud_gpu.so (include/apcloud_gpu.h).
+
+The GPU path has no fallback: if the library or a CUDA device is missing, construction
+raises.  ``GpuPath`` exposes the phase calls of the reference's Mover / Solver
+(mover.h:31-43, solver.h:53-62) with host numpy arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "libapcloud_gpu.so")
+
+APC_PREC_FP64 = 0
+APC_PREC_MIXED = 1
+
+EXPORTED = [
+    "apc_config_default", "apc_status_string", "apc_last_error", "apc_create", "apc_destroy",
+    "apc_set_particles", "apc_get_particles", "apc_set_particles_device", "apc_get_particles_device",
+    "apc_select", "apc_solve", "apc_move_velocity", "apc_move_position", "apc_step", "apc_synchronize",
+    "apc_get_cell_counts", "apc_get_cells", "apc_get_cell_codes", "apc_get_keys", "apc_get_octree_levels",
+    "apc_get_fields", "apc_get_stencils", "apc_get_solve_stats", "apc_get_matrix", "apc_kernel_launches",
+    "apc_get_phase_times",
+]
+
+
+class ApcConfig(C.Structure):
+    _fields_ = [
+        ("n_particles", C.c_int), ("depth", C.c_int), ("bc", C.c_int), ("box", C.c_double * 6),
+        ("gfd_c", C.c_double), ("lm", C.c_int), ("maxnc", C.c_int), ("nmax_cap", C.c_int),
+        ("gmres_restart", C.c_int), ("gmres_rtol", C.c_double), ("gmres_atol", C.c_double),
+        ("gmres_dtol", C.c_double), ("gmres_max_it", C.c_int), ("precision", C.c_int),
+        ("mixed_restart", C.c_int), ("mixed_inner_rtol", C.c_double), ("device", C.c_int),
+    ]
+
+
+class ApcSolveStats(C.Structure):
+    _fields_ = [
+        ("density_its", C.c_int), ("potential_its", C.c_int),
+        ("density_reason", C.c_int), ("potential_reason", C.c_int),
+        ("density_rnorm", C.c_double), ("potential_rnorm", C.c_double),
+        ("density_refinements", C.c_int), ("potential_refinements", C.c_int),
+    ]
+
+
+class ApcStepParams(C.Structure):
+    _fields_ = [("dt", C.c_double), ("c_dens", C.c_double), ("c_pot", C.c_double),
+                ("c_field", C.c_double), ("c_vel", C.c_double), ("c_pos", C.c_double)]
+
+
+class ApcError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str):
+        super().__init__(f"{where}: status {status} ({msg})")
+        self.status = status
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the CUDA library; raises if it is missing (no CPU fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with ap-cloud-cosmology_b200/build.py")
+    lib = C.CDLL(path)
+    vp, ip, dp, u64p = C.c_void_p, C.POINTER(C.c_int), C.c_void_p, C.c_void_p
+    sig = {
+        "apc_config_default": (None, [C.POINTER(ApcConfig)]),
+        "apc_status_string": (C.c_char_p, [C.c_int]),
+        "apc_last_error": (C.c_char_p, [vp]),
+        "apc_create": (C.c_int, [C.POINTER(ApcConfig), C.POINTER(C.c_void_p)]),
+        "apc_destroy": (C.c_int, [vp]),
+        "apc_set_particles": (C.c_int, [vp] + [dp] * 6),
+        "apc_get_particles": (C.c_int, [vp] + [dp] * 9),
+        "apc_set_particles_device": (C.c_int, [vp] + [dp] * 6),
+        "apc_get_particles_device": (C.c_int, [vp] + [dp] * 6),
+        "apc_select": (C.c_int, [vp, ip]),
+        "apc_solve": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),
+        "apc_move_velocity": (C.c_int, [vp, C.c_double, C.c_double, C.POINTER(C.c_double)]),
+        "apc_move_position": (C.c_int, [vp, C.c_double, C.c_double, C.POINTER(C.c_double)]),
+        "apc_step": (C.c_int, [vp, C.POINTER(ApcStepParams), ip, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "apc_synchronize": (C.c_int, [vp]),
+        "apc_get_cell_counts": (C.c_int, [vp, ip, ip, ip, ip]),
+        "apc_get_cells": (C.c_int, [vp] + [dp] * 4 + [vp] * 6),
+        "apc_get_cell_codes": (C.c_int, [vp, u64p]),
+        "apc_get_keys": (C.c_int, [vp, u64p, vp]),
+        "apc_get_octree_levels": (C.c_int, [vp, vp]),
+        "apc_get_fields": (C.c_int, [vp, dp, dp, dp]),
+        "apc_get_stencils": (C.c_int, [vp, vp, dp]),
+        "apc_get_solve_stats": (C.c_int, [vp, C.POINTER(ApcSolveStats)]),
+        "apc_get_matrix": (C.c_int, [vp, C.c_int, ip, ip, vp, vp, vp]),
+        "apc_kernel_launches": (C.c_int64, [vp]),
+        "apc_get_phase_times": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data
+
+
+@dataclass
+class GpuCells:
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    h: np.ndarray
+    first: np.ndarray
+    count: np.ndarray
+    type: np.ndarray
+    firstneigh: np.ndarray
+    numneigh: np.ndarray
+    neigh24: np.ndarray
+    nc: int
+    nv: int
+    nb: int
+
+    @property
+    def m(self) -> int:
+        return self.nc + self.nv
+
+
+@dataclass
+class GpuFields:
+    density: np.ndarray
+    potential: np.ndarray
+    deriv: np.ndarray
+
+
+class GpuPath:
+    """One particle set resident on the GPU, driven phase by phase through the C ABI."""
+
+    def __init__(self, parts, depth: int, gfd_c: float, lm: int = 17,
+                 box=(0.0, 1.0, 0.0, 1.0, 0.0, 1.0), bc: int = 1, precision: int = APC_PREC_FP64,
+                 restart: int = 30, rtol: float = 1e-10, atol: float = 1e-50, dtol: float = 1e5,
+                 max_it: int = 10000, mixed_restart: int = 0, mixed_inner_rtol: float = 0.0,
+                 device: int = 0, maxnc: int = 10000, nmax_cap: int = 0):
+        self.lib = load_library()
+        cfg = ApcConfig()
+        self.lib.apc_config_default(C.byref(cfg))
+        cfg.n_particles = parts.n
+        cfg.depth = depth
+        cfg.bc = bc
+        for k in range(6):
+            cfg.box[k] = box[k]
+        cfg.gfd_c = gfd_c
+        cfg.lm = lm
+        cfg.maxnc = maxnc
+        cfg.nmax_cap = nmax_cap
+        cfg.gmres_restart = restart
+        cfg.gmres_rtol = rtol
+        cfg.gmres_atol = atol
+        cfg.gmres_dtol = dtol
+        cfg.gmres_max_it = max_it
+        cfg.precision = precision
+        cfg.mixed_restart = mixed_restart
+        cfg.mixed_inner_rtol = mixed_inner_rtol
+        cfg.device = device
+        self.cfg = cfg
+        self.n = parts.n
+        self.depth = depth
+        self.lm = lm
+        h = C.c_void_p()
+        self._check(self.lib.apc_create(C.byref(cfg), C.byref(h)), "apc_create", None)
+        self.h = h
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in parts.as_tuple()]
+        self._check(self.lib.apc_set_particles(self.h, *[_ptr(a) for a in arrs]), "apc_set_particles")
+
+    def _check(self, rc: int, where: str, h="self"):
+        if rc != 0:
+            msg = self.lib.apc_status_string(rc).decode()
+            if h == "self" and getattr(self, "h", None):
+                detail = self.lib.apc_last_error(self.h).decode()
+                if detail:
+                    msg += "; " + detail
+            raise ApcError(rc, where, msg)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.apc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- phases ----
+    def select(self) -> int:
+        m = C.c_int()
+        self._check(self.lib.apc_select(self.h, C.byref(m)), "apc_select")
+        return m.value
+
+    def solve(self, c_dens: float, c_pot: float, c_field: float = -1.0) -> int:
+        self._check(self.lib.apc_solve(self.h, c_dens, c_pot, c_field), "apc_solve")
+        return 0
+
+    def move_velocity(self, dt: float, c_vel: float) -> float:
+        d = C.c_double()
+        self._check(self.lib.apc_move_velocity(self.h, dt, c_vel, C.byref(d)), "apc_move_velocity")
+        return d.value
+
+    def move_position(self, dt: float, c_pos: float) -> float:
+        d = C.c_double()
+        self._check(self.lib.apc_move_position(self.h, dt, c_pos, C.byref(d)), "apc_move_position")
+        return d.value
+
+    def step(self, dt, c_dens, c_pot, c_field, c_vel, c_pos):
+        p = ApcStepParams(dt, c_dens, c_pot, c_field, c_vel, c_pos)
+        m, dv, dx = C.c_int(), C.c_double(), C.c_double()
+        self._check(self.lib.apc_step(self.h, C.byref(p), C.byref(m), C.byref(dv), C.byref(dx)), "apc_step")
+        return m.value, dv.value, dx.value
+
+    def synchronize(self):
+        self._check(self.lib.apc_synchronize(self.h), "apc_synchronize")
+
+    # ---- results ----
+    def counts(self):
+        nc, nv, nb, nn = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        self._check(self.lib.apc_get_cell_counts(self.h, C.byref(nc), C.byref(nv), C.byref(nb), C.byref(nn)),
+                    "apc_get_cell_counts")
+        return nc.value, nv.value, nb.value, nn.value
+
+    def cells(self) -> GpuCells:
+        nc, nv, nb, nn = self.counts()
+        m = nc + nv
+        d = [np.zeros(m) for _ in range(4)]
+        i = [np.zeros(m, np.int32) for _ in range(5)]
+        nb24 = np.zeros(max(nn, 1), np.int32)
+        self._check(self.lib.apc_get_cells(self.h, *[_ptr(a) for a in d], *[_ptr(a) for a in i], _ptr(nb24)),
+                    "apc_get_cells")
+        return GpuCells(*d, *i, nb24[:nn], nc, nv, nb)
+
+    def codes(self) -> np.ndarray:
+        nc, nv, _, _ = self.counts()
+        out = np.zeros(nc + nv, np.uint64)
+        self._check(self.lib.apc_get_cell_codes(self.h, _ptr(out)), "apc_get_cell_codes")
+        return out
+
+    def keys(self):
+        k = np.zeros(self.n, np.uint64)
+        idx = np.zeros(self.n, np.int32)
+        self._check(self.lib.apc_get_keys(self.h, _ptr(k), _ptr(idx)), "apc_get_keys")
+        return k, idx
+
+    def octree_levels(self):
+        nn = np.zeros(self.depth + 1, np.int32)
+        self._check(self.lib.apc_get_octree_levels(self.h, _ptr(nn)), "apc_get_octree_levels")
+        return nn
+
+    def fields(self) -> GpuFields:
+        nc, nv, _, _ = self.counts()
+        m = nc + nv
+        rho, phi, der = np.zeros(m), np.zeros(m), np.zeros(9 * m)
+        self._check(self.lib.apc_get_fields(self.h, _ptr(rho), _ptr(phi), _ptr(der)), "apc_get_fields")
+        return GpuFields(rho, phi, der.reshape(m, 9))
+
+    def stencils(self):
+        nc, nv, _, _ = self.counts()
+        m = nc + nv
+        idx = np.zeros(m * self.lm, np.int32)
+        dist = np.zeros(m * self.lm)
+        self._check(self.lib.apc_get_stencils(self.h, _ptr(idx), _ptr(dist)), "apc_get_stencils")
+        return idx.reshape(m, self.lm), dist.reshape(m, self.lm)
+
+    def solve_stats(self) -> dict:
+        st = ApcSolveStats()
+        self._check(self.lib.apc_get_solve_stats(self.h, C.byref(st)), "apc_get_solve_stats")
+        return {f: getattr(st, f) for f, _ in ApcSolveStats._fields_}
+
+    def matrix(self, which: int):
+        n, nnz = C.c_int(), C.c_int()
+        self._check(self.lib.apc_get_matrix(self.h, which, C.byref(n), C.byref(nnz), None, None, None),
+                    "apc_get_matrix")
+        rp = np.zeros(n.value + 1, np.int32)
+        ci = np.zeros(max(nnz.value, 1), np.int32)
+        v = np.zeros(max(nnz.value, 1))
+        self._check(self.lib.apc_get_matrix(self.h, which, None, None, _ptr(rp), _ptr(ci), _ptr(v)),
+                    "apc_get_matrix")
+        return rp, ci[: nnz.value], v[: nnz.value]
+
+    def particles(self):
+        out = [np.zeros(self.n) for _ in range(9)]
+        self._check(self.lib.apc_get_particles(self.h, *[_ptr(a) for a in out]), "apc_get_particles")
+        return out
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.apc_kernel_launches(self.h))
+
+    def phase_times(self):
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        self._check(self.lib.apc_get_phase_times(self.h, C.byref(a), C.byref(b), C.byref(c)), "apc_get_phase_times")
+        return a.value, b.value, c.value

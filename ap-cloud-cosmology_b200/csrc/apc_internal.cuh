@@ -1,0 +1,223 @@
+// Internal declarations shared by the CUDA translation units of libapcloud_gpu.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/apcloud_gpu.h"
+
+// ------------------------------------------------------------------ errors
+
+// device-side error flags (bit set), read back by the host after each phase
+enum : int {
+  DERR_HASH_FULL = 1,      // a hash table probe ran past its bound
+  DERR_STENCIL_FEW = 2,    // < lm candidates after 5 expansions
+  DERR_STENCIL_MANY = 4,   // candidate buffers overflowed
+  DERR_RANK = 8,           // zero diagonal in R of a GFD least-squares system
+  DERR_NEIGH = 16,         // a face neighbour required by 2:1 balance was not found
+  DERR_NOT_FINITE = 32,
+  DERR_KRYLOV = 64,
+};
+
+#define APC_CUDA_TRY(ctx, call)                                                      \
+  do {                                                                               \
+    cudaError_t e__ = (call);                                                        \
+    if (e__ != cudaSuccess) {                                                        \
+      (ctx)->err = std::string(#call) + ": " + cudaGetErrorString(e__);              \
+      return APC_ERR_CUDA;                                                           \
+    }                                                                                \
+  } while (0)
+
+#define APC_TRY(...)                  \
+  do {                                \
+    int rc__ = (__VA_ARGS__);         \
+    if (rc__ != APC_OK) return rc__;  \
+  } while (0)
+
+// ----------------------------------------------------------------- context
+
+struct KrylovWork;  // krylov.cu
+
+struct apc_context {
+  apc_config cfg{};
+  int dev = 0;
+  cudaStream_t s = nullptr;
+  std::string err;
+  int64_t launches = 0;
+  bool have_particles = false, have_cells = false, have_fields = false;
+
+  // ---- particles, kept in Morton (sorted) order on the device ----
+  int n = 0;
+  double *px = nullptr, *py = nullptr, *pz = nullptr, *pvx = nullptr, *pvy = nullptr, *pvz = nullptr;
+  double *pax = nullptr, *pay = nullptr, *paz = nullptr;
+  int *pid = nullptr;  // caller index of each sorted particle
+  double *qx = nullptr, *qy = nullptr, *qz = nullptr, *qvx = nullptr, *qvy = nullptr, *qvz = nullptr;
+  int *qid = nullptr;
+  uint64_t *keys = nullptr, *keys_alt = nullptr;
+  uint32_t *perm = nullptr, *perm_alt = nullptr;
+  uint32_t *sort_hist = nullptr;
+  int sort_blocks = 0;
+  double *reduce_buf = nullptr;  // per-block partial maxima of the mover
+
+  // ---- selection ----
+  double h0 = 1.0, hx0 = 1.0, hy0 = 1.0, hz0 = 1.0;  // root cell sizes (octree.cpp:1127-1131)
+  double cx0 = 0.5, cy0 = 0.5, cz0 = 0.5;              // root centre (octree.cpp:1117-1119)
+  int hcap = 0;                  // opened-node hash capacity (power of two)
+  uint64_t *h_keys = nullptr;    // opened-node hash: location code
+  int *h_vals = nullptr;         //                   index into the opened list
+  int rcap = 0;                  // request hash capacity
+  uint64_t *r_keys = nullptr, *r_vals = nullptr;
+  int lcap = 0;                  // leaf hash capacity
+  uint64_t *l_keys = nullptr;
+  int *l_vals = nullptr;
+  int op_cap = 0;                // opened list capacity
+  uint64_t *op_code = nullptr;   // opened nodes: td in BFS order, then balance events in order
+  int *op_base = nullptr;        // temp index of the node's first child
+  int *op_first = nullptr, *op_count = nullptr;  // particle range (all opened nodes)
+  int n_open_td = 0, n_open = 0;
+  std::vector<int> td_level_off;  // [level] -> offset of level's td-opened nodes; size depth+2
+  uint64_t *req_key = nullptr, *req_key_alt = nullptr;  // balance requests: first-requester key
+  uint32_t *req_idx = nullptr, *req_idx_alt = nullptr;  //                   sort payload
+  uint64_t *req_code = nullptr;                         //                   requested cell
+  int *req_pos = nullptr;        // scan output of per-(node, octant) flags
+  long long maxnc_state = 10000; // temp-node budget, doubled like Mover::maxnc (mover.cpp:36-41)
+  int *counters = nullptr;       // small device counters
+  int *d_err = nullptr;          // device error flags
+  int *h_pinned = nullptr;       // pinned host mirror for small readbacks
+  int *scan_tmp = nullptr;
+  int scan_tmp_cap = 0;
+  int *flags = nullptr;          // per-(opened node, octant) flags / scan
+  int flags_cap = 0;
+  std::vector<int> numnodes;     // octree level sizes of the last build
+
+  // ---- cells (Computational_particle) in the reference's output order ----
+  int nc = 0, nv = 0, nb = 0, m_cap = 0;
+  double *cx = nullptr, *cy = nullptr, *cz = nullptr, *ch = nullptr;
+  int *cfirst = nullptr, *ccount = nullptr, *ctype = nullptr;
+  uint64_t *ccode = nullptr;
+  int *nb24 = nullptr;   // 24 per cell
+  int *nnb = nullptr;    // Neigh24 count per cell
+  int *cell_of = nullptr;  // sorted particle -> cell
+
+  // ---- GFD / solver ----
+  int lm = 17;
+  int *st_idx = nullptr;     // lm per cell
+  double *st_dist = nullptr; // lm per cell
+  double *gfd_x = nullptr;   // 9 x lm least-squares operator per cell
+  int ell_w = 18;            // ELL width lm + 1
+  int *ell_col = nullptr;    // [slot][row]
+  double *a1 = nullptr, *a2 = nullptr;  // [slot][row]
+  float *a1f = nullptr, *a2f = nullptr;
+  double *rhs = nullptr, *bcrhs = nullptr;
+  double *density = nullptr, *potential = nullptr, *deriv = nullptr;
+  double rot[9] = {0};       // octant rotation (solver.cpp:464-475), host-computed
+  KrylovWork *kw = nullptr;
+  apc_solve_stats stats{};
+
+  // ---- timing ----
+  cudaEvent_t ev[8] = {};
+  double t_select_ms = 0, t_solve_ms = 0, t_move_ms = 0;
+};
+
+// ----------------------------------------------------------- helpers (host)
+
+int apc_alloc(apc_context *c, void **p, size_t bytes);
+template <class T>
+int apc_ensure(apc_context *c, T **p, size_t count, size_t *cap_elems_io = nullptr);
+int apc_read_errors(apc_context *c, int *flags);
+
+// launch accounting
+inline void apc_count_launch(apc_context *c, int k = 1) { c->launches += k; }
+
+// subsystem entry points (each in its own .cu)
+int apc_octree_build(apc_context *c);        // keys, sort, permute (octree_build.cu)
+int apc_octree_levels_count(apc_context *c); // numnodes per level (octree_build.cu)
+int apc_selection(apc_context *c);           // top-down + balance + cells (selection.cu)
+int apc_gfd_assemble(apc_context *c, double c_dens);    // gfd.cu
+int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int *its,
+                     double *rnorm, int *reason, int *refinements);  // krylov.cu
+void apc_krylov_free(apc_context *c);
+int apc_potential_rhs(apc_context *c, double c_pot);    // gfd.cu
+int apc_differentiate(apc_context *c, double c_field);  // gfd.cu
+int apc_mover_velocity(apc_context *c, double dt, double c_vel, double *max_dv);  // mover.cu
+int apc_mover_position(apc_context *c, double dt, double c_pos, double *max_dx);  // mover.cu
+int apc_exclusive_scan(apc_context *c, const int *in, int *out, int n, int *total_dev);  // scan.cu
+int apc_radix_sort_u64(apc_context *c, uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
+                       uint32_t *vals_alt, int n, int lo_bit, int hi_bit, bool *result_in_alt);
+
+// grid sizing: a multiple of the SM count
+int apc_sm_count(apc_context *c);
+
+// ------------------------------------------------------- device helpers
+
+#ifdef __CUDACC__
+__device__ __forceinline__ int code_level(uint64_t code) {
+  // code = (1 << 3L) | prefix: L = (63 - clz) / 3
+  return (63 - __clzll((long long)code)) / 3;
+}
+
+__device__ __forceinline__ uint64_t hash_mix(uint64_t k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdULL;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ULL;
+  k ^= k >> 33;
+  return k;
+}
+
+// open-addressing hash set/map over location codes (0 = empty slot); bounded probing
+constexpr int kMaxProbe = 4096;
+
+__device__ __forceinline__ int hash_find(const uint64_t *keys, int cap, uint64_t code) {
+  uint32_t m = (uint32_t)cap - 1u;
+  uint32_t h = (uint32_t)hash_mix(code) & m;
+  for (int p = 0; p < kMaxProbe; ++p) {
+    uint64_t k = keys[h];
+    if (k == code) return (int)h;
+    if (k == 0) return -1;
+    h = (h + 1) & m;
+  }
+  return -1;
+}
+
+// insert; returns slot, sets *fresh when this call created the entry; -1 on overflow
+__device__ __forceinline__ int hash_insert(uint64_t *keys, int cap, uint64_t code, bool *fresh) {
+  uint32_t m = (uint32_t)cap - 1u;
+  uint32_t h = (uint32_t)hash_mix(code) & m;
+  *fresh = false;
+  for (int p = 0; p < kMaxProbe; ++p) {
+    unsigned long long prev =
+        atomicCAS((unsigned long long *)&keys[h], 0ULL, (unsigned long long)code);
+    if (prev == 0ULL) {
+      *fresh = true;
+      return (int)h;
+    }
+    if (prev == code) return (int)h;
+    h = (h + 1) & m;
+  }
+  return -1;
+}
+
+// Morton helpers: spread / compact 21-bit integers over every third bit
+__device__ __forceinline__ uint64_t spread3(uint64_t v) {
+  v &= 0x1fffffULL;
+  v = (v | v << 32) & 0x1f00000000ffffULL;
+  v = (v | v << 16) & 0x1f0000ff0000ffULL;
+  v = (v | v << 8) & 0x100f00f00f00f00fULL;
+  v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+  v = (v | v << 2) & 0x1249249249249249ULL;
+  return v;
+}
+__device__ __forceinline__ uint64_t compact3(uint64_t v) {
+  v &= 0x1249249249249249ULL;
+  v = (v ^ (v >> 2)) & 0x10c30c30c30c30c3ULL;
+  v = (v ^ (v >> 4)) & 0x100f00f00f00f00fULL;
+  v = (v ^ (v >> 8)) & 0x1f0000ff0000ffULL;
+  v = (v ^ (v >> 16)) & 0x1f00000000ffffULL;
+  v = (v ^ (v >> 32)) & 0x1fffffULL;
+  return v;
+}
+#endif

@@ -1,0 +1,536 @@
+// C ABI of libapcloud_gpu.so: context lifetime, particle I/O, the four phases of
+// Controller::solve (controller.cpp:133-197) and the result accessors.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+#include "apc_internal.cuh"
+
+// --------------------------------------------------------------- allocation
+
+namespace {
+struct CapTable {
+  std::unordered_map<const void *, size_t> cap;  // keyed by the address of the owning pointer
+};
+std::unordered_map<const apc_context *, CapTable> g_caps;
+}  // namespace
+
+int apc_alloc(apc_context *c, void **p, size_t bytes) {
+  *p = nullptr;
+  cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    c->err = std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? APC_ERR_OUT_OF_MEMORY : APC_ERR_CUDA;
+  }
+  return APC_OK;
+}
+
+template <class T>
+int apc_ensure(apc_context *c, T **p, size_t count, size_t *) {
+  CapTable &ct = g_caps[c];
+  size_t &cap = ct.cap[(const void *)p];
+  if (*p && cap >= count) return APC_OK;
+  if (*p) {
+    cudaStreamSynchronize(c->s);
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  size_t want = std::max<size_t>(count + count / 4, 64);
+  APC_TRY(apc_alloc(c, (void **)p, want * sizeof(T)));
+  cap = want;
+  return APC_OK;
+}
+template int apc_ensure<double>(apc_context *, double **, size_t, size_t *);
+template int apc_ensure<float>(apc_context *, float **, size_t, size_t *);
+template int apc_ensure<int>(apc_context *, int **, size_t, size_t *);
+template int apc_ensure<uint32_t>(apc_context *, uint32_t **, size_t, size_t *);
+template int apc_ensure<uint64_t>(apc_context *, uint64_t **, size_t, size_t *);
+
+int apc_read_errors(apc_context *c, int *flags) {
+  APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 1, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  *flags = c->h_pinned[1];
+  return APC_OK;
+}
+
+int apc_sm_count(apc_context *c) {
+  static int cached[64] = {0};
+  int d = c->dev;
+  if (d >= 0 && d < 64 && cached[d]) return cached[d];
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d);
+  if (v <= 0) v = 1;
+  if (d >= 0 && d < 64) cached[d] = v;
+  return v;
+}
+
+namespace {
+
+__global__ void iota_int(int n, int *p) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = i;
+}
+
+__global__ void unpermute(int n, const int *__restrict__ pid, const double *__restrict__ src, double *__restrict__ dst) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) dst[pid[s]] = src[s];
+}
+
+void free_all(apc_context *c) {
+  apc_krylov_free(c);
+  void *ptrs[] = {c->px, c->py, c->pz, c->pvx, c->pvy, c->pvz, c->pax, c->pay, c->paz, c->pid,
+                  c->qx, c->qy, c->qz, c->qvx, c->qvy, c->qvz, c->qid, c->keys, c->keys_alt, c->perm,
+                  c->perm_alt, c->sort_hist, c->reduce_buf, c->h_keys, c->h_vals, c->r_keys, c->r_vals,
+                  c->l_keys, c->l_vals, c->op_code, c->op_base, c->op_first, c->op_count, c->req_key,
+                  c->req_key_alt, c->req_idx, c->req_idx_alt, c->req_code, c->req_pos, c->counters,
+                  c->d_err, c->scan_tmp, c->flags, c->cx, c->cy, c->cz, c->ch, c->cfirst, c->ccount,
+                  c->ctype, c->ccode, c->nb24, c->nnb, c->cell_of, c->st_idx, c->st_dist, c->gfd_x,
+                  c->ell_col, c->a1, c->a2, c->a1f, c->a2f, c->rhs, c->bcrhs, c->density, c->potential,
+                  c->deriv};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  for (auto &e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->s) cudaStreamDestroy(c->s);
+  g_caps.erase(c);
+}
+
+int check_ready(apc_context *c, bool particles, bool cells, bool fields) {
+  if (!c) return APC_ERR_INVALID_ARG;
+  if ((particles && !c->have_particles) || (cells && !c->have_cells) || (fields && !c->have_fields)) {
+    c->err = "phase called before its inputs exist";
+    return APC_ERR_ORDER;
+  }
+  return APC_OK;
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------- API
+
+extern "C" {
+
+void apc_config_default(apc_config *cfg) {
+  if (!cfg) return;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->n_particles = 0;
+  cfg->depth = 21;
+  cfg->bc = 1;
+  cfg->box[0] = 0.0; cfg->box[1] = 1.0;
+  cfg->box[2] = 0.0; cfg->box[3] = 1.0;
+  cfg->box[4] = 0.0; cfg->box[5] = 1.0;
+  cfg->gfd_c = 5e-3;
+  cfg->lm = 17;
+  cfg->maxnc = 10000;
+  cfg->nmax_cap = 0;
+  cfg->gmres_restart = 30;
+  cfg->gmres_rtol = 1e-10;
+  cfg->gmres_atol = 1e-50;
+  cfg->gmres_dtol = 1e5;
+  cfg->gmres_max_it = 10000;
+  cfg->precision = APC_PREC_FP64;
+  cfg->mixed_restart = 0;
+  cfg->mixed_inner_rtol = 0.0;
+  cfg->device = 0;
+}
+
+const char *apc_status_string(int s) {
+  switch (s) {
+    case APC_OK: return "ok";
+    case APC_ERR_INVALID_ARG: return "invalid argument";
+    case APC_ERR_CUDA: return "CUDA error";
+    case APC_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case APC_ERR_ORDER: return "phase called out of order";
+    case APC_ERR_NMAX: return "temp-node budget exceeded";
+    case APC_ERR_STENCIL: return "GFD neighbour search failed";
+    case APC_ERR_RANK: return "rank-deficient GFD least squares";
+    case APC_ERR_NOT_FINITE: return "non-finite particle coordinates";
+    case APC_ERR_UNSUPPORTED: return "unsupported configuration";
+    case APC_ERR_TIMEOUT: return "device wait timed out";
+    default: return "unknown status";
+  }
+}
+
+const char *apc_last_error(const apc_context *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+int apc_create(const apc_config *cfg, apc_context **out) {
+  if (!cfg || !out) return APC_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (cfg->n_particles < 1 || cfg->depth < 1 || cfg->depth > 21 || cfg->lm < 9 || cfg->lm > 32 ||
+      (cfg->bc != 0 && cfg->bc != 1) || !(cfg->gfd_c >= 0.0) || cfg->gmres_restart < 1 ||
+      cfg->gmres_restart > 31 || cfg->mixed_restart < 0 || cfg->mixed_restart > 31 ||
+      (cfg->precision != APC_PREC_FP64 && cfg->precision != APC_PREC_MIXED))
+    return APC_ERR_INVALID_ARG;
+  for (int d = 0; d < 3; ++d)
+    if (!(cfg->box[2 * d + 1] > cfg->box[2 * d])) return APC_ERR_INVALID_ARG;
+  if (cfg->bc != 1) return APC_ERR_UNSUPPORTED;
+  apc_context *c = new apc_context();
+  c->cfg = *cfg;
+  c->dev = cfg->device;
+  c->n = cfg->n_particles;
+  c->lm = cfg->lm;
+  c->maxnc_state = cfg->maxnc > 0 ? cfg->maxnc : 10000;
+  auto fail = [&](int rc) {
+    free_all(c);
+    delete c;
+    return rc;
+  };
+  if (cudaSetDevice(c->dev) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(APC_ERR_CUDA);
+  }
+  if (cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking) != cudaSuccess) return fail(APC_ERR_CUDA);
+  for (auto &e : c->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return fail(APC_ERR_CUDA);
+  if (cudaMallocHost((void **)&c->h_pinned, 64 * sizeof(int)) != cudaSuccess) return fail(APC_ERR_CUDA);
+  const size_t n = (size_t)c->n;
+  double **dbl[] = {&c->px, &c->py, &c->pz, &c->pvx, &c->pvy, &c->pvz, &c->pax, &c->pay, &c->paz,
+                    &c->qx, &c->qy, &c->qz, &c->qvx, &c->qvy, &c->qvz};
+  for (double **p : dbl) {
+    int rc = apc_alloc(c, (void **)p, n * sizeof(double));
+    if (rc) return fail(rc);
+  }
+  int rc;
+  if ((rc = apc_alloc(c, (void **)&c->pid, n * sizeof(int)))) return fail(rc);
+  if ((rc = apc_alloc(c, (void **)&c->qid, n * sizeof(int)))) return fail(rc);
+  if ((rc = apc_alloc(c, (void **)&c->keys, n * sizeof(uint64_t)))) return fail(rc);
+  if ((rc = apc_alloc(c, (void **)&c->keys_alt, n * sizeof(uint64_t)))) return fail(rc);
+  if ((rc = apc_alloc(c, (void **)&c->perm, n * sizeof(uint32_t)))) return fail(rc);
+  if ((rc = apc_alloc(c, (void **)&c->perm_alt, n * sizeof(uint32_t)))) return fail(rc);
+  if ((rc = apc_alloc(c, (void **)&c->counters, 256 * sizeof(int)))) return fail(rc);
+  if ((rc = apc_alloc(c, (void **)&c->d_err, 4 * sizeof(int)))) return fail(rc);
+  cudaMemsetAsync(c->d_err, 0, 4 * sizeof(int), c->s);
+  cudaMemsetAsync(c->pax, 0, n * sizeof(double), c->s);
+  cudaMemsetAsync(c->pay, 0, n * sizeof(double), c->s);
+  cudaMemsetAsync(c->paz, 0, n * sizeof(double), c->s);
+  // root cell geometry (octree.cpp:1117-1131): centre from the box, h0 = volume^(1/3)
+  const double *b = cfg->box;
+  c->hx0 = b[1] - b[0];
+  c->hy0 = b[3] - b[2];
+  c->hz0 = b[5] - b[4];
+  c->h0 = std::pow(c->hx0 * c->hy0 * c->hz0, 1.0 / 3);
+  c->cx0 = (b[1] + b[0]) / 2;
+  c->cy0 = (b[3] + b[2]) / 2;
+  c->cz0 = (b[5] + b[4]) / 2;
+  // octant rotation of the neighbour search (solver.cpp:464-475), evaluated once on the host
+  const double al = 0.01, be = 0.001, ga = 0.0001;
+  double *A = c->rot;
+  A[0] = std::cos(al) * std::cos(ga) - std::sin(al) * std::sin(be) * std::sin(ga);
+  A[1] = -std::sin(al) * std::cos(be);
+  A[2] = -std::cos(al) * std::sin(ga) - std::sin(al) * std::sin(be) * std::cos(ga);
+  A[3] = std::cos(al) * std::sin(be) * std::sin(ga) + std::sin(al) * std::cos(ga);
+  A[4] = std::cos(al) * std::cos(be);
+  A[5] = std::cos(al) * std::sin(be) * std::cos(ga) - std::sin(al) * std::sin(ga);
+  A[6] = std::cos(be) * std::sin(ga);
+  A[7] = -std::sin(be);
+  A[8] = std::cos(be) * std::cos(ga);
+  if (cudaStreamSynchronize(c->s) != cudaSuccess) return fail(APC_ERR_CUDA);
+  *out = c;
+  return APC_OK;
+}
+
+int apc_destroy(apc_context *c) {
+  if (!c) return APC_ERR_INVALID_ARG;
+  cudaSetDevice(c->dev);
+  cudaStreamSynchronize(c->s);
+  free_all(c);
+  delete c;
+  return APC_OK;
+}
+
+static int set_particles_impl(apc_context *c, const double *const *src, cudaMemcpyKind kind) {
+  if (!c) return APC_ERR_INVALID_ARG;
+  for (int k = 0; k < 6; ++k)
+    if (!src[k]) return APC_ERR_INVALID_ARG;
+  cudaSetDevice(c->dev);
+  const size_t bytes = sizeof(double) * (size_t)c->n;
+  double *dst[6] = {c->px, c->py, c->pz, c->pvx, c->pvy, c->pvz};
+  for (int k = 0; k < 6; ++k) APC_CUDA_TRY(c, cudaMemcpyAsync(dst[k], src[k], bytes, kind, c->s));
+  iota_int<<<std::max(1, std::min((c->n + 255) / 256, apc_sm_count(c) * 8)), 256, 0, c->s>>>(c->n, c->pid);
+  apc_count_launch(c);
+  APC_CUDA_TRY(c, cudaGetLastError());
+  c->have_particles = true;
+  c->have_cells = false;
+  c->have_fields = false;
+  return APC_OK;
+}
+
+int apc_set_particles(apc_context *c, const double *x, const double *y, const double *z, const double *vx,
+                      const double *vy, const double *vz) {
+  const double *s[6] = {x, y, z, vx, vy, vz};
+  return set_particles_impl(c, s, cudaMemcpyHostToDevice);
+}
+
+int apc_set_particles_device(apc_context *c, const double *x, const double *y, const double *z,
+                             const double *vx, const double *vy, const double *vz) {
+  const double *s[6] = {x, y, z, vx, vy, vz};
+  return set_particles_impl(c, s, cudaMemcpyDeviceToDevice);
+}
+
+static int get_particles_impl(apc_context *c, double *const *dst, int count, cudaMemcpyKind kind) {
+  APC_TRY(check_ready(c, true, false, false));
+  cudaSetDevice(c->dev);
+  const double *src[9] = {c->px, c->py, c->pz, c->pvx, c->pvy, c->pvz, c->pax, c->pay, c->paz};
+  const size_t bytes = sizeof(double) * (size_t)c->n;
+  const int G = std::max(1, std::min((c->n + 255) / 256, apc_sm_count(c) * 8));
+  // caller order: scatter through the particle ids into the spare buffer, then copy
+  for (int k = 0; k < count; ++k) {
+    if (!dst[k]) continue;
+    unpermute<<<G, 256, 0, c->s>>>(c->n, c->pid, src[k], c->qx);
+    apc_count_launch(c);
+    APC_CUDA_TRY(c, cudaMemcpyAsync(dst[k], c->qx, bytes, kind, c->s));
+  }
+  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  return APC_OK;
+}
+
+int apc_get_particles(apc_context *c, double *x, double *y, double *z, double *vx, double *vy, double *vz,
+                      double *ax, double *ay, double *az) {
+  double *d[9] = {x, y, z, vx, vy, vz, ax, ay, az};
+  return get_particles_impl(c, d, 9, cudaMemcpyDeviceToHost);
+}
+
+int apc_get_particles_device(apc_context *c, double *x, double *y, double *z, double *vx, double *vy,
+                             double *vz) {
+  double *d[6] = {x, y, z, vx, vy, vz};
+  return get_particles_impl(c, d, 6, cudaMemcpyDeviceToDevice);
+}
+
+int apc_select(apc_context *c, int *n_cells) {
+  APC_TRY(check_ready(c, true, false, false));
+  cudaSetDevice(c->dev);
+  c->err.clear();
+  c->have_cells = false;
+  c->have_fields = false;
+  APC_CUDA_TRY(c, cudaEventRecord(c->ev[0], c->s));
+  APC_CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->s));
+  APC_TRY(apc_octree_build(c));
+  int derr = 0;
+  APC_TRY(apc_read_errors(c, &derr));
+  if (derr & DERR_NOT_FINITE) {
+    c->err = "non-finite particle coordinates";
+    return APC_ERR_NOT_FINITE;
+  }
+  APC_TRY(apc_selection(c));
+  APC_CUDA_TRY(c, cudaEventRecord(c->ev[1], c->s));
+  APC_CUDA_TRY(c, cudaEventSynchronize(c->ev[1]));
+  c->t_select_ms = elapsed(c->ev[0], c->ev[1]);
+  c->numnodes.clear();
+  c->have_cells = true;
+  if (n_cells) *n_cells = c->nc + c->nv + c->nb;
+  return APC_OK;
+}
+
+int apc_solve(apc_context *c, double c_dens, double c_pot, double c_field) {
+  APC_TRY(check_ready(c, true, true, false));
+  cudaSetDevice(c->dev);
+  c->err.clear();
+  APC_CUDA_TRY(c, cudaEventRecord(c->ev[2], c->s));
+  APC_TRY(apc_gfd_assemble(c, c_dens));
+  const int M = c->nc + c->nv;
+  if (c->cfg.precision == APC_PREC_MIXED) {
+    APC_TRY(apc_ensure(c, &c->a1f, (size_t)c->m_cap * c->ell_w, nullptr));
+    APC_TRY(apc_ensure(c, &c->a2f, (size_t)c->m_cap * c->ell_w, nullptr));
+  }
+  apc_solve_stats &st = c->stats;
+  APC_TRY(apc_krylov_solve(c, 0, c->rhs, c->density, &st.density_its, &st.density_rnorm, &st.density_reason,
+                           &st.density_refinements));
+  APC_TRY(apc_potential_rhs(c, c_pot));
+  APC_TRY(apc_krylov_solve(c, 1, c->rhs, c->potential, &st.potential_its, &st.potential_rnorm,
+                           &st.potential_reason, &st.potential_refinements));
+  APC_TRY(apc_differentiate(c, c_field));
+  (void)M;
+  APC_CUDA_TRY(c, cudaEventRecord(c->ev[3], c->s));
+  APC_CUDA_TRY(c, cudaEventSynchronize(c->ev[3]));
+  c->t_solve_ms = elapsed(c->ev[2], c->ev[3]);
+  c->have_fields = true;
+  return APC_OK;
+}
+
+int apc_move_velocity(apc_context *c, double dt, double c_vel, double *max_dv) {
+  APC_TRY(check_ready(c, true, true, true));
+  cudaSetDevice(c->dev);
+  APC_CUDA_TRY(c, cudaEventRecord(c->ev[4], c->s));
+  APC_TRY(apc_mover_velocity(c, dt, c_vel, max_dv));
+  APC_CUDA_TRY(c, cudaEventRecord(c->ev[5], c->s));
+  return APC_OK;
+}
+
+int apc_move_position(apc_context *c, double dt, double c_pos, double *max_dx) {
+  APC_TRY(check_ready(c, true, false, false));
+  cudaSetDevice(c->dev);
+  APC_TRY(apc_mover_position(c, dt, c_pos, max_dx));
+  APC_CUDA_TRY(c, cudaEventRecord(c->ev[6], c->s));
+  APC_CUDA_TRY(c, cudaEventSynchronize(c->ev[6]));
+  if (cudaEventQuery(c->ev[4]) == cudaSuccess) c->t_move_ms = elapsed(c->ev[4], c->ev[6]);
+  return APC_OK;
+}
+
+int apc_step(apc_context *c, const apc_step_params *p, int *n_cells, double *max_dv, double *max_dx) {
+  if (!p) return APC_ERR_INVALID_ARG;
+  APC_TRY(apc_select(c, n_cells));
+  APC_TRY(apc_solve(c, p->c_dens, p->c_pot, p->c_field));
+  APC_TRY(apc_move_velocity(c, p->dt, p->c_vel, max_dv));
+  APC_TRY(apc_move_position(c, p->dt, p->c_pos, max_dx));
+  return APC_OK;
+}
+
+int apc_synchronize(apc_context *c) {
+  if (!c) return APC_ERR_INVALID_ARG;
+  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  return APC_OK;
+}
+
+int apc_get_cell_counts(apc_context *c, int *nc, int *nv, int *nb, int *n_neigh24) {
+  APC_TRY(check_ready(c, true, true, false));
+  if (nc) *nc = c->nc;
+  if (nv) *nv = c->nv;
+  if (nb) *nb = c->nb;
+  if (n_neigh24) {
+    const int M = c->nc + c->nv;
+    std::vector<int> nn(M);
+    APC_CUDA_TRY(c, cudaMemcpy(nn.data(), c->nnb, sizeof(int) * M, cudaMemcpyDeviceToHost));
+    long long s = 0;
+    for (int v : nn) s += v;
+    *n_neigh24 = (int)s;
+  }
+  return APC_OK;
+}
+
+int apc_get_cells(apc_context *c, double *x, double *y, double *z, double *cell_length, int *first, int *count,
+                  int *type, int *first_neigh, int *number_neigh, int *neigh24) {
+  APC_TRY(check_ready(c, true, true, false));
+  cudaSetDevice(c->dev);
+  const int M = c->nc + c->nv;
+  const size_t db = sizeof(double) * M, ib = sizeof(int) * M;
+  if (x) APC_CUDA_TRY(c, cudaMemcpy(x, c->cx, db, cudaMemcpyDeviceToHost));
+  if (y) APC_CUDA_TRY(c, cudaMemcpy(y, c->cy, db, cudaMemcpyDeviceToHost));
+  if (z) APC_CUDA_TRY(c, cudaMemcpy(z, c->cz, db, cudaMemcpyDeviceToHost));
+  if (cell_length) APC_CUDA_TRY(c, cudaMemcpy(cell_length, c->ch, db, cudaMemcpyDeviceToHost));
+  if (first) APC_CUDA_TRY(c, cudaMemcpy(first, c->cfirst, ib, cudaMemcpyDeviceToHost));
+  if (count) APC_CUDA_TRY(c, cudaMemcpy(count, c->ccount, ib, cudaMemcpyDeviceToHost));
+  if (type) APC_CUDA_TRY(c, cudaMemcpy(type, c->ctype, ib, cudaMemcpyDeviceToHost));
+  if (first_neigh || number_neigh || neigh24) {
+    std::vector<int> nn(M), nb((size_t)M * 24);
+    APC_CUDA_TRY(c, cudaMemcpy(nn.data(), c->nnb, ib, cudaMemcpyDeviceToHost));
+    APC_CUDA_TRY(c, cudaMemcpy(nb.data(), c->nb24, ib * 24, cudaMemcpyDeviceToHost));
+    int tot = 0;
+    for (int i = 0; i < M; ++i) {
+      if (first_neigh) first_neigh[i] = tot;
+      if (number_neigh) number_neigh[i] = nn[i];
+      if (neigh24)
+        for (int k = 0; k < nn[i]; ++k) neigh24[tot + k] = nb[(size_t)i * 24 + k];
+      tot += nn[i];
+    }
+  }
+  return APC_OK;
+}
+
+int apc_get_cell_codes(apc_context *c, uint64_t *codes) {
+  APC_TRY(check_ready(c, true, true, false));
+  if (!codes) return APC_ERR_INVALID_ARG;
+  APC_CUDA_TRY(c, cudaMemcpy(codes, c->ccode, sizeof(uint64_t) * (c->nc + c->nv), cudaMemcpyDeviceToHost));
+  return APC_OK;
+}
+
+int apc_get_keys(apc_context *c, uint64_t *keys, int *index) {
+  APC_TRY(check_ready(c, true, true, false));
+  if (keys) APC_CUDA_TRY(c, cudaMemcpy(keys, c->keys, sizeof(uint64_t) * c->n, cudaMemcpyDeviceToHost));
+  if (index) APC_CUDA_TRY(c, cudaMemcpy(index, c->pid, sizeof(int) * c->n, cudaMemcpyDeviceToHost));
+  return APC_OK;
+}
+
+int apc_get_octree_levels(apc_context *c, int *numnodes) {
+  APC_TRY(check_ready(c, true, true, false));
+  if (!numnodes) return APC_ERR_INVALID_ARG;
+  if (c->numnodes.empty()) APC_TRY(apc_octree_levels_count(c));
+  for (int k = 0; k <= c->cfg.depth; ++k) numnodes[k] = c->numnodes[k];
+  return APC_OK;
+}
+
+int apc_get_fields(apc_context *c, double *density, double *potential, double *deriv9) {
+  APC_TRY(check_ready(c, true, true, true));
+  const int M = c->nc + c->nv;
+  if (density) APC_CUDA_TRY(c, cudaMemcpy(density, c->density, sizeof(double) * M, cudaMemcpyDeviceToHost));
+  if (potential) APC_CUDA_TRY(c, cudaMemcpy(potential, c->potential, sizeof(double) * M, cudaMemcpyDeviceToHost));
+  if (deriv9) APC_CUDA_TRY(c, cudaMemcpy(deriv9, c->deriv, sizeof(double) * 9 * M, cudaMemcpyDeviceToHost));
+  return APC_OK;
+}
+
+int apc_get_stencils(apc_context *c, int *idx, double *dist) {
+  APC_TRY(check_ready(c, true, true, true));
+  const size_t k = (size_t)(c->nc + c->nv) * c->lm;
+  if (idx) APC_CUDA_TRY(c, cudaMemcpy(idx, c->st_idx, sizeof(int) * k, cudaMemcpyDeviceToHost));
+  if (dist) APC_CUDA_TRY(c, cudaMemcpy(dist, c->st_dist, sizeof(double) * k, cudaMemcpyDeviceToHost));
+  return APC_OK;
+}
+
+int apc_get_solve_stats(apc_context *c, apc_solve_stats *st) {
+  APC_TRY(check_ready(c, true, true, true));
+  if (!st) return APC_ERR_INVALID_ARG;
+  *st = c->stats;
+  return APC_OK;
+}
+
+int apc_get_matrix(apc_context *c, int which, int *n, int *nnz, int *rowptr, int *col, double *val) {
+  APC_TRY(check_ready(c, true, true, true));
+  if (which != 0 && which != 1) return APC_ERR_INVALID_ARG;
+  const int M = c->nc + c->nv, W = c->ell_w;
+  const size_t ld = (size_t)c->m_cap;
+  std::vector<int> ec(ld * W);
+  std::vector<double> ev(ld * W);
+  APC_CUDA_TRY(c, cudaMemcpy(ec.data(), c->ell_col, sizeof(int) * ld * W, cudaMemcpyDeviceToHost));
+  APC_CUDA_TRY(c, cudaMemcpy(ev.data(), which == 0 ? c->a1 : c->a2, sizeof(double) * ld * W,
+                             cudaMemcpyDeviceToHost));
+  std::vector<std::vector<std::pair<int, double>>> rows(M);
+  for (int i = 0; i < M; ++i) {
+    const bool pin = which == 1 && c->cfg.bc == 1 && i == 0;
+    for (int s = 0; s < W; ++s) {
+      const int cj = ec[(size_t)s * ld + i];
+      if (s > 0 && (cj == i || pin)) continue;  // dropped slot
+      bool dup = false;
+      for (auto &e : rows[i])
+        if (e.first == cj) { e.second = ev[(size_t)s * ld + i]; dup = true; }
+      if (!dup) rows[i].push_back({cj, ev[(size_t)s * ld + i]});
+    }
+    std::sort(rows[i].begin(), rows[i].end());
+  }
+  int total = 0;
+  for (auto &r : rows) total += (int)r.size();
+  if (n) *n = M;
+  if (nnz) *nnz = total;
+  if (!rowptr) return APC_OK;
+  int k = 0;
+  for (int i = 0; i < M; ++i) {
+    rowptr[i] = k;
+    for (auto &e : rows[i]) {
+      if (col) col[k] = e.first;
+      if (val) val[k] = e.second;
+      ++k;
+    }
+  }
+  rowptr[M] = k;
+  return APC_OK;
+}
+
+int64_t apc_kernel_launches(const apc_context *c) { return c ? c->launches : 0; }
+
+int apc_get_phase_times(apc_context *c, double *a, double *b, double *d) {
+  if (!c) return APC_ERR_INVALID_ARG;
+  if (a) *a = c->t_select_ms;
+  if (b) *b = c->t_solve_ms;
+  if (d) *d = c->t_move_ms;
+  return APC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,536 @@
+// GFD stencils, density / Poisson system assembly and differentiation on the device.
+//
+// Reference: Solver::Build_Linear_System (solver.cpp:24-180), Solver::searchneighboroctant
+// (solver.cpp:456-570), Solver::Solve_Potential's right-hand side (solver.cpp:236-259)
+// and Solver::Differentiate (solver.cpp:295-362).
+//
+// One warp per cell (computational or vacuum particle):
+//  * Neighbour search.  The cell's Neigh24 entries are bucketed into 8 octants of a
+//    slightly rotated frame, then grown ring by ring through the neighbours' Neigh24
+//    lists until at least lm candidates exist.  Discovery order is kept exactly: one
+//    warp-wide batch per candidate, ordered appends by ballot, duplicates removed
+//    against the buckets and within the batch.  The rotation and distance products
+//    are evaluated without FMA contraction, in the reference's operand order, so the
+//    octant signs and distance ties are bit-identical.  Lane 0 then runs the
+//    reference's sort exactly:
+//      - quicksort of octant 0 only (solver.cpp:557 passes the running offset);
+//      - 1e4^rank penalties within each octant;
+//      - a global quicksort with the same partition scheme, so ties break identically.
+//  * Least squares.  The lm x 9 weighted monomial matrix is factored by FP64 Householder
+//    QR held one row per lane, with warp-shuffle reductions.  The full operator
+//    X = R^-1 Q1^T diag(w) (9 x lm) is formed, i.e. the dgels solution for the
+//    lm right-hand sides of solver.cpp:101-106, and kept for the differentiation step.
+//    The second neighbour search and QR of Solver::Differentiate (solver.cpp:307-342)
+//    repeat the same computation, so they are not redone.
+//  * Assembly.  A1 = I + (h^2/24) Lap and A2 = Lap go to slot-major ELL of width lm+1:
+//    slot 0 is the diagonal, slot 1+j neighbour j.  Row 0 of A2 is the Dirichlet pin of
+//    periodic boxes (solver.cpp:147-152).
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "apc_internal.cuh"
+
+namespace {
+
+constexpr int kWarps = 4;         // warps per block
+constexpr int kBucketCap = 48;    // entries per octant bucket
+constexpr int kListCap = 256;     // candidates entering the final sort
+constexpr int kMaxLm = 32;
+
+struct GfdParams {
+  int m, lm, bc, nc_nv, sort_cap;
+  double L[3], halfL[3];
+  double rot[9];
+  double e4;       // exp(-4)
+  double c_dens;
+  const double *cx, *cy, *cz, *ch;
+  const int *count, *type, *nb24, *nnb;
+  int *st_idx;
+  double *st_dist, *gx;
+  int *ell_col;
+  double *a1, *a2, *rhs;
+  size_t ld;  // ELL leading dimension (row capacity)
+  int *err;
+};
+
+__device__ __forceinline__ double pwrap(double x, double L, double halfL) {
+  // Solver::periodic_wrap (solver.cpp:574-594); |x| < L for points inside the box
+  for (int k = 0; k < 4 && x >= halfL; ++k) x = __dsub_rn(x, L);
+  for (int k = 0; k < 4 && x < -halfL; ++k) x = __dadd_rn(x, L);
+  return x;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// apartition / aquickSort (solver.cpp:600-632) with an explicit stack.  Sub-ranges are
+// disjoint, so processing order does not change the result; the smaller side is taken
+// first, which bounds the stack by log2(n).
+__device__ void aquicksort(double *a, int *b, int l, int r) {
+  int stack[64];
+  int sp = 0;
+  for (;;) {
+    if (l >= r) {
+      if (sp == 0) break;
+      r = stack[--sp];
+      l = stack[--sp];
+      continue;
+    }
+    double pivot = a[l], t;
+    int i = l, j = r + 1, ti;
+    for (;;) {
+      do ++i; while (i <= r && a[i] <= pivot);
+      do --j; while (a[j] > pivot);
+      if (i >= j) break;
+      t = a[i]; a[i] = a[j]; a[j] = t;
+      ti = b[i]; b[i] = b[j]; b[j] = ti;
+    }
+    t = a[l]; a[l] = a[j]; a[j] = t;
+    ti = b[l]; b[l] = b[j]; b[j] = ti;
+    if (j - l < r - j) {
+      stack[sp++] = j + 1;
+      stack[sp++] = r;
+      r = j - 1;
+    } else {
+      stack[sp++] = l;
+      stack[sp++] = j - 1;
+      l = j + 1;
+    }
+  }
+}
+
+struct WarpSmem {
+  int bidx[8][kBucketCap];
+  double bd2[8][kBucketCap];
+  double ldist[kListCap];
+  int lidx[kListCap];
+  double R[9][9];
+};
+
+__device__ __forceinline__ void offset_of(const GfdParams &P, int m, int i0, double &wx, double &wy,
+                                          double &wz) {
+  wx = pwrap(__dsub_rn(P.cx[m], P.cx[i0]), P.L[0], P.halfL[0]);
+  wy = pwrap(__dsub_rn(P.cy[m], P.cy[i0]), P.L[1], P.halfL[1]);
+  wz = pwrap(__dsub_rn(P.cz[m], P.cz[i0]), P.L[2], P.halfL[2]);
+}
+
+__device__ __forceinline__ int octant_of(const GfdParams &P, double wx, double wy, double wz) {
+  const double *A = P.rot;
+  double xt = __dadd_rn(__dadd_rn(__dmul_rn(A[0], wx), __dmul_rn(A[1], wy)), __dmul_rn(A[2], wz));
+  double yt = __dadd_rn(__dadd_rn(__dmul_rn(A[3], wx), __dmul_rn(A[4], wy)), __dmul_rn(A[5], wz));
+  double zt = __dadd_rn(__dadd_rn(__dmul_rn(A[6], wx), __dmul_rn(A[7], wy)), __dmul_rn(A[8], wz));
+  return (xt > 0) + 2 * (yt > 0) + 4 * (zt > 0);
+}
+
+__device__ __forceinline__ double sq3(double wx, double wy, double wz) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(wx, wx), __dmul_rn(wy, wy)), __dmul_rn(wz, wz));
+}
+
+// ordered append of the valid lanes' candidates to their octant buckets
+__device__ __forceinline__ bool append(WarpSmem &S, int (&nn)[8], bool valid, int m, int oct,
+                                       double d2, int lane) {
+  bool ok = true;
+  const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int o = 0; o < 8; ++o) {
+    unsigned bal = __ballot_sync(0xffffffffu, valid && oct == o);
+    if (valid && oct == o) {
+      int p = nn[o] + __popc(bal & lt);
+      if (p < kBucketCap) {
+        S.bidx[o][p] = m;
+        S.bd2[o][p] = d2;
+      }
+    }
+    nn[o] += __popc(bal);
+    if (nn[o] > kBucketCap) ok = false;
+  }
+  __syncwarp();
+  return ok;
+}
+
+__global__ void __launch_bounds__(32 * kWarps) gfd_stencil(GfdParams P) {
+  __shared__ WarpSmem smem[kWarps];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  WarpSmem &S = smem[w];
+  const int lm = P.lm;
+  for (int i0 = blockIdx.x * kWarps + w; i0 < P.m; i0 += gridDim.x * kWarps) {
+    int nn[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bool ok = true;   // false once a bucket overflowed
+    bool few = false; // true when 5 expansions did not reach lm candidates
+    // ---- first ring: Neigh24 of i0 (solver.cpp:479-492), no de-duplication ----
+    {
+      const int cnt = P.nnb[i0];
+      const bool v = lane < cnt;
+      int m = v ? P.nb24[24 * (size_t)i0 + lane] : -1;
+      double wx = 0, wy = 0, wz = 0;
+      int oct = 0;
+      double d2 = 0;
+      if (v) {
+        offset_of(P, m, i0, wx, wy, wz);
+        oct = octant_of(P, wx, wy, wz);
+        d2 = sq3(wx, wy, wz);
+      }
+      ok &= append(S, nn, v, m, oct, d2, lane);
+    }
+    int l = 0;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) l += nn[o];
+    // ---- expansion rings (solver.cpp:494-552) ----
+    int ite = 0;
+    while (ok && l < lm) {
+      // the reference exits on its sixth expansion whatever it finds (solver.cpp:544-550)
+      if (ite == 5) {
+        few = true;
+        break;
+      }
+      int snn[8];
+#pragma unroll
+      for (int o = 0; o < 8; ++o) snn[o] = nn[o];
+      for (int b = 0; b < 8 && ok; ++b) {
+        for (int e = 0; e < snn[b] && ok; ++e) {
+          const int p = S.bidx[b][e];
+          const int cnt = P.nnb[p];
+          bool v = lane < cnt;
+          int m = v ? P.nb24[24 * (size_t)p + lane] : -1;
+          int oct = 0;
+          double d2 = 0;
+          if (v) {
+            double wx, wy, wz;
+            offset_of(P, m, i0, wx, wy, wz);
+            oct = octant_of(P, wx, wy, wz);
+            d2 = sq3(wx, wy, wz);
+            bool dup = (m == i0);
+            const int cap = min(nn[oct], kBucketCap);
+            for (int q = 0; q < cap && !dup; ++q) dup = (S.bidx[oct][q] == m);
+            v = !dup;
+          }
+          // only the first lane holding a given index survives within the batch
+          unsigned peers = __match_any_sync(0xffffffffu, v ? m : -1 - lane);
+          if (v && lane != __ffs(peers) - 1) v = false;
+          ok &= append(S, nn, v, m, oct, d2, lane);
+        }
+      }
+      if (!ok) break;
+      ++ite;
+      l = 0;
+#pragma unroll
+      for (int o = 0; o < 8; ++o) l += nn[o];
+    }
+    if (few) {
+      if (lane == 0) atomicOr(P.err, DERR_STENCIL_FEW);
+      continue;
+    }
+    if (!ok || l > P.sort_cap) {
+      if (lane == 0) atomicOr(P.err, DERR_STENCIL_MANY);
+      continue;
+    }
+    // ---- sorting (solver.cpp:553-569), lane 0 ----
+    if (lane == 0) {
+      aquicksort(S.bd2[0], S.bidx[0], 0, nn[0] - 1);
+      int k = 0;
+      for (int b = 0; b < 8; ++b) {
+        double penalty = 1.0;
+        for (int e = 0; e < nn[b]; ++e) {
+          S.lidx[k] = S.bidx[b][e];
+          S.ldist[k] = __dmul_rn(penalty, S.bd2[b][e]);
+          penalty = __dmul_rn(penalty, 10000.0);
+          ++k;
+        }
+      }
+      aquicksort(S.ldist, S.lidx, 0, l - 1);
+    }
+    __syncwarp();
+    // ---- weights and weighted monomials (solver.cpp:75-103) ----
+    const bool act = lane < lm;
+    const int mj = act ? S.lidx[lane] : i0;
+    double wx, wy, wz;
+    offset_of(P, mj, i0, wx, wy, wz);
+    const double dist = act ? sqrt(sq3(wx, wy, wz)) : 0.0;
+    const double maxdis = warp_max(dist) * 0.7;
+    double weight = 0.0;
+    if (act) weight = (exp(-dist * dist / maxdis / maxdis) - P.e4) / (1 - P.e4);
+    const double h = P.ch[i0];
+    const double p1 = wx / h, p2 = wy / h, p3 = wz / h;
+    double b[9];
+    b[0] = p1; b[1] = p2; b[2] = p3;
+    b[3] = p1 * p1 / 2.0; b[4] = p2 * p2 / 2.0; b[5] = p3 * p3 / 2.0;
+    b[6] = p1 * p2; b[7] = p1 * p3; b[8] = p2 * p3;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) b[k] = act ? b[k] * weight : 0.0;
+    // ---- Householder QR, one row per lane ----
+    double v[9], tau[9];
+    bool rank_ok = true;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const double x = b[k];
+      const double xn2 = warp_sum(lane > k ? x * x : 0.0);
+      const double alpha = __shfl_sync(0xffffffffu, x, k);
+      const double xnorm = sqrt(xn2);
+      double beta = alpha, tk = 0.0, vr = (lane == k) ? 1.0 : 0.0;
+      if (xnorm != 0.0) {
+        beta = -copysign(hypot(alpha, xnorm), alpha);
+        tk = (beta - alpha) / beta;
+        const double scal = 1.0 / (alpha - beta);
+        if (lane > k) vr = x * scal;
+      }
+      tau[k] = tk;
+      v[k] = lane >= k ? vr : 0.0;
+      if (lane == k) b[k] = beta;
+      if (beta == 0.0) rank_ok = false;
+#pragma unroll
+      for (int c = k + 1; c < 9; ++c) {
+        const double s = warp_sum(v[k] * b[c]);
+        if (lane >= k) b[c] = b[c] + v[k] * (-tk * s);
+      }
+    }
+    if (!rank_ok) {
+      if (lane == 0) atomicOr(P.err, DERR_RANK);
+      continue;
+    }
+    if (lane < 9) {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) S.R[lane][c] = c >= lane ? b[c] : 0.0;
+    }
+    // ---- thin Q rows: Q1 = H0 H1 ... H8 [I; 0] (backward accumulation) ----
+    double q[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) q[c] = (lane == c) ? 1.0 : 0.0;
+#pragma unroll
+    for (int k = 8; k >= 0; --k) {
+#pragma unroll
+      for (int c = k; c < 9; ++c) {
+        const double s = warp_sum(v[k] * q[c]);
+        q[c] = q[c] - tau[k] * v[k] * s;
+      }
+    }
+    __syncwarp();
+    // ---- X(:, j) = w_j R^-1 Q1(j, :)^T, lane j ----
+    double y[9];
+#pragma unroll
+    for (int k = 8; k >= 0; --k) {
+      double t = q[k];
+#pragma unroll
+      for (int c = k + 1; c < 9; ++c) t -= S.R[k][c] * y[c];
+      y[k] = t / S.R[k][k];
+    }
+    double *X = P.gx + (size_t)i0 * 9 * lm;
+    if (act) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) X[k * lm + lane] = weight * y[k];
+      P.st_idx[(size_t)i0 * lm + lane] = mj;
+      P.st_dist[(size_t)i0 * lm + lane] = dist;
+    }
+    // ---- rows of A1, A2 and the density rhs (solver.cpp:116-172) ----
+    const double lap = act ? (weight * y[3] + weight * y[4]) + weight * y[5] : 0.0;
+    const double l24 = lap / 24.0;
+    const double lh2 = lap / h / h;
+    const bool in1 = act && mj < P.nc_nv;
+    const bool in2 = act && P.type[mj] < 1;
+    const bool pin = (i0 == 0) && (P.bc == 1);
+    if (act) {
+      const size_t at = (size_t)(1 + lane) * P.ld + i0;
+      P.ell_col[at] = in1 ? mj : i0;
+      P.a1[at] = in1 ? l24 : 0.0;
+      P.a2[at] = (in2 && !pin) ? lh2 : 0.0;
+    }
+    // diagonal sums in the reference's sequential order
+    double s1 = 0.0, s2 = 0.0;
+    for (int j = 0; j < lm; ++j) {
+      const double a = __shfl_sync(0xffffffffu, l24, j);
+      const double c = __shfl_sync(0xffffffffu, lh2, j);
+      s1 = s1 - a;
+      s2 = s2 - c;
+    }
+    if (lane == 0) {
+      const size_t at = (size_t)i0;
+      P.ell_col[at] = i0;
+      P.a1[at] = s1 + 1;
+      P.a2[at] = pin ? 1.0 : s2;
+      P.rhs[i0] = 1.0 * P.count[i0] / h / h / h * P.c_dens;
+    }
+    __syncwarp();
+  }
+}
+
+// -------------------------------------------------------------- potential rhs
+
+__global__ void mass_partials(const double *__restrict__ rho, const double *__restrict__ h, int m,
+                              double *partial) {
+  __shared__ double s1[256], s2[256];
+  double a = 0.0, b = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const double v = h[i] * h[i] * h[i];
+    a += rho[i] * h[i] * h[i] * h[i];
+    b += v;
+  }
+  s1[threadIdx.x] = a;
+  s2[threadIdx.x] = b;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      s1[threadIdx.x] += s1[threadIdx.x + o];
+      s2[threadIdx.x] += s2[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = s1[0];
+    partial[2 * blockIdx.x + 1] = s2[0];
+  }
+}
+
+// rhs = (rho - mean_volume_weighted(rho)) * c_pot (solver.cpp:244-259)
+__global__ void potential_rhs_kernel(const double *__restrict__ rho, int m, const double *partial,
+                                     int nparts, double c_pot, double *rhs) {
+  __shared__ double mean;
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int k = 0; k < nparts; ++k) {
+      a += partial[2 * k];
+      b += partial[2 * k + 1];
+    }
+    mean = a / b;
+  }
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    rhs[i] = (rho[i] - mean) * c_pot;
+}
+
+__global__ void potential_rhs_dirichlet(const double *__restrict__ rho, const double *__restrict__ bc,
+                                        int m, double c_pot, double *rhs) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    rhs[i] = (rho[i] + bc[i]) * c_pot;
+}
+
+// -------------------------------------------------------------- differentiate
+
+// gradient / Hessian of phi: y = X (phi_j - phi_i) c_field (solver.cpp:315-358), one warp per cell
+__global__ void __launch_bounds__(256) differentiate_kernel(int m, int lm, int nc_nv,
+                                                            const int *__restrict__ st_idx,
+                                                            const double *__restrict__ gx,
+                                                            const double *__restrict__ phi,
+                                                            const double *__restrict__ h,
+                                                            double c_field, double *deriv) {
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < m; i += gridDim.x * wpb) {
+    const double p4 = phi[i];
+    double r = 0.0;
+    if (lane < lm) {
+      const int k = st_idx[(size_t)i * lm + lane];
+      const double p1 = k < nc_nv ? phi[k] : 0.0;
+      r = (p1 - p4) * c_field;
+    }
+    const double *X = gx + (size_t)i * 9 * lm;
+    double out = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const double t = warp_sum(lane < lm ? X[k * lm + lane] * r : 0.0);
+      if (lane == k) out = t;
+    }
+    if (lane < 9) {
+      const double hi = h[i];
+      deriv[(size_t)i * 9 + lane] = lane < 3 ? out / hi : out / hi / hi;
+    }
+  }
+}
+
+}  // namespace
+
+int apc_gfd_assemble(apc_context *c, double c_dens) {
+  const int M = c->nc + c->nv;
+  const int lm = c->lm;
+  if (lm > kMaxLm || lm < 9) {
+    c->err = "lm must be in [9, 32]";
+    return APC_ERR_INVALID_ARG;
+  }
+  const size_t mc = (size_t)M + 1;
+  APC_TRY(apc_ensure(c, &c->st_idx, mc * lm, nullptr));
+  APC_TRY(apc_ensure(c, &c->st_dist, mc * lm, nullptr));
+  APC_TRY(apc_ensure(c, &c->gfd_x, mc * 9 * lm, nullptr));
+  c->ell_w = lm + 1;
+  if ((size_t)c->m_cap < mc) {
+    c->m_cap = (int)(mc + mc / 4 + 1024);
+  }
+  const size_t ld = (size_t)c->m_cap;
+  APC_TRY(apc_ensure(c, &c->ell_col, ld * c->ell_w, nullptr));
+  APC_TRY(apc_ensure(c, &c->a1, ld * c->ell_w, nullptr));
+  APC_TRY(apc_ensure(c, &c->a2, ld * c->ell_w, nullptr));
+  APC_TRY(apc_ensure(c, &c->rhs, ld, nullptr));
+  APC_TRY(apc_ensure(c, &c->bcrhs, ld, nullptr));
+  APC_TRY(apc_ensure(c, &c->density, ld, nullptr));
+  APC_TRY(apc_ensure(c, &c->potential, ld, nullptr));
+  APC_TRY(apc_ensure(c, &c->deriv, ld * 9, nullptr));
+  APC_CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->s));
+  APC_CUDA_TRY(c, cudaMemsetAsync(c->bcrhs, 0, sizeof(double) * M, c->s));
+  GfdParams P;
+  P.m = M;
+  P.lm = lm;
+  P.bc = c->cfg.bc;
+  P.nc_nv = M;
+  P.sort_cap = std::min(kListCap, 10 * lm);
+  for (int d = 0; d < 3; ++d) {
+    P.L[d] = c->cfg.box[2 * d + 1] - c->cfg.box[2 * d];
+    P.halfL[d] = c->cfg.bc == 1 ? 0.5 * P.L[d] : 1e308;
+  }
+  for (int k = 0; k < 9; ++k) P.rot[k] = c->rot[k];
+  P.e4 = std::exp(-4.0);
+  P.c_dens = c_dens;
+  P.cx = c->cx; P.cy = c->cy; P.cz = c->cz; P.ch = c->ch;
+  P.count = c->ccount; P.type = c->ctype; P.nb24 = c->nb24; P.nnb = c->nnb;
+  P.st_idx = c->st_idx; P.st_dist = c->st_dist; P.gx = c->gfd_x;
+  P.ell_col = c->ell_col; P.a1 = c->a1; P.a2 = c->a2; P.rhs = c->rhs;
+  P.ld = ld;
+  P.err = c->d_err;
+  const int blocks = std::max(1, std::min((M + kWarps - 1) / kWarps, apc_sm_count(c) * 16));
+  gfd_stencil<<<blocks, 32 * kWarps, 0, c->s>>>(P);
+  apc_count_launch(c);
+  APC_CUDA_TRY(c, cudaGetLastError());
+  int derr = 0;
+  APC_TRY(apc_read_errors(c, &derr));
+  if (derr & (DERR_STENCIL_FEW | DERR_STENCIL_MANY)) {
+    c->err = (derr & DERR_STENCIL_FEW) ? "GFD neighbour search: not enough neighbours after 5 expansions"
+                                       : "GFD neighbour search: candidate buffers exceeded";
+    return APC_ERR_STENCIL;
+  }
+  if (derr & DERR_RANK) {
+    c->err = "GFD least-squares system is rank deficient";
+    return APC_ERR_RANK;
+  }
+  return APC_OK;
+}
+
+int apc_potential_rhs(apc_context *c, double c_pot) {
+  const int M = c->nc + c->nv;
+  const int G = std::max(1, std::min((M + 255) / 256, apc_sm_count(c) * 4));
+  if (c->cfg.bc == 1) {
+    APC_TRY(apc_ensure(c, &c->reduce_buf, (size_t)2 * G + 2, nullptr));
+    mass_partials<<<G, 256, 0, c->s>>>(c->density, c->ch, M, c->reduce_buf);
+    potential_rhs_kernel<<<G, 256, 0, c->s>>>(c->density, M, c->reduce_buf, G, c_pot, c->rhs);
+    apc_count_launch(c, 2);
+  } else {
+    potential_rhs_dirichlet<<<G, 256, 0, c->s>>>(c->density, c->bcrhs, M, c_pot, c->rhs);
+    apc_count_launch(c);
+  }
+  APC_CUDA_TRY(c, cudaGetLastError());
+  return APC_OK;
+}
+
+int apc_differentiate(apc_context *c, double c_field) {
+  const int M = c->nc + c->nv;
+  const int G = std::max(1, std::min((M + 7) / 8, apc_sm_count(c) * 16));
+  differentiate_kernel<<<G, 256, 0, c->s>>>(M, c->lm, M, c->st_idx, c->gfd_x, c->potential, c->ch,
+                                            c_field, c->deriv);
+  apc_count_launch(c);
+  APC_CUDA_TRY(c, cudaGetLastError());
+  return APC_OK;
+}

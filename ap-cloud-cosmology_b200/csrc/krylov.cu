@@ -1,0 +1,670 @@
+// Restarted GMRES with left Jacobi preconditioning on the device, and the FP32-inner /
+// FP64-outer iterative refinement of the mixed-precision path.
+//
+// Reference: Solver::Solve_Density / Solve_Potential (solver.cpp:182-293) call PETSc
+// KSPGMRES + PCJACOBI (solver.cpp:196-204, 267-276).  The FP64 kernel follows PETSc
+// 3.5's GMRES control flow:
+//   - zero initial guess; left preconditioning r = D^-1 (b - A x);
+//   - classical Gram-Schmidt, refinement "never";
+//   - Givens rotations; happy-breakdown tolerance 1e-30;
+//   - convergence on the preconditioned residual estimate against
+//     max(rtol ||D^-1 b||, atol), divergence at dtol * ||D^-1 b||, DIVERGED_ITS at max_it.
+//
+// Design (B200): one persistent cooperative kernel per solve.  Every block owns a
+// strided set of rows.
+//   - Per Arnoldi step, one pass fuses SpMV + Jacobi + all dot products with the
+//     basis, and a second pass fuses the Gram-Schmidt update + norm.  That is two grid
+//     barriers per iteration.  With re-orthogonalisation (CGS2) it is three.
+//   - Basis vectors are stored un-normalised with a separate scale, so normalisation
+//     costs no pass.
+//   - Each block reduces the per-block partial sums itself in a fixed order, so all
+//     blocks hold identical Hessenberg / Givens state without another barrier.
+//   - Data other blocks write is read through L2 (ld.cg).
+//   - The grid barrier's spin is bounded.  On timeout it raises an error flag and an
+//     abort flag, and every block leaves.
+// At the problem sizes of interest the basis (M x (restart+1) words) and the ELL matrix
+// sit in the 126 MB L2, so an iteration runs at L2 bandwidth plus barrier latency.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "apc_internal.cuh"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarpsPB = kThreads / 32;
+constexpr int kPartStride = 72;  // doubles per block per partial-sum slot set
+constexpr long long kSpinLimit = 1ll << 24;  // ~1-2 s of __nanosleep(64)
+
+struct GridBar {
+  unsigned count;
+  unsigned gen;
+  int abort;
+  int pad;
+};
+
+enum {
+  KSP_CONVERGED_RTOL = 2,
+  KSP_CONVERGED_ATOL = 3,
+  KSP_DIVERGED_NULL = -2,
+  KSP_DIVERGED_ITS = -3,
+  KSP_DIVERGED_DTOL = -4,
+  KSP_DIVERGED_BREAKDOWN = -5,
+  KSP_DIVERGED_NANORINF = -9,
+};
+
+// bounded sense-free generation barrier; returns false when the grid must abort
+__device__ __forceinline__ bool grid_sync(GridBar *bar, unsigned nblocks, int *err) {
+  __syncthreads();
+  __shared__ int s_abort;
+  if (threadIdx.x == 0) {
+    volatile unsigned *vgen = &bar->gen;
+    volatile int *vab = &bar->abort;
+    const unsigned g = *vgen;
+    __threadfence();
+    const unsigned a = atomicAdd(&bar->count, 1u);
+    if (a == nblocks - 1) {
+      atomicExch(&bar->count, 0u);
+      __threadfence();
+      atomicAdd(&bar->gen, 1u);
+    } else {
+      long long spins = 0;
+      while (*vgen == g && !*vab) {
+        if (++spins > kSpinLimit) {
+          atomicOr(err, DERR_KRYLOV);
+          atomicExch(&bar->abort, 1);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_abort = *vab;
+  }
+  __syncthreads();
+  return s_abort == 0;
+}
+
+template <class T>
+struct GmresArgs {
+  int n;                // rows
+  int w;                // ELL width
+  size_t ld;            // ELL leading dimension
+  const int *col;       // [slot][row]
+  const T *val;         // [slot][row], slot 0 = diagonal
+  const T *b;           // rhs
+  T *x;                 // solution (out)
+  T *U;                 // (restart+1) x n basis, un-normalised
+  size_t un;            // basis leading dimension
+  double *part;         // 2 x nblocks x kPartStride partial sums
+  GridBar *bar;
+  int *err;
+  int restart;
+  double rtol, atol, dtol;
+  int max_it;
+  int *out_its;
+  int *out_reason;
+  double *out_rnorm;
+};
+
+template <class T>
+__device__ __forceinline__ T ldcg(const T *p) {
+  return __ldcg(p);
+}
+
+__device__ __forceinline__ double block_reduce_many(double (&acc)[33], int nv, double *sm_red) {
+  // per warp reduce each slot, then stage [warp][slot]; caller sums over warps
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < 33; ++j) {
+    if (j < nv) {
+      double v = acc[j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) sm_red[warp * 33 + j] = v;
+    }
+  }
+  return 0.0;
+}
+
+// sum of slot j over all blocks' partials, identical in every block
+__device__ __forceinline__ void gather_partials(const double *part, int nblocks, int nv, double *out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int j = warp; j < nv; j += kWarpsPB) {
+    double v = 0.0;
+    for (int b = lane; b < nblocks; b += 32) v += __ldcg(part + (size_t)b * kPartStride + j);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) out[j] = v;
+  }
+}
+
+__device__ __forceinline__ int converged_default(int n_its, double rnorm, double rtol, double atol,
+                                                 double dtol, double &ttol, double &rnorm0) {
+  if (n_its == 0) {
+    ttol = fmax(rtol * rnorm, atol);
+    rnorm0 = rnorm;
+  }
+  if (rnorm != rnorm) return KSP_DIVERGED_NANORINF;
+  if (rnorm <= ttol) return rnorm < atol ? KSP_CONVERGED_ATOL : KSP_CONVERGED_RTOL;
+  if (rnorm >= dtol * rnorm0) return KSP_DIVERGED_DTOL;
+  return 0;
+}
+
+template <class T, bool REORTH>
+__global__ void __launch_bounds__(kThreads) gmres_kernel(GmresArgs<T> A) {
+  constexpr int MAXV = 32;  // restart <= 31
+  __shared__ double sm_red[kWarpsPB * 33];
+  __shared__ double sh[MAXV + 1];      // reduced dots / norms of this step
+  __shared__ double HH[(MAXV + 1) * MAXV];
+  __shared__ double cc[MAXV], ss[MAXV], grs[MAXV + 1], scale[MAXV + 1], coef[MAXV + 1];
+  __shared__ int s_flow[4];  // reason, it, hapend, its
+  __shared__ double s_res, s_ttol, s_rnorm0;
+
+  const int nb = gridDim.x;
+  const int m = A.restart;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int stride = gridDim.x * blockDim.x;
+  double *partA = A.part;
+  double *partB = A.part + (size_t)nb * kPartStride;
+  double acc[33];
+
+  for (int i = tid; i < A.n; i += stride) A.x[i] = T(0);
+  int its = 0, reason = 0, itcount = 0;
+  bool guess_zero = true;
+  double ttol = 0.0, rnorm0 = 0.0, res = 0.0;
+  if (threadIdx.x == 0) {
+    s_ttol = 0.0;
+    s_rnorm0 = 0.0;
+  }
+  if (!grid_sync(A.bar, nb, A.err)) return;
+
+  while (!reason) {
+    // ---- initial residual: u0 = D^-1 (b - A x) ----
+    double nrm = 0.0;
+    for (int i = tid; i < A.n; i += stride) {
+      const T d = A.val[i];
+      const double di = d == T(0) ? 1.0 : 1.0 / (double)d;
+      double r = (double)A.b[i];
+      if (!guess_zero) {
+        double s = 0.0;
+        for (int k = 0; k < A.w; ++k) {
+          const size_t at = (size_t)k * A.ld + i;
+          s += (double)A.val[at] * (double)ldcg(A.x + A.col[at]);
+        }
+        r -= s;
+      }
+      const double u = di * r;
+      A.U[i] = T(u);
+      nrm += u * u;
+    }
+    acc[0] = nrm;
+    block_reduce_many(acc, 1, sm_red);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double v = 0.0;
+      for (int wv = 0; wv < kWarpsPB; ++wv) v += sm_red[wv * 33];
+      partB[(size_t)blockIdx.x * kPartStride] = v;
+    }
+    if (!grid_sync(A.bar, nb, A.err)) return;
+    gather_partials(partB, nb, 1, sh);
+    __syncthreads();
+    const double beta = sqrt(sh[0]);
+    if (threadIdx.x == 0) {
+      scale[0] = beta != 0.0 ? 1.0 / beta : 1.0;
+      grs[0] = beta;
+    }
+    res = beta;
+    if (res == 0.0) {
+      reason = KSP_CONVERGED_ATOL;
+      break;
+    }
+    reason = converged_default(its, res, A.rtol, A.atol, A.dtol, ttol, rnorm0);
+    int it = 0;
+    __syncthreads();
+    while (!reason && it < m && its < A.max_it) {
+      const T *uk = A.U + (size_t)it * A.un;
+      T *w = A.U + (size_t)(it + 1) * A.un;
+      const double sk = scale[it];
+      // ---- pass A: w = D^-1 A v_it, dots with u_0..u_it ----
+#pragma unroll
+      for (int j = 0; j < 33; ++j) acc[j] = 0.0;
+      for (int i = tid; i < A.n; i += stride) {
+        const T d = A.val[i];
+        const double di = d == T(0) ? 1.0 : 1.0 / (double)d;
+        double s = 0.0;
+        for (int k = 0; k < A.w; ++k) {
+          const size_t at = (size_t)k * A.ld + i;
+          s += (double)A.val[at] * (double)ldcg(uk + A.col[at]);
+        }
+        const T wi = T(di * sk * s);
+        w[i] = wi;
+#pragma unroll
+        for (int j = 0; j < MAXV; ++j)
+          if (j <= it) acc[j] += (double)wi * (double)ldcg(A.U + (size_t)j * A.un + i);
+      }
+      block_reduce_many(acc, it + 1, sm_red);
+      __syncthreads();
+      if (threadIdx.x <= it) {
+        double v = 0.0;
+        for (int wv = 0; wv < kWarpsPB; ++wv) v += sm_red[wv * 33 + threadIdx.x];
+        partA[(size_t)blockIdx.x * kPartStride + threadIdx.x] = v;
+      }
+      if (!grid_sync(A.bar, nb, A.err)) return;
+      gather_partials(partA, nb, it + 1, sh);
+      __syncthreads();
+      if (threadIdx.x <= it) {
+        const double h = sh[threadIdx.x] * scale[threadIdx.x];  // <v_j, w>
+        HH[it * (MAXV + 1) + threadIdx.x] = h;
+        coef[threadIdx.x] = h * scale[threadIdx.x];              // weight on u_j
+      }
+      __syncthreads();
+      // ---- pass B: w -= sum_j h_j v_j ; norm (or CGS2 second dots) ----
+#pragma unroll
+      for (int j = 0; j < 33; ++j) acc[j] = 0.0;
+      for (int i = tid; i < A.n; i += stride) {
+        double t = (double)ldcg(w + i);
+#pragma unroll
+        for (int j = 0; j < MAXV; ++j)
+          if (j <= it) t -= coef[j] * (double)ldcg(A.U + (size_t)j * A.un + i);
+        const T tv = T(t);
+        w[i] = tv;
+        if (REORTH) {
+#pragma unroll
+          for (int j = 0; j < MAXV; ++j)
+            if (j <= it) acc[j] += (double)tv * (double)ldcg(A.U + (size_t)j * A.un + i);
+        } else {
+          acc[0] += (double)tv * (double)tv;
+        }
+      }
+      const int nvb = REORTH ? it + 1 : 1;
+      block_reduce_many(acc, nvb, sm_red);
+      __syncthreads();
+      if (threadIdx.x < nvb) {
+        double v = 0.0;
+        for (int wv = 0; wv < kWarpsPB; ++wv) v += sm_red[wv * 33 + threadIdx.x];
+        partB[(size_t)blockIdx.x * kPartStride + threadIdx.x] = v;
+      }
+      if (!grid_sync(A.bar, nb, A.err)) return;
+      gather_partials(partB, nb, nvb, sh);
+      __syncthreads();
+      if (REORTH) {
+        // ---- pass C: second Gram-Schmidt sweep, then the norm ----
+        if (threadIdx.x <= it) {
+          const double h2 = sh[threadIdx.x] * scale[threadIdx.x];
+          HH[it * (MAXV + 1) + threadIdx.x] += h2;
+          coef[threadIdx.x] = h2 * scale[threadIdx.x];
+        }
+        __syncthreads();
+        double nr = 0.0;
+        for (int i = tid; i < A.n; i += stride) {
+          double t = (double)ldcg(w + i);
+#pragma unroll
+          for (int j = 0; j < MAXV; ++j)
+            if (j <= it) t -= coef[j] * (double)ldcg(A.U + (size_t)j * A.un + i);
+          const T tv = T(t);
+          w[i] = tv;
+          nr += (double)tv * (double)tv;
+        }
+        acc[0] = nr;
+        block_reduce_many(acc, 1, sm_red);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          double v = 0.0;
+          for (int wv = 0; wv < kWarpsPB; ++wv) v += sm_red[wv * 33];
+          partA[(size_t)blockIdx.x * kPartStride + 40] = v;
+        }
+        if (!grid_sync(A.bar, nb, A.err)) return;
+        gather_partials(partA + 40, nb, 1, sh);
+        __syncthreads();
+      }
+      // ---- Hessenberg / Givens (KSPGMRESUpdateHessenberg), every block alike ----
+      if (threadIdx.x == 0) {
+        const double tt = sqrt(sh[0]);
+        scale[it + 1] = tt != 0.0 ? 1.0 / tt : 1.0;
+        double *hh = HH + it * (MAXV + 1);
+        hh[it + 1] = tt;
+        double hapbnd = fabs(tt / grs[it]);
+        if (hapbnd > 1e-30) hapbnd = 1e-30;
+        const int hapend = tt < hapbnd;
+        for (int j = 1; j <= it; ++j) {
+          const double t0 = hh[j - 1];
+          hh[j - 1] = cc[j - 1] * t0 + ss[j - 1] * hh[j];
+          hh[j] = cc[j - 1] * hh[j] - ss[j - 1] * t0;
+        }
+        int rs = 0;
+        double r = 0.0;
+        if (!hapend) {
+          const double t = sqrt(hh[it] * hh[it] + hh[it + 1] * hh[it + 1]);
+          if (t == 0.0) {
+            rs = KSP_DIVERGED_NULL;
+          } else {
+            cc[it] = hh[it] / t;
+            ss[it] = hh[it + 1] / t;
+            grs[it + 1] = -(ss[it] * grs[it]);
+            grs[it] = cc[it] * grs[it];
+            hh[it] = cc[it] * hh[it] + ss[it] * hh[it + 1];
+            r = fabs(grs[it + 1]);
+          }
+        }
+        s_flow[0] = rs;
+        s_flow[2] = hapend;
+        s_res = rs ? s_res : r;
+      }
+      __syncthreads();
+      const int rs = s_flow[0], hapend = s_flow[2];
+      if (!rs) res = s_res;
+      ++it;
+      ++its;
+      if (rs) {
+        reason = rs;
+        break;
+      }
+      reason = converged_default(its, res, A.rtol, A.atol, A.dtol, ttol, rnorm0);
+      if (hapend) {
+        if (!reason) reason = KSP_DIVERGED_BREAKDOWN;
+        break;
+      }
+    }
+    // ---- KSPGMRESBuildSoln: back substitution, x += sum_j y_j v_j ----
+    const int last = it - 1;
+    if (last >= 0) {
+      if (threadIdx.x == 0) {
+        double *y = sh;
+        const double hl = HH[last * (MAXV + 1) + last];
+        y[last] = hl != 0.0 ? grs[last] / hl : 0.0;
+        for (int ii = 1; ii <= last; ++ii) {
+          const int k = last - ii;
+          double t = grs[k];
+          for (int j = k + 1; j <= last; ++j) t -= HH[j * (MAXV + 1) + k] * y[j];
+          const double hkk = HH[k * (MAXV + 1) + k];
+          y[k] = hkk != 0.0 ? t / hkk : 0.0;
+        }
+        for (int j = 0; j <= last; ++j) coef[j] = y[j] * scale[j];
+      }
+      __syncthreads();
+      for (int i = tid; i < A.n; i += stride) {
+        double t = 0.0;
+#pragma unroll
+        for (int j = 0; j < MAXV; ++j)
+          if (j <= last) t += coef[j] * (double)ldcg(A.U + (size_t)j * A.un + i);
+        A.x[i] = T((double)A.x[i] + t);
+      }
+    }
+    itcount += it;
+    if (itcount >= A.max_it) {
+      if (!reason) reason = KSP_DIVERGED_ITS;
+      break;
+    }
+    guess_zero = false;
+    if (!grid_sync(A.bar, nb, A.err)) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *A.out_its = its;
+    *A.out_reason = reason;
+    *A.out_rnorm = res;
+  }
+}
+
+// ------------------------------------------------------------ refinement helpers
+
+// r = b - A x (FP64), and per-block partials of ||D^-1 r||^2
+__global__ void __launch_bounds__(256) residual64(int n, int w, size_t ld, const int *__restrict__ col,
+                                                  const double *__restrict__ val,
+                                                  const double *__restrict__ b,
+                                                  const double *__restrict__ x, double *__restrict__ r,
+                                                  double *partial) {
+  double nrm = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < w; ++k) {
+      const size_t at = (size_t)k * ld + i;
+      s += val[at] * x[col[at]];
+    }
+    const double ri = b[i] - s;
+    r[i] = ri;
+    const double d = val[i];
+    const double pr = (d == 0.0 ? 1.0 : 1.0 / d) * ri;
+    nrm += pr * pr;
+  }
+  __shared__ double sm[256];
+  sm[threadIdx.x] = nrm;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sm[0];
+}
+
+__global__ void sum_partials(const double *partial, int n, double *out) {
+  __shared__ double sm[256];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v += partial[i];
+  sm[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sm[0];
+}
+
+// rhs32 = r / ||r||_inf-free scale s (FP32 copy of the FP64 residual)
+__global__ void to_f32_scaled(int n, const double *__restrict__ r, double inv_s, float *__restrict__ r32) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    r32[i] = (float)(r[i] * inv_s);
+}
+
+__global__ void axpy_f32(int n, double s, const float *__restrict__ d, double *__restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] += s * (double)d[i];
+}
+
+__global__ void ell_to_f32(size_t count, const double *__restrict__ a, float *__restrict__ f) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
+    f[i] = (float)a[i];
+}
+
+__global__ void zero_f64(int n, double *x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = 0.0;
+}
+
+}  // namespace
+
+struct KrylovWork {
+  size_t u_bytes = 0;
+  void *U = nullptr;
+  double *part = nullptr;
+  int part_blocks = 0;
+  GridBar *bar = nullptr;
+  int *ires = nullptr;     // its, reason
+  double *dres = nullptr;  // rnorm
+  double *r = nullptr, *partial = nullptr, *scalar = nullptr;
+  float *r32 = nullptr, *d32 = nullptr;
+  float *a32 = nullptr;
+  int cap_n = 0;
+  int occ64[2] = {0, 0}, occ32[2] = {0, 0};
+};
+
+void apc_krylov_free(apc_context *c) {
+  KrylovWork *k = c->kw;
+  if (!k) return;
+  cudaFree(k->U);
+  cudaFree(k->part);
+  cudaFree(k->bar);
+  cudaFree(k->ires);
+  cudaFree(k->dres);
+  cudaFree(k->r);
+  cudaFree(k->partial);
+  cudaFree(k->scalar);
+  cudaFree(k->r32);
+  cudaFree(k->d32);
+  cudaFree(k->a32);
+  delete k;
+  c->kw = nullptr;
+}
+
+template <class T, bool RE>
+static int launch_gmres(apc_context *c, int n, const T *val, const T *b, T *x, int restart, double rtol,
+                        double atol, double dtol, int max_it, int *its, double *rnorm, int *reason) {
+  KrylovWork *k = c->kw;
+  if (restart < 1 || restart > 31) {
+    c->err = "GMRES restart must be in [1, 31]";
+    return APC_ERR_INVALID_ARG;
+  }
+  const size_t un = ((size_t)n + 31) & ~(size_t)31;
+  const size_t need = un * (restart + 1) * sizeof(T);
+  if (need > k->u_bytes) {
+    cudaFree(k->U);
+    k->U = nullptr;
+    APC_TRY(apc_alloc(c, &k->U, need));
+    k->u_bytes = need;
+  }
+  int occ = 0;
+  APC_CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gmres_kernel<T, RE>, kThreads, 0));
+  occ = std::max(1, std::min(occ, 2));
+  int blocks = std::min(apc_sm_count(c) * occ, std::max(1, (n + kThreads - 1) / kThreads));
+  if (blocks > k->part_blocks) {
+    cudaFree(k->part);
+    k->part = nullptr;
+    APC_TRY(apc_alloc(c, (void **)&k->part, sizeof(double) * 2 * kPartStride * (size_t)blocks));
+    k->part_blocks = blocks;
+  }
+  APC_CUDA_TRY(c, cudaMemsetAsync(k->bar, 0, sizeof(GridBar), c->s));
+  GmresArgs<T> a;
+  a.n = n;
+  a.w = c->ell_w;
+  a.ld = (size_t)c->m_cap;
+  a.col = c->ell_col;
+  a.val = val;
+  a.b = b;
+  a.x = x;
+  a.U = (T *)k->U;
+  a.un = un;
+  a.part = k->part;
+  a.bar = k->bar;
+  a.err = c->d_err;
+  a.restart = restart;
+  a.rtol = rtol;
+  a.atol = atol;
+  a.dtol = dtol;
+  a.max_it = max_it;
+  a.out_its = k->ires;
+  a.out_reason = k->ires + 1;
+  a.out_rnorm = k->dres;
+  void *args[] = {&a};
+  APC_CUDA_TRY(c, cudaLaunchCooperativeKernel((const void *)gmres_kernel<T, RE>, dim3(blocks), dim3(kThreads),
+                                              args, 0, c->s));
+  apc_count_launch(c);
+  int hi[2];
+  double hd;
+  APC_CUDA_TRY(c, cudaMemcpyAsync(hi, k->ires, sizeof(hi), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, cudaMemcpyAsync(&hd, k->dres, sizeof(hd), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  int derr = 0;
+  APC_TRY(apc_read_errors(c, &derr));
+  if (derr & DERR_KRYLOV) {
+    c->err = "GMRES grid barrier timed out";
+    return APC_ERR_TIMEOUT;
+  }
+  *its = hi[0];
+  *reason = hi[1];
+  *rnorm = hd;
+  return APC_OK;
+}
+
+static int ensure_work(apc_context *c, int n) {
+  if (!c->kw) {
+    c->kw = new KrylovWork();
+    APC_TRY(apc_alloc(c, (void **)&c->kw->bar, sizeof(GridBar)));
+    APC_TRY(apc_alloc(c, (void **)&c->kw->ires, 4 * sizeof(int)));
+    APC_TRY(apc_alloc(c, (void **)&c->kw->dres, 2 * sizeof(double)));
+    APC_TRY(apc_alloc(c, (void **)&c->kw->scalar, 4 * sizeof(double)));
+    APC_TRY(apc_alloc(c, (void **)&c->kw->partial, 4096 * sizeof(double)));
+  }
+  KrylovWork *k = c->kw;
+  if (n > k->cap_n) {
+    cudaFree(k->r);
+    cudaFree(k->r32);
+    cudaFree(k->d32);
+    k->r = nullptr;
+    k->r32 = nullptr;
+    k->d32 = nullptr;
+    const int cap = n + n / 4 + 1024;
+    APC_TRY(apc_alloc(c, (void **)&k->r, sizeof(double) * cap));
+    APC_TRY(apc_alloc(c, (void **)&k->r32, sizeof(float) * cap));
+    APC_TRY(apc_alloc(c, (void **)&k->d32, sizeof(float) * cap));
+    k->cap_n = cap;
+  }
+  return APC_OK;
+}
+
+// Solve A_which x = b.  FP64: one PETSc-semantics GMRES.  Mixed: FP64 iterative
+// refinement on the true preconditioned residual, stopping at the same test
+// ||D^-1 (b - A x)|| <= max(rtol ||D^-1 b||, atol); each correction is an FP32
+// GMRES(CGS2) solve of A d = r to the inner tolerance.
+int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int *its, double *rnorm,
+                     int *reason, int *refinements) {
+  const int n = c->nc + c->nv;
+  APC_TRY(ensure_work(c, n));
+  KrylovWork *k = c->kw;
+  const double *val = which == 0 ? c->a1 : c->a2;
+  const apc_config &cfg = c->cfg;
+  *refinements = 0;
+  if (cfg.precision == APC_PREC_FP64) {
+    return launch_gmres<double, false>(c, n, val, b, x, cfg.gmres_restart, cfg.gmres_rtol, cfg.gmres_atol,
+                                       cfg.gmres_dtol, cfg.gmres_max_it, its, rnorm, reason);
+  }
+  // ---- mixed precision ----
+  const size_t ell_count = (size_t)c->m_cap * c->ell_w;
+  float *af = which == 0 ? c->a1f : c->a2f;
+  const int G = std::max(1, std::min((n + 255) / 256, std::min(apc_sm_count(c) * 8, 4096)));
+  {
+    ell_to_f32<<<std::min<size_t>((ell_count + 255) / 256, 8192), 256, 0, c->s>>>(ell_count, val, af);
+    zero_f64<<<G, 256, 0, c->s>>>(n, x);
+    apc_count_launch(c, 2);
+  }
+  const int m32 = cfg.mixed_restart > 0 ? cfg.mixed_restart : 30;
+  const double rtol_in = cfg.mixed_inner_rtol > 0 ? cfg.mixed_inner_rtol : 1e-5;
+  double ttol = 0.0, rn0 = 0.0;
+  int total_its = 0, rs = 0;
+  double rn = 0.0;
+  for (int outer = 0; outer < 40; ++outer) {
+    residual64<<<G, 256, 0, c->s>>>(n, c->ell_w, (size_t)c->m_cap, c->ell_col, val, b, x, k->r, k->partial);
+    sum_partials<<<1, 256, 0, c->s>>>(k->partial, G, k->scalar);
+    apc_count_launch(c, 2);
+    double nrm2 = 0.0;
+    APC_CUDA_TRY(c, cudaMemcpyAsync(&nrm2, k->scalar, sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+    rn = std::sqrt(nrm2);
+    if (outer == 0) {
+      ttol = std::max(cfg.gmres_rtol * rn, cfg.gmres_atol);
+      rn0 = rn;
+      if (rn == 0.0) { rs = KSP_CONVERGED_ATOL; break; }
+    }
+    if (rn != rn) { rs = KSP_DIVERGED_NANORINF; break; }
+    if (rn <= ttol) { rs = rn < cfg.gmres_atol ? KSP_CONVERGED_ATOL : KSP_CONVERGED_RTOL; break; }
+    if (rn >= cfg.gmres_dtol * rn0) { rs = KSP_DIVERGED_DTOL; break; }
+    if (total_its >= cfg.gmres_max_it) { rs = KSP_DIVERGED_ITS; break; }
+    // scale the correction problem to unit preconditioned-residual norm
+    const double s = rn;
+    to_f32_scaled<<<G, 256, 0, c->s>>>(n, k->r, 1.0 / s, k->r32);
+    apc_count_launch(c);
+    int iits = 0, ireason = 0;
+    double irn = 0.0;
+    APC_TRY(launch_gmres<float, true>(c, n, af, k->r32, k->d32, m32, rtol_in, 1e-30, 1e30,
+                                      std::max(1, cfg.gmres_max_it - total_its), &iits, &irn, &ireason));
+    total_its += iits;
+    axpy_f32<<<G, 256, 0, c->s>>>(n, s, k->d32, x);
+    apc_count_launch(c);
+    ++*refinements;
+  }
+  *its = total_its;
+  *rnorm = rn;
+  *reason = rs;
+  return APC_OK;
+}

@@ -1,0 +1,173 @@
+/*
+ * apcloud_gpu.h - C ABI of the B200 (sm_100a) AP-Cloud gravity step.
+ *
+ * One context owns one particle set resident in GPU memory and runs the reference's
+ * per-timestep gravity path on it:
+ *   octree build -> computational-particle selection -> GFD density + Laplacian
+ *   stencils -> density and potential GMRES solves -> differentiation ->
+ *   interpolation to particles + kick -> drift.
+ *
+ * The entry points replace these reference interfaces (paths relative to the
+ * reference project root):
+ *   apc_create / apc_set_particles   Physical_particle + Mover/Solver construction and
+ *                                     setters (particle.h:5-21, mover.h:31-40,
+ *                                     solver.h:53-60, controller.cpp:75-104)
+ *   apc_select                        Mover::select_computational_particles
+ *                                     (mover.cpp:17-49): Octree(...) (octree.h:224) +
+ *                                     Octree::select_computational_particles_2to1_3d
+ *                                     (octree.h:251, octree.cpp:1050-3001)
+ *   apc_solve                         Solver::solve (solver.h:62, solver.cpp:382-454)
+ *   apc_move_velocity                 Mover::move_velocity (mover.h:42, mover.cpp:51-89)
+ *                                     incl. Octree::interpolation_from_node_to_particle_2to1_3d
+ *                                     (octree.h:250, octree.cpp:3003-3031)
+ *   apc_move_position                 Mover::move_position (mover.h:41, mover.cpp:91-121)
+ *   apc_get_cells / apc_get_fields    the Computational_particle arrays
+ *                                     (particle.h:23-53) the reference fills
+ *
+ * Conventions: every call returns an apc_status (0 = success; never exit()).
+ * Host pointers are caller-owned; device buffers are owned by the context.  Each
+ * context issues its work on one CUDA stream of its own; a context is not
+ * thread-safe, distinct contexts are independent.
+ */
+#ifndef APCLOUD_GPU_H
+#define APCLOUD_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum apc_status {
+  APC_OK = 0,
+  APC_ERR_INVALID_ARG = -1,  /* bad size, pointer or parameter */
+  APC_ERR_CUDA = -2,         /* a CUDA runtime call failed (see apc_last_error) */
+  APC_ERR_OUT_OF_MEMORY = -3,
+  APC_ERR_ORDER = -4,        /* phase called before its inputs exist (e.g. solve before select) */
+  APC_ERR_NMAX = -5,         /* selection exceeded the temp-node budget even after doubling it
+                                to the reference's 1e6 cap (mover.cpp:20,36-41 returns -1) */
+  APC_ERR_STENCIL = -6,      /* GFD neighbour search failed where the reference exit()s:
+                                too few neighbours after 5 expansions (solver.cpp:544-550) or
+                                more candidates than the search buffers hold */
+  APC_ERR_RANK = -7,         /* rank-deficient GFD least-squares system (solver.cpp:107-115) */
+  APC_ERR_NOT_FINITE = -8,   /* NaN/Inf particle coordinates */
+  APC_ERR_UNSUPPORTED = -9,
+  APC_ERR_TIMEOUT = -10      /* a bounded device-side wait gave up */
+} apc_status;
+
+typedef enum apc_precision {
+  APC_PREC_FP64 = 0,  /* FP64 GMRES with the reference's semantics (the plain FP64 path) */
+  APC_PREC_MIXED = 1  /* FP32 SpMV/Krylov inside an FP64 iterative-refinement loop */
+} apc_precision;
+
+typedef struct apc_config {
+  int n_particles;       /* Physical_particle::size */
+  int depth;             /* MaxOctreeLevel: key bits = 3*depth, 1 <= depth <= 21 */
+  int bc;                /* 1 periodic, 0 non-periodic (Periodic) */
+  double box[6];         /* BoundingBox_min_x, max_x, min_y, max_y, min_z, max_z */
+  double gfd_c;          /* CellSizeParameter: refine while n*h^2 > c */
+  int lm;                /* NumberOfNeighbors: GFD stencil size, 10 <= lm <= 32 */
+  int maxnc;             /* first temp-node budget (Mover::Set_maxnc; controller sets 10000).
+                            The budget doubles on failure while below nmax_cap. */
+  int nmax_cap;          /* budget cap: 1000000 reproduces mover.cpp:20; 0 = no cap */
+  int gmres_restart;     /* -ksp_gmres_restart (PETSc default 30) */
+  double gmres_rtol;     /* -ksp_rtol */
+  double gmres_atol;     /* -ksp_atol */
+  double gmres_dtol;     /* -ksp_divtol */
+  int gmres_max_it;      /* -ksp_max_it */
+  int precision;         /* apc_precision */
+  int mixed_restart;     /* FP32 inner GMRES restart for APC_PREC_MIXED (0 = autotuned) */
+  double mixed_inner_rtol; /* FP32 inner solve relative tolerance (0 = 1e-5) */
+  int device;            /* CUDA device ordinal */
+} apc_config;
+
+typedef struct apc_solve_stats {
+  int density_its, potential_its;           /* inner iterations (FP32 ones in mixed mode) */
+  int density_reason, potential_reason;     /* PETSc KSPConvergedReason values */
+  double density_rnorm, potential_rnorm;    /* final preconditioned residual norm */
+  int density_refinements, potential_refinements; /* FP64 outer steps (mixed mode) */
+} apc_solve_stats;
+
+typedef struct apc_context apc_context;
+
+/* Defaults: depth 21, periodic unit box, lm 17, maxnc 10000, nmax_cap 0, GMRES(30)
+ * rtol 1e-10 atol 1e-50 dtol 1e5 max_it 10000, FP64. */
+void apc_config_default(apc_config *cfg);
+const char *apc_status_string(int status);
+/* The message of the last failing call on this context (empty when none). */
+const char *apc_last_error(const apc_context *ctx);
+
+int apc_create(const apc_config *cfg, apc_context **out);
+int apc_destroy(apc_context *ctx);
+
+/* Particles: SoA FP64 host arrays of n_particles each.  apc_get_particles may be
+ * given NULL for arrays the caller does not want; accelerations are those of the
+ * last apc_move_velocity.  Particle order is the caller's order throughout. */
+int apc_set_particles(apc_context *ctx, const double *x, const double *y, const double *z,
+                      const double *vx, const double *vy, const double *vz);
+int apc_get_particles(apc_context *ctx, double *x, double *y, double *z, double *vx, double *vy,
+                      double *vz, double *ax, double *ay, double *az);
+/* Same with device pointers (n_particles doubles each, on the context's device). */
+int apc_set_particles_device(apc_context *ctx, const double *x, const double *y, const double *z,
+                             const double *vx, const double *vy, const double *vz);
+int apc_get_particles_device(apc_context *ctx, double *x, double *y, double *z, double *vx,
+                             double *vy, double *vz);
+
+/* ---- phases, in Controller::solve order (controller.cpp:133-197) ---- */
+
+/* Octree build + selection.  *n_cells = nc + nv + nb, the reference's return value. */
+int apc_select(apc_context *ctx, int *n_cells);
+/* GFD assembly, density solve, potential solve, differentiation.  c_dens, c_pot,
+ * c_field are the constants of Solver::Set_Constant_For_* (controller.cpp:184-186). */
+int apc_solve(apc_context *ctx, double c_dens, double c_pot, double c_field);
+/* Interpolation + kick v += a c_vel dt; *max_dv = max |a| c_vel dt (may be NULL). */
+int apc_move_velocity(apc_context *ctx, double dt, double c_vel, double *max_dv);
+/* Drift x = wrap(x + v c_pos dt); *max_dx = max |v| c_pos dt (may be NULL). */
+int apc_move_position(apc_context *ctx, double dt, double c_pos, double *max_dx);
+
+/* One whole step {select; solve; move_velocity; move_position} with the constants of
+ * controller.cpp:182-186 for time t and step dt.  Outputs may be NULL. */
+typedef struct apc_step_params {
+  double dt, c_dens, c_pot, c_field, c_vel, c_pos;
+} apc_step_params;
+int apc_step(apc_context *ctx, const apc_step_params *p, int *n_cells, double *max_dv,
+             double *max_dx);
+
+/* Wait for all work of the context. */
+int apc_synchronize(apc_context *ctx);
+
+/* ---- results of the last select / solve (parity and diagnostics) ---- */
+
+int apc_get_cell_counts(apc_context *ctx, int *nc, int *nv, int *nb, int *n_neigh24);
+/* Computational_particle arrays in the reference's output order.  first[i] of a cell
+ * holding no particle is the sorted position where its particles would start. */
+int apc_get_cells(apc_context *ctx, double *x, double *y, double *z, double *cell_length,
+                  int *first, int *count, int *type, int *first_neigh, int *number_neigh,
+                  int *neigh24);
+/* Octree location code of every cell: (1 << 3*level) | Morton prefix. */
+int apc_get_cell_codes(apc_context *ctx, uint64_t *codes);
+/* Sorted Morton keys and the caller's particle index for each (octree.cpp:131-148). */
+int apc_get_keys(apc_context *ctx, uint64_t *keys, int *index);
+/* numnodes[0..depth]: octree node count per level (octree.cpp:174-191). */
+int apc_get_octree_levels(apc_context *ctx, int *numnodes);
+/* Density, Potential and p_x..p_yz (9 per cell, in that order) of cells 0..nc+nv-1. */
+int apc_get_fields(apc_context *ctx, double *density, double *potential, double *deriv9);
+/* GFD stencil of each cell: lm neighbour indices and distances, in search order. */
+int apc_get_stencils(apc_context *ctx, int *idx, double *dist);
+int apc_get_solve_stats(apc_context *ctx, apc_solve_stats *stats);
+/* Matrix A1 (which = 0) or A2 (which = 1) in CSR, columns sorted per row.  Call with
+ * rowptr == NULL to get *n and *nnz first. */
+int apc_get_matrix(apc_context *ctx, int which, int *n, int *nnz, int *rowptr, int *col,
+                   double *val);
+
+/* Number of kernels this context has launched since creation. */
+int64_t apc_kernel_launches(const apc_context *ctx);
+
+/* Device time (ms) of the last select / solve / move phases, from CUDA events. */
+int apc_get_phase_times(apc_context *ctx, double *select_ms, double *solve_ms, double *move_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* APCLOUD_GPU_H */
