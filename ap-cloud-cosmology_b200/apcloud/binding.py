@@ -24,7 +24,7 @@ EXPORTED = [
     "apc_select", "apc_solve", "apc_move_velocity", "apc_move_position", "apc_step", "apc_synchronize",
     "apc_get_cell_counts", "apc_get_cells", "apc_get_cell_codes", "apc_get_keys", "apc_get_octree_levels",
     "apc_get_fields", "apc_get_stencils", "apc_get_solve_stats", "apc_get_matrix", "apc_kernel_launches",
-    "apc_get_phase_times",
+    "apc_get_phase_times", "apc_get_profile", "apc_reset_profile",
 ]
 
 
@@ -45,6 +45,12 @@ class ApcSolveStats(C.Structure):
         ("density_rnorm", C.c_double), ("potential_rnorm", C.c_double),
         ("density_refinements", C.c_int), ("potential_refinements", C.c_int),
     ]
+
+
+class ApcProfile(C.Structure):
+    _fields_ = [("krylov_launches", C.c_int64), ("krylov_iterations", C.c_int64), ("krylov_ms", C.c_double),
+                ("krylov_bytes", C.c_double), ("select_ms", C.c_double), ("solve_ms", C.c_double),
+                ("move_ms", C.c_double), ("steps", C.c_int64), ("step_ms", C.c_double)]
 
 
 class ApcStepParams(C.Structure):
@@ -97,6 +103,8 @@ def load_library(path: str = LIB_PATH):
         "apc_get_matrix": (C.c_int, [vp, C.c_int, ip, ip, vp, vp, vp]),
         "apc_kernel_launches": (C.c_int64, [vp]),
         "apc_get_phase_times": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "apc_get_profile": (C.c_int, [vp, C.POINTER(ApcProfile)]),
+        "apc_reset_profile": (C.c_int, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -298,6 +306,14 @@ class GpuPath:
 
     def kernel_launches(self) -> int:
         return int(self.lib.apc_kernel_launches(self.h))
+
+    def profile(self) -> dict:
+        pr = ApcProfile()
+        self._check(self.lib.apc_get_profile(self.h, C.byref(pr)), "apc_get_profile")
+        return {f: getattr(pr, f) for f, _ in ApcProfile._fields_}
+
+    def reset_profile(self):
+        self._check(self.lib.apc_reset_profile(self.h), "apc_reset_profile")
 
     def phase_times(self):
         a, b, c = C.c_double(), C.c_double(), C.c_double()

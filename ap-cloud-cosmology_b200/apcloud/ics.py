@@ -101,7 +101,7 @@ def zeldovich(n_side: int, spectral_index: float, rms_spacing: float, a_start: f
         dk = wk * amp
         inv = np.where(k2 > 0, 1.0 / k2, 0.0)
     # psi_k = i k / k^2 delta_k  (delta = -div psi)
-    psi = [np.fft.irfftn(1j * K * inv * dk, s=(n, n, n)) for K in (KX, KY, KZ)]
+    psi = [np.fft.irfftn(1j * K * inv * dk, s=(n, n, n), axes=(0, 1, 2)) for K in (KX, KY, KZ)]
     rms = math.sqrt(float(np.mean(psi[0] ** 2 + psi[1] ** 2 + psi[2] ** 2)))
     scale = rms_spacing / n / rms
     psi = [p * scale for p in psi]

@@ -119,7 +119,11 @@ struct apc_context {
 
   // ---- timing ----
   cudaEvent_t ev[8] = {};
+  cudaEvent_t kev[2] = {};   // around each GMRES launch
   double t_select_ms = 0, t_solve_ms = 0, t_move_ms = 0;
+  apc_profile prof{};
+  bool step_open = false;    // a select has started a step that move_position will close
+  bool kick_recorded = false;  // ev[4] holds the start of a move_velocity
 };
 
 // ----------------------------------------------------------- helpers (host)

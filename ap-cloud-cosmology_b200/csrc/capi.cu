@@ -95,6 +95,8 @@ void free_all(apc_context *c) {
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
+  for (auto &e : c->kev)
+    if (e) cudaEventDestroy(e);
   if (c->s) cudaStreamDestroy(c->s);
   g_caps.erase(c);
 }
@@ -110,7 +112,10 @@ int check_ready(apc_context *c, bool particles, bool cells, bool fields) {
 
 float elapsed(cudaEvent_t a, cudaEvent_t b) {
   float ms = 0.f;
-  cudaEventElapsedTime(&ms, a, b);
+  if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+    cudaGetLastError();  // a timing query must not leave a sticky error behind
+    ms = 0.f;
+  }
   return ms;
 }
 
@@ -191,6 +196,8 @@ int apc_create(const apc_config *cfg, apc_context **out) {
   }
   if (cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking) != cudaSuccess) return fail(APC_ERR_CUDA);
   for (auto &e : c->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return fail(APC_ERR_CUDA);
+  for (auto &e : c->kev)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(APC_ERR_CUDA);
   if (cudaMallocHost((void **)&c->h_pinned, 64 * sizeof(int)) != cudaSuccess) return fail(APC_ERR_CUDA);
   const size_t n = (size_t)c->n;
@@ -313,6 +320,7 @@ int apc_select(apc_context *c, int *n_cells) {
   c->have_cells = false;
   c->have_fields = false;
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[0], c->s));
+  c->step_open = true;
   APC_CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->s));
   APC_TRY(apc_octree_build(c));
   int derr = 0;
@@ -325,6 +333,7 @@ int apc_select(apc_context *c, int *n_cells) {
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[1], c->s));
   APC_CUDA_TRY(c, cudaEventSynchronize(c->ev[1]));
   c->t_select_ms = elapsed(c->ev[0], c->ev[1]);
+  c->prof.select_ms += c->t_select_ms;
   c->numnodes.clear();
   c->have_cells = true;
   if (n_cells) *n_cells = c->nc + c->nv + c->nb;
@@ -353,6 +362,8 @@ int apc_solve(apc_context *c, double c_dens, double c_pot, double c_field) {
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[3], c->s));
   APC_CUDA_TRY(c, cudaEventSynchronize(c->ev[3]));
   c->t_solve_ms = elapsed(c->ev[2], c->ev[3]);
+  c->prof.solve_ms += c->t_solve_ms;
+  c->prof.steps += 1;
   c->have_fields = true;
   return APC_OK;
 }
@@ -361,6 +372,7 @@ int apc_move_velocity(apc_context *c, double dt, double c_vel, double *max_dv) {
   APC_TRY(check_ready(c, true, true, true));
   cudaSetDevice(c->dev);
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[4], c->s));
+  c->kick_recorded = true;
   APC_TRY(apc_mover_velocity(c, dt, c_vel, max_dv));
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[5], c->s));
   return APC_OK;
@@ -372,7 +384,15 @@ int apc_move_position(apc_context *c, double dt, double c_pos, double *max_dx) {
   APC_TRY(apc_mover_position(c, dt, c_pos, max_dx));
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[6], c->s));
   APC_CUDA_TRY(c, cudaEventSynchronize(c->ev[6]));
-  if (cudaEventQuery(c->ev[4]) == cudaSuccess) c->t_move_ms = elapsed(c->ev[4], c->ev[6]);
+  if (c->kick_recorded) {
+    c->t_move_ms = elapsed(c->ev[4], c->ev[6]);
+    c->prof.move_ms += c->t_move_ms;
+    c->kick_recorded = false;
+  }
+  if (c->step_open) {
+    c->prof.step_ms += elapsed(c->ev[0], c->ev[6]);
+    c->step_open = false;
+  }
   return APC_OK;
 }
 
@@ -524,6 +544,18 @@ int apc_get_matrix(apc_context *c, int which, int *n, int *nnz, int *rowptr, int
 }
 
 int64_t apc_kernel_launches(const apc_context *c) { return c ? c->launches : 0; }
+
+int apc_get_profile(apc_context *c, apc_profile *out) {
+  if (!c || !out) return APC_ERR_INVALID_ARG;
+  *out = c->prof;
+  return APC_OK;
+}
+
+int apc_reset_profile(apc_context *c) {
+  if (!c) return APC_ERR_INVALID_ARG;
+  c->prof = apc_profile{};
+  return APC_OK;
+}
 
 int apc_get_phase_times(apc_context *c, double *a, double *b, double *d) {
   if (!c) return APC_ERR_INVALID_ARG;

@@ -557,8 +557,10 @@ static int launch_gmres(apc_context *c, int n, const T *val, const T *b, T *x, i
   a.out_reason = k->ires + 1;
   a.out_rnorm = k->dres;
   void *args[] = {&a};
+  APC_CUDA_TRY(c, cudaEventRecord(c->kev[0], c->s));
   APC_CUDA_TRY(c, cudaLaunchCooperativeKernel((const void *)gmres_kernel<T, RE>, dim3(blocks), dim3(kThreads),
                                               args, 0, c->s));
+  APC_CUDA_TRY(c, cudaEventRecord(c->kev[1], c->s));
   apc_count_launch(c);
   int hi[2];
   double hd;
@@ -574,6 +576,25 @@ static int launch_gmres(apc_context *c, int n, const T *val, const T *b, T *x, i
   *its = hi[0];
   *reason = hi[1];
   *rnorm = hd;
+  float ms = 0.f;
+  APC_CUDA_TRY(c, cudaEventElapsedTime(&ms, c->kev[0], c->kev[1]));
+  // algorithmic bytes of this launch (model documented in apcloud_gpu.h)
+  const double S = sizeof(T), W = c->ell_w, rows = n;
+  double per_row = 0.0;
+  int left = hi[0], cycles = 0;
+  while (left > 0 || cycles == 0) {
+    const int in_cycle = std::min(left, restart);
+    per_row += W * (S + 4) + 3 * S;  // restart residual
+    for (int j = 0; j < in_cycle; ++j) per_row += W * (S + 4) + (2.0 * j + 6) * S + (RE ? (j + 3) * S : 0.0);
+    per_row += (in_cycle + 1) * S;  // solution update
+    left -= in_cycle;
+    ++cycles;
+    if (in_cycle == 0) break;
+  }
+  c->prof.krylov_launches += 1;
+  c->prof.krylov_iterations += hi[0];
+  c->prof.krylov_ms += ms;
+  c->prof.krylov_bytes += per_row * rows;
   return APC_OK;
 }
 

@@ -1,0 +1,414 @@
+#!/usr/bin/env python
+"""Benchmark: particle-steps/s of the AP-Cloud gravity step on one or more B200s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): the 128^3 LambdaCDM Zel'dovich box.
+  - 2,097,152 particles, P(k) ~ k^-1.5, rms displacement 0.3 lattice spacings at
+    a = 0.02; Omega0 = 0.3, OmegaL = 0.7;
+  - 128 leapfrog steps to a = 1, depth 21, c = 6.2e-3, lm = 17;
+  - GMRES(30), rtol 1e-10, max_it 10000.
+A step is one pass of the Controller sequence (select; solve; kick; drift) over the
+whole particle set.  The timed arm is the mixed-precision path: FP32 Krylov inside FP64
+iterative refinement, FP64 GFD moments and FP64 leapfrog.  The plain FP64 GPU path is
+timed beside it from the same state, and the force error between the two is reported.
+
+Timing: W warm-up steps, then K steps.
+  - Each step is timed on the device with the library's CUDA events, on its own stream.
+  - L2 is flushed (a 512 MiB write) before each timed step.
+  - Ranks run independent replicas; the time is the max over ranks.
+  - `e2e` repeats K steps through the public API from pinned host buffers (particles
+    copied in, step, particles and accelerations copied out) and times them on the host.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "ap-cloud-cosmology_b200")
+sys.path.insert(0, PKG)
+
+import numpy as np  # noqa: E402
+
+from apcloud import ics  # noqa: E402
+
+METRIC = "particle-steps/s at 128^3: mixed-prec vs FP64 GPU path at equal force error"
+UNIT = "particle-steps/s"
+WORKLOAD = "lcdm128"
+REF_GMRES_SAMPLE_ITS = 200
+
+
+def workload_desc(cfg) -> str:
+    return (f"{cfg.name}: {round(cfg.n ** (1 / 3))}^3={cfg.n} particles, LambdaCDM Zel'dovich "
+            f"(Omega0={cfg.omega0}, OmegaL={cfg.omegal}, P(k)~k^{cfg.spectral_index}, rms {cfg.rms_spacing} "
+            f"spacing at a={cfg.a_start}), {cfg.steps} steps to a={cfg.a_end}, depth {cfg.depth}, "
+            f"c={cfg.gfd_c}, lm={cfg.lm}, GMRES({cfg.restart}) rtol {cfg.rtol}")
+
+
+# ------------------------------------------------------------------ helpers
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Dist:
+    def __init__(self, device: int):
+        self.ws, self.rank, self.local = dist_env()
+        self.pg = None
+        if self.ws > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as td
+
+            torch.cuda.set_device(device)
+            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+            self.pg = td
+
+    def barrier(self):
+        if self.pg:
+            import torch
+
+            t = torch.zeros(1, device="cuda")
+            self.pg.all_reduce(t)
+            torch.cuda.synchronize()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if parts[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> tuple[float, str]:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_launch(kernel: str) -> float | None:
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        for ln in open(path):
+            ln = ln.strip()
+            if ln.startswith(kernel + ":"):
+                return float(ln.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+# ------------------------------------------------------------------ our arm
+
+def run_ours(args) -> dict:
+    import torch
+
+    from apcloud import binding
+    from apcloud.controller import for_config
+
+    ws, rank, local = dist_env()
+    dev = local
+    torch.cuda.set_device(dev)
+    dist = Dist(dev)
+    cfg = ics.config(args.workload)
+    parts = cfg.particles()
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def make(prec, p):
+        return binding.GpuPath(p, cfg.depth, cfg.gfd_c, cfg.lm, restart=cfg.restart, rtol=cfg.rtol,
+                               precision=prec, device=dev, mixed_restart=args.mixed_restart,
+                               mixed_inner_rtol=args.inner_rtol)
+
+    # ---- warm-up on the mixed path ----
+    mx = make(binding.APC_PREC_MIXED, parts)
+    ctl = for_config(mx, cfg)
+    ctl.start()
+    for _ in range(args.warmup):
+        ctl.step()
+    state = mx.particles()
+    state_parts = ics.Particles(*state[:6])
+    t_state = ctl.t
+
+    # ---- force error of the two paths on the same state ----
+    acc = {}
+    for prec, name in ((binding.APC_PREC_FP64, "fp64"), (binding.APC_PREC_MIXED, "mixed")):
+        g = make(prec, state_parts)
+        c2 = for_config(g, cfg)
+        c2.t = t_state
+        k = c2.constants(c2.t, cfg.delta_a)
+        g.select()
+        g.solve(k["c_dens"], k["c_pot"], k["c_field"])
+        g.move_velocity(cfg.delta_a, k["c_vel"])
+        acc[name] = (np.stack(g.particles()[6:9]), g.solve_stats())
+        g.close()
+    a64, amx = acc["fp64"][0], acc["mixed"][0]
+    force_err = float(np.sqrt(np.mean(np.sum((amx - a64) ** 2, 0)) / np.mean(np.sum(a64 ** 2, 0))))
+
+    def timed(g, c):
+        dist.barrier()
+        torch.cuda.synchronize()
+        g.reset_profile()
+        l0 = g.kernel_launches()
+        with ClockSampler(dev) as clk:
+            for _ in range(args.steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                c.step()
+        dist.barrier()
+        pr = g.profile()
+        return pr, g.kernel_launches() - l0, clk.summary()
+
+    prof, launches, clocks = timed(mx, ctl)
+    step_ms = dist.max(prof["step_ms"])
+    value = ws * cfg.n * args.steps / (step_ms / 1e3)
+
+    fp64_value = None
+    fp64_ms = None
+    if not args.no_fp64:
+        g64 = make(binding.APC_PREC_FP64, state_parts)
+        c64 = for_config(g64, cfg)
+        c64.t = t_state
+        p64, _, _ = timed(g64, c64)
+        fp64_ms = dist.max(p64["step_ms"])
+        fp64_value = ws * cfg.n * args.steps / (fp64_ms / 1e3)
+        fp64_stats = g64.solve_stats()
+        g64.close()
+
+    # ---- end to end through the public API with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        pin = [torch.empty(cfg.n, dtype=torch.float64).pin_memory().numpy() for _ in range(9)]
+        cur = mx.particles()
+        for a, b in zip(pin[:6], cur[:6]):
+            a[:] = b
+        lib = mx.lib
+        dist.barrier()
+        tot = 0.0
+        t = ctl.t
+        for _ in range(args.steps):
+            k = ctl.constants(t, cfg.delta_a)
+            t0 = time.perf_counter()
+            mx._check(lib.apc_set_particles(mx.h, *[a.ctypes.data for a in pin[:6]]), "apc_set_particles")
+            mx.step(cfg.delta_a, k["c_dens"], k["c_pot"], k["c_field"], k["c_vel"], k["c_pos"])
+            mx._check(lib.apc_get_particles(mx.h, *[a.ctypes.data for a in pin]), "apc_get_particles")
+            tot += time.perf_counter() - t0
+            t += cfg.delta_a
+        tot = dist.max(tot)
+        e2e = {"value": ws * cfg.n * args.steps / tot, "unit": UNIT, "h2d_bytes_per_step": 6 * 8 * cfg.n,
+               "d2h_bytes_per_step": 9 * 8 * cfg.n, "timing": "host wall clock per step, max over ranks"}
+
+    peak, peak_kind = measured_peaks()
+    kb = prof["krylov_bytes"] / max(prof["krylov_launches"], 1)
+    kms = prof["krylov_ms"] / max(prof["krylov_launches"], 1)
+    achieved = kb / (kms / 1e3) / 1e9 if kms > 0 else 0.0
+    st = mx.solve_stats()
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": step_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 Krylov / f64 refinement, GFD moments and leapfrog", "data": "synthetic",
+        "config": {"workload": workload_desc(cfg), "precision": "mixed", "parallelism": f"replicas x{ws}",
+                   "l2": "flushed (512 MiB write) before every timed step",
+                   "start_a": round(t_state, 6), "mixed_restart": args.mixed_restart or 30,
+                   "inner_rtol": args.inner_rtol or 1e-5},
+        "fp64": {"value": fp64_value, "ms_per_step": (fp64_ms / args.steps) if fp64_ms else None,
+                 "speedup_mixed_over_fp64": (value / fp64_value) if fp64_value else None,
+                 "potential_its": fp64_stats["potential_its"] if fp64_value else None,
+                 "potential_reason": fp64_stats["potential_reason"] if fp64_value else None},
+        "force_error": {"acc_rms_rel_mixed_vs_fp64": force_err, "bound": 1e-6,
+                        "fp64_potential_reason": acc["fp64"][1]["potential_reason"],
+                        "mixed_potential_reason": acc["mixed"][1]["potential_reason"]},
+        "phases_ms_per_step": {"select": prof["select_ms"] / args.steps, "solve": prof["solve_ms"] / args.steps,
+                               "move": prof["move_ms"] / args.steps,
+                               "krylov": prof["krylov_ms"] / args.steps},
+        "solve": {"potential_its": st["potential_its"], "potential_refinements": st["potential_refinements"],
+                  "potential_reason": st["potential_reason"], "density_its": st["density_its"],
+                  "krylov_iterations_per_step": prof["krylov_iterations"] / args.steps},
+        "roofline": {"kernel": "gmres_kernel<float,CGS2> (FP32 inner GMRES)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": ncu_traffic_per_launch("gmres_f32"),
+                     "bytes_per_launch": kb, "ms_per_launch": kms},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "e2e": e2e,
+    }
+    mx.close()
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(cfg, args)
+    dist.close()
+    return out if rank == 0 else None
+
+
+# ------------------------------------------------------------- CPU reference
+
+def reference_sample(cfg, parts_state, t, fp64_its: int | None, args):
+    """One bounded sample of a step through the reference's own code (oracle/_ref).
+    Select, GFD assembly, differentiation and mover run in full.  The potential GMRES
+    is timed for REF_GMRES_SAMPLE_ITS iterations and its time scaled per iteration to
+    the full step's iteration count: the FP64 path's count when known, else max_it,
+    which the reference reaches at this size.  GMRES(30) iterations cost the same
+    throughout a solve, so the scaling is linear."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refbind  # test infrastructure: only the CPU baseline leg loads it
+
+    r = refbind.CpuPath("ref", parts_state, cfg.depth, cfg.gfd_c, cfg.lm)
+    r.set_gmres(cfg.restart, cfg.rtol, 1e-50, 1e5, REF_GMRES_SAMPLE_ITS)
+    r.reset_solve_stats()
+    t0 = time.perf_counter()
+    r.select()
+    t1 = time.perf_counter()
+    k = dict(c_dens=1.0 / cfg.n, c_pot=1.5 * cfg.omega0 / t)
+    r.solve(k["c_dens"], k["c_pot"], -1.0)
+    t2 = time.perf_counter()
+    r.move_velocity(cfg.delta_a, ics.kick_factor(t, cfg.omega0, cfg.omegal))
+    r.move_position(cfg.delta_a, ics.drift_factor(t + cfg.delta_a / 2, cfg.omega0, cfg.omegal))
+    t3 = time.perf_counter()
+    st = r.solve_stats()
+    r.close()
+    its_s, sec_s = st[-1][0], st[-1][3]
+    full_its = fp64_its if fp64_its else 10000
+    per_it = sec_s / max(its_s, 1)
+    est = (t1 - t0) + (t2 - t1 - sec_s) + per_it * full_its + (t3 - t2)
+    return est, (t3 - t0), its_s, full_its, per_it
+
+
+def cpu_baseline(cfg, args) -> dict:
+    parts = cfg.particles()
+    t = cfg.a_start + 0.5 * cfg.delta_a
+    est, measured, its_s, full_its, per_it = reference_sample(cfg, parts, t, None, args)
+    return {"value": cfg.n / est, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+            "sample": (f"one 128^3 step through the reference code (oracle/_ref): select, GFD assembly, "
+                       f"differentiation and mover timed in full; potential GMRES timed for {its_s} iterations "
+                       f"({per_it * 1e3:.1f} ms each) and scaled to {full_its} iterations; {measured:.1f} s measured, "
+                       f"{est:.1f} s per step estimated; OpenMP regions on all cores, GMRES on one"),
+            "seconds_per_step": est}
+
+
+def run_reference(args) -> dict | None:
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return None
+    cfg = ics.config(args.workload)
+    ref_so = os.path.join(ROOT, "oracle", "_ref", "libapcref.so")
+    if not os.path.exists(ref_so):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libapcref.so not built (make -C oracle ref)"}
+    parts = cfg.particles()
+    t = cfg.a_start + 0.5 * cfg.delta_a
+    for _ in range(args.warmup):
+        reference_sample(cfg, parts, t, None, args)
+    ests = []
+    meas = 0.0
+    for _ in range(args.steps):
+        est, measured, its_s, full_its, per_it = reference_sample(cfg, parts, t, None, args)
+        ests.append(est)
+        meas += measured
+    total = sum(ests)
+    value = cfg.n * args.steps / total
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_desc(cfg), "precision": "fp64 (reference CPU path)"},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                             "sample": (f"each step: one 128^3 step of the reference code with the potential "
+                                        f"GMRES timed for {REF_GMRES_SAMPLE_ITS} iterations and scaled to "
+                                        f"{full_its}; {meas:.1f} s measured in total")},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--mixed-restart", type=int, default=0)
+    ap.add_argument("--inner-rtol", type=float, default=0.0)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

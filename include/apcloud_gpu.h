@@ -164,6 +164,23 @@ int apc_get_matrix(apc_context *ctx, int which, int *n, int *nnz, int *rowptr, i
 /* Number of kernels this context has launched since creation. */
 int64_t apc_kernel_launches(const apc_context *ctx);
 
+/* Counters of the GMRES kernel (the dominant kernel) since the last reset.
+ * krylov_bytes follows the algorithmic model: per Arnoldi step
+ * W*(S+4) + (2*j + 6)*S bytes per row for basis index j, where W is the ELL width and
+ * S the vector word size.  A CGS2 step adds (j + 3)*S.  Each restart adds
+ * W*(S+4) + 3*S and each solution update (j + 2)*S. */
+typedef struct apc_profile {
+  int64_t krylov_launches;
+  int64_t krylov_iterations;
+  double krylov_ms;      /* summed device time of those launches (CUDA events) */
+  double krylov_bytes;   /* algorithmic bytes of those launches */
+  double select_ms, solve_ms, move_ms;  /* summed phase device times */
+  int64_t steps;         /* completed solve phases */
+  double step_ms;        /* summed device time from each select to the next move_position */
+} apc_profile;
+int apc_get_profile(apc_context *ctx, apc_profile *out);
+int apc_reset_profile(apc_context *ctx);
+
 /* Device time (ms) of the last select / solve / move phases, from CUDA events. */
 int apc_get_phase_times(apc_context *ctx, double *select_ms, double *solve_ms, double *move_ms);
 

@@ -1,0 +1,77 @@
+"""CPU tests of the C ABI boundary: the library loads, exports every entry point that
+include/apcloud_gpu.h declares, and rejects invalid arguments before touching a device."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "apcloud_gpu.h")
+
+
+def declared_functions() -> list[str]:
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(apc_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_phase_entry_points():
+    names = declared_functions()
+    for n in ("apc_create", "apc_destroy", "apc_set_particles", "apc_select", "apc_solve",
+              "apc_move_velocity", "apc_move_position", "apc_get_cells", "apc_get_fields", "apc_step"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol(gpu_lib):
+    out = subprocess.run(["nm", "-D", "--defined-only", gpu_lib], capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r"\bT (apc_[a-z0-9_]+)\b", out))
+    missing = [n for n in declared_functions() if n not in exported]
+    assert not missing, missing
+
+
+def test_binding_covers_every_declared_symbol():
+    from apcloud import binding
+
+    assert sorted(binding.EXPORTED) == declared_functions()
+
+
+def test_library_loads_and_rejects_invalid_config(gpu_lib):
+    from apcloud import binding
+
+    lib = binding.load_library(gpu_lib)
+    assert lib.apc_status_string(0) == b"ok"
+    assert lib.apc_status_string(-5) == b"temp-node budget exceeded"
+    cfg = binding.ApcConfig()
+    lib.apc_config_default(C.byref(cfg))
+    assert (cfg.depth, cfg.lm, cfg.gmres_restart, cfg.maxnc) == (21, 17, 30, 10000)
+    assert cfg.gmres_rtol == pytest.approx(1e-10)
+    h = C.c_void_p()
+    assert lib.apc_create(None, C.byref(h)) == -1
+    for field, bad in (("n_particles", 0), ("depth", 22), ("depth", 0), ("lm", 8), ("lm", 33),
+                       ("gmres_restart", 0), ("gmres_restart", 32), ("precision", 7), ("bc", 2)):
+        c2 = binding.ApcConfig()
+        lib.apc_config_default(C.byref(c2))
+        c2.n_particles = 100
+        setattr(c2, field, bad)
+        assert lib.apc_create(C.byref(c2), C.byref(h)) == -1, field
+    c3 = binding.ApcConfig()
+    lib.apc_config_default(C.byref(c3))
+    c3.n_particles = 100
+    c3.box[1] = c3.box[0]  # empty box
+    assert lib.apc_create(C.byref(c3), C.byref(h)) == -1
+    # phase calls on a null context fail cleanly
+    assert lib.apc_select(None, None) == -1
+    assert lib.apc_destroy(None) == -1
+    assert lib.apc_kernel_launches(None) == 0
+
+
+def test_library_is_built_for_sm100a(gpu_lib):
+    out = subprocess.run(["cuobjdump", "--list-elf", gpu_lib], capture_output=True, text=True)
+    if out.returncode != 0:
+        pytest.skip("cuobjdump unavailable")
+    assert "sm_100a" in out.stdout
