@@ -24,7 +24,7 @@ EXPORTED = [
     "apc_select", "apc_solve", "apc_move_velocity", "apc_move_position", "apc_step", "apc_synchronize",
     "apc_get_cell_counts", "apc_get_cells", "apc_get_cell_codes", "apc_get_keys", "apc_get_octree_levels",
     "apc_get_fields", "apc_get_stencils", "apc_get_solve_stats", "apc_get_matrix", "apc_kernel_launches",
-    "apc_get_phase_times", "apc_get_profile", "apc_reset_profile",
+    "apc_get_phase_times", "apc_get_profile", "apc_reset_profile", "apc_move_velocity_noalloc",
 ]
 
 
@@ -105,6 +105,8 @@ def load_library(path: str = LIB_PATH):
         "apc_get_phase_times": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "apc_get_profile": (C.c_int, [vp, C.POINTER(ApcProfile)]),
         "apc_reset_profile": (C.c_int, [vp]),
+        "apc_move_velocity_noalloc": (C.c_int, [C.c_int, C.c_int] + [vp] * 15 + [C.c_double, C.c_double,
+                                                                                  C.POINTER(C.c_double), vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

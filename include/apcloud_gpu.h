@@ -181,6 +181,35 @@ typedef struct apc_profile {
 int apc_get_profile(apc_context *ctx, apc_profile *out);
 int apc_reset_profile(apc_context *ctx);
 
+/* Interpolation + kick (the work of apc_move_velocity) on caller-owned device buffers,
+ * for callers that cannot allocate device memory: embedders whose framework owns all
+ * device memory through its own allocator, or loops that cannot afford the device-wide
+ * synchronisation of cudaMalloc / cudaFree.  No counterpart in the reference: it has no
+ * GPU code and no caller with this constraint.
+ *
+ * This call allocates nothing.  Its scratch (particle -> cell map, max-change
+ * accumulator) is a fixed 4 MiB + 256 B array inside the library that every GPU loading
+ * the library keeps until the process exits, so n_particles may not exceed
+ * APC_NOALLOC_MAX_PARTICLES (larger sizes return APC_ERR_INVALID_ARG).  The first call
+ * on a device looks up the array's device address (once per device) and should come
+ * before any stream capture.  All calls share the one array: calls whose work overlaps
+ * on the GPU (other streams, other host threads) race and must be serialised by the
+ * caller.  Each call resets the parts of the scratch that must start cleared.
+ *
+ * Inputs, all device pointers on the current device: particles x, y, z in cell order
+ * (cell i owns particles first[i] .. first[i]+count[i]-1); cell centres cx, cy, cz;
+ * deriv9 = p_x p_y p_z p_xx p_yy p_zz p_xy p_xz p_yz per cell.  In/out: vx, vy, vz
+ * (v += a c_vel dt).  Out: ax, ay, az; *max_dv (host, may be NULL) as apc_move_velocity.
+ * stream: a cudaStream_t, or NULL for the default stream; the call returns after the
+ * stream has finished its work. */
+#define APC_NOALLOC_MAX_PARTICLES (1 << 20)
+int apc_move_velocity_noalloc(int n_particles, int n_cells, const int *first, const int *count,
+                              const double *cx, const double *cy, const double *cz,
+                              const double *deriv9, const double *x, const double *y,
+                              const double *z, double *vx, double *vy, double *vz, double *ax,
+                              double *ay, double *az, double dt, double c_vel, double *max_dv,
+                              void *stream);
+
 /* Device time (ms) of the last select / solve / move phases, from CUDA events. */
 int apc_get_phase_times(apc_context *ctx, double *select_ms, double *solve_ms, double *move_ms);
 
