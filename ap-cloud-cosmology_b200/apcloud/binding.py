@@ -50,7 +50,8 @@ class ApcSolveStats(C.Structure):
 class ApcProfile(C.Structure):
     _fields_ = [("krylov_launches", C.c_int64), ("krylov_iterations", C.c_int64), ("krylov_ms", C.c_double),
                 ("krylov_bytes", C.c_double), ("select_ms", C.c_double), ("solve_ms", C.c_double),
-                ("move_ms", C.c_double), ("steps", C.c_int64), ("step_ms", C.c_double)]
+                ("move_ms", C.c_double), ("steps", C.c_int64), ("step_ms", C.c_double),
+                ("gfd_ms", C.c_double)]
 
 
 class ApcStepParams(C.Structure):

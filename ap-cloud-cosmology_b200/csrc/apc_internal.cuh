@@ -120,6 +120,7 @@ struct apc_context {
   // ---- timing ----
   cudaEvent_t ev[8] = {};
   cudaEvent_t kev[2] = {};   // around each GMRES launch
+  cudaEvent_t gev[2] = {};   // around the GFD stencil kernel
   double t_select_ms = 0, t_solve_ms = 0, t_move_ms = 0;
   apc_profile prof{};
   bool step_open = false;    // a select has started a step that move_position will close

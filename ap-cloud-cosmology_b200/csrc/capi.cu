@@ -97,6 +97,8 @@ void free_all(apc_context *c) {
     if (e) cudaEventDestroy(e);
   for (auto &e : c->kev)
     if (e) cudaEventDestroy(e);
+  for (auto &e : c->gev)
+    if (e) cudaEventDestroy(e);
   if (c->s) cudaStreamDestroy(c->s);
   g_caps.erase(c);
 }
@@ -198,6 +200,8 @@ int apc_create(const apc_config *cfg, apc_context **out) {
   for (auto &e : c->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(APC_ERR_CUDA);
   for (auto &e : c->kev)
+    if (cudaEventCreate(&e) != cudaSuccess) return fail(APC_ERR_CUDA);
+  for (auto &e : c->gev)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(APC_ERR_CUDA);
   if (cudaMallocHost((void **)&c->h_pinned, 64 * sizeof(int)) != cudaSuccess) return fail(APC_ERR_CUDA);
   const size_t n = (size_t)c->n;

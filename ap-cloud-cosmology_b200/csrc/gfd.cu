@@ -492,11 +492,16 @@ int apc_gfd_assemble(apc_context *c, double c_dens) {
   P.ld = ld;
   P.err = c->d_err;
   const int blocks = std::max(1, std::min((M + kWarps - 1) / kWarps, apc_sm_count(c) * 16));
+  APC_CUDA_TRY(c, cudaEventRecord(c->gev[0], c->s));
   gfd_stencil<<<blocks, 32 * kWarps, 0, c->s>>>(P);
+  APC_CUDA_TRY(c, cudaEventRecord(c->gev[1], c->s));
   apc_count_launch(c);
   APC_CUDA_TRY(c, cudaGetLastError());
   int derr = 0;
   APC_TRY(apc_read_errors(c, &derr));
+  float gms = 0.f;
+  APC_CUDA_TRY(c, cudaEventElapsedTime(&gms, c->gev[0], c->gev[1]));
+  c->prof.gfd_ms += gms;
   if (derr & (DERR_STENCIL_FEW | DERR_STENCIL_MANY)) {
     c->err = (derr & DERR_STENCIL_FEW) ? "GFD neighbour search: not enough neighbours after 5 expansions"
                                        : "GFD neighbour search: candidate buffers exceeded";

@@ -34,9 +34,10 @@
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 1024;              // one block per SM
 constexpr int kWarpsPB = kThreads / 32;
-constexpr int kPartStride = 72;  // doubles per block per partial-sum slot set
+constexpr int kMaxBlocks = 256;             // partial sums are laid out [slot][block]
+constexpr int kSlots = 48;                  // slots per partial-sum buffer
 constexpr long long kSpinLimit = 1ll << 24;  // ~1-2 s of __nanosleep(64)
 
 struct GridBar {
@@ -99,7 +100,7 @@ struct GmresArgs {
   T *x;                 // solution (out)
   T *U;                 // (restart+1) x n basis, un-normalised
   size_t un;            // basis leading dimension
-  double *part;         // 2 x nblocks x kPartStride partial sums
+  double *part;         // 2 x kSlots x kMaxBlocks partial sums
   GridBar *bar;
   int *err;
   int restart;
@@ -115,31 +116,26 @@ __device__ __forceinline__ T ldcg(const T *p) {
   return __ldcg(p);
 }
 
-__device__ __forceinline__ double block_reduce_many(double (&acc)[33], int nv, double *sm_red) {
-  // per warp reduce each slot, then stage [warp][slot]; caller sums over warps
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int j = 0; j < 33; ++j) {
-    if (j < nv) {
-      double v = acc[j];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if (lane == 0) sm_red[warp * 33 + j] = v;
-    }
-  }
-  return 0.0;
-}
-
-// sum of slot j over all blocks' partials, identical in every block
+// sum of slot j over all blocks' partials, identical in every block: each lane adds a
+// fixed strided subset with independent loads (one L2 round trip), then a shuffle tree
 __device__ __forceinline__ void gather_partials(const double *part, int nblocks, int nv, double *out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int j = warp; j < nv; j += kWarpsPB) {
+    const double *row = part + (size_t)j * kMaxBlocks;
     double v = 0.0;
-    for (int b = lane; b < nblocks; b += 32) v += __ldcg(part + (size_t)b * kPartStride + j);
+#pragma unroll
+    for (int k = 0; k < kMaxBlocks / 32; ++k) {
+      const int b = lane + 32 * k;
+      if (b < nblocks) v += __ldcg(row + b);
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) out[j] = v;
   }
+}
+
+__device__ __forceinline__ void put_partial(double *part, int j, double v) {
+  part[(size_t)j * kMaxBlocks + blockIdx.x] = v;
 }
 
 __device__ __forceinline__ int converged_default(int n_its, double rnorm, double rtol, double atol,
@@ -154,60 +150,104 @@ __device__ __forceinline__ int converged_default(int n_its, double rnorm, double
   return 0;
 }
 
+// sum of one value per thread over the block; the result is valid in warp 0
+__device__ __forceinline__ double block_sum(double v, double *sm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0) sm[warp] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (warp == 0) {
+    r = lane < kWarpsPB ? sm[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+  }
+  __syncthreads();
+  return r;
+}
+
+// The block's partial dot products <a, u_j>, j < nv, over its row range [r0, r1):
+// every warp covers a contiguous sub-range with coalesced loads, four basis vectors per
+// sweep, then the warps' sums are added in a fixed order and published as partials.
+template <class T>
+__device__ __forceinline__ void block_dots(const T *a, const T *U, size_t un, int r0, int r1, int nv,
+                                           double *sm_red, double *part) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int per = (r1 - r0 + kWarpsPB - 1) / kWarpsPB;
+  const int ws = r0 + warp * per, we = min(r1, ws + per);
+  for (int j0 = 0; j0 < nv; j0 += 4) {
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int r = ws + lane; r < we; r += 32) {
+      const double ar = (double)ldcg(a + r);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (j0 + q < nv) v[q] += ar * (double)ldcg(U + (size_t)(j0 + q) * un + r);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      double t = v[q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (lane == 0 && j0 + q < nv) sm_red[warp * 33 + j0 + q] = t;
+    }
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < nv) {
+    double t = 0.0;
+    for (int wv = 0; wv < kWarpsPB; ++wv) t += sm_red[wv * 33 + threadIdx.x];
+    put_partial(part, threadIdx.x, t);
+  }
+}
+
+// Each block owns the contiguous rows [r0, r1); within a pass every thread takes rows
+// r0 + threadIdx.x + k * blockDim.x.
 template <class T, bool REORTH>
-__global__ void __launch_bounds__(kThreads) gmres_kernel(GmresArgs<T> A) {
+__global__ void __launch_bounds__(kThreads, 1) gmres_kernel(GmresArgs<T> A) {
   constexpr int MAXV = 32;  // restart <= 31
   __shared__ double sm_red[kWarpsPB * 33];
   __shared__ double sh[MAXV + 1];      // reduced dots / norms of this step
   __shared__ double HH[(MAXV + 1) * MAXV];
   __shared__ double cc[MAXV], ss[MAXV], grs[MAXV + 1], scale[MAXV + 1], coef[MAXV + 1];
-  __shared__ int s_flow[4];  // reason, it, hapend, its
-  __shared__ double s_res, s_ttol, s_rnorm0;
+  __shared__ int s_flow[4];
+  __shared__ double s_res;
 
   const int nb = gridDim.x;
   const int m = A.restart;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int stride = gridDim.x * blockDim.x;
+  const int rpb = (A.n + nb - 1) / nb;
+  const int r0 = min(A.n, (int)blockIdx.x * rpb), r1 = min(A.n, r0 + rpb);
   double *partA = A.part;
-  double *partB = A.part + (size_t)nb * kPartStride;
-  double acc[33];
+  double *partB = A.part + (size_t)kSlots * kMaxBlocks;
 
-  for (int i = tid; i < A.n; i += stride) A.x[i] = T(0);
+  for (int i = r0 + threadIdx.x; i < r1; i += kThreads) A.x[i] = T(0);
   int its = 0, reason = 0, itcount = 0;
   bool guess_zero = true;
   double ttol = 0.0, rnorm0 = 0.0, res = 0.0;
-  if (threadIdx.x == 0) {
-    s_ttol = 0.0;
-    s_rnorm0 = 0.0;
-  }
+  if (threadIdx.x == 0) s_res = 0.0;
   if (!grid_sync(A.bar, nb, A.err)) return;
 
   while (!reason) {
     // ---- initial residual: u0 = D^-1 (b - A x) ----
     double nrm = 0.0;
-    for (int i = tid; i < A.n; i += stride) {
+    for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
       const T d = A.val[i];
       const double di = d == T(0) ? 1.0 : 1.0 / (double)d;
       double r = (double)A.b[i];
       if (!guess_zero) {
-        double s = 0.0;
+        double sacc = 0.0;
         for (int k = 0; k < A.w; ++k) {
           const size_t at = (size_t)k * A.ld + i;
-          s += (double)A.val[at] * (double)ldcg(A.x + A.col[at]);
+          sacc += (double)A.val[at] * (double)ldcg(A.x + A.col[at]);
         }
-        r -= s;
+        r -= sacc;
       }
       const double u = di * r;
       A.U[i] = T(u);
       nrm += u * u;
     }
-    acc[0] = nrm;
-    block_reduce_many(acc, 1, sm_red);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double v = 0.0;
-      for (int wv = 0; wv < kWarpsPB; ++wv) v += sm_red[wv * 33];
-      partB[(size_t)blockIdx.x * kPartStride] = v;
+    {
+      const double v = block_sum(nrm, sm_red);
+      if (threadIdx.x == 0) put_partial(partB, 0, v);
     }
     if (!grid_sync(A.bar, nb, A.err)) return;
     gather_partials(partB, nb, 1, sh);
@@ -229,78 +269,53 @@ __global__ void __launch_bounds__(kThreads) gmres_kernel(GmresArgs<T> A) {
       const T *uk = A.U + (size_t)it * A.un;
       T *w = A.U + (size_t)(it + 1) * A.un;
       const double sk = scale[it];
-      // ---- pass A: w = D^-1 A v_it, dots with u_0..u_it ----
-#pragma unroll
-      for (int j = 0; j < 33; ++j) acc[j] = 0.0;
-      for (int i = tid; i < A.n; i += stride) {
+      // ---- pass A: w = D^-1 A v_it, then the block's dots with u_0..u_it ----
+      for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
         const T d = A.val[i];
         const double di = d == T(0) ? 1.0 : 1.0 / (double)d;
-        double s = 0.0;
+        double sacc = 0.0;
         for (int k = 0; k < A.w; ++k) {
           const size_t at = (size_t)k * A.ld + i;
-          s += (double)A.val[at] * (double)ldcg(uk + A.col[at]);
+          sacc += (double)A.val[at] * (double)ldcg(uk + A.col[at]);
         }
-        const T wi = T(di * sk * s);
-        w[i] = wi;
-#pragma unroll
-        for (int j = 0; j < MAXV; ++j)
-          if (j <= it) acc[j] += (double)wi * (double)ldcg(A.U + (size_t)j * A.un + i);
+        w[i] = T(di * sk * sacc);
       }
-      block_reduce_many(acc, it + 1, sm_red);
       __syncthreads();
-      if (threadIdx.x <= it) {
-        double v = 0.0;
-        for (int wv = 0; wv < kWarpsPB; ++wv) v += sm_red[wv * 33 + threadIdx.x];
-        partA[(size_t)blockIdx.x * kPartStride + threadIdx.x] = v;
-      }
+      block_dots(w, A.U, A.un, r0, r1, it + 1, sm_red, partA);
       if (!grid_sync(A.bar, nb, A.err)) return;
       gather_partials(partA, nb, it + 1, sh);
       __syncthreads();
-      if (threadIdx.x <= it) {
+      if ((int)threadIdx.x <= it) {
         const double h = sh[threadIdx.x] * scale[threadIdx.x];  // <v_j, w>
         HH[it * (MAXV + 1) + threadIdx.x] = h;
         coef[threadIdx.x] = h * scale[threadIdx.x];              // weight on u_j
       }
       __syncthreads();
-      // ---- pass B: w -= sum_j h_j v_j ; norm (or CGS2 second dots) ----
-#pragma unroll
-      for (int j = 0; j < 33; ++j) acc[j] = 0.0;
-      for (int i = tid; i < A.n; i += stride) {
+      // ---- pass B: w -= sum_j h_j v_j, then its norm (CGS) or a second sweep (CGS2) ----
+      double nr = 0.0;
+      for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
         double t = (double)ldcg(w + i);
 #pragma unroll
         for (int j = 0; j < MAXV; ++j)
           if (j <= it) t -= coef[j] * (double)ldcg(A.U + (size_t)j * A.un + i);
         const T tv = T(t);
         w[i] = tv;
-        if (REORTH) {
-#pragma unroll
-          for (int j = 0; j < MAXV; ++j)
-            if (j <= it) acc[j] += (double)tv * (double)ldcg(A.U + (size_t)j * A.un + i);
-        } else {
-          acc[0] += (double)tv * (double)tv;
-        }
+        nr += (double)tv * (double)tv;
       }
-      const int nvb = REORTH ? it + 1 : 1;
-      block_reduce_many(acc, nvb, sm_red);
-      __syncthreads();
-      if (threadIdx.x < nvb) {
-        double v = 0.0;
-        for (int wv = 0; wv < kWarpsPB; ++wv) v += sm_red[wv * 33 + threadIdx.x];
-        partB[(size_t)blockIdx.x * kPartStride + threadIdx.x] = v;
-      }
-      if (!grid_sync(A.bar, nb, A.err)) return;
-      gather_partials(partB, nb, nvb, sh);
-      __syncthreads();
       if (REORTH) {
-        // ---- pass C: second Gram-Schmidt sweep, then the norm ----
-        if (threadIdx.x <= it) {
+        __syncthreads();
+        block_dots(w, A.U, A.un, r0, r1, it + 1, sm_red, partB);
+        if (!grid_sync(A.bar, nb, A.err)) return;
+        gather_partials(partB, nb, it + 1, sh);
+        __syncthreads();
+        if ((int)threadIdx.x <= it) {
           const double h2 = sh[threadIdx.x] * scale[threadIdx.x];
           HH[it * (MAXV + 1) + threadIdx.x] += h2;
           coef[threadIdx.x] = h2 * scale[threadIdx.x];
         }
         __syncthreads();
-        double nr = 0.0;
-        for (int i = tid; i < A.n; i += stride) {
+        nr = 0.0;
+        for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
           double t = (double)ldcg(w + i);
 #pragma unroll
           for (int j = 0; j < MAXV; ++j)
@@ -309,16 +324,16 @@ __global__ void __launch_bounds__(kThreads) gmres_kernel(GmresArgs<T> A) {
           w[i] = tv;
           nr += (double)tv * (double)tv;
         }
-        acc[0] = nr;
-        block_reduce_many(acc, 1, sm_red);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-          double v = 0.0;
-          for (int wv = 0; wv < kWarpsPB; ++wv) v += sm_red[wv * 33];
-          partA[(size_t)blockIdx.x * kPartStride + 40] = v;
-        }
+        const double v = block_sum(nr, sm_red);
+        if (threadIdx.x == 0) put_partial(partA, 40, v);
         if (!grid_sync(A.bar, nb, A.err)) return;
-        gather_partials(partA + 40, nb, 1, sh);
+        gather_partials(partA + (size_t)40 * kMaxBlocks, nb, 1, sh);
+        __syncthreads();
+      } else {
+        const double v = block_sum(nr, sm_red);
+        if (threadIdx.x == 0) put_partial(partB, 0, v);
+        if (!grid_sync(A.bar, nb, A.err)) return;
+        gather_partials(partB, nb, 1, sh);
         __syncthreads();
       }
       // ---- Hessenberg / Givens (KSPGMRESUpdateHessenberg), every block alike ----
@@ -336,7 +351,7 @@ __global__ void __launch_bounds__(kThreads) gmres_kernel(GmresArgs<T> A) {
           hh[j] = cc[j - 1] * hh[j] - ss[j - 1] * t0;
         }
         int rs = 0;
-        double r = 0.0;
+        double rr = s_res;
         if (!hapend) {
           const double t = sqrt(hh[it] * hh[it] + hh[it + 1] * hh[it + 1]);
           if (t == 0.0) {
@@ -347,12 +362,14 @@ __global__ void __launch_bounds__(kThreads) gmres_kernel(GmresArgs<T> A) {
             grs[it + 1] = -(ss[it] * grs[it]);
             grs[it] = cc[it] * grs[it];
             hh[it] = cc[it] * hh[it] + ss[it] * hh[it + 1];
-            r = fabs(grs[it + 1]);
+            rr = fabs(grs[it + 1]);
           }
+        } else {
+          rr = 0.0;
         }
         s_flow[0] = rs;
         s_flow[2] = hapend;
-        s_res = rs ? s_res : r;
+        s_res = rr;
       }
       __syncthreads();
       const int rs = s_flow[0], hapend = s_flow[2];
@@ -386,7 +403,7 @@ __global__ void __launch_bounds__(kThreads) gmres_kernel(GmresArgs<T> A) {
         for (int j = 0; j <= last; ++j) coef[j] = y[j] * scale[j];
       }
       __syncthreads();
-      for (int i = tid; i < A.n; i += stride) {
+      for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
         double t = 0.0;
 #pragma unroll
         for (int j = 0; j < MAXV; ++j)
@@ -526,13 +543,14 @@ static int launch_gmres(apc_context *c, int n, const T *val, const T *b, T *x, i
   }
   int occ = 0;
   APC_CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gmres_kernel<T, RE>, kThreads, 0));
-  occ = std::max(1, std::min(occ, 2));
-  int blocks = std::min(apc_sm_count(c) * occ, std::max(1, (n + kThreads - 1) / kThreads));
-  if (blocks > k->part_blocks) {
-    cudaFree(k->part);
-    k->part = nullptr;
-    APC_TRY(apc_alloc(c, (void **)&k->part, sizeof(double) * 2 * kPartStride * (size_t)blocks));
-    k->part_blocks = blocks;
+  if (occ < 1) {
+    c->err = "GMRES kernel does not fit on an SM";
+    return APC_ERR_CUDA;
+  }
+  int blocks = std::min(std::min(apc_sm_count(c), kMaxBlocks), std::max(1, (n + kThreads - 1) / kThreads));
+  if (!k->part) {
+    APC_TRY(apc_alloc(c, (void **)&k->part, sizeof(double) * 2 * kSlots * (size_t)kMaxBlocks));
+    k->part_blocks = kMaxBlocks;
   }
   APC_CUDA_TRY(c, cudaMemsetAsync(k->bar, 0, sizeof(GridBar), c->s));
   GmresArgs<T> a;

@@ -177,6 +177,7 @@ typedef struct apc_profile {
   double select_ms, solve_ms, move_ms;  /* summed phase device times */
   int64_t steps;         /* completed solve phases */
   double step_ms;        /* summed device time from each select to the next move_position */
+  double gfd_ms;         /* summed device time of the GFD stencil + assembly kernel */
 } apc_profile;
 int apc_get_profile(apc_context *ctx, apc_profile *out);
 int apc_reset_profile(apc_context *ctx);
