@@ -17,6 +17,8 @@ LIB_PATH = os.path.join(PKG_DIR, "libapcloud_gpu.so")
 
 APC_PREC_FP64 = 0
 APC_PREC_MIXED = 1
+APC_PRECOND_JACOBI = 0
+APC_PRECOND_MULTIGRID = 1
 
 EXPORTED = [
     "apc_config_default", "apc_status_string", "apc_last_error", "apc_create", "apc_destroy",
@@ -35,6 +37,7 @@ class ApcConfig(C.Structure):
         ("gmres_restart", C.c_int), ("gmres_rtol", C.c_double), ("gmres_atol", C.c_double),
         ("gmres_dtol", C.c_double), ("gmres_max_it", C.c_int), ("precision", C.c_int),
         ("mixed_restart", C.c_int), ("mixed_inner_rtol", C.c_double), ("device", C.c_int),
+        ("mixed_precond", C.c_int), ("mg_sweeps", C.c_int), ("mg_omega", C.c_double), ("mg_alpha", C.c_double),
     ]
 
 
@@ -43,7 +46,7 @@ class ApcSolveStats(C.Structure):
         ("density_its", C.c_int), ("potential_its", C.c_int),
         ("density_reason", C.c_int), ("potential_reason", C.c_int),
         ("density_rnorm", C.c_double), ("potential_rnorm", C.c_double),
-        ("density_refinements", C.c_int), ("potential_refinements", C.c_int),
+        ("density_refinements", C.c_int), ("potential_refinements", C.c_int), ("mg_levels", C.c_int),
     ]
 
 
@@ -51,7 +54,8 @@ class ApcProfile(C.Structure):
     _fields_ = [("krylov_launches", C.c_int64), ("krylov_iterations", C.c_int64), ("krylov_ms", C.c_double),
                 ("krylov_bytes", C.c_double), ("select_ms", C.c_double), ("solve_ms", C.c_double),
                 ("move_ms", C.c_double), ("steps", C.c_int64), ("step_ms", C.c_double),
-                ("gfd_ms", C.c_double)]
+                ("gfd_ms", C.c_double), ("mg_build_ms", C.c_double), ("mg_solve_ms", C.c_double),
+                ("mg_iterations", C.c_int64)]
 
 
 class ApcStepParams(C.Structure):
@@ -156,7 +160,8 @@ class GpuPath:
                  box=(0.0, 1.0, 0.0, 1.0, 0.0, 1.0), bc: int = 1, precision: int = APC_PREC_FP64,
                  restart: int = 30, rtol: float = 1e-10, atol: float = 1e-50, dtol: float = 1e5,
                  max_it: int = 10000, mixed_restart: int = 0, mixed_inner_rtol: float = 0.0,
-                 device: int = 0, maxnc: int = 10000, nmax_cap: int = 0):
+                 device: int = 0, maxnc: int = 10000, nmax_cap: int = 0, precond: int = APC_PRECOND_MULTIGRID,
+                 mg_sweeps: int = 0, mg_omega: float = 0.0, mg_alpha: float = 0.0):
         self.lib = load_library()
         cfg = ApcConfig()
         self.lib.apc_config_default(C.byref(cfg))
@@ -178,6 +183,10 @@ class GpuPath:
         cfg.mixed_restart = mixed_restart
         cfg.mixed_inner_rtol = mixed_inner_rtol
         cfg.device = device
+        cfg.mixed_precond = precond
+        cfg.mg_sweeps = mg_sweeps
+        cfg.mg_omega = mg_omega
+        cfg.mg_alpha = mg_alpha
         self.cfg = cfg
         self.n = parts.n
         self.depth = depth

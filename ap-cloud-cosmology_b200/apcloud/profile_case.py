@@ -34,6 +34,7 @@ def main():
     print(f"cells {rec.n_cells} wall {dt * 1e3:.1f} ms  krylov {pr['krylov_ms']:.2f} ms over {pr['krylov_launches']} "
           f"launches, {pr['krylov_iterations']} iterations, {pr['krylov_bytes'] / 1e9:.3f} GB algorithmic; "
           f"stats {g.solve_stats()}")
+    print("profile", {k: (round(v, 3) if isinstance(v, float) else v) for k, v in pr.items()})
     g.close()
 
 

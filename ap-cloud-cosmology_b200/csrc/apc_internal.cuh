@@ -40,6 +40,7 @@ enum : int {
 // ----------------------------------------------------------------- context
 
 struct KrylovWork;  // krylov.cu
+struct MgWork;      // mg.cu
 
 struct apc_context {
   apc_config cfg{};
@@ -115,6 +116,7 @@ struct apc_context {
   double *density = nullptr, *potential = nullptr, *deriv = nullptr;
   double rot[9] = {0};       // octant rotation (solver.cpp:464-475), host-computed
   KrylovWork *kw = nullptr;
+  MgWork *mg = nullptr;
   apc_solve_stats stats{};
 
   // ---- timing ----
@@ -145,6 +147,11 @@ int apc_gfd_assemble(apc_context *c, double c_dens);    // gfd.cu
 int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int *its,
                      double *rnorm, int *reason, int *refinements);  // krylov.cu
 void apc_krylov_free(apc_context *c);
+void apc_mg_free(apc_context *c);
+// FP32 FGMRES with the octree-aggregation V-cycle (mg.cu); rebuilds the hierarchy from
+// the current potential operator when asked
+int apc_mg_fgmres(apc_context *c, bool rebuild, const float *r, float *d, int restart, double rtol_in,
+                  int max_it, int *its, int *levels);
 int apc_potential_rhs(apc_context *c, double c_pot);    // gfd.cu
 int apc_differentiate(apc_context *c, double c_field);  // gfd.cu
 int apc_mover_velocity(apc_context *c, double dt, double c_vel, double *max_dv);  // mover.cu

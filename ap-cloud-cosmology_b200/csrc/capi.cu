@@ -81,6 +81,7 @@ __global__ void unpermute(int n, const int *__restrict__ pid, const double *__re
 
 void free_all(apc_context *c) {
   apc_krylov_free(c);
+  apc_mg_free(c);
   void *ptrs[] = {c->px, c->py, c->pz, c->pvx, c->pvy, c->pvz, c->pax, c->pay, c->paz, c->pid,
                   c->qx, c->qy, c->qz, c->qvx, c->qvy, c->qvz, c->qid, c->keys, c->keys_alt, c->perm,
                   c->perm_alt, c->sort_hist, c->reduce_buf, c->h_keys, c->h_vals, c->r_keys, c->r_vals,
@@ -149,6 +150,10 @@ void apc_config_default(apc_config *cfg) {
   cfg->mixed_restart = 0;
   cfg->mixed_inner_rtol = 0.0;
   cfg->device = 0;
+  cfg->mixed_precond = APC_PRECOND_MULTIGRID;
+  cfg->mg_sweeps = 0;
+  cfg->mg_omega = 0.0;
+  cfg->mg_alpha = 0.0;
 }
 
 const char *apc_status_string(int s) {
@@ -175,7 +180,8 @@ int apc_create(const apc_config *cfg, apc_context **out) {
   *out = nullptr;
   if (cfg->n_particles < 1 || cfg->depth < 1 || cfg->depth > 21 || cfg->lm < 9 || cfg->lm > 32 ||
       (cfg->bc != 0 && cfg->bc != 1) || !(cfg->gfd_c >= 0.0) || cfg->gmres_restart < 1 ||
-      cfg->gmres_restart > 31 || cfg->mixed_restart < 0 || cfg->mixed_restart > 31 ||
+      cfg->gmres_restart > 31 || cfg->mixed_restart < 0 || cfg->mixed_restart > 31 || cfg->mg_sweeps < 0 ||
+      (cfg->mixed_precond != APC_PRECOND_JACOBI && cfg->mixed_precond != APC_PRECOND_MULTIGRID) ||
       (cfg->precision != APC_PREC_FP64 && cfg->precision != APC_PREC_MIXED))
     return APC_ERR_INVALID_ARG;
   for (int d = 0; d < 3; ++d)

@@ -470,10 +470,13 @@ __global__ void sum_partials(const double *partial, int n, double *out) {
   if (threadIdx.x == 0) *out = sm[0];
 }
 
-// rhs32 = r / ||r||_inf-free scale s (FP32 copy of the FP64 residual)
-__global__ void to_f32_scaled(int n, const double *__restrict__ r, double inv_s, float *__restrict__ r32) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    r32[i] = (float)(r[i] * inv_s);
+// rhs32 = D^-1 r / s: the FP64 residual, Jacobi-scaled, in FP32 (diagonal = ELL slot 0)
+__global__ void to_f32_scaled(int n, const double *__restrict__ r, const double *__restrict__ diag, double inv_s,
+                              float *__restrict__ r32) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double d = diag[i];
+    r32[i] = (float)((d == 0.0 ? r[i] : r[i] / d) * inv_s);
+  }
 }
 
 __global__ void axpy_f32(int n, double s, const float *__restrict__ d, double *__restrict__ x) {
@@ -481,9 +484,21 @@ __global__ void axpy_f32(int n, double s, const float *__restrict__ d, double *_
     x[i] += s * (double)d[i];
 }
 
-__global__ void ell_to_f32(size_t count, const double *__restrict__ a, float *__restrict__ f) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
-    f[i] = (float)a[i];
+// FP32 copy of D^-1 A (rows scaled by their FP64 diagonal before rounding).  The
+// potential operator's rows sum to zero and its Dirichlet row is a unit row, so the
+// constant mode has a singular value ~1/sqrt(n).  Unscaled, FP32 rounding of rows of
+// size ~1/h^2 would perturb that mode by O(1); scaled rows keep it at O(eps32 sqrt(n)).
+__global__ void ell_to_f32_scaled(size_t ld, int w, int n, const double *__restrict__ a, float *__restrict__ f) {
+  const size_t count = ld * (size_t)w;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < count; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = e % ld;
+    if ((int)i >= n) {
+      f[e] = 0.f;
+      continue;
+    }
+    const double d = a[i];
+    f[e] = (float)(d == 0.0 ? a[e] : a[e] / d);
+  }
 }
 
 __global__ void zero_f64(int n, double *x) {
@@ -644,8 +659,10 @@ static int ensure_work(apc_context *c, int n) {
 
 // Solve A_which x = b.  FP64: one PETSc-semantics GMRES.  Mixed: FP64 iterative
 // refinement on the true preconditioned residual, stopping at the same test
-// ||D^-1 (b - A x)|| <= max(rtol ||D^-1 b||, atol); each correction is an FP32
-// GMRES(CGS2) solve of A d = r to the inner tolerance.
+// ||D^-1 (b - A x)|| <= max(rtol ||D^-1 b||, atol); each correction solves the
+// Jacobi-scaled system (D^-1 A) d = D^-1 r / ||D^-1 r|| in FP32 to the inner tolerance,
+// by GMRES(CGS2) or, for the potential with the multigrid option, by FGMRES with the
+// octree-aggregation V-cycle.
 int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int *its, double *rnorm,
                      int *reason, int *refinements) {
   const int n = c->nc + c->nv;
@@ -663,7 +680,8 @@ int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int 
   float *af = which == 0 ? c->a1f : c->a2f;
   const int G = std::max(1, std::min((n + 255) / 256, std::min(apc_sm_count(c) * 8, 4096)));
   {
-    ell_to_f32<<<std::min<size_t>((ell_count + 255) / 256, 8192), 256, 0, c->s>>>(ell_count, val, af);
+    ell_to_f32_scaled<<<std::min<size_t>((ell_count + 255) / 256, 8192), 256, 0, c->s>>>((size_t)c->m_cap,
+                                                                                         c->ell_w, n, val, af);
     zero_f64<<<G, 256, 0, c->s>>>(n, x);
     apc_count_launch(c, 2);
   }
@@ -691,12 +709,19 @@ int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int 
     if (total_its >= cfg.gmres_max_it) { rs = KSP_DIVERGED_ITS; break; }
     // scale the correction problem to unit preconditioned-residual norm
     const double s = rn;
-    to_f32_scaled<<<G, 256, 0, c->s>>>(n, k->r, 1.0 / s, k->r32);
+    to_f32_scaled<<<G, 256, 0, c->s>>>(n, k->r, val, 1.0 / s, k->r32);
     apc_count_launch(c);
     int iits = 0, ireason = 0;
     double irn = 0.0;
-    APC_TRY(launch_gmres<float, true>(c, n, af, k->r32, k->d32, m32, rtol_in, 1e-30, 1e30,
-                                      std::max(1, cfg.gmres_max_it - total_its), &iits, &irn, &ireason));
+    if (which == 1 && cfg.mixed_precond == APC_PRECOND_MULTIGRID) {
+      int levels = 0;
+      APC_TRY(apc_mg_fgmres(c, outer == 0, k->r32, k->d32, m32, rtol_in,
+                            std::max(1, cfg.gmres_max_it - total_its), &iits, &levels));
+      c->stats.mg_levels = levels;
+    } else {
+      APC_TRY(launch_gmres<float, true>(c, n, af, k->r32, k->d32, m32, rtol_in, 1e-30, 1e30,
+                                        std::max(1, cfg.gmres_max_it - total_its), &iits, &irn, &ireason));
+    }
     total_its += iits;
     axpy_f32<<<G, 256, 0, c->s>>>(n, s, k->d32, x);
     apc_count_launch(c);

@@ -1,0 +1,692 @@
+// Multigrid-preconditioned FP32 Krylov solve of the potential system (mixed path).
+//
+// The reference solves the Poisson system with GMRES + Jacobi (solver.cpp:267-276).  At
+// 262k cells that reaches max_it before rtol (KSP_DIVERGED_ITS), in the reference and on
+// the GPU alike.  The mixed path keeps the reference's stopping test on the FP64 residual
+// (krylov.cu).  Its FP32 correction solves use this preconditioner:
+//   * Aggregation by the octree.  A node of the next coarser level is the parent cell
+//     (location code >> 3); its aggregate is the set of its children present on the
+//     finer level.  Coarse node order is sorted location code, so Morton order.
+//   * Galerkin coarse operators A_c = P^T A P, P piecewise constant.  Each (I, J, a_ij)
+//     contribution is sorted by (I, J) with the library's stable radix sort and summed
+//     in sorted order, so the hierarchy is deterministic.  Rows sum to zero except the
+//     Dirichlet pin's aggregate, so the constant mode is reproduced exactly on every
+//     level.
+//   * Damped Jacobi smoothing on ELL operators; an explicit dense inverse (FP64, formed
+//     on the host) on the coarsest level of <= 128 nodes.
+//   * Flexible GMRES with classical Gram-Schmidt and re-orthogonalisation, right
+//     preconditioned, so the residual it monitors is the true residual of the correction
+//     equation.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <vector>
+
+#include "apc_internal.cuh"
+
+namespace {
+
+constexpr int kT = 256;
+constexpr int kMaxLevels = 24;
+constexpr int kCoarsest = 128;
+
+int grid_for(long long n, int cap = 4096) {
+  return (int)std::max<long long>(1, std::min<long long>((n + kT - 1) / kT, cap));
+}
+
+// ------------------------------------------------------------ hierarchy build
+
+__global__ void parent_codes(int n, const uint64_t *__restrict__ code, uint64_t *__restrict__ key,
+                             uint32_t *__restrict__ idx) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint64_t c = code[i];
+    key[i] = c > 1ull ? (c >> 3) : 1ull;
+    idx[i] = (uint32_t)i;
+  }
+}
+
+__global__ void change_flags_u64(int n, const uint64_t *__restrict__ key, int *__restrict__ flag) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    flag[k] = (k == 0 || key[k] != key[k - 1]) ? 1 : 0;
+}
+
+// after the scan: aggregate map, coarse codes, member CSR of the coarse nodes
+__global__ void aggregate_map(int n, const uint64_t *__restrict__ key, const uint32_t *__restrict__ idx,
+                              const int *__restrict__ flag, const int *__restrict__ pos, int *__restrict__ agg,
+                              uint64_t *__restrict__ ccode, int *__restrict__ mptr, int *__restrict__ mem) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int I = pos[k] + flag[k] - 1;  // inclusive count - 1
+    agg[idx[k]] = I;
+    mem[k] = (int)idx[k];
+    if (flag[k]) {
+      ccode[I] = key[k];
+      mptr[I] = k;
+    }
+  }
+}
+
+// every ELL entry of the fine operator becomes a (I, J) contribution
+__global__ void galerkin_entries(int n, int w, size_t ld, const int *__restrict__ col, const int *__restrict__ agg,
+                                 uint64_t *__restrict__ ekey, uint32_t *__restrict__ eidx) {
+  const long long total = (long long)n * w;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int s = (int)(e / n), i = (int)(e % n);
+    const size_t at = (size_t)s * ld + i;
+    const uint64_t I = (uint64_t)agg[i], J = (uint64_t)agg[col[at]];
+    ekey[e] = (I << 32) | J;
+    eidx[e] = (uint32_t)at;
+  }
+}
+
+__global__ void segment_starts(long long ne, const int *__restrict__ flag, const int *__restrict__ pos,
+                               int *__restrict__ ustart) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < ne; k += (long long)gridDim.x * blockDim.x)
+    if (flag[k]) ustart[pos[k]] = (int)k;
+}
+
+// sum each (I, J) segment in sorted order; record row starts
+__global__ void segment_sums(int nu, long long ne, const int *__restrict__ ustart, const uint64_t *__restrict__ ekey,
+                             const uint32_t *__restrict__ eidx, const float *__restrict__ fval,
+                             int *__restrict__ ucol, float *__restrict__ uval, int *__restrict__ rowstart) {
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nu; u += gridDim.x * blockDim.x) {
+    const int a = ustart[u];
+    const long long b = (u + 1 < nu) ? ustart[u + 1] : ne;
+    double s = 0.0;
+    for (long long k = a; k < b; ++k) s += (double)fval[eidx[k]];
+    const uint64_t key = ekey[a];
+    const int I = (int)(key >> 32);
+    ucol[u] = (int)(key & 0xffffffffull);
+    uval[u] = (float)s;
+    if (u == 0 || (int)(ekey[ustart[u - 1]] >> 32) != I) rowstart[I] = u;
+  }
+}
+
+__global__ void csr_to_ell(int n, int w, size_t ld, const int *__restrict__ rowstart, int nu,
+                           const int *__restrict__ ucol, const float *__restrict__ uval, int *__restrict__ col,
+                           float *__restrict__ val, float *__restrict__ dinv) {
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < n; I += gridDim.x * blockDim.x) {
+    const int a = rowstart[I], b = (I + 1 < n) ? rowstart[I + 1] : nu;
+    float d = 0.f;
+    for (int s = 0; s < w; ++s) {
+      const int u = a + s;
+      const bool in = u < b;
+      const int c = in ? ucol[u] : I;
+      const float v = in ? uval[u] : 0.f;
+      col[(size_t)s * ld + I] = c;
+      val[(size_t)s * ld + I] = v;
+      if (in && c == I) d += v;
+    }
+    dinv[I] = d != 0.f ? 1.f / d : 1.f;
+  }
+}
+
+__global__ void ell_f32_dinv(int n, size_t ld, const float *__restrict__ val, float *__restrict__ dinv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float d = val[i];
+    dinv[i] = d != 0.f ? 1.f / d : 1.f;
+  }
+}
+
+// ------------------------------------------------------------------ V-cycle
+
+__global__ void jacobi_first(int n, const float *__restrict__ dinv, const float *__restrict__ b, float omega,
+                             float *__restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = omega * dinv[i] * b[i];
+}
+
+__global__ void jacobi_sweep(int n, int w, size_t ld, const int *__restrict__ col, const float *__restrict__ val,
+                             const float *__restrict__ dinv, const float *__restrict__ b,
+                             const float *__restrict__ xin, float omega, float *__restrict__ xout) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int k = 0; k < w; ++k) {
+      const size_t at = (size_t)k * ld + i;
+      s += val[at] * xin[col[at]];
+    }
+    xout[i] = xin[i] + omega * dinv[i] * (b[i] - s);
+  }
+}
+
+// b_c[I] = sum over the members i of I of (b - A x)_i
+__global__ void restrict_residual(int nc, const int *__restrict__ mptr, int nf, const int *__restrict__ mem, int w,
+                                  size_t ld, const int *__restrict__ col, const float *__restrict__ val,
+                                  const float *__restrict__ b, const float *__restrict__ x, float *__restrict__ bc) {
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
+    const int a = mptr[I], e = (I + 1 < nc) ? mptr[I + 1] : nf;
+    float r = 0.f;
+    for (int k = a; k < e; ++k) {
+      const int i = mem[k];
+      float s = 0.f;
+      for (int q = 0; q < w; ++q) {
+        const size_t at = (size_t)q * ld + i;
+        s += val[at] * x[col[at]];
+      }
+      r += b[i] - s;
+    }
+    bc[I] = r;
+  }
+}
+
+__global__ void prolong_add(int n, const int *__restrict__ agg, const float *__restrict__ xc, float alpha,
+                            float *__restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] += alpha * xc[agg[i]];
+}
+
+__global__ void dense_apply(int n, const float *__restrict__ inv, const float *__restrict__ b, float *__restrict__ x) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    float s = 0.f;
+    for (int j = 0; j < n; ++j) s += inv[(size_t)i * n + j] * b[j];
+    x[i] = s;
+  }
+}
+
+// ------------------------------------------------------------------ FGMRES
+
+__global__ void combine(int n, int nv, const float *__restrict__ Z, size_t vn, const double *__restrict__ y,
+                        float *__restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double t = 0.0;
+    for (int j = 0; j < nv; ++j) t += y[j] * (double)Z[(size_t)j * vn + i];
+    x[i] = (float)t;
+  }
+}
+
+// ---- fused FGMRES kernels: every reduction finishes in the last block to arrive, which
+//      adds the per-block partials in a fixed order (deterministic) ----
+
+constexpr int kRedBlocks = 296;  // grid of the reduction kernels (2 per SM)
+
+__device__ __forceinline__ bool last_block_arrived(unsigned *counter) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  return last;
+}
+
+// the last block: out[j] = sum_b partial[j * G + b] for j < nv, then re-arm the counter
+__device__ __forceinline__ void finish_sums(int nv, const double *partial, unsigned *counter, double *out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, G = gridDim.x;
+  for (int j = warp; j < nv; j += blockDim.x / 32) {
+    double v = 0.0;
+#pragma unroll
+    for (int k = 0; k < (kRedBlocks + 31) / 32; ++k) {
+      const int b = lane + 32 * k;
+      if (b < G) v += __ldcg(partial + (size_t)j * G + b);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) out[j] = v;
+  }
+  if (threadIdx.x == 0) atomicExch(counter, 0u);
+}
+
+// per-thread values t[j] (j < nv) -> block partials at partial[j * G + block]
+__device__ __forceinline__ void block_partials(const double *t, int nv, double *partial) {
+  __shared__ double sm[kT / 32][33];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (j < nv) {
+      double v = t[j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) sm[warp][j] = v;
+    }
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < nv) {
+    double v = 0.0;
+    for (int k = 0; k < kT / 32; ++k) v += sm[k][threadIdx.x];
+    partial[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = v;
+  }
+}
+
+// mode 0: h = V^T w.  mode 1: w -= V h_in; h = V^T w.  mode 2: w -= V h_in; h[0] = ||w||^2
+template <int MODE>
+__global__ void __launch_bounds__(kT) cgs_pass(int n, int nv, const float *__restrict__ V, size_t vn, float *w,
+                                                const double *__restrict__ h_in, double *partial, unsigned *counter,
+                                                double *out) {
+  double t[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) t[j] = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double wi = (double)w[i];
+    if (MODE > 0) {
+      for (int j = 0; j < nv; ++j) wi -= h_in[j] * (double)V[(size_t)j * vn + i];
+      w[i] = (float)wi;
+      wi = (double)(float)wi;
+    }
+    if (MODE < 2) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < nv) t[j] += wi * (double)V[(size_t)j * vn + i];
+    } else {
+      t[0] += wi * wi;
+    }
+  }
+  const int nout = MODE < 2 ? nv : 1;
+  block_partials(t, nout, partial);
+  if (last_block_arrived(counter)) finish_sums(nout, partial, counter, out);
+}
+
+// z kept for the solution, w = A z
+__global__ void spmv_keep(int n, int w, size_t ld, const int *__restrict__ col, const float *__restrict__ val,
+                          const float *__restrict__ z, float *__restrict__ zkeep, float *__restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int k = 0; k < w; ++k) {
+      const size_t at = (size_t)k * ld + i;
+      s += val[at] * z[col[at]];
+    }
+    zkeep[i] = z[i];
+    y[i] = s;
+  }
+}
+
+// v_next = f w, and the same into the V-cycle's fixed input buffer
+__global__ void scale2(int n, const float *__restrict__ w, float f, float *__restrict__ v, float *__restrict__ vin) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float u = w[i] * f;
+    v[i] = u;
+    vin[i] = u;
+  }
+}
+
+}  // namespace
+
+struct MgLevel {
+  int n = 0, w = 0;
+  size_t ld = 0;
+  int *col = nullptr;
+  float *val = nullptr, *dinv = nullptr;
+  uint64_t *code = nullptr;
+  int *agg = nullptr;                   // node -> coarser node
+  int *mptr = nullptr, *mem = nullptr;  // members on the finer level (levels >= 1)
+  float *x = nullptr, *x2 = nullptr, *b = nullptr;
+  bool owns_matrix = true;
+};
+
+struct MgWork {
+  MgLevel lv[kMaxLevels];
+  int nlev = 0;
+  float *coarse_inv = nullptr;
+  int coarse_n = 0;
+  // Galerkin temporaries
+  uint64_t *ekey = nullptr, *ekey_alt = nullptr, *pkey = nullptr, *pkey_alt = nullptr;
+  uint32_t *eidx = nullptr, *eidx_alt = nullptr, *pidx = nullptr, *pidx_alt = nullptr;
+  int *eflag = nullptr, *epos = nullptr, *ustart = nullptr, *ucol = nullptr, *rowstart = nullptr;
+  float *uval = nullptr;
+  // FGMRES
+  float *V = nullptr, *Z = nullptr, *w = nullptr, *vin = nullptr, *vout = nullptr;
+  double *partial = nullptr, *dots = nullptr;
+  unsigned *counter = nullptr;
+  double *host = nullptr;  // pinned readback buffer
+  int *total = nullptr;
+  // the V-cycle of the current hierarchy as a CUDA graph (vin -> vout)
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  int64_t graph_nodes = 0;
+};
+
+static MgWork *mg(apc_context *c) {
+  if (!c->mg) c->mg = new MgWork();
+  return c->mg;
+}
+
+void apc_mg_free(apc_context *c) {
+  MgWork *m = c->mg;
+  if (!m) return;
+  for (auto &L : m->lv) {
+    if (L.owns_matrix) {
+      cudaFree(L.col);
+      cudaFree(L.val);
+    }
+    cudaFree(L.dinv);
+    cudaFree(L.code);
+    cudaFree(L.agg);
+    cudaFree(L.mptr);
+    cudaFree(L.mem);
+    cudaFree(L.x);
+    cudaFree(L.x2);
+    cudaFree(L.b);
+  }
+  void *p[] = {m->coarse_inv, m->ekey, m->ekey_alt, m->pkey, m->pkey_alt, m->eidx, m->eidx_alt, m->pidx,
+               m->pidx_alt, m->eflag, m->epos, m->ustart, m->ucol, m->rowstart, m->uval, m->V, m->Z, m->w,
+               m->vin, m->vout, m->partial, m->dots, m->counter, m->total};
+  for (void *q : p) cudaFree(q);
+  if (m->host) cudaFreeHost(m->host);
+  if (m->graph_exec) cudaGraphExecDestroy(m->graph_exec);
+  if (m->graph) cudaGraphDestroy(m->graph);
+  delete m;
+  c->mg = nullptr;
+}
+
+static int read_int(apc_context *c, const int *dev, int *host) {
+  APC_CUDA_TRY(c, cudaMemcpyAsync(host, dev, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  return APC_OK;
+}
+
+// Build the hierarchy over the current f32 potential operator (c->a2f) and cell codes.
+static int mg_build(apc_context *c) {
+  MgWork *m = mg(c);
+  const int n0 = c->nc + c->nv;
+  MgLevel &L0 = m->lv[0];
+  L0.n = n0;
+  L0.w = c->ell_w;
+  L0.ld = (size_t)c->m_cap;
+  L0.col = c->ell_col;
+  L0.val = c->a2f;
+  L0.owns_matrix = false;
+  APC_TRY(apc_ensure(c, &L0.dinv, (size_t)n0 + 1));
+  APC_TRY(apc_ensure(c, &L0.code, (size_t)n0 + 1));
+  APC_TRY(apc_ensure(c, &L0.x, (size_t)n0 + 1));
+  APC_TRY(apc_ensure(c, &L0.x2, (size_t)n0 + 1));
+  APC_TRY(apc_ensure(c, &L0.b, (size_t)n0 + 1));
+  APC_CUDA_TRY(c, cudaMemcpyAsync(L0.code, c->ccode, sizeof(uint64_t) * n0, cudaMemcpyDeviceToDevice, c->s));
+  ell_f32_dinv<<<grid_for(n0), kT, 0, c->s>>>(n0, L0.ld, L0.val, L0.dinv);
+  apc_count_launch(c);
+  if (!m->total) APC_TRY(apc_alloc(c, (void **)&m->total, 4 * sizeof(int)));
+  int lev = 0;
+  while (m->lv[lev].n > kCoarsest && lev + 1 < kMaxLevels) {
+    MgLevel &F = m->lv[lev];
+    MgLevel &C = m->lv[lev + 1];
+    const int nf = F.n;
+    // ---- aggregates: parents of this level's nodes ----
+    APC_TRY(apc_ensure(c, &m->pkey, (size_t)nf));
+    APC_TRY(apc_ensure(c, &m->pkey_alt, (size_t)nf));
+    APC_TRY(apc_ensure(c, &m->pidx, (size_t)nf));
+    APC_TRY(apc_ensure(c, &m->pidx_alt, (size_t)nf));
+    APC_TRY(apc_ensure(c, &F.agg, (size_t)nf));
+    parent_codes<<<grid_for(nf), kT, 0, c->s>>>(nf, F.code, m->pkey, m->pidx);
+    apc_count_launch(c);
+    bool alt = false;
+    APC_TRY(apc_radix_sort_u64(c, m->pkey, m->pidx, m->pkey_alt, m->pidx_alt, nf, 0, 64, &alt));
+    uint64_t *pk = alt ? m->pkey_alt : m->pkey;
+    uint32_t *pi = alt ? m->pidx_alt : m->pidx;
+    APC_TRY(apc_ensure(c, &m->eflag, (size_t)nf + 1));
+    APC_TRY(apc_ensure(c, &m->epos, (size_t)nf + 1));
+    change_flags_u64<<<grid_for(nf), kT, 0, c->s>>>(nf, pk, m->eflag);
+    apc_count_launch(c);
+    APC_TRY(apc_exclusive_scan(c, m->eflag, m->epos, nf, m->total));
+    int nc = 0;
+    APC_TRY(read_int(c, m->total, &nc));
+    if (nc >= nf) break;  // no coarsening left
+    C.n = nc;
+    APC_TRY(apc_ensure(c, &C.code, (size_t)nc + 1));
+    APC_TRY(apc_ensure(c, &C.mptr, (size_t)nc + 1));
+    APC_TRY(apc_ensure(c, &C.mem, (size_t)nf + 1));
+    aggregate_map<<<grid_for(nf), kT, 0, c->s>>>(nf, pk, pi, m->eflag, m->epos, F.agg, C.code, C.mptr, C.mem);
+    apc_count_launch(c);
+    // ---- Galerkin product ----
+    const long long ne = (long long)nf * F.w;
+    APC_TRY(apc_ensure(c, &m->ekey, (size_t)ne));
+    APC_TRY(apc_ensure(c, &m->ekey_alt, (size_t)ne));
+    APC_TRY(apc_ensure(c, &m->eidx, (size_t)ne));
+    APC_TRY(apc_ensure(c, &m->eidx_alt, (size_t)ne));
+    galerkin_entries<<<grid_for(ne), kT, 0, c->s>>>(nf, F.w, F.ld, F.col, F.agg, m->ekey, m->eidx);
+    apc_count_launch(c);
+    int bits = 1;
+    while ((1ll << bits) < nc) ++bits;
+    APC_TRY(apc_radix_sort_u64(c, m->ekey, m->eidx, m->ekey_alt, m->eidx_alt, (int)ne, 0, 32 + bits, &alt));
+    uint64_t *ek = alt ? m->ekey_alt : m->ekey;
+    uint32_t *ei = alt ? m->eidx_alt : m->eidx;
+    APC_TRY(apc_ensure(c, &m->eflag, (size_t)ne + 1));
+    APC_TRY(apc_ensure(c, &m->epos, (size_t)ne + 1));
+    change_flags_u64<<<grid_for(ne), kT, 0, c->s>>>((int)ne, ek, m->eflag);
+    apc_count_launch(c);
+    APC_TRY(apc_exclusive_scan(c, m->eflag, m->epos, (int)ne, m->total));
+    int nu = 0;
+    APC_TRY(read_int(c, m->total, &nu));
+    APC_TRY(apc_ensure(c, &m->ustart, (size_t)nu + 1));
+    APC_TRY(apc_ensure(c, &m->ucol, (size_t)nu + 1));
+    APC_TRY(apc_ensure(c, &m->uval, (size_t)nu + 1));
+    APC_TRY(apc_ensure(c, &m->rowstart, (size_t)nc + 1));
+    segment_starts<<<grid_for(ne), kT, 0, c->s>>>(ne, m->eflag, m->epos, m->ustart);
+    segment_sums<<<grid_for(nu), kT, 0, c->s>>>(nu, ne, m->ustart, ek, ei, F.val, m->ucol, m->uval, m->rowstart);
+    apc_count_launch(c, 2);
+    std::vector<int> rs(nc);
+    APC_CUDA_TRY(c, cudaMemcpyAsync(rs.data(), m->rowstart, sizeof(int) * nc, cudaMemcpyDeviceToHost, c->s));
+    APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+    int wc = 0;
+    for (int I = 0; I < nc; ++I) wc = std::max(wc, (I + 1 < nc ? rs[I + 1] : nu) - rs[I]);
+    C.w = wc;
+    C.ld = (size_t)nc;
+    APC_TRY(apc_ensure(c, &C.col, C.ld * wc));
+    APC_TRY(apc_ensure(c, &C.val, C.ld * wc));
+    APC_TRY(apc_ensure(c, &C.dinv, (size_t)nc + 1));
+    APC_TRY(apc_ensure(c, &C.x, (size_t)nc + 1));
+    APC_TRY(apc_ensure(c, &C.x2, (size_t)nc + 1));
+    APC_TRY(apc_ensure(c, &C.b, (size_t)nc + 1));
+    csr_to_ell<<<grid_for(nc), kT, 0, c->s>>>(nc, wc, C.ld, m->rowstart, nu, m->ucol, m->uval, C.col, C.val, C.dinv);
+    apc_count_launch(c);
+    APC_CUDA_TRY(c, cudaGetLastError());
+    ++lev;
+  }
+  m->nlev = lev + 1;
+  // ---- coarsest level: explicit inverse in FP64 on the host ----
+  MgLevel &K = m->lv[lev];
+  const int n = K.n;
+  if (n > 4 * kCoarsest) {
+    c->err = "multigrid coarsening stalled";
+    return APC_ERR_UNSUPPORTED;
+  }
+  std::vector<int> col(K.ld * K.w);
+  std::vector<float> val(K.ld * K.w);
+  APC_CUDA_TRY(c, cudaMemcpyAsync(col.data(), K.col, sizeof(int) * col.size(), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, cudaMemcpyAsync(val.data(), K.val, sizeof(float) * val.size(), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  std::vector<double> a((size_t)n * n, 0.0), inv((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    for (int s = 0; s < K.w; ++s) a[(size_t)i * n + col[(size_t)s * K.ld + i]] += val[(size_t)s * K.ld + i];
+    inv[(size_t)i * n + i] = 1.0;
+  }
+  for (int k = 0; k < n; ++k) {  // Gauss-Jordan with partial pivoting
+    int p = k;
+    for (int i = k + 1; i < n; ++i)
+      if (std::fabs(a[(size_t)i * n + k]) > std::fabs(a[(size_t)p * n + k])) p = i;
+    if (a[(size_t)p * n + k] == 0.0) {
+      c->err = "singular coarsest multigrid operator";
+      return APC_ERR_RANK;
+    }
+    if (p != k)
+      for (int j = 0; j < n; ++j) {
+        std::swap(a[(size_t)p * n + j], a[(size_t)k * n + j]);
+        std::swap(inv[(size_t)p * n + j], inv[(size_t)k * n + j]);
+      }
+    const double d = 1.0 / a[(size_t)k * n + k];
+    for (int j = 0; j < n; ++j) {
+      a[(size_t)k * n + j] *= d;
+      inv[(size_t)k * n + j] *= d;
+    }
+    for (int i = 0; i < n; ++i) {
+      if (i == k) continue;
+      const double f = a[(size_t)i * n + k];
+      if (f == 0.0) continue;
+      for (int j = 0; j < n; ++j) {
+        a[(size_t)i * n + j] -= f * a[(size_t)k * n + j];
+        inv[(size_t)i * n + j] -= f * inv[(size_t)k * n + j];
+      }
+    }
+  }
+  std::vector<float> invf(inv.begin(), inv.end());
+  APC_TRY(apc_ensure(c, &m->coarse_inv, (size_t)n * n + 1));
+  APC_CUDA_TRY(c, cudaMemcpyAsync(m->coarse_inv, invf.data(), sizeof(float) * invf.size(), cudaMemcpyHostToDevice,
+                                  c->s));
+  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  m->coarse_n = n;
+  return APC_OK;
+}
+
+// x = V-cycle(b) on level l; b and x are that level's buffers
+static void vcycle(apc_context *c, int l, const float *b, float *x) {
+  MgWork *m = c->mg;
+  MgLevel &L = m->lv[l];
+  const int n = L.n;
+  const int sweeps = c->cfg.mg_sweeps > 0 ? c->cfg.mg_sweeps : 2;
+  const float omega = (float)(c->cfg.mg_omega > 0 ? c->cfg.mg_omega : 0.7);
+  const float alpha = (float)(c->cfg.mg_alpha > 0 ? c->cfg.mg_alpha : 1.0);
+  if (l == m->nlev - 1) {
+    dense_apply<<<1, 256, 0, c->s>>>(n, m->coarse_inv, b, x);
+    apc_count_launch(c);
+    return;
+  }
+  MgLevel &C = m->lv[l + 1];
+  const int G = grid_for(n);
+  jacobi_first<<<G, kT, 0, c->s>>>(n, L.dinv, b, omega, x);
+  float *cur = x, *nxt = L.x2;
+  for (int k = 1; k < sweeps; ++k) {
+    jacobi_sweep<<<G, kT, 0, c->s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, cur, omega, nxt);
+    std::swap(cur, nxt);
+  }
+  restrict_residual<<<grid_for(C.n), kT, 0, c->s>>>(C.n, C.mptr, n, C.mem, L.w, L.ld, L.col, L.val, b, cur, C.b);
+  apc_count_launch(c, sweeps + 1);
+  vcycle(c, l + 1, C.b, C.x);
+  prolong_add<<<G, kT, 0, c->s>>>(n, L.agg, C.x, alpha, cur);
+  apc_count_launch(c);
+  for (int k = 0; k < sweeps; ++k) {
+    jacobi_sweep<<<G, kT, 0, c->s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, cur, omega, nxt);
+    std::swap(cur, nxt);
+  }
+  apc_count_launch(c, sweeps);
+  if (cur != x) {
+    cudaMemcpyAsync(x, cur, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->s);
+  }
+}
+
+// Capture the V-cycle of the freshly built hierarchy (fixed buffers vin -> vout).
+static int capture_vcycle(apc_context *c) {
+  MgWork *m = c->mg;
+  if (m->graph_exec) {
+    cudaGraphExecDestroy(m->graph_exec);
+    m->graph_exec = nullptr;
+  }
+  if (m->graph) {
+    cudaGraphDestroy(m->graph);
+    m->graph = nullptr;
+  }
+  const int64_t l0 = c->launches;
+  APC_CUDA_TRY(c, cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal));
+  vcycle(c, 0, m->vin, m->vout);
+  cudaError_t e = cudaStreamEndCapture(c->s, &m->graph);
+  m->graph_nodes = c->launches - l0;
+  c->launches = l0;
+  if (e != cudaSuccess) {
+    c->err = std::string("V-cycle capture: ") + cudaGetErrorString(e);
+    cudaGetLastError();
+    return APC_ERR_CUDA;
+  }
+  APC_CUDA_TRY(c, cudaGraphInstantiate(&m->graph_exec, m->graph, 0));
+  return APC_OK;
+}
+
+// FP32 FGMRES(m) with the V-cycle as right preconditioner: solve A d = r to rtol_in.
+// r is Jacobi-scaled to unit norm by the caller.
+int apc_mg_fgmres(apc_context *c, bool rebuild, const float *r, float *d, int restart, double rtol_in, int max_it,
+                  int *its, int *levels) {
+  MgWork *m = mg(c);
+  const int n = c->nc + c->nv;
+  const size_t vn = ((size_t)n + 31) & ~(size_t)31;
+  const int M = std::max(1, std::min(restart, 31));
+  APC_TRY(apc_ensure(c, &m->V, vn * (M + 1)));
+  APC_TRY(apc_ensure(c, &m->Z, vn * M));
+  APC_TRY(apc_ensure(c, &m->vin, vn));
+  APC_TRY(apc_ensure(c, &m->vout, vn));
+  APC_TRY(apc_ensure(c, &m->partial, (size_t)kRedBlocks * 34));
+  APC_TRY(apc_ensure(c, &m->dots, (size_t)4 * 34));
+  if (!m->counter) {
+    APC_TRY(apc_alloc(c, (void **)&m->counter, 4 * sizeof(unsigned)));
+    APC_CUDA_TRY(c, cudaMemsetAsync(m->counter, 0, 4 * sizeof(unsigned), c->s));
+  }
+  if (!m->host) APC_CUDA_TRY(c, cudaMallocHost((void **)&m->host, sizeof(double) * 4 * 34));
+  if (rebuild || m->nlev == 0 || !m->graph_exec) {
+    APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+    const auto t0 = std::chrono::steady_clock::now();
+    APC_TRY(mg_build(c));
+    APC_TRY(capture_vcycle(c));
+    APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+    c->prof.mg_build_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  const auto ts = std::chrono::steady_clock::now();
+  *levels = m->nlev;
+  MgLevel &L0 = m->lv[0];
+  const int G = std::min(kRedBlocks, grid_for(n));
+  const int Gs = grid_for(n, 1184);
+  double *h1 = m->dots, *h2 = m->dots + 34, *nr = m->dots + 68;
+  // beta = ||r||, v0 = r / beta
+  cgs_pass<0><<<G, kT, 0, c->s>>>(n, 1, r, vn, const_cast<float *>(r), nullptr, m->partial, m->counter, nr);
+  apc_count_launch(c);
+  APC_CUDA_TRY(c, cudaMemcpyAsync(m->host, nr, sizeof(double), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  const double beta = std::sqrt(m->host[0]);
+  *its = 0;
+  if (beta == 0.0) {
+    APC_CUDA_TRY(c, cudaMemsetAsync(d, 0, sizeof(float) * n, c->s));
+    return APC_OK;
+  }
+  scale2<<<Gs, kT, 0, c->s>>>(n, r, (float)(1.0 / beta), m->V, m->vin);
+  apc_count_launch(c);
+  std::vector<double> H((size_t)(M + 1) * M, 0.0), cs(M), sn(M), g(M + 1, 0.0);
+  g[0] = beta;
+  int it = 0;
+  for (; it < M && it < max_it; ++it) {
+    float *zk = m->Z + (size_t)it * vn, *w = m->V + (size_t)(it + 1) * vn;
+    APC_CUDA_TRY(c, cudaGraphLaunch(m->graph_exec, c->s));  // vout = V-cycle(vin)
+    apc_count_launch(c, (int)m->graph_nodes);
+    spmv_keep<<<Gs, kT, 0, c->s>>>(n, L0.w, L0.ld, L0.col, L0.val, m->vout, zk, w);
+    cgs_pass<0><<<G, kT, 0, c->s>>>(n, it + 1, m->V, vn, w, nullptr, m->partial, m->counter, h1);
+    cgs_pass<1><<<G, kT, 0, c->s>>>(n, it + 1, m->V, vn, w, h1, m->partial, m->counter, h2);
+    cgs_pass<2><<<G, kT, 0, c->s>>>(n, it + 1, m->V, vn, w, h2, m->partial, m->counter, nr);
+    apc_count_launch(c, 4);
+    APC_CUDA_TRY(c, cudaMemcpyAsync(m->host, m->dots, sizeof(double) * 69, cudaMemcpyDeviceToHost, c->s));
+    APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+    const double tt = std::sqrt(m->host[68]);
+    double *hc = H.data() + (size_t)it * (M + 1);
+    for (int j = 0; j <= it; ++j) hc[j] = m->host[j] + m->host[34 + j];
+    hc[it + 1] = tt;
+    for (int j = 1; j <= it; ++j) {
+      const double t0 = hc[j - 1];
+      hc[j - 1] = cs[j - 1] * t0 + sn[j - 1] * hc[j];
+      hc[j] = cs[j - 1] * hc[j] - sn[j - 1] * t0;
+    }
+    const double t = std::sqrt(hc[it] * hc[it] + hc[it + 1] * hc[it + 1]);
+    if (t == 0.0) {
+      ++it;
+      break;
+    }
+    cs[it] = hc[it] / t;
+    sn[it] = hc[it + 1] / t;
+    g[it + 1] = -sn[it] * g[it];
+    g[it] = cs[it] * g[it];
+    hc[it] = cs[it] * hc[it] + sn[it] * hc[it + 1];
+    if (std::fabs(g[it + 1]) <= rtol_in * beta || tt == 0.0) {
+      ++it;
+      break;
+    }
+    scale2<<<Gs, kT, 0, c->s>>>(n, w, (float)(1.0 / tt), w, m->vin);
+    apc_count_launch(c);
+  }
+  *its = it;
+  // y = H^-1 g (upper triangular), d = Z y
+  std::vector<double> y(std::max(it, 1), 0.0);
+  for (int k = it - 1; k >= 0; --k) {
+    double sacc = g[k];
+    for (int j = k + 1; j < it; ++j) sacc -= H[(size_t)j * (M + 1) + k] * y[j];
+    const double hkk = H[(size_t)k * (M + 1) + k];
+    y[k] = hkk != 0.0 ? sacc / hkk : 0.0;
+  }
+  for (int j = 0; j < it; ++j) m->host[j] = y[j];
+  APC_CUDA_TRY(c, cudaMemcpyAsync(m->dots, m->host, sizeof(double) * std::max(it, 1), cudaMemcpyHostToDevice, c->s));
+  combine<<<Gs, kT, 0, c->s>>>(n, it, m->Z, vn, m->dots, d);
+  apc_count_launch(c);
+  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, cudaGetLastError());
+  c->prof.mg_solve_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ts).count();
+  c->prof.mg_iterations += it;
+  return APC_OK;
+}

@@ -204,10 +204,14 @@ def run_ours(args) -> dict:
     state_parts = ics.Particles(*state[:6])
     t_state = ctl.t
 
-    # ---- force error of the two paths on the same state ----
+    # ---- force error of the two paths on the same state, against a solve converged
+    #      to 1e-13 (the FP64 GMRES(30)+Jacobi path stops at max_it at this size) ----
     acc = {}
-    for prec, name in ((binding.APC_PREC_FP64, "fp64"), (binding.APC_PREC_MIXED, "mixed")):
-        g = make(prec, state_parts)
+    for prec, name in ((binding.APC_PREC_FP64, "fp64"), (binding.APC_PREC_MIXED, "mixed"),
+                       (binding.APC_PREC_MIXED, "converged")):
+        g = make(prec, state_parts) if name != "converged" else binding.GpuPath(
+            state_parts, cfg.depth, cfg.gfd_c, cfg.lm, restart=cfg.restart, rtol=1e-13,
+            precision=prec, device=dev)
         c2 = for_config(g, cfg)
         c2.t = t_state
         k = c2.constants(c2.t, cfg.delta_a)
@@ -216,8 +220,13 @@ def run_ours(args) -> dict:
         g.move_velocity(cfg.delta_a, k["c_vel"])
         acc[name] = (np.stack(g.particles()[6:9]), g.solve_stats())
         g.close()
-    a64, amx = acc["fp64"][0], acc["mixed"][0]
-    force_err = float(np.sqrt(np.mean(np.sum((amx - a64) ** 2, 0)) / np.mean(np.sum(a64 ** 2, 0))))
+    a64, amx, aref = acc["fp64"][0], acc["mixed"][0], acc["converged"][0]
+
+    def rms(a, b):
+        return float(np.sqrt(np.mean(np.sum((a - b) ** 2, 0)) / np.mean(np.sum(b ** 2, 0))))
+
+    force_err = rms(amx, a64)
+    err_mixed, err_fp64 = rms(amx, aref), rms(a64, aref)
 
     def timed(g, c):
         dist.barrier()
@@ -289,16 +298,22 @@ def run_ours(args) -> dict:
                  "speedup_mixed_over_fp64": (value / fp64_value) if fp64_value else None,
                  "potential_its": fp64_stats["potential_its"] if fp64_value else None,
                  "potential_reason": fp64_stats["potential_reason"] if fp64_value else None},
-        "force_error": {"acc_rms_rel_mixed_vs_fp64": force_err, "bound": 1e-6,
+        "force_error": {"mixed_vs_converged": err_mixed, "fp64_vs_converged": err_fp64,
+                        "mixed_vs_fp64": force_err, "bound": 1e-6,
+                        "measure": "acceleration RMS relative error on the same state; 'converged' = potential "
+                                   "solved to rtol 1e-13",
                         "fp64_potential_reason": acc["fp64"][1]["potential_reason"],
-                        "mixed_potential_reason": acc["mixed"][1]["potential_reason"]},
+                        "fp64_potential_its": acc["fp64"][1]["potential_its"],
+                        "mixed_potential_reason": acc["mixed"][1]["potential_reason"],
+                        "mixed_potential_its": acc["mixed"][1]["potential_its"]},
         "phases_ms_per_step": {"select": prof["select_ms"] / args.steps, "solve": prof["solve_ms"] / args.steps,
                                "move": prof["move_ms"] / args.steps,
                                "krylov": prof["krylov_ms"] / args.steps},
         "solve": {"potential_its": st["potential_its"], "potential_refinements": st["potential_refinements"],
                   "potential_reason": st["potential_reason"], "density_its": st["density_its"],
                   "krylov_iterations_per_step": prof["krylov_iterations"] / args.steps},
-        "roofline": {"kernel": "gmres_kernel<float,CGS2> (FP32 inner GMRES)", "bound": "hbm",
+        "roofline": {"kernel": "gmres_kernel (persistent GMRES; the density solve on the mixed path)",
+                     "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "traffic": ncu_traffic_per_launch("gmres_f32"),
                      "bytes_per_launch": kb, "ms_per_launch": kms},

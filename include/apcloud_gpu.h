@@ -80,19 +80,28 @@ typedef struct apc_config {
   int mixed_restart;     /* FP32 inner GMRES restart for APC_PREC_MIXED (0 = autotuned) */
   double mixed_inner_rtol; /* FP32 inner solve relative tolerance (0 = 1e-5) */
   int device;            /* CUDA device ordinal */
+  int mixed_precond;     /* APC_PREC_MIXED potential solve: APC_PRECOND_JACOBI or APC_PRECOND_MULTIGRID */
+  int mg_sweeps;         /* multigrid: Jacobi sweeps before and after each coarse correction (0 = 2) */
+  double mg_omega;       /* multigrid: Jacobi damping (0 = 0.7) */
+  double mg_alpha;       /* multigrid: coarse-correction scaling (0 = 1.0) */
 } apc_config;
 
+enum { APC_PRECOND_JACOBI = 0, APC_PRECOND_MULTIGRID = 1 };
+
 typedef struct apc_solve_stats {
-  int density_its, potential_its;           /* inner iterations (FP32 ones in mixed mode) */
+  int density_its, potential_its;           /* inner iterations (FP32 ones in mixed mode; with the
+                                               multigrid preconditioner, preconditioned iterations) */
   int density_reason, potential_reason;     /* PETSc KSPConvergedReason values */
   double density_rnorm, potential_rnorm;    /* final preconditioned residual norm */
   int density_refinements, potential_refinements; /* FP64 outer steps (mixed mode) */
+  int mg_levels;                            /* multigrid levels of the last potential solve (0 = none) */
 } apc_solve_stats;
 
 typedef struct apc_context apc_context;
 
 /* Defaults: depth 21, periodic unit box, lm 17, maxnc 10000, nmax_cap 0, GMRES(30)
- * rtol 1e-10 atol 1e-50 dtol 1e5 max_it 10000, FP64. */
+ * rtol 1e-10 atol 1e-50 dtol 1e5 max_it 10000, FP64; the mixed path's potential solve
+ * uses the multigrid preconditioner. */
 void apc_config_default(apc_config *cfg);
 const char *apc_status_string(int status);
 /* The message of the last failing call on this context (empty when none). */
@@ -178,6 +187,9 @@ typedef struct apc_profile {
   int64_t steps;         /* completed solve phases */
   double step_ms;        /* summed device time from each select to the next move_position */
   double gfd_ms;         /* summed device time of the GFD stencil + assembly kernel */
+  double mg_build_ms;    /* summed time to build multigrid hierarchies (incl. host work) */
+  double mg_solve_ms;    /* summed time of the multigrid-preconditioned FGMRES solves */
+  int64_t mg_iterations; /* their FGMRES iterations */
 } apc_profile;
 int apc_get_profile(apc_context *ctx, apc_profile *out);
 int apc_reset_profile(apc_context *ctx);

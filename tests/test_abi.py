@@ -50,6 +50,7 @@ def test_library_loads_and_rejects_invalid_config(gpu_lib):
     lib.apc_config_default(C.byref(cfg))
     assert (cfg.depth, cfg.lm, cfg.gmres_restart, cfg.maxnc) == (21, 17, 30, 10000)
     assert cfg.gmres_rtol == pytest.approx(1e-10)
+    assert cfg.mixed_precond == binding.APC_PRECOND_MULTIGRID
     h = C.c_void_p()
     assert lib.apc_create(None, C.byref(h)) == -1
     for field, bad in (("n_particles", 0), ("depth", 22), ("depth", 0), ("lm", 8), ("lm", 33),
