@@ -7,11 +7,11 @@
 //   * Aggregation by the octree.  A node of the next coarser level is the parent cell
 //     (location code >> 3); its aggregate is the set of its children present on the
 //     finer level.  Coarse node order is sorted location code, so Morton order.
-//   * Galerkin coarse operators A_c = P^T A P, P piecewise constant.  Each (I, J, a_ij)
-//     contribution is sorted by (I, J) with the library's stable radix sort and summed
-//     in sorted order, so the hierarchy is deterministic.  Rows sum to zero except the
-//     Dirichlet pin's aggregate, so the constant mode is reproduced exactly on every
-//     level.
+//   * Galerkin coarse operators A_c = P^T A P, P piecewise constant, one warp per
+//     coarse row: the members' (J, a_ij) contributions are sorted in shared memory by a
+//     bitonic network and summed in sorted order, so the hierarchy is deterministic.
+//     Rows sum to zero except the Dirichlet pin's aggregate, so the constant mode is
+//     reproduced exactly on every level.
 //   * Damped Jacobi smoothing on ELL operators; an explicit dense inverse (FP64, formed
 //     on the host) on the coarsest level of <= 128 nodes.
 //   * Flexible GMRES with classical Gram-Schmidt and re-orthogonalisation, right
@@ -67,54 +67,111 @@ __global__ void aggregate_map(int n, const uint64_t *__restrict__ key, const uin
   }
 }
 
-// every ELL entry of the fine operator becomes a (I, J) contribution
-__global__ void galerkin_entries(int n, int w, size_t ld, const int *__restrict__ col, const int *__restrict__ agg,
-                                 uint64_t *__restrict__ ekey, uint32_t *__restrict__ eidx) {
-  const long long total = (long long)n * w;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int s = (int)(e / n), i = (int)(e % n);
-    const size_t at = (size_t)s * ld + i;
-    const uint64_t I = (uint64_t)agg[i], J = (uint64_t)agg[col[at]];
-    ekey[e] = (I << 32) | J;
-    eidx[e] = (uint32_t)at;
+__global__ void ell_f32_dinv(int n, size_t ld, const float *__restrict__ val, float *__restrict__ dinv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float d = val[i];
+    dinv[i] = d != 0.f ? 1.f / d : 1.f;
   }
 }
 
-__global__ void segment_starts(long long ne, const int *__restrict__ flag, const int *__restrict__ pos,
-                               int *__restrict__ ustart) {
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < ne; k += (long long)gridDim.x * blockDim.x)
-    if (flag[k]) ustart[pos[k]] = (int)k;
-}
+// Galerkin row I of A_c = P^T A P, one warp per coarse row: the (J, a) contributions of
+// the members' rows are gathered in shared memory, sorted by J with a bitonic network
+// (data-independent, so deterministic), and equal-J runs summed in sorted order.
+constexpr int kGalWarps = 2;
+constexpr int kGalCap = 2048;  // contributions per coarse row
 
-// sum each (I, J) segment in sorted order; record row starts
-__global__ void segment_sums(int nu, long long ne, const int *__restrict__ ustart, const uint64_t *__restrict__ ekey,
-                             const uint32_t *__restrict__ eidx, const float *__restrict__ fval,
-                             int *__restrict__ ucol, float *__restrict__ uval, int *__restrict__ rowstart) {
-  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nu; u += gridDim.x * blockDim.x) {
-    const int a = ustart[u];
-    const long long b = (u + 1 < nu) ? ustart[u + 1] : ne;
-    double s = 0.0;
-    for (long long k = a; k < b; ++k) s += (double)fval[eidx[k]];
-    const uint64_t key = ekey[a];
-    const int I = (int)(key >> 32);
-    ucol[u] = (int)(key & 0xffffffffull);
-    uval[u] = (float)s;
-    if (u == 0 || (int)(ekey[ustart[u - 1]] >> 32) != I) rowstart[I] = u;
+__global__ void __launch_bounds__(32 * kGalWarps) galerkin_rows(int nc, const int *__restrict__ mptr, int nf,
+                                                              const int *__restrict__ mem, int wf, size_t ldf,
+                                                              const int *__restrict__ colf,
+                                                              const float *__restrict__ valf,
+                                                              const int *__restrict__ agg, int wcap,
+                                                              int *__restrict__ rowlen, int *__restrict__ tcol,
+                                                              float *__restrict__ tval, int *__restrict__ err) {
+  __shared__ unsigned long long buf[kGalWarps][kGalCap];  // (J << 32) | float bits
+  const int lane = threadIdx.x & 31, wv = threadIdx.x >> 5;
+  unsigned long long *B = buf[wv];
+  for (int I = blockIdx.x * kGalWarps + wv; I < nc; I += gridDim.x * kGalWarps) {
+    const int a = mptr[I], e = (I + 1 < nc) ? mptr[I + 1] : nf;
+    const int cnt = (e - a) * wf;
+    if (cnt > kGalCap) {
+      if (lane == 0) atomicOr(err, DERR_STENCIL_MANY);
+      continue;
+    }
+    int P = 1;
+    while (P < cnt) P <<= 1;
+    for (int t = lane; t < P; t += 32) {
+      unsigned long long v = ~0ull;  // padding sorts last
+      if (t < cnt) {
+        const int i = mem[a + t / wf], sl = t % wf;
+        const size_t at = (size_t)sl * ldf + i;
+        const unsigned J = (unsigned)agg[colf[at]];
+        v = ((unsigned long long)J << 32) | (unsigned long long)__float_as_uint(valf[at]);
+      }
+      B[t] = v;
+    }
+    __syncwarp();
+    for (int k = 2; k <= P; k <<= 1) {
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int t = lane; t < P; t += 32) {
+          const int u = t ^ j;
+          if (u > t) {
+            const unsigned long long x = B[t], y = B[u];
+            const bool up = (t & k) == 0;
+            // order by J only (upper 32 bits), ties by the raw word, so the network is total
+            if ((x > y) == up) {
+              B[t] = y;
+              B[u] = x;
+            }
+          }
+        }
+        __syncwarp();
+      }
+    }
+    // segmented sums in sorted order by lane 0 (rows are short)
+    if (lane == 0) {
+      int len = 0;
+      int curJ = -1;
+      double acc = 0.0;
+      for (int t = 0; t < cnt; ++t) {
+        const int J = (int)(B[t] >> 32);
+        const float v = __uint_as_float((unsigned)(B[t] & 0xffffffffull));
+        if (J != curJ) {
+          if (curJ >= 0) {
+            if (len < wcap) {
+              tcol[(size_t)I * wcap + len] = curJ;
+              tval[(size_t)I * wcap + len] = (float)acc;
+            }
+            ++len;
+          }
+          curJ = J;
+          acc = 0.0;
+        }
+        acc += (double)v;
+      }
+      if (curJ >= 0) {
+        if (len < wcap) {
+          tcol[(size_t)I * wcap + len] = curJ;
+          tval[(size_t)I * wcap + len] = (float)acc;
+        }
+        ++len;
+      }
+      rowlen[I] = len;
+      if (len > wcap) atomicOr(err, DERR_STENCIL_MANY);
+    }
+    __syncwarp();
   }
 }
 
-__global__ void csr_to_ell(int n, int w, size_t ld, const int *__restrict__ rowstart, int nu,
-                           const int *__restrict__ ucol, const float *__restrict__ uval, int *__restrict__ col,
-                           float *__restrict__ val, float *__restrict__ dinv) {
+__global__ void rows_to_ell(int n, int w, size_t ld, int wcap, const int *__restrict__ rowlen,
+                            const int *__restrict__ tcol, const float *__restrict__ tval, int *__restrict__ col,
+                            float *__restrict__ val, float *__restrict__ dinv) {
   for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < n; I += gridDim.x * blockDim.x) {
-    const int a = rowstart[I], b = (I + 1 < n) ? rowstart[I + 1] : nu;
+    const int len = rowlen[I];
     float d = 0.f;
     for (int s = 0; s < w; ++s) {
-      const int u = a + s;
-      const bool in = u < b;
-      const int c = in ? ucol[u] : I;
-      const float v = in ? uval[u] : 0.f;
+      const bool in = s < len;
+      const int c = in ? tcol[(size_t)I * wcap + s] : I;
+      const float v = in ? tval[(size_t)I * wcap + s] : 0.f;
       col[(size_t)s * ld + I] = c;
       val[(size_t)s * ld + I] = v;
       if (in && c == I) d += v;
@@ -123,11 +180,12 @@ __global__ void csr_to_ell(int n, int w, size_t ld, const int *__restrict__ rows
   }
 }
 
-__global__ void ell_f32_dinv(int n, size_t ld, const float *__restrict__ val, float *__restrict__ dinv) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const float d = val[i];
-    dinv[i] = d != 0.f ? 1.f / d : 1.f;
-  }
+__global__ void max_int(int n, const int *__restrict__ a, int *out) {
+  int m = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = max(m, a[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
 // ------------------------------------------------------------------ V-cycle
@@ -150,23 +208,27 @@ __global__ void jacobi_sweep(int n, int w, size_t ld, const int *__restrict__ co
   }
 }
 
-// b_c[I] = sum over the members i of I of (b - A x)_i
-__global__ void restrict_residual(int nc, const int *__restrict__ mptr, int nf, const int *__restrict__ mem, int w,
-                                  size_t ld, const int *__restrict__ col, const float *__restrict__ val,
-                                  const float *__restrict__ b, const float *__restrict__ x, float *__restrict__ bc) {
+// r = b - A x, one thread per row
+__global__ void residual_f32(int n, int w, size_t ld, const int *__restrict__ col, const float *__restrict__ val,
+                             const float *__restrict__ b, const float *__restrict__ x, float *__restrict__ r) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int k = 0; k < w; ++k) {
+      const size_t at = (size_t)k * ld + i;
+      s += val[at] * x[col[at]];
+    }
+    r[i] = b[i] - s;
+  }
+}
+
+// b_c[I] = sum of r over the members of I, in member order
+__global__ void restrict_sum(int nc, const int *__restrict__ mptr, int nf, const int *__restrict__ mem,
+                             const float *__restrict__ r, float *__restrict__ bc) {
   for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
     const int a = mptr[I], e = (I + 1 < nc) ? mptr[I + 1] : nf;
-    float r = 0.f;
-    for (int k = a; k < e; ++k) {
-      const int i = mem[k];
-      float s = 0.f;
-      for (int q = 0; q < w; ++q) {
-        const size_t at = (size_t)q * ld + i;
-        s += val[at] * x[col[at]];
-      }
-      r += b[i] - s;
-    }
-    bc[I] = r;
+    float s = 0.f;
+    for (int k = a; k < e; ++k) s += r[mem[k]];
+    bc[I] = s;
   }
 }
 
@@ -307,7 +369,7 @@ struct MgLevel {
   uint64_t *code = nullptr;
   int *agg = nullptr;                   // node -> coarser node
   int *mptr = nullptr, *mem = nullptr;  // members on the finer level (levels >= 1)
-  float *x = nullptr, *x2 = nullptr, *b = nullptr;
+  float *x = nullptr, *x2 = nullptr, *b = nullptr, *r = nullptr;
   bool owns_matrix = true;
 };
 
@@ -316,10 +378,10 @@ struct MgWork {
   int nlev = 0;
   float *coarse_inv = nullptr;
   int coarse_n = 0;
-  // Galerkin temporaries
-  uint64_t *ekey = nullptr, *ekey_alt = nullptr, *pkey = nullptr, *pkey_alt = nullptr;
-  uint32_t *eidx = nullptr, *eidx_alt = nullptr, *pidx = nullptr, *pidx_alt = nullptr;
-  int *eflag = nullptr, *epos = nullptr, *ustart = nullptr, *ucol = nullptr, *rowstart = nullptr;
+  // hierarchy temporaries: parent-code sort, flags, coarse rows before the ELL transpose
+  uint64_t *pkey = nullptr, *pkey_alt = nullptr;
+  uint32_t *pidx = nullptr, *pidx_alt = nullptr;
+  int *eflag = nullptr, *epos = nullptr, *ucol = nullptr, *rowstart = nullptr;
   float *uval = nullptr;
   // FGMRES
   float *V = nullptr, *Z = nullptr, *w = nullptr, *vin = nullptr, *vout = nullptr;
@@ -354,9 +416,10 @@ void apc_mg_free(apc_context *c) {
     cudaFree(L.x);
     cudaFree(L.x2);
     cudaFree(L.b);
+    cudaFree(L.r);
   }
-  void *p[] = {m->coarse_inv, m->ekey, m->ekey_alt, m->pkey, m->pkey_alt, m->eidx, m->eidx_alt, m->pidx,
-               m->pidx_alt, m->eflag, m->epos, m->ustart, m->ucol, m->rowstart, m->uval, m->V, m->Z, m->w,
+  void *p[] = {m->coarse_inv, m->pkey, m->pkey_alt, m->pidx, m->pidx_alt, m->eflag, m->epos, m->ucol,
+               m->rowstart, m->uval, m->V, m->Z, m->w,
                m->vin, m->vout, m->partial, m->dots, m->counter, m->total};
   for (void *q : p) cudaFree(q);
   if (m->host) cudaFreeHost(m->host);
@@ -388,6 +451,7 @@ static int mg_build(apc_context *c) {
   APC_TRY(apc_ensure(c, &L0.x, (size_t)n0 + 1));
   APC_TRY(apc_ensure(c, &L0.x2, (size_t)n0 + 1));
   APC_TRY(apc_ensure(c, &L0.b, (size_t)n0 + 1));
+  APC_TRY(apc_ensure(c, &L0.r, (size_t)n0 + 1));
   APC_CUDA_TRY(c, cudaMemcpyAsync(L0.code, c->ccode, sizeof(uint64_t) * n0, cudaMemcpyDeviceToDevice, c->s));
   ell_f32_dinv<<<grid_for(n0), kT, 0, c->s>>>(n0, L0.ld, L0.val, L0.dinv);
   apc_count_launch(c);
@@ -423,38 +487,25 @@ static int mg_build(apc_context *c) {
     APC_TRY(apc_ensure(c, &C.mem, (size_t)nf + 1));
     aggregate_map<<<grid_for(nf), kT, 0, c->s>>>(nf, pk, pi, m->eflag, m->epos, F.agg, C.code, C.mptr, C.mem);
     apc_count_launch(c);
-    // ---- Galerkin product ----
-    const long long ne = (long long)nf * F.w;
-    APC_TRY(apc_ensure(c, &m->ekey, (size_t)ne));
-    APC_TRY(apc_ensure(c, &m->ekey_alt, (size_t)ne));
-    APC_TRY(apc_ensure(c, &m->eidx, (size_t)ne));
-    APC_TRY(apc_ensure(c, &m->eidx_alt, (size_t)ne));
-    galerkin_entries<<<grid_for(ne), kT, 0, c->s>>>(nf, F.w, F.ld, F.col, F.agg, m->ekey, m->eidx);
-    apc_count_launch(c);
-    int bits = 1;
-    while ((1ll << bits) < nc) ++bits;
-    APC_TRY(apc_radix_sort_u64(c, m->ekey, m->eidx, m->ekey_alt, m->eidx_alt, (int)ne, 0, 32 + bits, &alt));
-    uint64_t *ek = alt ? m->ekey_alt : m->ekey;
-    uint32_t *ei = alt ? m->eidx_alt : m->eidx;
-    APC_TRY(apc_ensure(c, &m->eflag, (size_t)ne + 1));
-    APC_TRY(apc_ensure(c, &m->epos, (size_t)ne + 1));
-    change_flags_u64<<<grid_for(ne), kT, 0, c->s>>>((int)ne, ek, m->eflag);
-    apc_count_launch(c);
-    APC_TRY(apc_exclusive_scan(c, m->eflag, m->epos, (int)ne, m->total));
-    int nu = 0;
-    APC_TRY(read_int(c, m->total, &nu));
-    APC_TRY(apc_ensure(c, &m->ustart, (size_t)nu + 1));
-    APC_TRY(apc_ensure(c, &m->ucol, (size_t)nu + 1));
-    APC_TRY(apc_ensure(c, &m->uval, (size_t)nu + 1));
+    // ---- Galerkin product, one warp per coarse row ----
+    const int wcap = 256;
     APC_TRY(apc_ensure(c, &m->rowstart, (size_t)nc + 1));
-    segment_starts<<<grid_for(ne), kT, 0, c->s>>>(ne, m->eflag, m->epos, m->ustart);
-    segment_sums<<<grid_for(nu), kT, 0, c->s>>>(nu, ne, m->ustart, ek, ei, F.val, m->ucol, m->uval, m->rowstart);
+    APC_TRY(apc_ensure(c, &m->ucol, (size_t)nc * wcap));
+    APC_TRY(apc_ensure(c, &m->uval, (size_t)nc * wcap));
+    APC_CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->s));
+    APC_CUDA_TRY(c, cudaMemsetAsync(m->total, 0, sizeof(int), c->s));
+    galerkin_rows<<<std::max(1, std::min((nc + kGalWarps - 1) / kGalWarps, apc_sm_count(c) * 8)), 32 * kGalWarps, 0,
+                    c->s>>>(nc, C.mptr, nf, C.mem, F.w, F.ld, F.col, F.val, F.agg, wcap, m->rowstart, m->ucol,
+                            m->uval, c->d_err);
+    max_int<<<grid_for(nc, 256), kT, 0, c->s>>>(nc, m->rowstart, m->total);
     apc_count_launch(c, 2);
-    std::vector<int> rs(nc);
-    APC_CUDA_TRY(c, cudaMemcpyAsync(rs.data(), m->rowstart, sizeof(int) * nc, cudaMemcpyDeviceToHost, c->s));
-    APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
-    int wc = 0;
-    for (int I = 0; I < nc; ++I) wc = std::max(wc, (I + 1 < nc ? rs[I + 1] : nu) - rs[I]);
+    int wc = 0, derr = 0;
+    APC_TRY(read_int(c, m->total, &wc));
+    APC_TRY(apc_read_errors(c, &derr));
+    if (derr & DERR_STENCIL_MANY) {
+      c->err = "multigrid coarse row exceeds its buffers";
+      return APC_ERR_UNSUPPORTED;
+    }
     C.w = wc;
     C.ld = (size_t)nc;
     APC_TRY(apc_ensure(c, &C.col, C.ld * wc));
@@ -463,7 +514,9 @@ static int mg_build(apc_context *c) {
     APC_TRY(apc_ensure(c, &C.x, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &C.x2, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &C.b, (size_t)nc + 1));
-    csr_to_ell<<<grid_for(nc), kT, 0, c->s>>>(nc, wc, C.ld, m->rowstart, nu, m->ucol, m->uval, C.col, C.val, C.dinv);
+    APC_TRY(apc_ensure(c, &C.r, (size_t)nc + 1));
+    rows_to_ell<<<grid_for(nc), kT, 0, c->s>>>(nc, wc, C.ld, wcap, m->rowstart, m->ucol, m->uval, C.col, C.val,
+                                              C.dinv);
     apc_count_launch(c);
     APC_CUDA_TRY(c, cudaGetLastError());
     ++lev;
@@ -544,8 +597,9 @@ static void vcycle(apc_context *c, int l, const float *b, float *x) {
     jacobi_sweep<<<G, kT, 0, c->s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, cur, omega, nxt);
     std::swap(cur, nxt);
   }
-  restrict_residual<<<grid_for(C.n), kT, 0, c->s>>>(C.n, C.mptr, n, C.mem, L.w, L.ld, L.col, L.val, b, cur, C.b);
-  apc_count_launch(c, sweeps + 1);
+  residual_f32<<<G, kT, 0, c->s>>>(n, L.w, L.ld, L.col, L.val, b, cur, L.r);
+  restrict_sum<<<grid_for(C.n), kT, 0, c->s>>>(C.n, C.mptr, n, C.mem, L.r, C.b);
+  apc_count_launch(c, sweeps + 2);
   vcycle(c, l + 1, C.b, C.x);
   prolong_add<<<G, kT, 0, c->s>>>(n, L.agg, C.x, alpha, cur);
   apc_count_launch(c);
