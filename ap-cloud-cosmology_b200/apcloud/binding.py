@@ -38,6 +38,7 @@ class ApcConfig(C.Structure):
         ("gmres_dtol", C.c_double), ("gmres_max_it", C.c_int), ("precision", C.c_int),
         ("mixed_restart", C.c_int), ("mixed_inner_rtol", C.c_double), ("device", C.c_int),
         ("mixed_precond", C.c_int), ("mg_sweeps", C.c_int), ("mg_omega", C.c_double), ("mg_alpha", C.c_double),
+        ("mg_reorth", C.c_int),
     ]
 
 
@@ -161,7 +162,7 @@ class GpuPath:
                  restart: int = 30, rtol: float = 1e-10, atol: float = 1e-50, dtol: float = 1e5,
                  max_it: int = 10000, mixed_restart: int = 0, mixed_inner_rtol: float = 0.0,
                  device: int = 0, maxnc: int = 10000, nmax_cap: int = 0, precond: int = APC_PRECOND_MULTIGRID,
-                 mg_sweeps: int = 0, mg_omega: float = 0.0, mg_alpha: float = 0.0):
+                 mg_sweeps: int = 0, mg_omega: float = 0.0, mg_alpha: float = 0.0, mg_reorth: int = 0):
         self.lib = load_library()
         cfg = ApcConfig()
         self.lib.apc_config_default(C.byref(cfg))
@@ -187,6 +188,7 @@ class GpuPath:
         cfg.mg_sweeps = mg_sweeps
         cfg.mg_omega = mg_omega
         cfg.mg_alpha = mg_alpha
+        cfg.mg_reorth = mg_reorth
         self.cfg = cfg
         self.n = parts.n
         self.depth = depth

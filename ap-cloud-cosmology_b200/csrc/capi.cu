@@ -154,6 +154,7 @@ void apc_config_default(apc_config *cfg) {
   cfg->mg_sweeps = 0;
   cfg->mg_omega = 0.0;
   cfg->mg_alpha = 0.0;
+  cfg->mg_reorth = 0;
 }
 
 const char *apc_status_string(int s) {

@@ -109,6 +109,7 @@ __device__ void aquicksort(double *a, int *b, int l, int r) {
 }
 
 struct WarpSmem {
+  int soff[32], sp[32];  // expansion ring: item offset and cell of each candidate
   int bidx[8][kBucketCap];
   double bd2[8][kBucketCap];
   double ldist[kListCap];
@@ -192,32 +193,53 @@ __global__ void __launch_bounds__(32 * kWarps) gfd_stencil(GfdParams P) {
         few = true;
         break;
       }
-      int snn[8];
+      // the ring's (candidate, Neigh24 entry) items in the reference's order, processed 32
+      // at a time: candidates of the snapshot are < lm <= 32, so one lane holds each
+      int pre[9];
+      pre[0] = 0;
 #pragma unroll
-      for (int o = 0; o < 8; ++o) snn[o] = nn[o];
-      for (int b = 0; b < 8 && ok; ++b) {
-        for (int e = 0; e < snn[b] && ok; ++e) {
-          const int p = S.bidx[b][e];
-          const int cnt = P.nnb[p];
-          bool v = lane < cnt;
-          int m = v ? P.nb24[24 * (size_t)p + lane] : -1;
-          int oct = 0;
-          double d2 = 0;
-          if (v) {
-            double wx, wy, wz;
-            offset_of(P, m, i0, wx, wy, wz);
-            oct = octant_of(P, wx, wy, wz);
-            d2 = sq3(wx, wy, wz);
-            bool dup = (m == i0);
-            const int cap = min(nn[oct], kBucketCap);
-            for (int q = 0; q < cap && !dup; ++q) dup = (S.bidx[oct][q] == m);
-            v = !dup;
-          }
-          // only the first lane holding a given index survives within the batch
-          unsigned peers = __match_any_sync(0xffffffffu, v ? m : -1 - lane);
-          if (v && lane != __ffs(peers) - 1) v = false;
-          ok &= append(S, nn, v, m, oct, d2, lane);
+      for (int o = 0; o < 8; ++o) pre[o + 1] = pre[o] + nn[o];
+      const int lsnap = pre[8];
+      int pc = 0, cc = 0;
+      if (lane < lsnap) {
+        int b = 0;
+#pragma unroll
+        for (int o = 1; o < 8; ++o) b += (lane >= pre[o]) ? 1 : 0;
+        pc = S.bidx[b][lane - pre[b]];
+        cc = P.nnb[pc];
+      }
+      int incl = cc;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      S.soff[lane] = incl - cc;
+      S.sp[lane] = pc;
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      __syncwarp();
+      for (int f0 = 0; f0 < total && ok; f0 += 32) {
+        const int f = f0 + lane;
+        bool v = f < total;
+        int m = -1, oct = 0;
+        double d2 = 0;
+        if (v) {
+          int c = 0;
+          for (int q = 1; q < lsnap; ++q) c += (S.soff[q] <= f) ? 1 : 0;
+          m = P.nb24[24 * (size_t)S.sp[c] + (f - S.soff[c])];
+          double wx, wy, wz;
+          offset_of(P, m, i0, wx, wy, wz);
+          oct = octant_of(P, wx, wy, wz);
+          d2 = sq3(wx, wy, wz);
+          bool dup = (m == i0);
+          const int cap = min(nn[oct], kBucketCap);
+          for (int q = 0; q < cap && !dup; ++q) dup = (S.bidx[oct][q] == m);
+          v = !dup;
         }
+        // only the first lane holding a given index survives within the chunk
+        unsigned peers = __match_any_sync(0xffffffffu, v ? m : -1 - lane);
+        if (v && lane != __ffs(peers) - 1) v = false;
+        ok &= append(S, nn, v, m, oct, d2, lane);
       }
       if (!ok) break;
       ++ite;

@@ -685,7 +685,10 @@ int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int 
     zero_f64<<<G, 256, 0, c->s>>>(n, x);
     apc_count_launch(c, 2);
   }
-  const int m32 = cfg.mixed_restart > 0 ? cfg.mixed_restart : 30;
+  // inner restart: 16 for the multigrid FGMRES (a V-cycle per step makes short cycles
+  // cheapest at 128^3), 30 for Jacobi GMRES
+  const bool use_mg = which == 1 && cfg.mixed_precond == APC_PRECOND_MULTIGRID;
+  const int m32 = cfg.mixed_restart > 0 ? cfg.mixed_restart : (use_mg ? 16 : 30);
   const double rtol_in = cfg.mixed_inner_rtol > 0 ? cfg.mixed_inner_rtol : 1e-5;
   double ttol = 0.0, rn0 = 0.0;
   int total_its = 0, rs = 0;
@@ -713,7 +716,7 @@ int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int 
     apc_count_launch(c);
     int iits = 0, ireason = 0;
     double irn = 0.0;
-    if (which == 1 && cfg.mixed_precond == APC_PRECOND_MULTIGRID) {
+    if (use_mg) {
       int levels = 0;
       APC_TRY(apc_mg_fgmres(c, outer == 0, k->r32, k->d32, m32, rtol_in,
                             std::max(1, cfg.gmres_max_it - total_its), &iits, &levels));

@@ -14,9 +14,9 @@
 //     reproduced exactly on every level.
 //   * Damped Jacobi smoothing on ELL operators; an explicit dense inverse (FP64, formed
 //     on the host) on the coarsest level of <= 128 nodes.
-//   * Flexible GMRES with classical Gram-Schmidt and re-orthogonalisation, right
-//     preconditioned, so the residual it monitors is the true residual of the correction
-//     equation.
+//   * Flexible GMRES with classical Gram-Schmidt (optionally a second, re-orthogonalising
+//     sweep), right preconditioned, so the residual it monitors is the true residual of
+//     the correction equation.  The SpMV is fused with the first dot-product pass.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,7 +30,7 @@ namespace {
 
 constexpr int kT = 256;
 constexpr int kMaxLevels = 24;
-constexpr int kCoarsest = 128;
+constexpr int kCoarsest = 64;
 
 int grid_for(long long n, int cap = 4096) {
   return (int)std::max<long long>(1, std::min<long long>((n + kT - 1) / kT, cap));
@@ -237,14 +237,6 @@ __global__ void prolong_add(int n, const int *__restrict__ agg, const float *__r
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] += alpha * xc[agg[i]];
 }
 
-__global__ void dense_apply(int n, const float *__restrict__ inv, const float *__restrict__ b, float *__restrict__ x) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    float s = 0.f;
-    for (int j = 0; j < n; ++j) s += inv[(size_t)i * n + j] * b[j];
-    x[i] = s;
-  }
-}
-
 // ------------------------------------------------------------------ FGMRES
 
 __global__ void combine(int n, int nv, const float *__restrict__ Z, size_t vn, const double *__restrict__ y,
@@ -287,67 +279,108 @@ __device__ __forceinline__ void finish_sums(int nv, const double *partial, unsig
   if (threadIdx.x == 0) atomicExch(counter, 0u);
 }
 
-// per-thread values t[j] (j < nv) -> block partials at partial[j * G + block]
-__device__ __forceinline__ void block_partials(const double *t, int nv, double *partial) {
-  __shared__ double sm[kT / 32][33];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int j = 0; j < 32; ++j) {
-    if (j < nv) {
-      double v = t[j];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if (lane == 0) sm[warp][j] = v;
-    }
-  }
-  __syncthreads();
-  if ((int)threadIdx.x < nv) {
-    double v = 0.0;
-    for (int k = 0; k < kT / 32; ++k) v += sm[k][threadIdx.x];
-    partial[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = v;
-  }
-}
-
-// mode 0: h = V^T w.  mode 1: w -= V h_in; h = V^T w.  mode 2: w -= V h_in; h[0] = ||w||^2
+// mode 0: h = V^T w.  mode 1: w -= V h_in; h = V^T w.  mode 2: w -= V h_in; h[0] = ||w||^2.
+// Each warp takes tiles of 32 consecutive rows (one per lane); the basis values of a row
+// stay in registers for the update and the dots; every dot is reduced across the warp at
+// once and kept by lane j, so one accumulator per lane covers all basis vectors.
 template <int MODE>
 __global__ void __launch_bounds__(kT) cgs_pass(int n, int nv, const float *__restrict__ V, size_t vn, float *w,
                                                 const double *__restrict__ h_in, double *partial, unsigned *counter,
                                                 double *out) {
-  double t[32];
+  __shared__ double hsh[32];
+  __shared__ double sm[kT / 32][32];
+  if (MODE > 0 && (int)threadIdx.x < nv) hsh[threadIdx.x] = h_in[threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double acc = 0.0;
+  const int ntiles = (n + 31) / 32;
+  for (int tile = blockIdx.x * nw + warp; tile < ntiles; tile += gridDim.x * nw) {
+    const int i = tile * 32 + lane;
+    const bool ok = i < n;
+    float vj[32];
 #pragma unroll
-  for (int j = 0; j < 32; ++j) t[j] = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double wi = (double)w[i];
+    for (int j = 0; j < 32; ++j) vj[j] = (j < nv && ok) ? V[(size_t)j * vn + i] : 0.f;
+    double wi = ok ? (double)w[i] : 0.0;
     if (MODE > 0) {
-      for (int j = 0; j < nv; ++j) wi -= h_in[j] * (double)V[(size_t)j * vn + i];
-      w[i] = (float)wi;
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < nv) wi -= hsh[j] * (double)vj[j];
+      if (ok) w[i] = (float)wi;
       wi = (double)(float)wi;
     }
     if (MODE < 2) {
 #pragma unroll
-      for (int j = 0; j < 32; ++j)
-        if (j < nv) t[j] += wi * (double)V[(size_t)j * vn + i];
+      for (int j = 0; j < 32; ++j) {
+        if (j < nv) {
+          double p = wi * (double)vj[j];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
+          if (lane == j) acc += p;
+        }
+      }
     } else {
-      t[0] += wi * wi;
+      double p = wi * wi;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
+      if (lane == 0) acc += p;
     }
   }
+  sm[warp][lane] = acc;
+  __syncthreads();
   const int nout = MODE < 2 ? nv : 1;
-  block_partials(t, nout, partial);
+  if ((int)threadIdx.x < nout) {
+    double v = 0.0;
+    for (int k = 0; k < nw; ++k) v += sm[k][threadIdx.x];
+    partial[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = v;
+  }
   if (last_block_arrived(counter)) finish_sums(nout, partial, counter, out);
 }
 
-// z kept for the solution, w = A z
-__global__ void spmv_keep(int n, int w, size_t ld, const int *__restrict__ col, const float *__restrict__ val,
-                          const float *__restrict__ z, float *__restrict__ zkeep, float *__restrict__ y) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    float s = 0.f;
-    for (int k = 0; k < w; ++k) {
-      const size_t at = (size_t)k * ld + i;
-      s += val[at] * z[col[at]];
+// w = A z (z kept for the solution), then the block's dots <w, V_j>, j < nv, in the same
+// warp-tile pass as cgs_pass<0>
+__global__ void __launch_bounds__(kT) spmv_dots(int n, int ew, size_t ld, const int *__restrict__ col,
+                                                 const float *__restrict__ val, const float *__restrict__ z,
+                                                 float *__restrict__ zkeep, float *__restrict__ w, int nv,
+                                                 const float *__restrict__ V, size_t vn, double *partial,
+                                                 unsigned *counter, double *out) {
+  __shared__ double sm[kT / 32][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double acc = 0.0;
+  const int ntiles = (n + 31) / 32;
+  for (int tile = blockIdx.x * nw + warp; tile < ntiles; tile += gridDim.x * nw) {
+    const int i = tile * 32 + lane;
+    const bool ok = i < n;
+    float vj[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) vj[j] = (j < nv && ok) ? V[(size_t)j * vn + i] : 0.f;
+    float sacc = 0.f;
+    if (ok) {
+      for (int k = 0; k < ew; ++k) {
+        const size_t at = (size_t)k * ld + i;
+        sacc += val[at] * z[col[at]];
+      }
+      zkeep[i] = z[i];
+      w[i] = sacc;
     }
-    zkeep[i] = z[i];
-    y[i] = s;
+    const double wi = (double)sacc;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      if (j < nv) {
+        double p = wi * (double)vj[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
+        if (lane == j) acc += p;
+      }
+    }
   }
+  sm[warp][lane] = acc;
+  __syncthreads();
+  if ((int)threadIdx.x < nv) {
+    double v = 0.0;
+    for (int k = 0; k < nw; ++k) v += sm[k][threadIdx.x];
+    partial[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = v;
+  }
+  if (last_block_arrived(counter)) finish_sums(nv, partial, counter, out);
 }
 
 // v_next = f w, and the same into the V-cycle's fixed input buffer
@@ -356,6 +389,101 @@ __global__ void scale2(int n, const float *__restrict__ w, float f, float *__res
     const float u = w[i] * f;
     v[i] = u;
     vin[i] = u;
+  }
+}
+
+
+// ---- the coarse end of the V-cycle in one block: every level with <= kTail nodes,
+//      down (smooth, residual, restrict), the dense coarsest solve, and up (prolong,
+//      smooth), separated by block barriers instead of kernel launches ----
+constexpr int kTail = 512;
+constexpr int kTailLevels = 12;
+
+struct TailLevel {
+  int n, w;
+  size_t ld;
+  const int *col;
+  const float *val, *dinv;
+  const int *agg;             // node -> next coarser node
+  const int *mptr, *mem;      // members of this level's nodes on the finer level
+  float *x, *x2, *b, *r;
+};
+struct TailArgs {
+  int nl;                     // levels in the tail, the last one solved densely
+  TailLevel L[kTailLevels];
+  const float *inv;
+  int sweeps;
+  float omega, alpha;
+};
+
+__device__ __forceinline__ void tail_sweep(const TailLevel &L, const float *xin, float *xout, float omega) {
+  for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+    float sacc = 0.f;
+    for (int k = 0; k < L.w; ++k) {
+      const size_t at = (size_t)k * L.ld + i;
+      sacc += L.val[at] * xin[L.col[at]];
+    }
+    xout[i] = xin[i] + omega * L.dinv[i] * (L.b[i] - sacc);
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(1024) vcycle_tail(TailArgs A) {
+  float *cur[kTailLevels];
+  for (int l = 0; l < A.nl - 1; ++l) {
+    const TailLevel &L = A.L[l];
+    for (int i = threadIdx.x; i < L.n; i += blockDim.x) L.x[i] = A.omega * L.dinv[i] * L.b[i];
+    __syncthreads();
+    float *c = L.x, *o = L.x2;
+    for (int k = 1; k < A.sweeps; ++k) {
+      tail_sweep(L, c, o, A.omega);
+      float *t = c; c = o; o = t;
+    }
+    cur[l] = c;
+    for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+      float sacc = 0.f;
+      for (int k = 0; k < L.w; ++k) {
+        const size_t at = (size_t)k * L.ld + i;
+        sacc += L.val[at] * c[L.col[at]];
+      }
+      L.r[i] = L.b[i] - sacc;
+    }
+    __syncthreads();
+    const TailLevel &C = A.L[l + 1];
+    for (int I = threadIdx.x; I < C.n; I += blockDim.x) {
+      const int a = C.mptr[I], e = (I + 1 < C.n) ? C.mptr[I + 1] : L.n;
+      float sacc = 0.f;
+      for (int q = a; q < e; ++q) sacc += L.r[C.mem[q]];
+      C.b[I] = sacc;
+    }
+    __syncthreads();
+  }
+  {
+    const TailLevel &K = A.L[A.nl - 1];
+    for (int i = threadIdx.x; i < K.n; i += blockDim.x) {
+      float sacc = 0.f;
+      for (int j = 0; j < K.n; ++j) sacc += A.inv[(size_t)i * K.n + j] * K.b[j];
+      K.x[i] = sacc;
+    }
+    __syncthreads();
+    cur[A.nl - 1] = K.x;
+  }
+  for (int l = A.nl - 2; l >= 0; --l) {
+    const TailLevel &L = A.L[l];
+    float *c = cur[l];
+    float *o = (c == L.x) ? L.x2 : L.x;
+    const float *xc = cur[l + 1];
+    for (int i = threadIdx.x; i < L.n; i += blockDim.x) c[i] += A.alpha * xc[L.agg[i]];
+    __syncthreads();
+    for (int k = 0; k < A.sweeps; ++k) {
+      tail_sweep(L, c, o, A.omega);
+      float *t = c; c = o; o = t;
+    }
+    if (c != L.x) {
+      for (int i = threadIdx.x; i < L.n; i += blockDim.x) L.x[i] = c[i];
+      __syncthreads();
+    }
+    cur[l] = L.x;
   }
 }
 
@@ -470,7 +598,9 @@ static int mg_build(apc_context *c) {
     parent_codes<<<grid_for(nf), kT, 0, c->s>>>(nf, F.code, m->pkey, m->pidx);
     apc_count_launch(c);
     bool alt = false;
-    APC_TRY(apc_radix_sort_u64(c, m->pkey, m->pidx, m->pkey_alt, m->pidx_alt, nf, 0, 64, &alt));
+    // level 0 is in the reference's cell order; coarser levels are already sorted by
+    // code, and so are their parents' codes
+    if (lev == 0) APC_TRY(apc_radix_sort_u64(c, m->pkey, m->pidx, m->pkey_alt, m->pidx_alt, nf, 0, 64, &alt));
     uint64_t *pk = alt ? m->pkey_alt : m->pkey;
     uint32_t *pi = alt ? m->pidx_alt : m->pidx;
     APC_TRY(apc_ensure(c, &m->eflag, (size_t)nf + 1));
@@ -522,6 +652,14 @@ static int mg_build(apc_context *c) {
     ++lev;
   }
   m->nlev = lev + 1;
+  {
+    int first_tail = 0;
+    while (first_tail < m->nlev - 1 && m->lv[first_tail].n > kTail) ++first_tail;
+    if (m->nlev - first_tail > kTailLevels) {
+      c->err = "multigrid hierarchy deeper than the single-block tail supports";
+      return APC_ERR_UNSUPPORTED;
+    }
+  }
   // ---- coarsest level: explicit inverse in FP64 on the host ----
   MgLevel &K = m->lv[lev];
   const int n = K.n;
@@ -584,8 +722,32 @@ static void vcycle(apc_context *c, int l, const float *b, float *x) {
   const int sweeps = c->cfg.mg_sweeps > 0 ? c->cfg.mg_sweeps : 2;
   const float omega = (float)(c->cfg.mg_omega > 0 ? c->cfg.mg_omega : 0.7);
   const float alpha = (float)(c->cfg.mg_alpha > 0 ? c->cfg.mg_alpha : 1.0);
-  if (l == m->nlev - 1) {
-    dense_apply<<<1, 256, 0, c->s>>>(n, m->coarse_inv, b, x);
+  if (n <= kTail || l == m->nlev - 1) {
+    // this level and every coarser one in a single block
+    TailArgs A{};
+    A.nl = std::min(m->nlev - l, kTailLevels);
+    A.inv = m->coarse_inv;
+    A.sweeps = sweeps;
+    A.omega = omega;
+    A.alpha = alpha;
+    for (int k = 0; k < A.nl; ++k) {
+      MgLevel &T = m->lv[l + k];
+      TailLevel &D = A.L[k];
+      D.n = T.n;
+      D.w = T.w;
+      D.ld = T.ld;
+      D.col = T.col;
+      D.val = T.val;
+      D.dinv = T.dinv;
+      D.agg = T.agg;
+      D.mptr = T.mptr;
+      D.mem = T.mem;
+      D.x = k == 0 ? x : T.x;
+      D.b = k == 0 ? const_cast<float *>(b) : T.b;
+      D.x2 = T.x2;
+      D.r = T.r;
+    }
+    vcycle_tail<<<1, 1024, 0, c->s>>>(A);
     apc_count_launch(c);
     return;
   }
@@ -669,6 +831,7 @@ int apc_mg_fgmres(apc_context *c, bool rebuild, const float *r, float *d, int re
   const auto ts = std::chrono::steady_clock::now();
   *levels = m->nlev;
   MgLevel &L0 = m->lv[0];
+  const bool reorth = c->cfg.mg_reorth != 0;
   const int G = std::min(kRedBlocks, grid_for(n));
   const int Gs = grid_for(n, 1184);
   double *h1 = m->dots, *h2 = m->dots + 34, *nr = m->dots + 68;
@@ -692,11 +855,16 @@ int apc_mg_fgmres(apc_context *c, bool rebuild, const float *r, float *d, int re
     float *zk = m->Z + (size_t)it * vn, *w = m->V + (size_t)(it + 1) * vn;
     APC_CUDA_TRY(c, cudaGraphLaunch(m->graph_exec, c->s));  // vout = V-cycle(vin)
     apc_count_launch(c, (int)m->graph_nodes);
-    spmv_keep<<<Gs, kT, 0, c->s>>>(n, L0.w, L0.ld, L0.col, L0.val, m->vout, zk, w);
-    cgs_pass<0><<<G, kT, 0, c->s>>>(n, it + 1, m->V, vn, w, nullptr, m->partial, m->counter, h1);
-    cgs_pass<1><<<G, kT, 0, c->s>>>(n, it + 1, m->V, vn, w, h1, m->partial, m->counter, h2);
-    cgs_pass<2><<<G, kT, 0, c->s>>>(n, it + 1, m->V, vn, w, h2, m->partial, m->counter, nr);
-    apc_count_launch(c, 4);
+    spmv_dots<<<G, kT, 0, c->s>>>(n, L0.w, L0.ld, L0.col, L0.val, m->vout, zk, w, it + 1, m->V, vn, m->partial,
+                                  m->counter, h1);
+    if (reorth) {
+      cgs_pass<1><<<G, kT, 0, c->s>>>(n, it + 1, m->V, vn, w, h1, m->partial, m->counter, h2);
+      cgs_pass<2><<<G, kT, 0, c->s>>>(n, it + 1, m->V, vn, w, h2, m->partial, m->counter, nr);
+    } else {
+      cgs_pass<2><<<G, kT, 0, c->s>>>(n, it + 1, m->V, vn, w, h1, m->partial, m->counter, nr);
+    }
+    apc_count_launch(c, reorth ? 3 : 2);
+    if (!reorth) APC_CUDA_TRY(c, cudaMemsetAsync(h2, 0, sizeof(double) * (it + 1), c->s));
     APC_CUDA_TRY(c, cudaMemcpyAsync(m->host, m->dots, sizeof(double) * 69, cudaMemcpyDeviceToHost, c->s));
     APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
     const double tt = std::sqrt(m->host[68]);

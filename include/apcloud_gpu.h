@@ -77,13 +77,14 @@ typedef struct apc_config {
   double gmres_dtol;     /* -ksp_divtol */
   int gmres_max_it;      /* -ksp_max_it */
   int precision;         /* apc_precision */
-  int mixed_restart;     /* FP32 inner GMRES restart for APC_PREC_MIXED (0 = autotuned) */
+  int mixed_restart;     /* FP32 inner restart for APC_PREC_MIXED (0 = 16 with multigrid, 30 without) */
   double mixed_inner_rtol; /* FP32 inner solve relative tolerance (0 = 1e-5) */
   int device;            /* CUDA device ordinal */
   int mixed_precond;     /* APC_PREC_MIXED potential solve: APC_PRECOND_JACOBI or APC_PRECOND_MULTIGRID */
   int mg_sweeps;         /* multigrid: Jacobi sweeps before and after each coarse correction (0 = 2) */
   double mg_omega;       /* multigrid: Jacobi damping (0 = 0.7) */
   double mg_alpha;       /* multigrid: coarse-correction scaling (0 = 1.0) */
+  int mg_reorth;         /* multigrid FGMRES: 1 = classical Gram-Schmidt twice, 0 = once (default) */
 } apc_config;
 
 enum { APC_PRECOND_JACOBI = 0, APC_PRECOND_MULTIGRID = 1 };
