@@ -56,7 +56,8 @@ class ApcProfile(C.Structure):
                 ("krylov_bytes", C.c_double), ("select_ms", C.c_double), ("solve_ms", C.c_double),
                 ("move_ms", C.c_double), ("steps", C.c_int64), ("step_ms", C.c_double),
                 ("gfd_ms", C.c_double), ("mg_build_ms", C.c_double), ("mg_solve_ms", C.c_double),
-                ("mg_iterations", C.c_int64)]
+                ("mg_iterations", C.c_int64), ("assemble_ms", C.c_double), ("density_ms", C.c_double),
+                ("potential_ms", C.c_double)]
 
 
 class ApcStepParams(C.Structure):

@@ -123,6 +123,7 @@ struct apc_context {
   cudaEvent_t ev[8] = {};
   cudaEvent_t kev[2] = {};   // around each GMRES launch
   cudaEvent_t gev[2] = {};   // around the GFD stencil kernel
+  cudaEvent_t sev[3] = {};   // solve phase: after assembly, after the density solve, after the potential rhs
   double t_select_ms = 0, t_solve_ms = 0, t_move_ms = 0;
   apc_profile prof{};
   bool step_open = false;    // a select has started a step that move_position will close
@@ -148,10 +149,13 @@ int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int 
                      double *rnorm, int *reason, int *refinements);  // krylov.cu
 void apc_krylov_free(apc_context *c);
 void apc_mg_free(apc_context *c);
-// FP32 FGMRES with the octree-aggregation V-cycle (mg.cu); rebuilds the hierarchy from
-// the current potential operator when asked
-int apc_mg_fgmres(apc_context *c, bool rebuild, const float *r, float *d, int restart, double rtol_in,
-                  int max_it, int *its, int *levels);
+// One solve of the mixed path (mg.cu): FP64 refinement with FP32 (F)GMRES corrections on
+// the Jacobi-scaled operator valf, run on the device as one CUDA graph; with use_mg the
+// corrections are right-preconditioned by the octree-aggregation V-cycle, whose hierarchy
+// is rebuilt from valf
+int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, const float *valf, const double *b,
+                 double *x, double *r, int restart, double rtol_in, int *its, double *rnorm, int *reason,
+                 int *refinements, int *levels);
 int apc_potential_rhs(apc_context *c, double c_pot);    // gfd.cu
 int apc_differentiate(apc_context *c, double c_field);  // gfd.cu
 int apc_mover_velocity(apc_context *c, double dt, double c_vel, double *max_dv);  // mover.cu

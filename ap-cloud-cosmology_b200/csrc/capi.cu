@@ -100,6 +100,8 @@ void free_all(apc_context *c) {
     if (e) cudaEventDestroy(e);
   for (auto &e : c->gev)
     if (e) cudaEventDestroy(e);
+  for (auto &e : c->sev)
+    if (e) cudaEventDestroy(e);
   if (c->s) cudaStreamDestroy(c->s);
   g_caps.erase(c);
 }
@@ -209,6 +211,8 @@ int apc_create(const apc_config *cfg, apc_context **out) {
   for (auto &e : c->kev)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(APC_ERR_CUDA);
   for (auto &e : c->gev)
+    if (cudaEventCreate(&e) != cudaSuccess) return fail(APC_ERR_CUDA);
+  for (auto &e : c->sev)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(APC_ERR_CUDA);
   if (cudaMallocHost((void **)&c->h_pinned, 64 * sizeof(int)) != cudaSuccess) return fail(APC_ERR_CUDA);
   const size_t n = (size_t)c->n;
@@ -363,16 +367,23 @@ int apc_solve(apc_context *c, double c_dens, double c_pot, double c_field) {
     APC_TRY(apc_ensure(c, &c->a2f, (size_t)c->m_cap * c->ell_w, nullptr));
   }
   apc_solve_stats &st = c->stats;
+  APC_CUDA_TRY(c, cudaEventRecord(c->sev[0], c->s));
   APC_TRY(apc_krylov_solve(c, 0, c->rhs, c->density, &st.density_its, &st.density_rnorm, &st.density_reason,
                            &st.density_refinements));
+  APC_CUDA_TRY(c, cudaEventRecord(c->sev[1], c->s));
   APC_TRY(apc_potential_rhs(c, c_pot));
+  APC_CUDA_TRY(c, cudaEventRecord(c->sev[2], c->s));
   APC_TRY(apc_krylov_solve(c, 1, c->rhs, c->potential, &st.potential_its, &st.potential_rnorm,
                            &st.potential_reason, &st.potential_refinements));
+  APC_CUDA_TRY(c, cudaEventRecord(c->ev[7], c->s));
   APC_TRY(apc_differentiate(c, c_field));
   (void)M;
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[3], c->s));
   APC_CUDA_TRY(c, cudaEventSynchronize(c->ev[3]));
   c->t_solve_ms = elapsed(c->ev[2], c->ev[3]);
+  c->prof.assemble_ms += elapsed(c->ev[2], c->sev[0]);
+  c->prof.density_ms += elapsed(c->sev[0], c->sev[1]);
+  c->prof.potential_ms += elapsed(c->sev[2], c->ev[7]);
   c->prof.solve_ms += c->t_solve_ms;
   c->prof.steps += 1;
   c->have_fields = true;

@@ -1,5 +1,5 @@
-// Restarted GMRES with left Jacobi preconditioning on the device, and the FP32-inner /
-// FP64-outer iterative refinement of the mixed-precision path.
+// Restarted GMRES with left Jacobi preconditioning on the device (the FP64 path), and
+// the solve entry point, which hands the mixed-precision path to mg.cu.
 //
 // Reference: Solver::Solve_Density / Solve_Potential (solver.cpp:182-293) call PETSc
 // KSPGMRES + PCJACOBI (solver.cpp:196-204, 267-276).  The FP64 kernel follows PETSc
@@ -426,68 +426,8 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_kernel(GmresArgs<T> A) {
   }
 }
 
-// ------------------------------------------------------------ refinement helpers
+// ------------------------------------------------------------ mixed-path helpers
 
-// r = b - A x (FP64), and per-block partials of ||D^-1 r||^2
-__global__ void __launch_bounds__(256) residual64(int n, int w, size_t ld, const int *__restrict__ col,
-                                                  const double *__restrict__ val,
-                                                  const double *__restrict__ b,
-                                                  const double *__restrict__ x, double *__restrict__ r,
-                                                  double *partial) {
-  double nrm = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double s = 0.0;
-    for (int k = 0; k < w; ++k) {
-      const size_t at = (size_t)k * ld + i;
-      s += val[at] * x[col[at]];
-    }
-    const double ri = b[i] - s;
-    r[i] = ri;
-    const double d = val[i];
-    const double pr = (d == 0.0 ? 1.0 : 1.0 / d) * ri;
-    nrm += pr * pr;
-  }
-  __shared__ double sm[256];
-  sm[threadIdx.x] = nrm;
-  __syncthreads();
-  for (int o = 128; o > 0; o >>= 1) {
-    if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) partial[blockIdx.x] = sm[0];
-}
-
-__global__ void sum_partials(const double *partial, int n, double *out) {
-  __shared__ double sm[256];
-  double v = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) v += partial[i];
-  sm[threadIdx.x] = v;
-  __syncthreads();
-  for (int o = 128; o > 0; o >>= 1) {
-    if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) *out = sm[0];
-}
-
-// rhs32 = D^-1 r / s: the FP64 residual, Jacobi-scaled, in FP32 (diagonal = ELL slot 0)
-__global__ void to_f32_scaled(int n, const double *__restrict__ r, const double *__restrict__ diag, double inv_s,
-                              float *__restrict__ r32) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double d = diag[i];
-    r32[i] = (float)((d == 0.0 ? r[i] : r[i] / d) * inv_s);
-  }
-}
-
-__global__ void axpy_f32(int n, double s, const float *__restrict__ d, double *__restrict__ x) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    x[i] += s * (double)d[i];
-}
-
-// FP32 copy of D^-1 A (rows scaled by their FP64 diagonal before rounding).  The
-// potential operator's rows sum to zero and its Dirichlet row is a unit row, so the
-// constant mode has a singular value ~1/sqrt(n).  Unscaled, FP32 rounding of rows of
-// size ~1/h^2 would perturb that mode by O(1); scaled rows keep it at O(eps32 sqrt(n)).
 __global__ void ell_to_f32_scaled(size_t ld, int w, int n, const double *__restrict__ a, float *__restrict__ f) {
   const size_t count = ld * (size_t)w;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < count; e += (size_t)gridDim.x * blockDim.x) {
@@ -515,8 +455,7 @@ struct KrylovWork {
   GridBar *bar = nullptr;
   int *ires = nullptr;     // its, reason
   double *dres = nullptr;  // rnorm
-  double *r = nullptr, *partial = nullptr, *scalar = nullptr;
-  float *r32 = nullptr, *d32 = nullptr;
+  double *r = nullptr;  // FP64 residual of the mixed path
   float *a32 = nullptr;
   int cap_n = 0;
   int occ64[2] = {0, 0}, occ32[2] = {0, 0};
@@ -531,10 +470,6 @@ void apc_krylov_free(apc_context *c) {
   cudaFree(k->ires);
   cudaFree(k->dres);
   cudaFree(k->r);
-  cudaFree(k->partial);
-  cudaFree(k->scalar);
-  cudaFree(k->r32);
-  cudaFree(k->d32);
   cudaFree(k->a32);
   delete k;
   c->kw = nullptr;
@@ -637,21 +572,13 @@ static int ensure_work(apc_context *c, int n) {
     APC_TRY(apc_alloc(c, (void **)&c->kw->bar, sizeof(GridBar)));
     APC_TRY(apc_alloc(c, (void **)&c->kw->ires, 4 * sizeof(int)));
     APC_TRY(apc_alloc(c, (void **)&c->kw->dres, 2 * sizeof(double)));
-    APC_TRY(apc_alloc(c, (void **)&c->kw->scalar, 4 * sizeof(double)));
-    APC_TRY(apc_alloc(c, (void **)&c->kw->partial, 4096 * sizeof(double)));
   }
   KrylovWork *k = c->kw;
   if (n > k->cap_n) {
     cudaFree(k->r);
-    cudaFree(k->r32);
-    cudaFree(k->d32);
     k->r = nullptr;
-    k->r32 = nullptr;
-    k->d32 = nullptr;
     const int cap = n + n / 4 + 1024;
     APC_TRY(apc_alloc(c, (void **)&k->r, sizeof(double) * cap));
-    APC_TRY(apc_alloc(c, (void **)&k->r32, sizeof(float) * cap));
-    APC_TRY(apc_alloc(c, (void **)&k->d32, sizeof(float) * cap));
     k->cap_n = cap;
   }
   return APC_OK;
@@ -675,63 +602,23 @@ int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int 
     return launch_gmres<double, false>(c, n, val, b, x, cfg.gmres_restart, cfg.gmres_rtol, cfg.gmres_atol,
                                        cfg.gmres_dtol, cfg.gmres_max_it, its, rnorm, reason);
   }
-  // ---- mixed precision ----
+  // ---- mixed precision: the refinement loop and its FP32 corrections run on the device
+  //      as one graph per solve (mg.cu) ----
   const size_t ell_count = (size_t)c->m_cap * c->ell_w;
   float *af = which == 0 ? c->a1f : c->a2f;
   const int G = std::max(1, std::min((n + 255) / 256, std::min(apc_sm_count(c) * 8, 4096)));
-  {
-    ell_to_f32_scaled<<<std::min<size_t>((ell_count + 255) / 256, 8192), 256, 0, c->s>>>((size_t)c->m_cap,
-                                                                                         c->ell_w, n, val, af);
-    zero_f64<<<G, 256, 0, c->s>>>(n, x);
-    apc_count_launch(c, 2);
-  }
-  // inner restart: 16 for the multigrid FGMRES (a V-cycle per step makes short cycles
-  // cheapest at 128^3), 30 for Jacobi GMRES
+  ell_to_f32_scaled<<<std::min<size_t>((ell_count + 255) / 256, 8192), 256, 0, c->s>>>((size_t)c->m_cap, c->ell_w,
+                                                                                       n, val, af);
+  zero_f64<<<G, 256, 0, c->s>>>(n, x);
+  apc_count_launch(c, 2);
+  // inner restart: 16 for the multigrid FGMRES (a V-cycle per iteration makes short
+  // cycles cheapest at 128^3), 30 without a preconditioner
   const bool use_mg = which == 1 && cfg.mixed_precond == APC_PRECOND_MULTIGRID;
   const int m32 = cfg.mixed_restart > 0 ? cfg.mixed_restart : (use_mg ? 16 : 30);
   const double rtol_in = cfg.mixed_inner_rtol > 0 ? cfg.mixed_inner_rtol : 1e-5;
-  double ttol = 0.0, rn0 = 0.0;
-  int total_its = 0, rs = 0;
-  double rn = 0.0;
-  for (int outer = 0; outer < 40; ++outer) {
-    residual64<<<G, 256, 0, c->s>>>(n, c->ell_w, (size_t)c->m_cap, c->ell_col, val, b, x, k->r, k->partial);
-    sum_partials<<<1, 256, 0, c->s>>>(k->partial, G, k->scalar);
-    apc_count_launch(c, 2);
-    double nrm2 = 0.0;
-    APC_CUDA_TRY(c, cudaMemcpyAsync(&nrm2, k->scalar, sizeof(double), cudaMemcpyDeviceToHost, c->s));
-    APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
-    rn = std::sqrt(nrm2);
-    if (outer == 0) {
-      ttol = std::max(cfg.gmres_rtol * rn, cfg.gmres_atol);
-      rn0 = rn;
-      if (rn == 0.0) { rs = KSP_CONVERGED_ATOL; break; }
-    }
-    if (rn != rn) { rs = KSP_DIVERGED_NANORINF; break; }
-    if (rn <= ttol) { rs = rn < cfg.gmres_atol ? KSP_CONVERGED_ATOL : KSP_CONVERGED_RTOL; break; }
-    if (rn >= cfg.gmres_dtol * rn0) { rs = KSP_DIVERGED_DTOL; break; }
-    if (total_its >= cfg.gmres_max_it) { rs = KSP_DIVERGED_ITS; break; }
-    // scale the correction problem to unit preconditioned-residual norm
-    const double s = rn;
-    to_f32_scaled<<<G, 256, 0, c->s>>>(n, k->r, val, 1.0 / s, k->r32);
-    apc_count_launch(c);
-    int iits = 0, ireason = 0;
-    double irn = 0.0;
-    if (use_mg) {
-      int levels = 0;
-      APC_TRY(apc_mg_fgmres(c, outer == 0, k->r32, k->d32, m32, rtol_in,
-                            std::max(1, cfg.gmres_max_it - total_its), &iits, &levels));
-      c->stats.mg_levels = levels;
-    } else {
-      APC_TRY(launch_gmres<float, true>(c, n, af, k->r32, k->d32, m32, rtol_in, 1e-30, 1e30,
-                                        std::max(1, cfg.gmres_max_it - total_its), &iits, &irn, &ireason));
-    }
-    total_its += iits;
-    axpy_f32<<<G, 256, 0, c->s>>>(n, s, k->d32, x);
-    apc_count_launch(c);
-    ++*refinements;
-  }
-  *its = total_its;
-  *rnorm = rn;
-  *reason = rs;
+  int levels = 0;
+  APC_TRY(apc_ir_solve(c, which, use_mg, val, af, b, x, k->r, m32, rtol_in, its, rnorm, reason, refinements,
+                       &levels));
+  if (use_mg) c->stats.mg_levels = levels;
   return APC_OK;
 }

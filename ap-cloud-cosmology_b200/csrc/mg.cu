@@ -1,9 +1,16 @@
-// Multigrid-preconditioned FP32 Krylov solve of the potential system (mixed path).
+// The mixed-precision solves: FP64 iterative refinement with FP32 Krylov corrections,
+// run on the device as one CUDA graph per solve, and the multigrid preconditioner of the
+// potential solve.
 //
 // The reference solves the Poisson system with GMRES + Jacobi (solver.cpp:267-276).  At
 // 262k cells that reaches max_it before rtol (KSP_DIVERGED_ITS), in the reference and on
 // the GPU alike.  The mixed path keeps the reference's stopping test on the FP64 residual
-// (krylov.cu).  Its FP32 correction solves use this preconditioner:
+// ||D^-1 (b - A x)|| <= max(rtol ||D^-1 b||, atol), with dtol and max_it.  Each
+// correction solves the Jacobi-scaled system (D^-1 A) d = D^-1 r / ||D^-1 r|| in FP32:
+//   * Loops on the device.  The refinement loop and the (F)GMRES cycle are nested
+//     conditional WHILE nodes of one graph; kernels hold every scalar (Hessenberg
+//     column, Givens rotations, stopping tests) in device memory and set the loop
+//     conditions, so a solve costs the host one launch and one readback.
 //   * Aggregation by the octree.  A node of the next coarser level is the parent cell
 //     (location code >> 3); its aggregate is the set of its children present on the
 //     finer level.  Coarse node order is sorted location code, so Morton order.
@@ -12,11 +19,13 @@
 //     bitonic network and summed in sorted order, so the hierarchy is deterministic.
 //     Rows sum to zero except the Dirichlet pin's aggregate, so the constant mode is
 //     reproduced exactly on every level.
-//   * Damped Jacobi smoothing on ELL operators; an explicit dense inverse (FP64, formed
-//     on the host) on the coarsest level of <= 128 nodes.
+//   * Damped Jacobi smoothing on ELL operators, over-scaled coarse corrections; the
+//     levels of <= 512 nodes in one single-block kernel; an explicit dense inverse (FP64,
+//     formed on the host) on the coarsest level of <= 64 nodes.
 //   * Flexible GMRES with classical Gram-Schmidt (optionally a second, re-orthogonalising
 //     sweep), right preconditioned, so the residual it monitors is the true residual of
-//     the correction equation.  The SpMV is fused with the first dot-product pass.
+//     the correction equation.  The SpMV is fused with the first dot-product pass.  The
+//     density solve runs the same loop without a preconditioner.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -232,25 +241,42 @@ __global__ void restrict_sum(int nc, const int *__restrict__ mptr, int nf, const
   }
 }
 
+// out = in + alpha P xc (in place when out == in)
 __global__ void prolong_add(int n, const int *__restrict__ agg, const float *__restrict__ xc, float alpha,
-                            float *__restrict__ x) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] += alpha * xc[agg[i]];
+                            const float *in, float *out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = in[i] + alpha * xc[agg[i]];
 }
 
 // ------------------------------------------------------------------ FGMRES
 
-__global__ void combine(int n, int nv, const float *__restrict__ Z, size_t vn, const double *__restrict__ y,
-                        float *__restrict__ x) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double t = 0.0;
-    for (int j = 0; j < nv; ++j) t += y[j] * (double)Z[(size_t)j * vn + i];
-    x[i] = (float)t;
-  }
-}
+// State of the device-resident mixed solve: the FP64 refinement loop and the FP32
+// FGMRES cycle both run as conditional WHILE nodes of one CUDA graph, so every
+// scalar of the iteration lives here.  The leading fields are read back by the host
+// once the graph has run.
+constexpr int kMaxM = 31;
 
-// ---- fused FGMRES kernels: every reduction finishes in the last block to arrive, which
-//      adds the per-block partials in a fixed order (deterministic) ----
+struct IrState {
+  int outer;      // corrections applied (refinements)
+  int total_its;  // FGMRES iterations over all corrections
+  int reason;     // KSP convergence reason of the refinement loop
+  int it;         // iteration of the current FGMRES cycle
+  double rn;      // ||D^-1 (b - A x)|| of the current iterate
+  double rn0, ttol;
+  double rtol, atol, dtol, rtol_in;
+  int max_it, max_outer, M, inner_max;
+  double beta;    // ||v_0|| of the current cycle
+  double scale;   // factor that normalises the newest basis vector
+  double H[(kMaxM + 1) * kMaxM];  // column j at H[j * (M + 1)]
+  double cs[kMaxM], sn[kMaxM], g[kMaxM + 1], y[kMaxM];
+};
 
+// KSPConvergedReason values of the stopping test (petsc 3.5 kspconvergedreason)
+constexpr int kConvergedRtol = 2, kConvergedAtol = 3, kDivergedIts = -3, kDivergedDtol = -4,
+              kDivergedNanOrInf = -9;
+
+// Every reduction finishes in the last block to arrive, which adds the per-block
+// partials in a fixed order (deterministic).
 constexpr int kRedBlocks = 296;  // grid of the reduction kernels (2 per SM)
 
 __device__ __forceinline__ bool last_block_arrived(unsigned *counter) {
@@ -279,117 +305,300 @@ __device__ __forceinline__ void finish_sums(int nv, const double *partial, unsig
   if (threadIdx.x == 0) atomicExch(counter, 0u);
 }
 
-// mode 0: h = V^T w.  mode 1: w -= V h_in; h = V^T w.  mode 2: w -= V h_in; h[0] = ||w||^2.
-// Each warp takes tiles of 32 consecutive rows (one per lane); the basis values of a row
-// stay in registers for the update and the dots; every dot is reduced across the warp at
-// once and kept by lane j, so one accumulator per lane covers all basis vectors.
-template <int MODE>
-__global__ void __launch_bounds__(kT) cgs_pass(int n, int nv, const float *__restrict__ V, size_t vn, float *w,
-                                                const double *__restrict__ h_in, double *partial, unsigned *counter,
-                                                double *out) {
-  __shared__ double hsh[32];
-  __shared__ double sm[kT / 32][32];
-  if (MODE > 0 && (int)threadIdx.x < nv) hsh[threadIdx.x] = h_in[threadIdx.x];
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  double acc = 0.0;
-  const int ntiles = (n + 31) / 32;
-  for (int tile = blockIdx.x * nw + warp; tile < ntiles; tile += gridDim.x * nw) {
-    const int i = tile * 32 + lane;
-    const bool ok = i < n;
-    float vj[32];
+__device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
-    for (int j = 0; j < 32; ++j) vj[j] = (j < nv && ok) ? V[(size_t)j * vn + i] : 0.f;
-    double wi = ok ? (double)w[i] : 0.0;
-    if (MODE > 0) {
-#pragma unroll
-      for (int j = 0; j < 32; ++j)
-        if (j < nv) wi -= hsh[j] * (double)vj[j];
-      if (ok) w[i] = (float)wi;
-      wi = (double)(float)wi;
-    }
-    if (MODE < 2) {
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        if (j < nv) {
-          double p = wi * (double)vj[j];
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
-          if (lane == j) acc += p;
-        }
-      }
-    } else {
-      double p = wi * wi;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
-      if (lane == 0) acc += p;
-    }
-  }
-  sm[warp][lane] = acc;
-  __syncthreads();
-  const int nout = MODE < 2 ? nv : 1;
-  if ((int)threadIdx.x < nout) {
-    double v = 0.0;
-    for (int k = 0; k < nw; ++k) v += sm[k][threadIdx.x];
-    partial[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = v;
-  }
-  if (last_block_arrived(counter)) finish_sums(nout, partial, counter, out);
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
 }
 
-// w = A z (z kept for the solution), then the block's dots <w, V_j>, j < nv, in the same
-// warp-tile pass as cgs_pass<0>
-__global__ void __launch_bounds__(kT) spmv_dots(int n, int ew, size_t ld, const int *__restrict__ col,
-                                                 const float *__restrict__ val, const float *__restrict__ z,
-                                                 float *__restrict__ zkeep, float *__restrict__ w, int nv,
-                                                 const float *__restrict__ V, size_t vn, double *partial,
-                                                 unsigned *counter, double *out) {
+// block partials of nv per-lane accumulators: reduced across each warp once, then
+// across the block's warps in warp order
+__device__ __forceinline__ void block_partials(const double (&acc)[32], int nv, double *partial) {
   __shared__ double sm[kT / 32][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  double acc = 0.0;
-  const int ntiles = (n + 31) / 32;
-  for (int tile = blockIdx.x * nw + warp; tile < ntiles; tile += gridDim.x * nw) {
-    const int i = tile * 32 + lane;
-    const bool ok = i < n;
-    float vj[32];
+  double mine = 0.0;
 #pragma unroll
-    for (int j = 0; j < 32; ++j) vj[j] = (j < nv && ok) ? V[(size_t)j * vn + i] : 0.f;
-    float sacc = 0.f;
-    if (ok) {
-      for (int k = 0; k < ew; ++k) {
-        const size_t at = (size_t)k * ld + i;
-        sacc += val[at] * z[col[at]];
-      }
-      zkeep[i] = z[i];
-      w[i] = sacc;
-    }
-    const double wi = (double)sacc;
-#pragma unroll
-    for (int j = 0; j < 32; ++j) {
-      if (j < nv) {
-        double p = wi * (double)vj[j];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
-        if (lane == j) acc += p;
-      }
+  for (int j = 0; j < 32; ++j) {
+    if (j < nv) {
+      const double p = warp_sum(acc[j]);
+      if (lane == j) mine = p;
     }
   }
-  sm[warp][lane] = acc;
+  sm[warp][lane] = mine;
   __syncthreads();
   if ((int)threadIdx.x < nv) {
     double v = 0.0;
     for (int k = 0; k < nw; ++k) v += sm[k][threadIdx.x];
     partial[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = v;
   }
+}
+
+__device__ __forceinline__ void block_partial1(double acc, double *partial) {
+  __shared__ double sm1[kT / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  acc = warp_sum(acc);
+  if (lane == 0) sm1[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int k = 0; k < nw; ++k) v += sm1[k];
+    partial[blockIdx.x] = v;
+  }
+}
+
+// Basis vectors V_0..V_it are rows of V (stride vn); the vector being orthogonalised is
+// V_{it+1}, with it read from the state.  Each warp takes tiles of 32 consecutive rows
+// (one per lane); a row's basis values stay in registers for the update and the dots.
+//   MODE 1: w -= V h_in; h = V^T w.   MODE 2: w -= V h_in; out[0] = ||w||^2.
+template <int MODE>
+__global__ void __launch_bounds__(kT) cgs_pass(int n, const IrState *__restrict__ S, float *V, size_t vn,
+                                                const double *__restrict__ h_in, double *partial, unsigned *counter,
+                                                double *out) {
+  __shared__ double hsh[32];
+  const int nv = S->it + 1;
+  float *w = V + (size_t)nv * vn;
+  if ((int)threadIdx.x < nv) hsh[threadIdx.x] = h_in[threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double acc[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+  double acc1 = 0.0;
+  const int ntiles = (n + 31) / 32;
+  for (int tile = blockIdx.x * nw + warp; tile < ntiles; tile += gridDim.x * nw) {
+    const int i = tile * 32 + lane;
+    const bool ok = i < n;
+    if (MODE == 1) {
+      float vj[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) vj[j] = (j < nv && ok) ? V[(size_t)j * vn + i] : 0.f;
+      double wi = ok ? (double)w[i] : 0.0;
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < nv) wi -= hsh[j] * (double)vj[j];
+      if (ok) w[i] = (float)wi;
+      wi = (double)(float)wi;
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < nv) acc[j] += wi * (double)vj[j];
+    } else if (ok) {
+      double wi = (double)w[i];
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < nv) wi -= hsh[j] * (double)V[(size_t)j * vn + i];
+      w[i] = (float)wi;
+      wi = (double)(float)wi;
+      acc1 += wi * wi;
+    }
+  }
+  if (MODE == 1) {
+    block_partials(acc, nv, partial);
+    if (last_block_arrived(counter)) finish_sums(nv, partial, counter, out);
+  } else {
+    block_partial1(acc1, partial);
+    if (last_block_arrived(counter)) finish_sums(1, partial, counter, out);
+  }
+}
+
+// V_{it+1} = A z and the dots <V_{it+1}, V_j>, j <= it, in the same warp-tile pass.
+// With a preconditioner z is its output, kept as Z_it for the solution; without one
+// (Z == nullptr) z is V_it itself.
+__global__ void __launch_bounds__(kT) spmv_dots(int n, int ew, size_t ld, const int *__restrict__ col,
+                                                 const float *__restrict__ val, const float *zin, float *Z,
+                                                 float *V, size_t vn, const IrState *__restrict__ S, double *partial,
+                                                 unsigned *counter, double *out) {
+  const int it = S->it, nv = it + 1;
+  const float *z = Z ? zin : V + (size_t)it * vn;
+  float *zk = Z ? Z + (size_t)it * vn : nullptr;
+  float *w = V + (size_t)nv * vn;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double acc[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+  const int ntiles = (n + 31) / 32;
+  for (int tile = blockIdx.x * nw + warp; tile < ntiles; tile += gridDim.x * nw) {
+    const int i = tile * 32 + lane;
+    if (i >= n) continue;
+    float sacc = 0.f;
+    for (int k = 0; k < ew; ++k) {
+      const size_t at = (size_t)k * ld + i;
+      sacc += val[at] * z[col[at]];
+    }
+    if (zk) zk[i] = z[i];
+    w[i] = sacc;
+    const double wi = (double)sacc;
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      if (j < nv) acc[j] += wi * (double)V[(size_t)j * vn + i];
+  }
+  block_partials(acc, nv, partial);
   if (last_block_arrived(counter)) finish_sums(nv, partial, counter, out);
 }
 
-// v_next = f w, and the same into the V-cycle's fixed input buffer
-__global__ void scale2(int n, const float *__restrict__ w, float f, float *__restrict__ v, float *__restrict__ vin) {
+// V_it *= scale (the newest basis vector), and the same into the V-cycle's input if any
+__global__ void scale_next(int n, const IrState *__restrict__ S, float *__restrict__ V, size_t vn,
+                           float *__restrict__ vin) {
+  const float f = (float)S->scale;
+  float *v = V + (size_t)S->it * vn;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const float u = w[i] * f;
+    const float u = v[i] * f;
     v[i] = u;
-    vin[i] = u;
+    if (vin) vin[i] = u;
   }
+}
+
+// One Arnoldi step's scalar work: Hessenberg column, Givens rotations, residual
+// estimate, and whether the cycle goes on (sets the inner loop's condition).
+template <bool REORTH>
+__global__ void arnoldi(IrState *S, const double *__restrict__ h1, const double *__restrict__ h2,
+                        const double *__restrict__ nr, cudaGraphConditionalHandle cond) {
+  if (threadIdx.x != 0) return;
+  const int it = S->it, M1 = S->M + 1;
+  const double tt = sqrt(*nr);
+  double *hc = S->H + (size_t)it * M1;
+  for (int j = 0; j <= it; ++j) hc[j] = h1[j] + (REORTH ? h2[j] : 0.0);
+  hc[it + 1] = tt;
+  for (int j = 1; j <= it; ++j) {
+    const double t0 = hc[j - 1];
+    hc[j - 1] = S->cs[j - 1] * t0 + S->sn[j - 1] * hc[j];
+    hc[j] = S->cs[j - 1] * hc[j] - S->sn[j - 1] * t0;
+  }
+  const double t = sqrt(hc[it] * hc[it] + hc[it + 1] * hc[it + 1]);
+  bool more = false;
+  if (t != 0.0 && t == t) {
+    const double cs = hc[it] / t, sn = hc[it + 1] / t;
+    S->cs[it] = cs;
+    S->sn[it] = sn;
+    S->g[it + 1] = -sn * S->g[it];
+    S->g[it] = cs * S->g[it];
+    hc[it] = cs * hc[it] + sn * hc[it + 1];
+    more = !(fabs(S->g[it + 1]) <= S->rtol_in * S->beta) && tt != 0.0;
+  }
+  S->it = it + 1;
+  more = more && S->it < S->inner_max;
+  S->scale = tt > 0.0 ? 1.0 / tt : 0.0;
+  cudaGraphSetConditional(cond, more ? 1u : 0u);
+}
+
+// y = H^-1 g (upper triangular) for the cycle's iterations
+__global__ void fg_finish(IrState *S) {
+  if (threadIdx.x != 0) return;
+  const int it = S->it, M1 = S->M + 1;
+  for (int k = it - 1; k >= 0; --k) {
+    double s = S->g[k];
+    for (int j = k + 1; j < it; ++j) s -= S->H[(size_t)j * M1 + k] * S->y[j];
+    const double hkk = S->H[(size_t)k * M1 + k];
+    S->y[k] = hkk != 0.0 ? s / hkk : 0.0;
+  }
+  S->total_its += it;
+}
+
+// d = Z y
+__global__ void combine(int n, const float *__restrict__ Z, size_t vn, const IrState *__restrict__ S,
+                        float *__restrict__ d) {
+  const int nv = S->it;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double t = 0.0;
+    for (int j = 0; j < nv; ++j) t += S->y[j] * (double)Z[(size_t)j * vn + i];
+    d[i] = (float)t;
+  }
+}
+
+// ---- the FP64 refinement loop ----
+
+__global__ void ir_init(IrState *S, double rtol, double atol, double dtol, double rtol_in, int max_it, int max_outer,
+                        int M) {
+  S->outer = 0;
+  S->total_its = 0;
+  S->reason = 0;
+  S->it = 0;
+  S->rn = S->rn0 = S->ttol = 0.0;
+  S->rtol = rtol;
+  S->atol = atol;
+  S->dtol = dtol;
+  S->rtol_in = rtol_in;
+  S->max_it = max_it;
+  S->max_outer = max_outer;
+  S->M = M;
+}
+
+// r = b - A x in FP64 and ||D^-1 r||; the last block applies the stopping test of the
+// reference's KSP (rtol on the first residual, atol, dtol, max_it) and sets the
+// refinement loop's condition
+__global__ void __launch_bounds__(kT) ir_residual(int n, int w, size_t ld, const int *__restrict__ col,
+                                                   const double *__restrict__ val, const double *__restrict__ b,
+                                                   const double *__restrict__ x, double *__restrict__ r,
+                                                   IrState *S, double *partial, unsigned *counter, double *tmp,
+                                                   cudaGraphConditionalHandle cond) {
+  double nrm = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < w; ++k) {
+      const size_t at = (size_t)k * ld + i;
+      s += val[at] * x[col[at]];
+    }
+    const double ri = b[i] - s;
+    r[i] = ri;
+    const double d = val[i];
+    const double pr = (d == 0.0 ? 1.0 : 1.0 / d) * ri;
+    nrm += pr * pr;
+  }
+  block_partial1(nrm, partial);
+  if (!last_block_arrived(counter)) return;
+  finish_sums(1, partial, counter, tmp);
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const double rn = sqrt(__ldcg(tmp));
+  if (S->outer == 0) {
+    S->ttol = fmax(S->rtol * rn, S->atol);
+    S->rn0 = rn;
+  }
+  int reason = 0;
+  bool stop = true;
+  if (S->outer == 0 && rn == 0.0) reason = kConvergedAtol;
+  else if (!(rn == rn)) reason = kDivergedNanOrInf;
+  else if (rn <= S->ttol) reason = rn < S->atol ? kConvergedAtol : kConvergedRtol;
+  else if (rn >= S->dtol * S->rn0) reason = kDivergedDtol;
+  else if (S->total_its >= S->max_it) reason = kDivergedIts;
+  else if (S->outer >= S->max_outer) reason = 0;
+  else stop = false;
+  S->rn = rn;
+  S->reason = reason;
+  cudaGraphSetConditional(cond, stop ? 0u : 1u);
+}
+
+// v_0 = D^-1 r / ||D^-1 r|| rounded to FP32, and beta = ||v_0||; the last block opens
+// the FGMRES cycle (sets the inner loop's condition)
+__global__ void __launch_bounds__(kT) ir_to_f32(int n, const double *__restrict__ r, const double *__restrict__ diag,
+                                                 IrState *S, float *__restrict__ v0, double *partial,
+                                                 unsigned *counter, double *tmp, cudaGraphConditionalHandle cond) {
+  const double inv_s = 1.0 / S->rn;
+  double nrm = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double d = diag[i];
+    const float v = (float)((d == 0.0 ? r[i] : r[i] / d) * inv_s);
+    v0[i] = v;
+    nrm += (double)v * (double)v;
+  }
+  block_partial1(nrm, partial);
+  if (!last_block_arrived(counter)) return;
+  finish_sums(1, partial, counter, tmp);
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const double beta = sqrt(__ldcg(tmp));
+  S->beta = beta;
+  S->it = 0;
+  S->g[0] = beta;
+  S->scale = beta > 0.0 ? 1.0 / beta : 0.0;
+  S->inner_max = min(S->M, max(1, S->max_it - S->total_its));
+  cudaGraphSetConditional(cond, beta > 0.0 ? 1u : 0u);
+}
+
+// x += ||D^-1 r|| d: apply the correction of the scaled system
+__global__ void ir_axpy(int n, IrState *S, const float *__restrict__ d, double *__restrict__ x) {
+  const double s = S->rn;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] += s * (double)d[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0) S->outer += 1;
 }
 
 
@@ -511,16 +720,20 @@ struct MgWork {
   uint32_t *pidx = nullptr, *pidx_alt = nullptr;
   int *eflag = nullptr, *epos = nullptr, *ucol = nullptr, *rowstart = nullptr;
   float *uval = nullptr;
-  // FGMRES
-  float *V = nullptr, *Z = nullptr, *w = nullptr, *vin = nullptr, *vout = nullptr;
+  // FGMRES: basis V, preconditioned vectors Z, V-cycle in/out, correction
+  float *V = nullptr, *Z = nullptr, *vin = nullptr, *vout = nullptr, *dvec = nullptr;
+  size_t vn = 0;
   double *partial = nullptr, *dots = nullptr;
   unsigned *counter = nullptr;
-  double *host = nullptr;  // pinned readback buffer
+  IrState *state = nullptr;
+  void *host = nullptr;  // pinned readback of the state
   int *total = nullptr;
-  // the V-cycle of the current hierarchy as a CUDA graph (vin -> vout)
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t graph_exec = nullptr;
-  int64_t graph_nodes = 0;
+  // each mixed solve of the step as one graph, captured on c->s with the loop bodies on
+  // two side streams
+  cudaStream_t cap[2] = {nullptr, nullptr};
+  cudaGraph_t solve_graph[2] = {nullptr, nullptr};  // density, potential
+  cudaGraphExec_t solve_exec[2] = {nullptr, nullptr};
+  int64_t vcycle_nodes[2] = {0, 0};
 };
 
 static MgWork *mg(apc_context *c) {
@@ -547,12 +760,16 @@ void apc_mg_free(apc_context *c) {
     cudaFree(L.r);
   }
   void *p[] = {m->coarse_inv, m->pkey, m->pkey_alt, m->pidx, m->pidx_alt, m->eflag, m->epos, m->ucol,
-               m->rowstart, m->uval, m->V, m->Z, m->w,
-               m->vin, m->vout, m->partial, m->dots, m->counter, m->total};
+               m->rowstart, m->uval, m->V, m->Z, m->vin, m->vout, m->dvec,
+               m->partial, m->dots, m->counter, m->state, m->total};
   for (void *q : p) cudaFree(q);
   if (m->host) cudaFreeHost(m->host);
-  if (m->graph_exec) cudaGraphExecDestroy(m->graph_exec);
-  if (m->graph) cudaGraphDestroy(m->graph);
+  for (int k = 0; k < 2; ++k) {
+    if (m->solve_exec[k]) cudaGraphExecDestroy(m->solve_exec[k]);
+    if (m->solve_graph[k]) cudaGraphDestroy(m->solve_graph[k]);
+  }
+  for (cudaStream_t q : m->cap)
+    if (q) cudaStreamDestroy(q);
   delete m;
   c->mg = nullptr;
 }
@@ -714,14 +931,17 @@ static int mg_build(apc_context *c) {
   return APC_OK;
 }
 
-// x = V-cycle(b) on level l; b and x are that level's buffers
-static void vcycle(apc_context *c, int l, const float *b, float *x) {
+// x = V-cycle(b) on level l, launched on stream s; b and x are that level's buffers
+static void vcycle(apc_context *c, cudaStream_t s, int l, const float *b, float *x) {
   MgWork *m = c->mg;
   MgLevel &L = m->lv[l];
   const int n = L.n;
   const int sweeps = c->cfg.mg_sweeps > 0 ? c->cfg.mg_sweeps : 2;
-  const float omega = (float)(c->cfg.mg_omega > 0 ? c->cfg.mg_omega : 0.7);
-  const float alpha = (float)(c->cfg.mg_alpha > 0 ? c->cfg.mg_alpha : 1.0);
+  // piecewise-constant prolongation under-corrects smooth errors; over-scaling the
+  // coarse correction (1.8) with lightly damped Jacobi (0.95) took the 128^3 potential
+  // solve from 48 to 29 FGMRES iterations
+  const float omega = (float)(c->cfg.mg_omega > 0 ? c->cfg.mg_omega : 0.95);
+  const float alpha = (float)(c->cfg.mg_alpha > 0 ? c->cfg.mg_alpha : 1.8);
   if (n <= kTail || l == m->nlev - 1) {
     // this level and every coarser one in a single block
     TailArgs A{};
@@ -747,168 +967,256 @@ static void vcycle(apc_context *c, int l, const float *b, float *x) {
       D.x2 = T.x2;
       D.r = T.r;
     }
-    vcycle_tail<<<1, 1024, 0, c->s>>>(A);
+    vcycle_tail<<<1, 1024, 0, s>>>(A);
     apc_count_launch(c);
     return;
   }
   MgLevel &C = m->lv[l + 1];
   const int G = grid_for(n);
-  jacobi_first<<<G, kT, 0, c->s>>>(n, L.dinv, b, omega, x);
+  jacobi_first<<<G, kT, 0, s>>>(n, L.dinv, b, omega, x);
   float *cur = x, *nxt = L.x2;
   for (int k = 1; k < sweeps; ++k) {
-    jacobi_sweep<<<G, kT, 0, c->s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, cur, omega, nxt);
+    jacobi_sweep<<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, cur, omega, nxt);
     std::swap(cur, nxt);
   }
-  residual_f32<<<G, kT, 0, c->s>>>(n, L.w, L.ld, L.col, L.val, b, cur, L.r);
-  restrict_sum<<<grid_for(C.n), kT, 0, c->s>>>(C.n, C.mptr, n, C.mem, L.r, C.b);
+  residual_f32<<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, b, cur, L.r);
+  restrict_sum<<<grid_for(C.n), kT, 0, s>>>(C.n, C.mptr, n, C.mem, L.r, C.b);
   apc_count_launch(c, sweeps + 2);
-  vcycle(c, l + 1, C.b, C.x);
-  prolong_add<<<G, kT, 0, c->s>>>(n, L.agg, C.x, alpha, cur);
-  apc_count_launch(c);
+  vcycle(c, s, l + 1, C.b, C.x);
+  // the correction goes to the buffer from which the post-smoothing sweeps, alternating,
+  // end in x
+  float *other = L.x2;
+  float *p = (sweeps % 2 == 0) ? x : other;
+  prolong_add<<<G, kT, 0, s>>>(n, L.agg, C.x, alpha, cur, p);
+  cur = p;
+  nxt = (p == x) ? other : x;
   for (int k = 0; k < sweeps; ++k) {
-    jacobi_sweep<<<G, kT, 0, c->s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, cur, omega, nxt);
+    jacobi_sweep<<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, cur, omega, nxt);
     std::swap(cur, nxt);
   }
-  apc_count_launch(c, sweeps);
-  if (cur != x) {
-    cudaMemcpyAsync(x, cur, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->s);
-  }
+  apc_count_launch(c, sweeps + 1);
 }
 
-// Capture the V-cycle of the freshly built hierarchy (fixed buffers vin -> vout).
-static int capture_vcycle(apc_context *c) {
+// Add a conditional WHILE node after the current capture dependencies of stream s and
+// make it the new dependency; *body receives the node's body graph.
+static cudaError_t add_while(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraph_t *body) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd);
+  if (e != cudaSuccess) return e;
+  if (st != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureInvalidated;
+  cudaGraphNodeParams p{};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  e = cudaGraphAddNode(&node, g, deps, nd, &p);
+  if (e != cudaSuccess) return e;
+  *body = p.conditional.phGraph_out[0];
+  return cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+}
+
+struct IrSolveArgs {
+  int which;               // 0 density, 1 potential
+  bool mg;                 // V-cycle preconditioner (else none: GMRES on the scaled system)
+  int n, w;
+  size_t ld;
+  const int *col;          // ELL columns shared by both operators
+  const float *valf;       // Jacobi-scaled FP32 operator D^-1 A
+  const double *val, *b;   // FP64 operator (diagonal in slot 0) and rhs
+  double *x, *r;           // solution, FP64 residual
+  double rtol, atol, dtol, rtol_in;
+  int max_it, max_outer, M;
+};
+
+// Capture one mixed solve:
+//   init; residual (sets cond_outer)
+//   while (cond_outer) {                       -- FP64 iterative refinement
+//     v0 = D^-1 r / ||D^-1 r|| (sets cond_inner); normalise v0
+//     while (cond_inner) {                     -- FP32 (F)GMRES cycle, right preconditioned
+//       z = V-cycle(v_it) or v_it; v_it+1 = A z; CGS; Arnoldi scalars (sets cond_inner);
+//       normalise
+//     }
+//     y = H^-1 g; d = Z y; x += ||D^-1 r|| d; residual (sets cond_outer)
+//   }
+// Both loops end by counters the kernels advance: at most max_outer corrections, M
+// iterations per cycle, max_it iterations in all.
+static int capture_solve(apc_context *c, const IrSolveArgs &a) {
   MgWork *m = c->mg;
-  if (m->graph_exec) {
-    cudaGraphExecDestroy(m->graph_exec);
-    m->graph_exec = nullptr;
+  const int n = a.n, slot = a.which;
+  const size_t vn = m->vn;
+  const int G = std::min(kRedBlocks, grid_for(n));
+  const int Gs = grid_for(n, 1184);
+  const bool reorth = c->cfg.mg_reorth != 0;
+  double *h1 = m->dots, *h2 = m->dots + 34, *nr = m->dots + 68, *tmp = m->dots + 70;
+  float *Z = a.mg ? m->Z : nullptr;
+  float *vin = a.mg ? m->vin : nullptr;
+  if (m->solve_exec[slot]) {
+    cudaGraphExecDestroy(m->solve_exec[slot]);
+    m->solve_exec[slot] = nullptr;
   }
-  if (m->graph) {
-    cudaGraphDestroy(m->graph);
-    m->graph = nullptr;
+  if (m->solve_graph[slot]) {
+    cudaGraphDestroy(m->solve_graph[slot]);
+    m->solve_graph[slot] = nullptr;
   }
   const int64_t l0 = c->launches;
-  APC_CUDA_TRY(c, cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal));
-  vcycle(c, 0, m->vin, m->vout);
-  cudaError_t e = cudaStreamEndCapture(c->s, &m->graph);
-  m->graph_nodes = c->launches - l0;
-  c->launches = l0;
+  cudaStream_t s = c->s, s1 = m->cap[0], s2 = m->cap[1];
+  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) {
-    c->err = std::string("V-cycle capture: ") + cudaGetErrorString(e);
-    cudaGetLastError();
+    c->err = std::string("solve capture: ") + cudaGetErrorString(e);
     return APC_ERR_CUDA;
   }
-  APC_CUDA_TRY(c, cudaGraphInstantiate(&m->graph_exec, m->graph, 0));
+  auto ok = [&](cudaError_t r) {
+    if (e == cudaSuccess && r != cudaSuccess) e = r;
+    return e == cudaSuccess;
+  };
+  cudaStreamCaptureStatus st;
+  cudaGraph_t top = nullptr, body_out = nullptr, body_in = nullptr;
+  cudaGraphConditionalHandle cond_out = 0, cond_in = 0;
+  bool cap1 = false, cap2 = false;
+  if (ok(cudaStreamGetCaptureInfo(s, &st, nullptr, &top, nullptr, nullptr)) &&
+      ok(cudaGraphConditionalHandleCreate(&cond_out, top, 0, 0))) {
+    ir_init<<<1, 1, 0, s>>>(m->state, a.rtol, a.atol, a.dtol, a.rtol_in, a.max_it, a.max_outer, a.M);
+    ir_residual<<<G, kT, 0, s>>>(n, a.w, a.ld, a.col, a.val, a.b, a.x, a.r, m->state, m->partial, m->counter, tmp,
+                                 cond_out);
+    if (ok(cudaGetLastError()) && ok(add_while(s, cond_out, &body_out)) &&
+        ok(cudaStreamBeginCaptureToGraph(s1, body_out, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal))) {
+      cap1 = true;
+      if (ok(cudaGraphConditionalHandleCreate(&cond_in, body_out, 0, 0))) {
+        ir_to_f32<<<G, kT, 0, s1>>>(n, a.r, a.val, m->state, m->V, m->partial, m->counter, tmp, cond_in);
+        scale_next<<<Gs, kT, 0, s1>>>(n, m->state, m->V, vn, vin);
+        if (ok(cudaGetLastError()) && ok(add_while(s1, cond_in, &body_in)) &&
+            ok(cudaStreamBeginCaptureToGraph(s2, body_in, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal))) {
+          cap2 = true;
+          const int64_t v0 = c->launches;
+          if (a.mg) vcycle(c, s2, 0, m->vin, m->vout);
+          m->vcycle_nodes[slot] = c->launches - v0;
+          spmv_dots<<<G, kT, 0, s2>>>(n, a.w, a.ld, a.col, a.valf, a.mg ? m->vout : nullptr, Z, m->V, vn, m->state,
+                                      m->partial, m->counter, h1);
+          if (reorth) {
+            cgs_pass<1><<<G, kT, 0, s2>>>(n, m->state, m->V, vn, h1, m->partial, m->counter, h2);
+            cgs_pass<2><<<G, kT, 0, s2>>>(n, m->state, m->V, vn, h2, m->partial, m->counter, nr);
+            arnoldi<true><<<1, 32, 0, s2>>>(m->state, h1, h2, nr, cond_in);
+          } else {
+            cgs_pass<2><<<G, kT, 0, s2>>>(n, m->state, m->V, vn, h1, m->partial, m->counter, nr);
+            arnoldi<false><<<1, 32, 0, s2>>>(m->state, h1, h2, nr, cond_in);
+          }
+          scale_next<<<Gs, kT, 0, s2>>>(n, m->state, m->V, vn, vin);
+          ok(cudaGetLastError());
+        }
+        if (cap2) {
+          cudaGraph_t g2 = nullptr;
+          ok(cudaStreamEndCapture(s2, &g2));
+        }
+        fg_finish<<<1, 32, 0, s1>>>(m->state);
+        combine<<<Gs, kT, 0, s1>>>(n, a.mg ? m->Z : m->V, vn, m->state, m->dvec);
+        ir_axpy<<<Gs, kT, 0, s1>>>(n, m->state, m->dvec, a.x);
+        ir_residual<<<G, kT, 0, s1>>>(n, a.w, a.ld, a.col, a.val, a.b, a.x, a.r, m->state, m->partial, m->counter,
+                                      tmp, cond_out);
+        ok(cudaGetLastError());
+      }
+    }
+    if (cap1) {
+      cudaGraph_t g1 = nullptr;
+      ok(cudaStreamEndCapture(s1, &g1));
+    }
+  }
+  cudaGraph_t g = nullptr;
+  ok(cudaStreamEndCapture(s, &g));
+  c->launches = l0;
+  if (e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    c->err = std::string("solve capture: ") + cudaGetErrorString(e);
+    return APC_ERR_CUDA;
+  }
+  m->solve_graph[slot] = g;
+  APC_CUDA_TRY(c, cudaGraphInstantiate(&m->solve_exec[slot], g, 0));
   return APC_OK;
 }
 
-// FP32 FGMRES(m) with the V-cycle as right preconditioner: solve A d = r to rtol_in.
-// r is Jacobi-scaled to unit norm by the caller.
-int apc_mg_fgmres(apc_context *c, bool rebuild, const float *r, float *d, int restart, double rtol_in, int max_it,
-                  int *its, int *levels) {
+// One solve of the mixed path: FP64 iterative refinement on the true Jacobi-
+// preconditioned residual, each correction an FP32 (F)GMRES cycle on the Jacobi-scaled
+// system.  For the potential with the multigrid option, builds the hierarchy over the
+// current operator and right-preconditions with its V-cycle.  The solve is captured as
+// one graph and run; the host reads the outcome once.
+int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, const float *valf, const double *b,
+                 double *x, double *r, int restart, double rtol_in, int *its, double *rnorm, int *reason,
+                 int *refinements, int *levels) {
   MgWork *m = mg(c);
   const int n = c->nc + c->nv;
   const size_t vn = ((size_t)n + 31) & ~(size_t)31;
-  const int M = std::max(1, std::min(restart, 31));
+  const int M = std::max(1, std::min(restart, kMaxM));
   APC_TRY(apc_ensure(c, &m->V, vn * (M + 1)));
-  APC_TRY(apc_ensure(c, &m->Z, vn * M));
-  APC_TRY(apc_ensure(c, &m->vin, vn));
-  APC_TRY(apc_ensure(c, &m->vout, vn));
+  if (use_mg) {
+    APC_TRY(apc_ensure(c, &m->Z, vn * M));
+    APC_TRY(apc_ensure(c, &m->vin, vn));
+    APC_TRY(apc_ensure(c, &m->vout, vn));
+  }
+  APC_TRY(apc_ensure(c, &m->dvec, vn));
   APC_TRY(apc_ensure(c, &m->partial, (size_t)kRedBlocks * 34));
   APC_TRY(apc_ensure(c, &m->dots, (size_t)4 * 34));
+  m->vn = vn;
   if (!m->counter) {
     APC_TRY(apc_alloc(c, (void **)&m->counter, 4 * sizeof(unsigned)));
     APC_CUDA_TRY(c, cudaMemsetAsync(m->counter, 0, 4 * sizeof(unsigned), c->s));
   }
-  if (!m->host) APC_CUDA_TRY(c, cudaMallocHost((void **)&m->host, sizeof(double) * 4 * 34));
-  if (rebuild || m->nlev == 0 || !m->graph_exec) {
+  if (!m->state) APC_TRY(apc_alloc(c, (void **)&m->state, sizeof(IrState)));
+  if (!m->host) APC_CUDA_TRY(c, cudaMallocHost((void **)&m->host, sizeof(IrState)));
+  for (int k = 0; k < 2; ++k)
+    if (!m->cap[k]) APC_CUDA_TRY(c, cudaStreamCreateWithFlags(&m->cap[k], cudaStreamNonBlocking));
+  const apc_config &cfg = c->cfg;
+  const auto t0 = std::chrono::steady_clock::now();
+  if (use_mg) {
     APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
-    const auto t0 = std::chrono::steady_clock::now();
     APC_TRY(mg_build(c));
-    APC_TRY(capture_vcycle(c));
-    APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  }
+  IrSolveArgs a{};
+  a.which = which;
+  a.mg = use_mg;
+  a.n = n;
+  a.w = c->ell_w;
+  a.ld = (size_t)c->m_cap;
+  a.col = c->ell_col;
+  a.valf = valf;
+  a.val = val;
+  a.b = b;
+  a.x = x;
+  a.r = r;
+  a.rtol = cfg.gmres_rtol;
+  a.atol = cfg.gmres_atol;
+  a.dtol = cfg.gmres_dtol;
+  a.rtol_in = rtol_in;
+  a.max_it = cfg.gmres_max_it;
+  // the multigrid corrections gain ~5 digits each; without a preconditioner a correction
+  // may gain little, and max_it bounds the loop
+  a.max_outer = use_mg ? 40 : std::max(40, cfg.gmres_max_it);
+  a.M = M;
+  APC_TRY(capture_solve(c, a));
+  if (use_mg)
     c->prof.mg_build_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-  }
-  const auto ts = std::chrono::steady_clock::now();
-  *levels = m->nlev;
-  MgLevel &L0 = m->lv[0];
-  const bool reorth = c->cfg.mg_reorth != 0;
-  const int G = std::min(kRedBlocks, grid_for(n));
-  const int Gs = grid_for(n, 1184);
-  double *h1 = m->dots, *h2 = m->dots + 34, *nr = m->dots + 68;
-  // beta = ||r||, v0 = r / beta
-  cgs_pass<0><<<G, kT, 0, c->s>>>(n, 1, r, vn, const_cast<float *>(r), nullptr, m->partial, m->counter, nr);
-  apc_count_launch(c);
-  APC_CUDA_TRY(c, cudaMemcpyAsync(m->host, nr, sizeof(double), cudaMemcpyDeviceToHost, c->s));
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
-  const double beta = std::sqrt(m->host[0]);
-  *its = 0;
-  if (beta == 0.0) {
-    APC_CUDA_TRY(c, cudaMemsetAsync(d, 0, sizeof(float) * n, c->s));
-    return APC_OK;
-  }
-  scale2<<<Gs, kT, 0, c->s>>>(n, r, (float)(1.0 / beta), m->V, m->vin);
-  apc_count_launch(c);
-  std::vector<double> H((size_t)(M + 1) * M, 0.0), cs(M), sn(M), g(M + 1, 0.0);
-  g[0] = beta;
-  int it = 0;
-  for (; it < M && it < max_it; ++it) {
-    float *zk = m->Z + (size_t)it * vn, *w = m->V + (size_t)(it + 1) * vn;
-    APC_CUDA_TRY(c, cudaGraphLaunch(m->graph_exec, c->s));  // vout = V-cycle(vin)
-    apc_count_launch(c, (int)m->graph_nodes);
-    spmv_dots<<<G, kT, 0, c->s>>>(n, L0.w, L0.ld, L0.col, L0.val, m->vout, zk, w, it + 1, m->V, vn, m->partial,
-                                  m->counter, h1);
-    if (reorth) {
-      cgs_pass<1><<<G, kT, 0, c->s>>>(n, it + 1, m->V, vn, w, h1, m->partial, m->counter, h2);
-      cgs_pass<2><<<G, kT, 0, c->s>>>(n, it + 1, m->V, vn, w, h2, m->partial, m->counter, nr);
-    } else {
-      cgs_pass<2><<<G, kT, 0, c->s>>>(n, it + 1, m->V, vn, w, h1, m->partial, m->counter, nr);
-    }
-    apc_count_launch(c, reorth ? 3 : 2);
-    if (!reorth) APC_CUDA_TRY(c, cudaMemsetAsync(h2, 0, sizeof(double) * (it + 1), c->s));
-    APC_CUDA_TRY(c, cudaMemcpyAsync(m->host, m->dots, sizeof(double) * 69, cudaMemcpyDeviceToHost, c->s));
-    APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
-    const double tt = std::sqrt(m->host[68]);
-    double *hc = H.data() + (size_t)it * (M + 1);
-    for (int j = 0; j <= it; ++j) hc[j] = m->host[j] + m->host[34 + j];
-    hc[it + 1] = tt;
-    for (int j = 1; j <= it; ++j) {
-      const double t0 = hc[j - 1];
-      hc[j - 1] = cs[j - 1] * t0 + sn[j - 1] * hc[j];
-      hc[j] = cs[j - 1] * hc[j] - sn[j - 1] * t0;
-    }
-    const double t = std::sqrt(hc[it] * hc[it] + hc[it + 1] * hc[it + 1]);
-    if (t == 0.0) {
-      ++it;
-      break;
-    }
-    cs[it] = hc[it] / t;
-    sn[it] = hc[it + 1] / t;
-    g[it + 1] = -sn[it] * g[it];
-    g[it] = cs[it] * g[it];
-    hc[it] = cs[it] * hc[it] + sn[it] * hc[it + 1];
-    if (std::fabs(g[it + 1]) <= rtol_in * beta || tt == 0.0) {
-      ++it;
-      break;
-    }
-    scale2<<<Gs, kT, 0, c->s>>>(n, w, (float)(1.0 / tt), w, m->vin);
-    apc_count_launch(c);
-  }
-  *its = it;
-  // y = H^-1 g (upper triangular), d = Z y
-  std::vector<double> y(std::max(it, 1), 0.0);
-  for (int k = it - 1; k >= 0; --k) {
-    double sacc = g[k];
-    for (int j = k + 1; j < it; ++j) sacc -= H[(size_t)j * (M + 1) + k] * y[j];
-    const double hkk = H[(size_t)k * (M + 1) + k];
-    y[k] = hkk != 0.0 ? sacc / hkk : 0.0;
-  }
-  for (int j = 0; j < it; ++j) m->host[j] = y[j];
-  APC_CUDA_TRY(c, cudaMemcpyAsync(m->dots, m->host, sizeof(double) * std::max(it, 1), cudaMemcpyHostToDevice, c->s));
-  combine<<<Gs, kT, 0, c->s>>>(n, it, m->Z, vn, m->dots, d);
-  apc_count_launch(c);
+  APC_CUDA_TRY(c, cudaEventRecord(c->kev[0], c->s));
+  APC_CUDA_TRY(c, cudaGraphLaunch(m->solve_exec[which], c->s));
+  APC_CUDA_TRY(c, cudaEventRecord(c->kev[1], c->s));
+  APC_CUDA_TRY(c, cudaMemcpyAsync(m->host, m->state, sizeof(IrState), cudaMemcpyDeviceToHost, c->s));
   APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
   APC_CUDA_TRY(c, cudaGetLastError());
-  c->prof.mg_solve_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ts).count();
-  c->prof.mg_iterations += it;
+  const IrState &S = *reinterpret_cast<const IrState *>(m->host);
+  float ms = 0.f;
+  APC_CUDA_TRY(c, cudaEventElapsedTime(&ms, c->kev[0], c->kev[1]));
+  *its = S.total_its;
+  *rnorm = S.rn;
+  *reason = S.reason;
+  *refinements = S.outer;
+  *levels = use_mg ? m->nlev : 0;
+  const int per_it = (int)m->vcycle_nodes[which] + 4 + (cfg.mg_reorth != 0 ? 1 : 0);
+  apc_count_launch(c, 2 + 6 * S.outer + per_it * S.total_its);
+  if (use_mg) {
+    c->prof.mg_solve_ms += ms;
+    c->prof.mg_iterations += S.total_its;
+  }
   return APC_OK;
 }

@@ -82,8 +82,8 @@ typedef struct apc_config {
   int device;            /* CUDA device ordinal */
   int mixed_precond;     /* APC_PREC_MIXED potential solve: APC_PRECOND_JACOBI or APC_PRECOND_MULTIGRID */
   int mg_sweeps;         /* multigrid: Jacobi sweeps before and after each coarse correction (0 = 2) */
-  double mg_omega;       /* multigrid: Jacobi damping (0 = 0.7) */
-  double mg_alpha;       /* multigrid: coarse-correction scaling (0 = 1.0) */
+  double mg_omega;       /* multigrid: Jacobi damping (0 = 0.95) */
+  double mg_alpha;       /* multigrid: coarse-correction over-scaling (0 = 1.8) */
   int mg_reorth;         /* multigrid FGMRES: 1 = classical Gram-Schmidt twice, 0 = once (default) */
 } apc_config;
 
@@ -191,6 +191,9 @@ typedef struct apc_profile {
   double mg_build_ms;    /* summed time to build multigrid hierarchies (incl. host work) */
   double mg_solve_ms;    /* summed time of the multigrid-preconditioned FGMRES solves */
   int64_t mg_iterations; /* their FGMRES iterations */
+  double assemble_ms;    /* summed device-timeline span of GFD assembly (stencils, matrices, rhs) */
+  double density_ms;     /* ... of the density solve */
+  double potential_ms;   /* ... of the potential solve (incl. hierarchy build and capture) */
 } apc_profile;
 int apc_get_profile(apc_context *ctx, apc_profile *out);
 int apc_reset_profile(apc_context *ctx);
