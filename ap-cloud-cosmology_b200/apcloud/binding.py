@@ -57,7 +57,7 @@ class ApcProfile(C.Structure):
                 ("move_ms", C.c_double), ("steps", C.c_int64), ("step_ms", C.c_double),
                 ("gfd_ms", C.c_double), ("mg_build_ms", C.c_double), ("mg_solve_ms", C.c_double),
                 ("mg_iterations", C.c_int64), ("assemble_ms", C.c_double), ("density_ms", C.c_double),
-                ("potential_ms", C.c_double)]
+                ("potential_ms", C.c_double), ("graph_instantiations", C.c_int64), ("graph_updates", C.c_int64)]
 
 
 class ApcStepParams(C.Structure):

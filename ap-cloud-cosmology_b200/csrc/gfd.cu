@@ -74,12 +74,14 @@ __device__ __forceinline__ double warp_max(double v) {
 
 // apartition / aquickSort (solver.cpp:600-632) with an explicit stack.  Sub-ranges are
 // disjoint, so processing order does not change the result; the smaller side is taken
-// first, which bounds the stack by log2(n).
-__device__ void aquicksort(double *a, int *b, int l, int r) {
+// first, which bounds the stack by log2(n).  Only positions below `limit` are wanted:
+// a sub-range starting at or beyond it only permutes unwanted positions, so it is not
+// entered, and positions below the limit end exactly as in the full sort.
+__device__ void aquicksort(double *a, int *b, int l, int r, int limit) {
   int stack[64];
   int sp = 0;
   for (;;) {
-    if (l >= r) {
+    if (l >= r || l >= limit) {
       if (sp == 0) break;
       r = stack[--sp];
       l = stack[--sp];
@@ -105,6 +107,71 @@ __device__ void aquicksort(double *a, int *b, int l, int r) {
       stack[sp++] = j - 1;
       l = j + 1;
     }
+  }
+}
+
+// position of the (k+1)-th lowest set bit of mask (k < popc(mask)), by binary search
+__device__ __forceinline__ int select_bit(unsigned mask, int k) {
+  int p = 0;
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    const int c = __popc(mask & ((1u << s) - 1u));
+    if (k >= c) {
+      k -= c;
+      mask >>= s;
+      p += s;
+    }
+  }
+  return p;
+}
+
+// aquicksort (solver.cpp:600-632) of n <= 32 (key, idx) pairs held one per lane, lane =
+// position.  Each partition is the reference's: with pivot a[l], the i scan stops at the
+// elements > pivot in (l, r] (g_0 < g_1 < ...), the j scan at the elements <= pivot in
+// [l, r] (s_0 > s_1 > ...); the k-th swap exchanges g_k and s_k while g_k < s_k, and
+// the pivot goes to j = s_0 (no swap) or max(s_K, g_{K-1}) after K swaps.  A warp does
+// one partition in a few ballots and shuffles; sub-ranges are disjoint, so taking the
+// lowest unsorted one first ends in the reference's order, ties included.  Sub-ranges
+// starting at or beyond `limit` are left unsorted.
+__device__ void warp_aquicksort(double &key, int &idx, int n, int limit, int lane) {
+  constexpr unsigned kAll = 0xffffffffu;
+  unsigned U = n >= 32 ? kAll : ((1u << n) - 1u);  // positions not yet final
+  while (U) {
+    const int l = __ffs(U) - 1;
+    if (l >= limit) break;
+    const unsigned run = ~(U >> l);
+    const int len = run ? __ffs(run) - 1 : 32 - l;
+    if (len == 1) {
+      U &= ~(1u << l);
+      continue;
+    }
+    const int r = l + len - 1;
+    const double pivot = __shfl_sync(kAll, key, l);
+    const bool in = lane >= l && lane <= r;
+    const unsigned gt = __ballot_sync(kAll, in && lane > l && key > pivot);
+    const unsigned le = __ballot_sync(kAll, in && key <= pivot);
+    const int nle = __popc(le);
+    int partner = -1;
+    if ((gt >> lane) & 1u) {
+      const int k = __popc(gt & ((1u << lane) - 1u));
+      if (k < nle) {
+        const int sk = select_bit(le, nle - 1 - k);
+        if (sk > lane) partner = sk;
+      }
+    }
+    const int K = __popc(__ballot_sync(kAll, partner >= 0));
+    if ((le >> lane) & 1u) {
+      const int k = nle - 1 - __popc(le & ((1u << lane) - 1u));
+      if (k < K) partner = select_bit(gt, k);
+    }
+    const int src = partner >= 0 ? partner : lane;
+    key = __shfl_sync(kAll, key, src);
+    idx = __shfl_sync(kAll, idx, src);
+    const int j = K == 0 ? 31 - __clz(le) : max(select_bit(le, nle - 1 - K), select_bit(gt, K - 1));
+    const int src2 = lane == l ? j : (lane == j ? l : lane);
+    key = __shfl_sync(kAll, key, src2);
+    idx = __shfl_sync(kAll, idx, src2);
+    U &= ~(1u << j);
   }
 }
 
@@ -255,9 +322,39 @@ __global__ void __launch_bounds__(32 * kWarps) gfd_stencil(GfdParams P) {
       if (lane == 0) atomicOr(P.err, DERR_STENCIL_MANY);
       continue;
     }
-    // ---- sorting (solver.cpp:553-569), lane 0 ----
-    if (lane == 0) {
-      aquicksort(S.bd2[0], S.bidx[0], 0, nn[0] - 1);
+    // ---- sorting (solver.cpp:553-569) ----
+    if (l <= 32 && nn[0] <= 32) {
+      // bucket 0, then the penalised list, by the warp-parallel quicksort
+      double key = 0.0;
+      int idx = 0;
+      if (lane < nn[0]) {
+        key = S.bd2[0][lane];
+        idx = S.bidx[0][lane];
+      }
+      warp_aquicksort(key, idx, nn[0], nn[0], lane);
+      if (lane < nn[0]) {
+        S.bd2[0][lane] = key;
+        S.bidx[0][lane] = idx;
+      }
+      __syncwarp();
+      if (lane < l) {
+        int b = 0, e = lane;
+#pragma unroll
+        for (int o = 0; o < 8; ++o) {
+          if (b == o && e >= nn[o]) {
+            e -= nn[o];
+            b = o + 1;
+          }
+        }
+        double penalty = 1.0;
+        for (int t = 0; t < e; ++t) penalty = __dmul_rn(penalty, 10000.0);
+        key = __dmul_rn(penalty, S.bd2[b][e]);
+        idx = S.bidx[b][e];
+      }
+      warp_aquicksort(key, idx, l, lm, lane);
+      if (lane < l) S.lidx[lane] = idx;
+    } else if (lane == 0) {
+      aquicksort(S.bd2[0], S.bidx[0], 0, nn[0] - 1, nn[0]);
       int k = 0;
       for (int b = 0; b < 8; ++b) {
         double penalty = 1.0;
@@ -268,7 +365,7 @@ __global__ void __launch_bounds__(32 * kWarps) gfd_stencil(GfdParams P) {
           ++k;
         }
       }
-      aquicksort(S.ldist, S.lidx, 0, l - 1);
+      aquicksort(S.ldist, S.lidx, 0, l - 1, lm);
     }
     __syncwarp();
     // ---- weights and weighted monomials (solver.cpp:75-103) ----

@@ -83,11 +83,15 @@ __global__ void ell_f32_dinv(int n, size_t ld, const float *__restrict__ val, fl
   }
 }
 
-// Galerkin row I of A_c = P^T A P, one warp per coarse row: the (J, a) contributions of
-// the members' rows are gathered in shared memory, sorted by J with a bitonic network
-// (data-independent, so deterministic), and equal-J runs summed in sorted order.
-constexpr int kGalWarps = 2;
-constexpr int kGalCap = 2048;  // contributions per coarse row
+// Galerkin row I of A_c = P^T A P, one warp per coarse row.  The (J, a) contributions of
+// the members' rows are taken 32 at a time in member-then-slot order; lanes with equal J
+// are merged by their lowest lane, which adds the values in lane order into a shared-
+// memory hash table keyed by J (one writer per J per round, so every coarse entry is
+// summed in contribution order).  The distinct entries are then written sorted by J.
+// The result does not depend on scheduling, so the hierarchy is deterministic.
+constexpr int kGalWarps = 4;
+constexpr int kGalTab = 512;   // hash slots per warp
+constexpr int kGalRows = 256;  // distinct coarse columns per row
 
 __global__ void __launch_bounds__(32 * kGalWarps) galerkin_rows(int nc, const int *__restrict__ mptr, int nf,
                                                               const int *__restrict__ mem, int wf, size_t ldf,
@@ -96,76 +100,79 @@ __global__ void __launch_bounds__(32 * kGalWarps) galerkin_rows(int nc, const in
                                                               const int *__restrict__ agg, int wcap,
                                                               int *__restrict__ rowlen, int *__restrict__ tcol,
                                                               float *__restrict__ tval, int *__restrict__ err) {
-  __shared__ unsigned long long buf[kGalWarps][kGalCap];  // (J << 32) | float bits
+  __shared__ int tkey[kGalWarps][kGalTab];
+  __shared__ double tsum[kGalWarps][kGalTab];
+  __shared__ double stage[kGalWarps][32];
+  __shared__ int dkey[kGalWarps][kGalRows];
+  __shared__ double dval[kGalWarps][kGalRows];
   const int lane = threadIdx.x & 31, wv = threadIdx.x >> 5;
-  unsigned long long *B = buf[wv];
+  int *K = tkey[wv];
+  double *T = tsum[wv];
   for (int I = blockIdx.x * kGalWarps + wv; I < nc; I += gridDim.x * kGalWarps) {
     const int a = mptr[I], e = (I + 1 < nc) ? mptr[I + 1] : nf;
     const int cnt = (e - a) * wf;
-    if (cnt > kGalCap) {
-      if (lane == 0) atomicOr(err, DERR_STENCIL_MANY);
-      continue;
-    }
-    int P = 1;
-    while (P < cnt) P <<= 1;
-    for (int t = lane; t < P; t += 32) {
-      unsigned long long v = ~0ull;  // padding sorts last
+    for (int t = lane; t < kGalTab; t += 32) K[t] = -1;
+    __syncwarp();
+    bool bad = false;
+    for (int t0 = 0; t0 < cnt; t0 += 32) {
+      const int t = t0 + lane;
+      int J = -1;
+      double v = 0.0;
       if (t < cnt) {
         const int i = mem[a + t / wf], sl = t % wf;
         const size_t at = (size_t)sl * ldf + i;
-        const unsigned J = (unsigned)agg[colf[at]];
-        v = ((unsigned long long)J << 32) | (unsigned long long)__float_as_uint(valf[at]);
+        J = agg[colf[at]];
+        v = (double)valf[at];
       }
-      B[t] = v;
+      stage[wv][lane] = v;
+      __syncwarp();
+      const unsigned peers = __match_any_sync(0xffffffffu, J);
+      if (J >= 0 && lane == __ffs(peers) - 1) {
+        double sum = 0.0;
+        for (unsigned q = peers; q; q &= q - 1) sum += stage[wv][__ffs(q) - 1];
+        unsigned h = ((unsigned)J * 2654435761u) >> (32 - 9);
+        bool placed = false;
+        for (int probe = 0; probe < kGalTab && !placed; ++probe, h = (h + 1) & (kGalTab - 1)) {
+          const int cur = atomicCAS(&K[h], -1, J);
+          if (cur == -1) {
+            T[h] = sum;
+            placed = true;
+          } else if (cur == J) {
+            T[h] += sum;
+            placed = true;
+          }
+        }
+        if (!placed) bad = true;
+      }
+      __syncwarp();
+    }
+    // compact the occupied slots, then place each by its rank in J
+    int nd = 0;
+    for (int t0 = 0; t0 < kGalTab; t0 += 32) {
+      const int key = K[t0 + lane];
+      const unsigned occ = __ballot_sync(0xffffffffu, key >= 0);
+      const int pos = nd + __popc(occ & ((1u << lane) - 1u));
+      if (key >= 0 && pos < kGalRows) {
+        dkey[wv][pos] = key;
+        dval[wv][pos] = T[t0 + lane];
+      }
+      nd += __popc(occ);
     }
     __syncwarp();
-    for (int k = 2; k <= P; k <<= 1) {
-      for (int j = k >> 1; j > 0; j >>= 1) {
-        for (int t = lane; t < P; t += 32) {
-          const int u = t ^ j;
-          if (u > t) {
-            const unsigned long long x = B[t], y = B[u];
-            const bool up = (t & k) == 0;
-            // order by J only (upper 32 bits), ties by the raw word, so the network is total
-            if ((x > y) == up) {
-              B[t] = y;
-              B[u] = x;
-            }
-          }
-        }
-        __syncwarp();
+    const int len = min(nd, kGalRows);
+    for (int q = lane; q < len; q += 32) {
+      const int key = dkey[wv][q];
+      int rank = 0;
+      for (int u = 0; u < len; ++u) rank += dkey[wv][u] < key ? 1 : 0;
+      if (rank < wcap) {
+        tcol[(size_t)I * wcap + rank] = key;
+        tval[(size_t)I * wcap + rank] = (float)dval[wv][q];
       }
     }
-    // segmented sums in sorted order by lane 0 (rows are short)
+    bad = __any_sync(0xffffffffu, bad);
     if (lane == 0) {
-      int len = 0;
-      int curJ = -1;
-      double acc = 0.0;
-      for (int t = 0; t < cnt; ++t) {
-        const int J = (int)(B[t] >> 32);
-        const float v = __uint_as_float((unsigned)(B[t] & 0xffffffffull));
-        if (J != curJ) {
-          if (curJ >= 0) {
-            if (len < wcap) {
-              tcol[(size_t)I * wcap + len] = curJ;
-              tval[(size_t)I * wcap + len] = (float)acc;
-            }
-            ++len;
-          }
-          curJ = J;
-          acc = 0.0;
-        }
-        acc += (double)v;
-      }
-      if (curJ >= 0) {
-        if (len < wcap) {
-          tcol[(size_t)I * wcap + len] = curJ;
-          tval[(size_t)I * wcap + len] = (float)acc;
-        }
-        ++len;
-      }
-      rowlen[I] = len;
-      if (len > wcap) atomicOr(err, DERR_STENCIL_MANY);
+      rowlen[I] = nd;
+      if (bad || nd > wcap || nd > kGalRows) atomicOr(err, DERR_STENCIL_MANY);
     }
     __syncwarp();
   }
@@ -817,7 +824,13 @@ static int mg_build(apc_context *c) {
     bool alt = false;
     // level 0 is in the reference's cell order; coarser levels are already sorted by
     // code, and so are their parents' codes
-    if (lev == 0) APC_TRY(apc_radix_sort_u64(c, m->pkey, m->pidx, m->pkey_alt, m->pidx_alt, nf, 0, 64, &alt));
+    if (lev == 0) {
+      // parent codes of cells at level <= D have at most 3 D - 2 significant bits; the
+      // deepest cell level is one below the deepest top-down opened level
+      const int deepest = (int)c->td_level_off.size();
+      const int bits = std::min(64, 3 * deepest + 1);
+      APC_TRY(apc_radix_sort_u64(c, m->pkey, m->pidx, m->pkey_alt, m->pidx_alt, nf, 0, bits, &alt));
+    }
     uint64_t *pk = alt ? m->pkey_alt : m->pkey;
     uint32_t *pi = alt ? m->pidx_alt : m->pidx;
     APC_TRY(apc_ensure(c, &m->eflag, (size_t)nf + 1));
@@ -1054,14 +1067,6 @@ static int capture_solve(apc_context *c, const IrSolveArgs &a) {
   double *h1 = m->dots, *h2 = m->dots + 34, *nr = m->dots + 68, *tmp = m->dots + 70;
   float *Z = a.mg ? m->Z : nullptr;
   float *vin = a.mg ? m->vin : nullptr;
-  if (m->solve_exec[slot]) {
-    cudaGraphExecDestroy(m->solve_exec[slot]);
-    m->solve_exec[slot] = nullptr;
-  }
-  if (m->solve_graph[slot]) {
-    cudaGraphDestroy(m->solve_graph[slot]);
-    m->solve_graph[slot] = nullptr;
-  }
   const int64_t l0 = c->launches;
   cudaStream_t s = c->s, s1 = m->cap[0], s2 = m->cap[1];
   cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
@@ -1133,8 +1138,24 @@ static int capture_solve(apc_context *c, const IrSolveArgs &a) {
     c->err = std::string("solve capture: ") + cudaGetErrorString(e);
     return APC_ERR_CUDA;
   }
+  // the graph of the previous step usually differs only in kernel parameters: update
+  // the executable in place, and instantiate only when the topology changed
+  if (m->solve_exec[slot]) {
+    cudaGraphExecUpdateResultInfo info{};
+    if (cudaGraphExecUpdate(m->solve_exec[slot], g, &info) == cudaSuccess) {
+      if (m->solve_graph[slot]) cudaGraphDestroy(m->solve_graph[slot]);
+      m->solve_graph[slot] = g;
+      c->prof.graph_updates += 1;
+      return APC_OK;
+    }
+    cudaGetLastError();
+    cudaGraphExecDestroy(m->solve_exec[slot]);
+    m->solve_exec[slot] = nullptr;
+  }
+  if (m->solve_graph[slot]) cudaGraphDestroy(m->solve_graph[slot]);
   m->solve_graph[slot] = g;
   APC_CUDA_TRY(c, cudaGraphInstantiate(&m->solve_exec[slot], g, 0));
+  c->prof.graph_instantiations += 1;
   return APC_OK;
 }
 

@@ -194,6 +194,8 @@ typedef struct apc_profile {
   double assemble_ms;    /* summed device-timeline span of GFD assembly (stencils, matrices, rhs) */
   double density_ms;     /* ... of the density solve */
   double potential_ms;   /* ... of the potential solve (incl. hierarchy build and capture) */
+  int64_t graph_instantiations;  /* solve graphs instantiated */
+  int64_t graph_updates;         /* solve graphs updated in place from a new capture */
 } apc_profile;
 int apc_get_profile(apc_context *ctx, apc_profile *out);
 int apc_reset_profile(apc_context *ctx);
