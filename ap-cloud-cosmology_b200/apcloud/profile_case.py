@@ -1,39 +1,58 @@
 """A short, fixed workload for kernel profiling under ncu.
 
-    python -m apcloud.profile_case [--max-it N] [--precision fp64|mixed] [--workload lcdm128]
+    python -m apcloud.profile_case [--precision fp64|mixed] [--workload lcdm128]
+                                   [--warm K] [--max-it N]
 
-Runs one Controller step of the named workload with the GMRES iteration cap lowered to
---max-it, so that each GMRES launch is short enough for a multi-pass ncu capture.  The
-density solve is the first GMRES launch of the step and the potential solve the second.
+Runs K unprofiled Controller steps of the named workload, then one more step bracketed
+by cudaProfilerStart / cudaProfilerStop, so that `ncu --profile-from-start off` sees
+exactly one steady-state step.  --max-it lowers the GMRES iteration cap of the FP64
+path, so that each of its GMRES launches is short enough for a multi-pass capture.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import time
 
 from . import binding, ics
 from .controller import for_config
 
 
+def _cudart():
+    for name in ("libcudart.so.12", "libcudart.so"):
+        try:
+            return ctypes.CDLL(name)
+        except OSError:
+            continue
+    return None
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--max-it", type=int, default=200)
-    ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
+    ap.add_argument("--max-it", type=int, default=10000)
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default="mixed")
     ap.add_argument("--workload", default="lcdm128")
+    ap.add_argument("--warm", type=int, default=2)
     args = ap.parse_args()
     cfg = ics.config(args.workload)
     prec = binding.APC_PREC_FP64 if args.precision == "fp64" else binding.APC_PREC_MIXED
     g = binding.GpuPath(cfg.particles(), cfg.depth, cfg.gfd_c, cfg.lm, precision=prec, max_it=args.max_it)
     ctl = for_config(g, cfg)
     ctl.start()
+    for _ in range(args.warm):
+        ctl.step()
+    rt = _cudart()
     g.reset_profile()
+    g.synchronize()
+    if rt is not None:
+        rt.cudaProfilerStart()
     t0 = time.perf_counter()
     rec = ctl.step()
     dt = time.perf_counter() - t0
+    if rt is not None:
+        rt.cudaProfilerStop()
     pr = g.profile()
-    print(f"cells {rec.n_cells} wall {dt * 1e3:.1f} ms  krylov {pr['krylov_ms']:.2f} ms over {pr['krylov_launches']} "
-          f"launches, {pr['krylov_iterations']} iterations, {pr['krylov_bytes'] / 1e9:.3f} GB algorithmic; "
-          f"stats {g.solve_stats()}")
+    print(f"cells {rec.n_cells} wall {dt * 1e3:.1f} ms; stats {g.solve_stats()}")
     print("profile", {k: (round(v, 3) if isinstance(v, float) else v) for k, v in pr.items()})
     g.close()
 
