@@ -20,7 +20,7 @@
 //     Rows sum to zero except the Dirichlet pin's aggregate, so the constant mode is
 //     reproduced exactly on every level.
 //   * Damped Jacobi smoothing on ELL operators, over-scaled coarse corrections; the
-//     levels of <= 512 nodes in one single-block kernel; an explicit dense inverse (FP64,
+//     levels of <= 1024 nodes in one single-block kernel; an explicit dense inverse (FP64,
 //     formed on the host) on the coarsest level of <= 64 nodes.
 //   * Flexible GMRES with classical Gram-Schmidt (optionally a second, re-orthogonalising
 //     sweep), right preconditioned, so the residual it monitors is the true residual of
@@ -216,6 +216,7 @@ __global__ void jacobi_sweep(int n, int w, size_t ld, const int *__restrict__ co
                              const float *__restrict__ xin, float omega, float *__restrict__ xout) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float s = 0.f;
+#pragma unroll 6
     for (int k = 0; k < w; ++k) {
       const size_t at = (size_t)k * ld + i;
       s += val[at] * xin[col[at]];
@@ -224,11 +225,30 @@ __global__ void jacobi_sweep(int n, int w, size_t ld, const int *__restrict__ co
   }
 }
 
+// Two damped Jacobi sweeps from x = 0 in one pass: x1 = omega D^-1 b is formed on the fly
+// at the row and at its neighbours, x2 = x1 + omega D^-1 (b - A x1).
+__global__ void jacobi_first2(int n, int w, size_t ld, const int *__restrict__ col, const float *__restrict__ val,
+                              const float *__restrict__ dinv, const float *__restrict__ b, float omega,
+                              float *__restrict__ xout) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float s = 0.f;
+#pragma unroll 6
+    for (int k = 0; k < w; ++k) {
+      const size_t at = (size_t)k * ld + i;
+      const int j = col[at];
+      s += val[at] * (omega * dinv[j] * b[j]);
+    }
+    const float x1 = omega * dinv[i] * b[i];
+    xout[i] = x1 + omega * dinv[i] * (b[i] - s);
+  }
+}
+
 // r = b - A x, one thread per row
 __global__ void residual_f32(int n, int w, size_t ld, const int *__restrict__ col, const float *__restrict__ val,
                              const float *__restrict__ b, const float *__restrict__ x, float *__restrict__ r) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float s = 0.f;
+#pragma unroll 6
     for (int k = 0; k < w; ++k) {
       const size_t at = (size_t)k * ld + i;
       s += val[at] * x[col[at]];
@@ -248,11 +268,23 @@ __global__ void restrict_sum(int nc, const int *__restrict__ mptr, int nf, const
   }
 }
 
-// out = in + alpha P xc (in place when out == in)
-__global__ void prolong_add(int n, const int *__restrict__ agg, const float *__restrict__ xc, float alpha,
-                            const float *in, float *out) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    out[i] = in[i] + alpha * xc[agg[i]];
+// The first post-smoothing sweep with the coarse correction applied on the fly:
+// y = x + alpha P xc at the row and at its neighbours, out = y + omega D^-1 (b - A y).
+__global__ void prolong_sweep(int n, int w, size_t ld, const int *__restrict__ col, const float *__restrict__ val,
+                              const float *__restrict__ dinv, const float *__restrict__ b,
+                              const float *__restrict__ xin, const int *__restrict__ agg,
+                              const float *__restrict__ xc, float alpha, float omega, float *__restrict__ xout) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float s = 0.f;
+#pragma unroll 6
+    for (int k = 0; k < w; ++k) {
+      const size_t at = (size_t)k * ld + i;
+      const int j = col[at];
+      s += val[at] * (xin[j] + alpha * xc[agg[j]]);
+    }
+    const float y = xin[i] + alpha * xc[agg[i]];
+    xout[i] = y + omega * dinv[i] * (b[i] - s);
+  }
 }
 
 // ------------------------------------------------------------------ FGMRES
@@ -353,14 +385,48 @@ __device__ __forceinline__ void block_partial1(double acc, double *partial) {
   }
 }
 
+// One Arnoldi step's scalar work, by one thread: Hessenberg column (h1 + h2, h2 the
+// re-orthogonalisation pass or null), Givens rotations, residual estimate, and whether
+// the cycle goes on (sets the inner loop's condition).
+__device__ void arnoldi_step(IrState *S, const double *h1, const double *h2, double nr,
+                             cudaGraphConditionalHandle cond) {
+  const int it = S->it, M1 = S->M + 1;
+  const double tt = sqrt(nr);
+  double *hc = S->H + (size_t)it * M1;
+  for (int j = 0; j <= it; ++j) hc[j] = __ldcg(h1 + j) + (h2 ? __ldcg(h2 + j) : 0.0);
+  hc[it + 1] = tt;
+  for (int j = 1; j <= it; ++j) {
+    const double t0 = hc[j - 1];
+    hc[j - 1] = S->cs[j - 1] * t0 + S->sn[j - 1] * hc[j];
+    hc[j] = S->cs[j - 1] * hc[j] - S->sn[j - 1] * t0;
+  }
+  const double t = sqrt(hc[it] * hc[it] + hc[it + 1] * hc[it + 1]);
+  bool more = false;
+  if (t != 0.0 && t == t) {
+    const double cs = hc[it] / t, sn = hc[it + 1] / t;
+    S->cs[it] = cs;
+    S->sn[it] = sn;
+    S->g[it + 1] = -sn * S->g[it];
+    S->g[it] = cs * S->g[it];
+    hc[it] = cs * hc[it] + sn * hc[it + 1];
+    more = !(fabs(S->g[it + 1]) <= S->rtol_in * S->beta) && tt != 0.0;
+  }
+  S->it = it + 1;
+  more = more && S->it < S->inner_max;
+  S->scale = tt > 0.0 ? 1.0 / tt : 0.0;
+  cudaGraphSetConditional(cond, more ? 1u : 0u);
+}
+
 // Basis vectors V_0..V_it are rows of V (stride vn); the vector being orthogonalised is
 // V_{it+1}, with it read from the state.  Each warp takes tiles of 32 consecutive rows
 // (one per lane); a row's basis values stay in registers for the update and the dots.
 //   MODE 1: w -= V h_in; h = V^T w.   MODE 2: w -= V h_in; out[0] = ||w||^2.
+// MODE 2 also finishes the Arnoldi step in its last block (h1, h2 as arnoldi_step).
 template <int MODE>
-__global__ void __launch_bounds__(kT) cgs_pass(int n, const IrState *__restrict__ S, float *V, size_t vn,
+__global__ void __launch_bounds__(kT) cgs_pass(int n, IrState *S, float *V, size_t vn,
                                                 const double *__restrict__ h_in, double *partial, unsigned *counter,
-                                                double *out) {
+                                                double *out, const double *h1, const double *h2,
+                                                cudaGraphConditionalHandle cond) {
   __shared__ double hsh[32];
   const int nv = S->it + 1;
   float *w = V + (size_t)nv * vn;
@@ -403,7 +469,11 @@ __global__ void __launch_bounds__(kT) cgs_pass(int n, const IrState *__restrict_
     if (last_block_arrived(counter)) finish_sums(nv, partial, counter, out);
   } else {
     block_partial1(acc1, partial);
-    if (last_block_arrived(counter)) finish_sums(1, partial, counter, out);
+    if (last_block_arrived(counter)) {
+      finish_sums(1, partial, counter, out);
+      __syncthreads();
+      if (threadIdx.x == 0) arnoldi_step(S, h1, h2, __ldcg(out), cond);
+    }
   }
 }
 
@@ -452,39 +522,6 @@ __global__ void scale_next(int n, const IrState *__restrict__ S, float *__restri
     v[i] = u;
     if (vin) vin[i] = u;
   }
-}
-
-// One Arnoldi step's scalar work: Hessenberg column, Givens rotations, residual
-// estimate, and whether the cycle goes on (sets the inner loop's condition).
-template <bool REORTH>
-__global__ void arnoldi(IrState *S, const double *__restrict__ h1, const double *__restrict__ h2,
-                        const double *__restrict__ nr, cudaGraphConditionalHandle cond) {
-  if (threadIdx.x != 0) return;
-  const int it = S->it, M1 = S->M + 1;
-  const double tt = sqrt(*nr);
-  double *hc = S->H + (size_t)it * M1;
-  for (int j = 0; j <= it; ++j) hc[j] = h1[j] + (REORTH ? h2[j] : 0.0);
-  hc[it + 1] = tt;
-  for (int j = 1; j <= it; ++j) {
-    const double t0 = hc[j - 1];
-    hc[j - 1] = S->cs[j - 1] * t0 + S->sn[j - 1] * hc[j];
-    hc[j] = S->cs[j - 1] * hc[j] - S->sn[j - 1] * t0;
-  }
-  const double t = sqrt(hc[it] * hc[it] + hc[it + 1] * hc[it + 1]);
-  bool more = false;
-  if (t != 0.0 && t == t) {
-    const double cs = hc[it] / t, sn = hc[it + 1] / t;
-    S->cs[it] = cs;
-    S->sn[it] = sn;
-    S->g[it + 1] = -sn * S->g[it];
-    S->g[it] = cs * S->g[it];
-    hc[it] = cs * hc[it] + sn * hc[it + 1];
-    more = !(fabs(S->g[it + 1]) <= S->rtol_in * S->beta) && tt != 0.0;
-  }
-  S->it = it + 1;
-  more = more && S->it < S->inner_max;
-  S->scale = tt > 0.0 ? 1.0 / tt : 0.0;
-  cudaGraphSetConditional(cond, more ? 1u : 0u);
 }
 
 // y = H^-1 g (upper triangular) for the cycle's iterations
@@ -612,7 +649,7 @@ __global__ void ir_axpy(int n, IrState *S, const float *__restrict__ d, double *
 // ---- the coarse end of the V-cycle in one block: every level with <= kTail nodes,
 //      down (smooth, residual, restrict), the dense coarsest solve, and up (prolong,
 //      smooth), separated by block barriers instead of kernel launches ----
-constexpr int kTail = 512;
+constexpr int kTail = 1024;
 constexpr int kTailLevels = 12;
 
 struct TailLevel {
@@ -986,28 +1023,35 @@ static void vcycle(apc_context *c, cudaStream_t s, int l, const float *b, float 
   }
   MgLevel &C = m->lv[l + 1];
   const int G = grid_for(n);
-  jacobi_first<<<G, kT, 0, s>>>(n, L.dinv, b, omega, x);
-  float *cur = x, *nxt = L.x2;
+  // Buffers alternate between x and L.x2.  The pre-smoothing result is placed so that the
+  // `sweeps` post-smoothing sweeps, each flipping buffers, end in x.
+  float *cur, *nxt;
+  if (sweeps >= 2) {
+    jacobi_first2<<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, omega, x);
+    cur = x;
+    nxt = L.x2;
+    for (int k = 2; k < sweeps; ++k) {
+      jacobi_sweep<<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, cur, omega, nxt);
+      std::swap(cur, nxt);
+    }
+    apc_count_launch(c, sweeps - 1);
+  } else {
+    jacobi_first<<<G, kT, 0, s>>>(n, L.dinv, b, omega, L.x2);
+    cur = L.x2;
+    nxt = x;
+    apc_count_launch(c);
+  }
+  residual_f32<<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, b, cur, L.r);
+  restrict_sum<<<grid_for(C.n), kT, 0, s>>>(C.n, C.mptr, n, C.mem, L.r, C.b);
+  apc_count_launch(c, 2);
+  vcycle(c, s, l + 1, C.b, C.x);
+  prolong_sweep<<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, cur, L.agg, C.x, alpha, omega, nxt);
+  std::swap(cur, nxt);
   for (int k = 1; k < sweeps; ++k) {
     jacobi_sweep<<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, cur, omega, nxt);
     std::swap(cur, nxt);
   }
-  residual_f32<<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, b, cur, L.r);
-  restrict_sum<<<grid_for(C.n), kT, 0, s>>>(C.n, C.mptr, n, C.mem, L.r, C.b);
-  apc_count_launch(c, sweeps + 2);
-  vcycle(c, s, l + 1, C.b, C.x);
-  // the correction goes to the buffer from which the post-smoothing sweeps, alternating,
-  // end in x
-  float *other = L.x2;
-  float *p = (sweeps % 2 == 0) ? x : other;
-  prolong_add<<<G, kT, 0, s>>>(n, L.agg, C.x, alpha, cur, p);
-  cur = p;
-  nxt = (p == x) ? other : x;
-  for (int k = 0; k < sweeps; ++k) {
-    jacobi_sweep<<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, cur, omega, nxt);
-    std::swap(cur, nxt);
-  }
-  apc_count_launch(c, sweeps + 1);
+  apc_count_launch(c, sweeps);
 }
 
 // Add a conditional WHILE node after the current capture dependencies of stream s and
@@ -1102,12 +1146,12 @@ static int capture_solve(apc_context *c, const IrSolveArgs &a) {
           spmv_dots<<<G, kT, 0, s2>>>(n, a.w, a.ld, a.col, a.valf, a.mg ? m->vout : nullptr, Z, m->V, vn, m->state,
                                       m->partial, m->counter, h1);
           if (reorth) {
-            cgs_pass<1><<<G, kT, 0, s2>>>(n, m->state, m->V, vn, h1, m->partial, m->counter, h2);
-            cgs_pass<2><<<G, kT, 0, s2>>>(n, m->state, m->V, vn, h2, m->partial, m->counter, nr);
-            arnoldi<true><<<1, 32, 0, s2>>>(m->state, h1, h2, nr, cond_in);
+            cgs_pass<1><<<G, kT, 0, s2>>>(n, m->state, m->V, vn, h1, m->partial, m->counter, h2, nullptr, nullptr,
+                                          cond_in);
+            cgs_pass<2><<<G, kT, 0, s2>>>(n, m->state, m->V, vn, h2, m->partial, m->counter, nr, h1, h2, cond_in);
           } else {
-            cgs_pass<2><<<G, kT, 0, s2>>>(n, m->state, m->V, vn, h1, m->partial, m->counter, nr);
-            arnoldi<false><<<1, 32, 0, s2>>>(m->state, h1, h2, nr, cond_in);
+            cgs_pass<2><<<G, kT, 0, s2>>>(n, m->state, m->V, vn, h1, m->partial, m->counter, nr, h1, nullptr,
+                                          cond_in);
           }
           scale_next<<<Gs, kT, 0, s2>>>(n, m->state, m->V, vn, vin);
           ok(cudaGetLastError());
@@ -1233,7 +1277,7 @@ int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, cons
   *reason = S.reason;
   *refinements = S.outer;
   *levels = use_mg ? m->nlev : 0;
-  const int per_it = (int)m->vcycle_nodes[which] + 4 + (cfg.mg_reorth != 0 ? 1 : 0);
+  const int per_it = (int)m->vcycle_nodes[which] + 3 + (cfg.mg_reorth != 0 ? 1 : 0);
   apc_count_launch(c, 2 + 6 * S.outer + per_it * S.total_its);
   if (use_mg) {
     c->prof.mg_solve_ms += ms;

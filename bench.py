@@ -283,17 +283,21 @@ def run_ours(args) -> dict:
         dist.barrier()
         tot = 0.0
         t = ctl.t
+        per_step = []
         for _ in range(args.steps):
             k = ctl.constants(t, cfg.delta_a)
             t0 = time.perf_counter()
             mx._check(lib.apc_set_particles(mx.h, *[a.ctypes.data for a in pin[:6]]), "apc_set_particles")
             mx.step(cfg.delta_a, k["c_dens"], k["c_pot"], k["c_field"], k["c_vel"], k["c_pos"])
             mx._check(lib.apc_get_particles(mx.h, *[a.ctypes.data for a in pin]), "apc_get_particles")
-            tot += time.perf_counter() - t0
+            dt = time.perf_counter() - t0
+            per_step.append(round(dt * 1e3, 2))
+            tot += dt
             t += cfg.delta_a
         tot = dist.max(tot)
         e2e = {"value": ws * cfg.n * args.steps / tot, "unit": UNIT, "h2d_bytes_per_step": 6 * 8 * cfg.n,
-               "d2h_bytes_per_step": 9 * 8 * cfg.n, "timing": "host wall clock per step, max over ranks"}
+               "d2h_bytes_per_step": 9 * 8 * cfg.n, "timing": "host wall clock per step, max over ranks",
+               "ms_per_step": per_step}
 
     peak, peak_kind = measured_peaks()
     # ---- roofline of the dominant kernel: gfd_stencil, one launch per step over the M
