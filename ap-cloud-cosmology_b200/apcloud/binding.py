@@ -27,6 +27,7 @@ EXPORTED = [
     "apc_get_cell_counts", "apc_get_cells", "apc_get_cell_codes", "apc_get_keys", "apc_get_octree_levels",
     "apc_get_fields", "apc_get_stencils", "apc_get_solve_stats", "apc_get_matrix", "apc_kernel_launches",
     "apc_get_phase_times", "apc_get_profile", "apc_reset_profile", "apc_move_velocity_noalloc",
+    "apc_batch_create", "apc_batch_destroy", "apc_batch_size", "apc_batch_context", "apc_batch_step",
 ]
 
 
@@ -114,6 +115,11 @@ def load_library(path: str = LIB_PATH):
         "apc_reset_profile": (C.c_int, [vp]),
         "apc_move_velocity_noalloc": (C.c_int, [C.c_int, C.c_int] + [vp] * 15 + [C.c_double, C.c_double,
                                                                                   C.POINTER(C.c_double), vp]),
+        "apc_batch_create": (C.c_int, [C.POINTER(ApcConfig), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+        "apc_batch_destroy": (C.c_int, [vp]),
+        "apc_batch_size": (C.c_int, [vp]),
+        "apc_batch_context": (C.c_void_p, [vp, C.c_int]),
+        "apc_batch_step": (C.c_int, [vp, C.POINTER(ApcStepParams), ip, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -155,41 +161,49 @@ class GpuFields:
     deriv: np.ndarray
 
 
+def make_config(n: int, depth: int, gfd_c: float, lm: int = 17,
+                box=(0.0, 1.0, 0.0, 1.0, 0.0, 1.0), bc: int = 1, precision: int = APC_PREC_FP64,
+                restart: int = 30, rtol: float = 1e-10, atol: float = 1e-50, dtol: float = 1e5,
+                max_it: int = 10000, mixed_restart: int = 0, mixed_inner_rtol: float = 0.0,
+                device: int = 0, maxnc: int = 10000, nmax_cap: int = 0, precond: int = APC_PRECOND_MULTIGRID,
+                mg_sweeps: int = 0, mg_omega: float = 0.0, mg_alpha: float = 0.0, mg_reorth: int = 0) -> "ApcConfig":
+    """An apc_config: the library defaults with the given fields set."""
+    lib = load_library()
+    cfg = ApcConfig()
+    lib.apc_config_default(C.byref(cfg))
+    cfg.n_particles = n
+    cfg.depth = depth
+    cfg.bc = bc
+    for k in range(6):
+        cfg.box[k] = box[k]
+    cfg.gfd_c = gfd_c
+    cfg.lm = lm
+    cfg.maxnc = maxnc
+    cfg.nmax_cap = nmax_cap
+    cfg.gmres_restart = restart
+    cfg.gmres_rtol = rtol
+    cfg.gmres_atol = atol
+    cfg.gmres_dtol = dtol
+    cfg.gmres_max_it = max_it
+    cfg.precision = precision
+    cfg.mixed_restart = mixed_restart
+    cfg.mixed_inner_rtol = mixed_inner_rtol
+    cfg.device = device
+    cfg.mixed_precond = precond
+    cfg.mg_sweeps = mg_sweeps
+    cfg.mg_omega = mg_omega
+    cfg.mg_alpha = mg_alpha
+    cfg.mg_reorth = mg_reorth
+    return cfg
+
+
 class GpuPath:
     """One particle set resident on the GPU, driven phase by phase through the C ABI."""
 
-    def __init__(self, parts, depth: int, gfd_c: float, lm: int = 17,
-                 box=(0.0, 1.0, 0.0, 1.0, 0.0, 1.0), bc: int = 1, precision: int = APC_PREC_FP64,
-                 restart: int = 30, rtol: float = 1e-10, atol: float = 1e-50, dtol: float = 1e5,
-                 max_it: int = 10000, mixed_restart: int = 0, mixed_inner_rtol: float = 0.0,
-                 device: int = 0, maxnc: int = 10000, nmax_cap: int = 0, precond: int = APC_PRECOND_MULTIGRID,
-                 mg_sweeps: int = 0, mg_omega: float = 0.0, mg_alpha: float = 0.0, mg_reorth: int = 0):
+    def __init__(self, parts, depth: int, gfd_c: float, lm: int = 17, **kw):
         self.lib = load_library()
-        cfg = ApcConfig()
-        self.lib.apc_config_default(C.byref(cfg))
-        cfg.n_particles = parts.n
-        cfg.depth = depth
-        cfg.bc = bc
-        for k in range(6):
-            cfg.box[k] = box[k]
-        cfg.gfd_c = gfd_c
-        cfg.lm = lm
-        cfg.maxnc = maxnc
-        cfg.nmax_cap = nmax_cap
-        cfg.gmres_restart = restart
-        cfg.gmres_rtol = rtol
-        cfg.gmres_atol = atol
-        cfg.gmres_dtol = dtol
-        cfg.gmres_max_it = max_it
-        cfg.precision = precision
-        cfg.mixed_restart = mixed_restart
-        cfg.mixed_inner_rtol = mixed_inner_rtol
-        cfg.device = device
-        cfg.mixed_precond = precond
-        cfg.mg_sweeps = mg_sweeps
-        cfg.mg_omega = mg_omega
-        cfg.mg_alpha = mg_alpha
-        cfg.mg_reorth = mg_reorth
+        cfg = make_config(parts.n, depth, gfd_c, lm, **kw)
+        self._owned = True
         self.cfg = cfg
         self.n = parts.n
         self.depth = depth
@@ -209,9 +223,18 @@ class GpuPath:
                     msg += "; " + detail
             raise ApcError(rc, where, msg)
 
+    @classmethod
+    def view(cls, lib, h, cfg: "ApcConfig") -> "GpuPath":
+        """A GpuPath over a context owned elsewhere (a batch box); close() leaves it alone."""
+        g = cls.__new__(cls)
+        g.lib, g.h, g.cfg, g._owned = lib, h, cfg, False
+        g.n, g.depth, g.lm = cfg.n_particles, cfg.depth, cfg.lm
+        return g
+
     def close(self):
         if getattr(self, "h", None):
-            self.lib.apc_destroy(self.h)
+            if getattr(self, "_owned", True):
+                self.lib.apc_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -334,3 +357,55 @@ class GpuPath:
         a, b, c = C.c_double(), C.c_double(), C.c_double()
         self._check(self.lib.apc_get_phase_times(self.h, C.byref(a), C.byref(b), C.byref(c)), "apc_get_phase_times")
         return a.value, b.value, c.value
+
+
+class BatchPath:
+    """Independent boxes stepped together through apc_batch_step (one context each)."""
+
+    def __init__(self, boxes, n_workers: int = 0):
+        """boxes: sequence of (Particles, dict of make_config keywords incl. depth, gfd_c)."""
+        self.lib = load_library()
+        n = len(boxes)
+        cfgs = (ApcConfig * n)()
+        for i, (parts, kw) in enumerate(boxes):
+            kw = dict(kw)
+            cfgs[i] = make_config(parts.n, kw.pop("depth"), kw.pop("gfd_c"), **kw)
+        h = C.c_void_p()
+        rc = self.lib.apc_batch_create(cfgs, n, n_workers, C.byref(h))
+        if rc != 0:
+            raise ApcError(rc, "apc_batch_create", self.lib.apc_status_string(rc).decode())
+        self.h = h
+        self.cfgs = cfgs
+        self.boxes = [GpuPath.view(self.lib, C.c_void_p(self.lib.apc_batch_context(h, i)), cfgs[i]) for i in range(n)]
+        for g, (parts, _) in zip(self.boxes, boxes):
+            arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in parts.as_tuple()]
+            g._check(self.lib.apc_set_particles(g.h, *[_ptr(a) for a in arrs]), "apc_set_particles")
+
+    def __len__(self) -> int:
+        return len(self.boxes)
+
+    def step(self, params):
+        """params: one (dt, c_dens, c_pot, c_field, c_vel, c_pos) per box."""
+        n = len(self.boxes)
+        p = (ApcStepParams * n)(*[ApcStepParams(*q) for q in params])
+        st = (C.c_int * n)()
+        dv = np.zeros(n)
+        dx = np.zeros(n)
+        rc = self.lib.apc_batch_step(self.h, p, st, _ptr(dv), _ptr(dx))
+        if rc != 0:
+            bad = [i for i in range(n) if st[i] != 0]
+            raise ApcError(rc, "apc_batch_step", f"boxes {bad}: " + self.lib.apc_status_string(rc).decode())
+        return dv, dx
+
+    def close(self):
+        if getattr(self, "h", None):
+            for g in self.boxes:
+                g.h = None
+            self.lib.apc_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -167,3 +167,53 @@ def config(name: str, **over) -> RunConfig:
     }[name]
     base.update(over)
     return RunConfig(name=name, **base)
+
+
+# ---------------------------------------------------------------- batched boxes
+
+BATCH_SIDES = (16, 24, 32, 48, 64)
+
+
+def batch_boxes(n_boxes: int = 96, seed: int = 2024, a_start: float = 0.05, a_end: float = 0.5,
+                steps: int = 32, sides=BATCH_SIDES) -> list:
+    """Independent periodic EdS boxes of uneven size, each with its own seed.
+
+    Particle counts are drawn uniformly from sides^3.  Even-numbered boxes are cold
+    uniform-ball collapses (radius uniform in [0.15, 0.35], zero velocity); odd ones
+    are Zel'dovich lattices with P(k) ~ k^-2 and rms displacement uniform in [0.1, 0.3]
+    spacings at a_start.  Refinement constants follow c = cap^(5/3) rho^(-2/3) with a
+    cap of 8 particles per cell (rho the mean density inside the ball, or N for a
+    lattice box, scaled by 1.28 as for the 64^3 box)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for b in range(n_boxes):
+        side = int(rng.choice(sides))
+        n = side ** 3
+        box_seed = int(rng.integers(1, 2 ** 31 - 1))
+        if b % 2 == 0:
+            radius = float(rng.uniform(0.15, 0.35))
+            rho = n / (4.0 / 3.0 * math.pi * radius ** 3)
+            out.append(RunConfig(name=f"box{b}-ball{side}", kind="ball", n=n, depth=21,
+                                 gfd_c=8.0 ** (5.0 / 3.0) * rho ** (-2.0 / 3.0), omega0=1.0, omegal=0.0,
+                                 a_start=a_start, a_end=a_end, steps=steps, seed=box_seed, radius=radius))
+        else:
+            rms = float(rng.uniform(0.1, 0.3))
+            out.append(RunConfig(name=f"box{b}-zel{side}", kind="zeldovich", n=n, depth=21,
+                                 gfd_c=1.28 * 8.0 ** (5.0 / 3.0) * n ** (-2.0 / 3.0), omega0=1.0, omegal=0.0,
+                                 a_start=a_start, a_end=a_end, steps=steps, seed=box_seed,
+                                 spectral_index=-2.0, rms_spacing=rms))
+    return out
+
+
+def lpt_partition(costs, parts: int) -> list:
+    """Longest-processing-time assignment of items to `parts` bins: items by decreasing
+    cost (ties by index), each to the currently lightest bin (ties by bin index).
+    Deterministic, so every rank computes the same assignment."""
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * parts
+    bins = [[] for _ in range(parts)]
+    for i in order:
+        k = min(range(parts), key=lambda j: (load[j], j))
+        bins[k].append(i)
+        load[k] += costs[i]
+    return [sorted(b) for b in bins]

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/apcloud_gpu.h"
@@ -45,6 +46,9 @@ struct MgWork;      // mg.cu
 struct apc_context {
   apc_config cfg{};
   int dev = 0;
+  // capacity (elements) of every buffer grown by apc_ensure, keyed by the address of the
+  // owning pointer; per context, so contexts can be driven from different host threads
+  std::unordered_map<const void *, size_t> caps;
   cudaStream_t s = nullptr;
   std::string err;
   int64_t launches = 0;

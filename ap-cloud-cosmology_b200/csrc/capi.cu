@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <unordered_map>
@@ -11,13 +12,6 @@
 #include "apc_internal.cuh"
 
 // --------------------------------------------------------------- allocation
-
-namespace {
-struct CapTable {
-  std::unordered_map<const void *, size_t> cap;  // keyed by the address of the owning pointer
-};
-std::unordered_map<const apc_context *, CapTable> g_caps;
-}  // namespace
 
 int apc_alloc(apc_context *c, void **p, size_t bytes) {
   *p = nullptr;
@@ -32,8 +26,7 @@ int apc_alloc(apc_context *c, void **p, size_t bytes) {
 
 template <class T>
 int apc_ensure(apc_context *c, T **p, size_t count, size_t *) {
-  CapTable &ct = g_caps[c];
-  size_t &cap = ct.cap[(const void *)p];
+  size_t &cap = c->caps[(const void *)p];
   if (*p && cap >= count) return APC_OK;
   if (*p) {
     cudaStreamSynchronize(c->s);
@@ -59,13 +52,16 @@ int apc_read_errors(apc_context *c, int *flags) {
 }
 
 int apc_sm_count(apc_context *c) {
-  static int cached[64] = {0};
+  static std::atomic<int> cached[64];
   int d = c->dev;
-  if (d >= 0 && d < 64 && cached[d]) return cached[d];
+  if (d >= 0 && d < 64) {
+    const int v = cached[d].load(std::memory_order_relaxed);
+    if (v) return v;
+  }
   int v = 0;
   cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d);
   if (v <= 0) v = 1;
-  if (d >= 0 && d < 64) cached[d] = v;
+  if (d >= 0 && d < 64) cached[d].store(v, std::memory_order_relaxed);
   return v;
 }
 
@@ -103,7 +99,6 @@ void free_all(apc_context *c) {
   for (auto &e : c->sev)
     if (e) cudaEventDestroy(e);
   if (c->s) cudaStreamDestroy(c->s);
-  g_caps.erase(c);
 }
 
 int check_ready(apc_context *c, bool particles, bool cells, bool fields) {

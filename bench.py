@@ -63,34 +63,49 @@ def dist_env():
 
 
 class Dist:
-    def __init__(self, device: int):
+    """Rank plumbing: NCCL on GPUs for the bench, gloo on CPU for the tests.  Only
+    barriers and a max over ranks cross ranks; the step itself has no collective."""
+
+    def __init__(self, device: int, backend: str = "nccl"):
         self.ws, self.rank, self.local = dist_env()
         self.pg = None
+        self.dev = "cuda" if backend == "nccl" else "cpu"
         if self.ws > 1:
             import datetime
 
             import torch
             import torch.distributed as td
 
-            torch.cuda.set_device(device)
-            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+            if backend == "nccl":
+                torch.cuda.set_device(device)
+            td.init_process_group(backend, timeout=datetime.timedelta(seconds=900 if backend == "nccl" else 60))
             self.pg = td
 
     def barrier(self):
         if self.pg:
             import torch
 
-            t = torch.zeros(1, device="cuda")
+            t = torch.zeros(1, device=self.dev)
             self.pg.all_reduce(t)
-            torch.cuda.synchronize()
+            if self.dev == "cuda":
+                torch.cuda.synchronize()
 
     def max(self, v: float) -> float:
         if not self.pg:
             return v
         import torch
 
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        t = torch.tensor([v], dtype=torch.float64, device=self.dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64, device=self.dev)
+        self.pg.all_reduce(t)
         return float(t.item())
 
     def close(self):
@@ -185,6 +200,12 @@ def ncu_traffic_per_unit(kernel: str) -> float | None:
     except OSError:
         pass
     return None
+
+
+def batch_shard(cfgs, ws: int, rank: int) -> list:
+    """The boxes of `rank`: longest-processing-time partition by particle-steps, the
+    same on every rank, so the ranks share no data and need no collective."""
+    return ics.lpt_partition([c.n * c.steps for c in cfgs], ws)[rank]
 
 
 # ------------------------------------------------------------------ our arm
@@ -358,6 +379,59 @@ def run_ours(args) -> dict:
     return out if rank == 0 else None
 
 
+# ------------------------------------------------------------- batched boxes
+
+def run_batch(args) -> dict | None:
+    """96 independent boxes (16^3..64^3 balls and Zel'dovich lattices), each rank taking
+    a longest-processing-time share; every step of every box goes through one
+    apc_batch_step call per rank.  Timed on the host around whole batch steps, with the
+    device synchronised on both sides (the boxes run on many streams); max over ranks."""
+    import torch
+
+    from apcloud import binding
+    from apcloud.batch import BatchRun, load_tuned
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = Dist(local)
+    cfgs = ics.batch_boxes()
+    mine = [cfgs[i] for i in batch_shard(cfgs, ws, rank)]
+    br = BatchRun(mine, precision=binding.APC_PREC_MIXED, n_workers=args.batch_workers, tuned=load_tuned())
+    br.start()
+    for _ in range(args.warmup):
+        br.step()
+    for g in br.path.boxes:
+        g.reset_profile()
+    dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        br.step()
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    dist.barrier()
+    dt = dist.max(dt)
+    launches = sum(g.kernel_launches() for g in br.path.boxes)
+    dev_ms = sum(g.profile()["step_ms"] for g in br.path.boxes)
+    br.close()
+    total = sum(c.n for c in cfgs)
+    value = total * args.steps / dt
+    dist.close()
+    if rank != 0:
+        return None
+    return {"metric": "particle-steps/s over 96 batched boxes (16^3..64^3, mixed path)", "value": value,
+            "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32 Krylov / f64 refinement, GFD moments and leapfrog",
+            "data": "synthetic",
+            "config": {"workload": f"batch96: {len(cfgs)} EdS boxes, {total} particles, a 0.05->0.5 in 32 steps",
+                       "parallelism": f"boxes sharded over {ws} ranks by LPT; {args.batch_workers or 8} "
+                                      f"host workers per rank",
+                       "timing": "host clock around whole batch steps, device synchronised, max over ranks"},
+            "rank0": {"boxes": len(mine), "sum_of_box_device_ms_per_step": dev_ms / args.steps},
+            "gpu_launches": launches}
+
+
 # ------------------------------------------------------------- CPU reference
 
 def reference_sample(cfg, parts_state, t, fp64_its: int | None, args):
@@ -447,10 +521,16 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-workers", type=int, default=0, help="host worker threads per rank (batch96)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if args.impl == "reference":
+        out = run_reference(args)
+    elif args.workload == "batch96":
+        out = run_batch(args)
+    else:
+        out = run_ours(args)
     if out is not None:
         print(json.dumps(out), flush=True)
 

@@ -232,6 +232,32 @@ int apc_move_velocity_noalloc(int n_particles, int n_cells, const int *first, co
 /* Device time (ms) of the last select / solve / move phases, from CUDA events. */
 int apc_get_phase_times(apc_context *ctx, double *select_ms, double *solve_ms, double *move_ms);
 
+/* ---- batches of independent boxes ----
+ * The reference runs one box per process (test.cpp:16-80); it has no batched
+ * interface.  A batch owns one context per box (each with its own stream) and steps
+ * them together: host worker threads take boxes from a queue, largest first, and each
+ * runs that box's apc_step (controller.cpp:133-197, the same code path as a single
+ * context), so the GPU overlaps the kernels of many small boxes.  Per-box results are
+ * those of the single-box path. */
+typedef struct apc_batch apc_batch;
+
+/* Create n_boxes contexts from cfgs[0..n_boxes-1] (all on cfgs[i].device), stepped by
+ * n_workers host threads (0 = min(n_boxes, 8)). */
+int apc_batch_create(const apc_config *cfgs, int n_boxes, int n_workers, apc_batch **out);
+int apc_batch_destroy(apc_batch *b);
+int apc_batch_size(const apc_batch *b);
+
+/* The context of box i: use it for particles I/O, selection, results and profiles.
+ * Do not use it from another thread while apc_batch_step runs. */
+apc_context *apc_batch_context(apc_batch *b, int box);
+
+/* One step of every box: select, solve, kick and drift with params[i] for box i.
+ * status[i] (optional) receives box i's apc_status; the call returns the first
+ * non-zero status, or APC_OK.  max_dv / max_dx (optional, n_boxes each) receive the
+ * boxes' kick and drift maxima. */
+int apc_batch_step(apc_batch *b, const apc_step_params *params, int *status, double *max_dv,
+                   double *max_dx);
+
 #ifdef __cplusplus
 }
 #endif
