@@ -28,6 +28,7 @@ EXPORTED = [
     "apc_get_fields", "apc_get_stencils", "apc_get_solve_stats", "apc_get_matrix", "apc_kernel_launches",
     "apc_get_phase_times", "apc_get_profile", "apc_reset_profile", "apc_move_velocity_noalloc",
     "apc_batch_create", "apc_batch_destroy", "apc_batch_size", "apc_batch_context", "apc_batch_step",
+    "apc_get_hessians_device", "apc_vjp_kick_drift", "apc_trajectory_vjp",
 ]
 
 
@@ -64,6 +65,11 @@ class ApcProfile(C.Structure):
 class ApcStepParams(C.Structure):
     _fields_ = [("dt", C.c_double), ("c_dens", C.c_double), ("c_pot", C.c_double),
                 ("c_field", C.c_double), ("c_vel", C.c_double), ("c_pos", C.c_double)]
+
+
+class ApcTrajectory(C.Structure):
+    _fields_ = [("n_steps", C.c_int), ("steps", C.POINTER(ApcStepParams)), ("start_dt", C.c_double),
+                ("start_c_pos", C.c_double), ("checkpoint_every", C.c_int)]
 
 
 class ApcError(RuntimeError):
@@ -120,6 +126,11 @@ def load_library(path: str = LIB_PATH):
         "apc_batch_size": (C.c_int, [vp]),
         "apc_batch_context": (C.c_void_p, [vp, C.c_int]),
         "apc_batch_step": (C.c_int, [vp, C.POINTER(ApcStepParams), ip, vp, vp]),
+        "apc_get_hessians_device": (C.c_int, [vp] + [vp] * 6),
+        "apc_vjp_kick_drift": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.c_double, C.c_double,
+                                         C.POINTER(C.c_void_p), vp]),
+        "apc_trajectory_vjp": (C.c_int, [vp, C.POINTER(ApcTrajectory), C.POINTER(C.c_void_p),
+                                         C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -271,6 +282,23 @@ class GpuPath:
 
     def synchronize(self):
         self._check(self.lib.apc_synchronize(self.h), "apc_synchronize")
+
+    # ---- derivatives (device pointers: ints, e.g. torch tensor data_ptr()) ----
+    def hessians_device(self, ptrs):
+        self._check(self.lib.apc_get_hessians_device(self.h, *[C.c_void_p(p) for p in ptrs]),
+                    "apc_get_hessians_device")
+
+    def trajectory_vjp(self, steps, start_dt: float, start_c_pos: float, every: int, state0_ptrs, cot_ptrs,
+                       statef_ptrs=None):
+        """steps: (dt, c_dens, c_pot, c_field, c_vel, c_pos) per step; *_ptrs: 6 device
+        pointers each (x, y, z, vx, vy, vz) in caller order; cot is updated in place."""
+        k = len(steps)
+        arr = (ApcStepParams * max(k, 1))(*[ApcStepParams(*q) for q in steps])
+        t = ApcTrajectory(k, arr, start_dt, start_c_pos, every)
+        s0 = (C.c_void_p * 6)(*state0_ptrs)
+        ct = (C.c_void_p * 6)(*cot_ptrs)
+        sf = (C.c_void_p * 6)(*statef_ptrs) if statef_ptrs is not None else None
+        self._check(self.lib.apc_trajectory_vjp(self.h, C.byref(t), s0, ct, sf), "apc_trajectory_vjp")
 
     # ---- results ----
     def counts(self):

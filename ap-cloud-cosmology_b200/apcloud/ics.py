@@ -82,9 +82,10 @@ def drift_factor(a: float, omega0: float, omegal: float) -> float:
     return kick_factor(a, omega0, omegal) / (a * a)
 
 
-def zeldovich(n_side: int, spectral_index: float, rms_spacing: float, a_start: float,
-              omega0: float, omegal: float, seed: int = 0) -> Particles:
-    """Lattice + Zel'dovich displacement with growing-mode momenta."""
+def zeldovich_field(n_side: int, spectral_index: float, rms_spacing: float, a_start: float,
+                    omega0: float, omegal: float, seed: int = 0):
+    """The Zel'dovich displacement field psi (3, n, n, n), in box units at a_start, and the
+    growing-mode factor fac with momenta p = fac psi."""
     rng = np.random.default_rng(seed)
     n = n_side
     white = rng.standard_normal((n, n, n))
@@ -104,17 +105,31 @@ def zeldovich(n_side: int, spectral_index: float, rms_spacing: float, a_start: f
     psi = [np.fft.irfftn(1j * K * inv * dk, s=(n, n, n), axes=(0, 1, 2)) for K in (KX, KY, KZ)]
     rms = math.sqrt(float(np.mean(psi[0] ** 2 + psi[1] ** 2 + psi[2] ** 2)))
     scale = rms_spacing / n / rms
-    psi = [p * scale for p in psi]
+    psi = np.stack([p * scale for p in psi])
+    d, dd = growth(a_start, omega0, omegal)
+    # p = a^2 dx/da / F(a),  dx/da = (D'/D) psi
+    fac = a_start * a_start * (dd / d) / kick_factor(a_start, omega0, omegal)
+    return psi, fac
+
+
+def particles_from_field(psi, fac: float) -> Particles:
+    """Lattice q = (i + 1/2)/n displaced by psi (3, n, n, n), wrapped into [0, 1)."""
+    n = psi.shape[1]
+    psi = np.asarray(psi, dtype=np.float64)
     q = (np.arange(n, dtype=np.float64) + 0.5) / n
     QX, QY, QZ = np.meshgrid(q, q, q, indexing="ij")
     pos = [np.mod(Q + P, 1.0).ravel() for Q, P in zip((QX, QY, QZ), psi)]
     for p in pos:
         p[p >= 1.0] -= 1.0
-    d, dd = growth(a_start, omega0, omegal)
-    # p = a^2 dx/da / F(a),  dx/da = (D'/D) psi
-    fac = a_start * a_start * (dd / d) / kick_factor(a_start, omega0, omegal)
     vel = [(fac * P).ravel() for P in psi]
     return Particles(pos[0], pos[1], pos[2], vel[0], vel[1], vel[2])
+
+
+def zeldovich(n_side: int, spectral_index: float, rms_spacing: float, a_start: float,
+              omega0: float, omegal: float, seed: int = 0) -> Particles:
+    """Lattice + Zel'dovich displacement with growing-mode momenta."""
+    psi, fac = zeldovich_field(n_side, spectral_index, rms_spacing, a_start, omega0, omegal, seed)
+    return particles_from_field(psi, fac)
 
 
 @dataclass

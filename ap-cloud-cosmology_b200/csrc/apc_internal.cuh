@@ -106,6 +106,7 @@ struct apc_context {
   int *nb24 = nullptr;   // 24 per cell
   int *nnb = nullptr;    // Neigh24 count per cell
   int *cell_of = nullptr;  // sorted particle -> cell
+  double *adj_ckpt = nullptr, *adj_tape = nullptr;  // trajectory VJP: checkpoints, Hessian tape
 
   // ---- GFD / solver ----
   int lm = 17;

@@ -86,7 +86,7 @@ void free_all(apc_context *c) {
                   c->d_err, c->scan_tmp, c->flags, c->cx, c->cy, c->cz, c->ch, c->cfirst, c->ccount,
                   c->ctype, c->ccode, c->nb24, c->nnb, c->cell_of, c->st_idx, c->st_dist, c->gfd_x,
                   c->ell_col, c->a1, c->a2, c->a1f, c->a2f, c->rhs, c->bcrhs, c->density, c->potential,
-                  c->deriv};
+                  c->deriv, c->adj_ckpt, c->adj_tape};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->h_pinned) cudaFreeHost(c->h_pinned);

@@ -232,6 +232,43 @@ int apc_move_velocity_noalloc(int n_particles, int n_cells, const int *first, co
 /* Device time (ms) of the last select / solve / move phases, from CUDA events. */
 int apc_get_phase_times(apc_context *ctx, double *select_ms, double *solve_ms, double *move_ms);
 
+/* ---- derivatives ----
+ * The reference computes no derivatives.  These entry points are the reverse mode of
+ * the Controller step sequence (controller.cpp:88-208) with the octree, the selected
+ * cells and their particle counts held fixed.  Under that assumption the cell fields of
+ * a step do not depend on the positions (the density is n_p / h^3, solver.cpp:116-172),
+ * and the Jacobian of the interpolated acceleration a = g + H (x - x_c)
+ * (octree.cpp:3003-3031) is the cell's Hessian H. */
+
+/* Per-particle Hessian (xx, yy, zz, xy, xz, yz) of the cell each particle was kicked in
+ * by the last apc_move_velocity; device arrays of n_particles, caller order. */
+int apc_get_hessians_device(apc_context *ctx, double *hxx, double *hyy, double *hzz, double *hxy,
+                            double *hxz, double *hyz);
+
+/* Reverse of one kick + drift: given the cotangents cot = (x, y, z, vx, vy, vz) of the
+ * state after the step (device, caller order), overwrite them with those of the state
+ * before it.  hess: the step's per-particle Hessians (apc_get_hessians_device);
+ * kdt = C_vel dt, ddt = C_pos dt.  stream: cudaStream_t or NULL; returns when done. */
+int apc_vjp_kick_drift(int n_particles, const double *const hess[6], double kdt, double ddt,
+                       double *const cot[6], void *stream);
+
+typedef struct apc_trajectory {
+  int n_steps;                   /* Controller steps after the start */
+  const apc_step_params *steps;  /* one per step */
+  double start_dt, start_c_pos;  /* the initial half drift: dt/2 and C_pos(start_a) */
+  int checkpoint_every;          /* forward states kept every k steps, k >= 1 */
+} apc_trajectory;
+
+/* Vector-Jacobian product of a whole trajectory: select + half drift, then n_steps
+ * apc_step calls, from the initial state state0 = (x, y, z, vx, vy, vz) (device, caller
+ * order).  On entry cot holds the cotangents of the final state; on return those of
+ * state0.  statef (optional, device) receives the final state.  The forward pass keeps
+ * the state every checkpoint_every steps; the backward pass reruns each segment to
+ * record its Hessians (bit-identical to the forward run) and applies the reverse steps.
+ * Memory: 6 n doubles per checkpoint and per step of a segment. */
+int apc_trajectory_vjp(apc_context *ctx, const apc_trajectory *t, const double *const state0[6],
+                       double *const cot[6], double *const statef[6]);
+
 /* ---- batches of independent boxes ----
  * The reference runs one box per process (test.cpp:16-80); it has no batched
  * interface.  A batch owns one context per box (each with its own stream) and steps
