@@ -28,7 +28,8 @@ EXPORTED = [
     "apc_get_fields", "apc_get_stencils", "apc_get_solve_stats", "apc_get_matrix", "apc_kernel_launches",
     "apc_get_phase_times", "apc_get_profile", "apc_reset_profile", "apc_move_velocity_noalloc",
     "apc_batch_create", "apc_batch_destroy", "apc_batch_size", "apc_batch_context", "apc_batch_step",
-    "apc_get_hessians_device", "apc_vjp_kick_drift", "apc_trajectory_vjp",
+    "apc_get_hessians_device", "apc_vjp_kick_drift", "apc_trajectory_vjp", "apc_fields_from_rhs",
+    "apc_solve_vjp",
 ]
 
 
@@ -50,6 +51,8 @@ class ApcSolveStats(C.Structure):
         ("density_reason", C.c_int), ("potential_reason", C.c_int),
         ("density_rnorm", C.c_double), ("potential_rnorm", C.c_double),
         ("density_refinements", C.c_int), ("potential_refinements", C.c_int), ("mg_levels", C.c_int),
+        ("adjoint_density_its", C.c_int), ("adjoint_potential_its", C.c_int),
+        ("adjoint_density_reason", C.c_int), ("adjoint_potential_reason", C.c_int),
     ]
 
 
@@ -127,6 +130,8 @@ def load_library(path: str = LIB_PATH):
         "apc_batch_context": (C.c_void_p, [vp, C.c_int]),
         "apc_batch_step": (C.c_int, [vp, C.POINTER(ApcStepParams), ip, vp, vp]),
         "apc_get_hessians_device": (C.c_int, [vp] + [vp] * 6),
+        "apc_fields_from_rhs": (C.c_int, [vp, vp]),
+        "apc_solve_vjp": (C.c_int, [vp, vp, vp, vp, vp]),
         "apc_vjp_kick_drift": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.c_double, C.c_double,
                                          C.POINTER(C.c_void_p), vp]),
         "apc_trajectory_vjp": (C.c_int, [vp, C.POINTER(ApcTrajectory), C.POINTER(C.c_void_p),
@@ -287,6 +292,14 @@ class GpuPath:
     def hessians_device(self, ptrs):
         self._check(self.lib.apc_get_hessians_device(self.h, *[C.c_void_p(p) for p in ptrs]),
                     "apc_get_hessians_device")
+
+    def fields_from_rhs(self, rhs_ptr: int):
+        self._check(self.lib.apc_fields_from_rhs(self.h, C.c_void_p(rhs_ptr)), "apc_fields_from_rhs")
+
+    def solve_vjp(self, g_deriv_ptr: int, g_rhs_ptr: int, g_rho_ptr: int | None = None, g_phi_ptr: int | None = None):
+        self._check(self.lib.apc_solve_vjp(self.h, C.c_void_p(g_deriv_ptr), C.c_void_p(g_rhs_ptr),
+                                           C.c_void_p(g_rho_ptr) if g_rho_ptr else None,
+                                           C.c_void_p(g_phi_ptr) if g_phi_ptr else None), "apc_solve_vjp")
 
     def trajectory_vjp(self, steps, start_dt: float, start_c_pos: float, every: int, state0_ptrs, cot_ptrs,
                        statef_ptrs=None):

@@ -73,7 +73,172 @@ __global__ void reverse_drift(int n, double ddt, const double *__restrict__ lx, 
 
 int grid_of(int n) { return std::max(1, std::min((n + 255) / 256, 4096)); }
 
+// ---- transposition of a sparsity pattern ----
+// Source entries (i, s), i < n, s in [s0, w): column col[s * ss + i * si].  Entries whose
+// column is i itself or outside [0, n) are skipped (ELL padding and the diagonal slot).
+// The transposed pattern has, per row t, the flat sources i * w + s with column t, sorted
+// ascending, so every sum over it runs in a fixed order.
+
+__global__ void tr_count(int n, int w, int s0, size_t ss, size_t si, const int *__restrict__ col,
+                         int *__restrict__ cnt) {
+  const long long total = (long long)n * w;
+  for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < total;
+       f += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(f / w), sl = (int)(f % w);
+    if (sl < s0) continue;
+    const int t = col[sl * ss + i * si];
+    if (t >= 0 && t < n && t != i) atomicAdd(&cnt[t], 1);
+  }
+}
+
+__global__ void tr_fill(int n, int w, int s0, size_t ss, size_t si, const int *__restrict__ col,
+                        int *__restrict__ cur, int *__restrict__ tmp) {
+  const long long total = (long long)n * w;
+  for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < total;
+       f += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(f / w), sl = (int)(f % w);
+    if (sl < s0) continue;
+    const int t = col[sl * ss + i * si];
+    if (t >= 0 && t < n && t != i) tmp[atomicAdd(&cur[t], 1)] = (int)f;
+  }
+}
+
+__global__ void max_count(int n, const int *__restrict__ cnt, int *out) {
+  int m = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = max(m, cnt[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// sort each row's sources and write the transposed ELL (slot-major, leading dimension n):
+// slot 0 = the row's own diagonal source (diag_w > 0: flat t * diag_w) or none, slots
+// 1.. = the sorted sources, padding = (column t, source -1)
+__global__ void tr_emit(int n, int w, int wt, int diag_w, const int *__restrict__ off, const int *__restrict__ cnt,
+                        int *__restrict__ tmp, int *__restrict__ tcol, int *__restrict__ tsrc) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    int *seg = tmp + off[t];
+    const int k = cnt[t];
+    for (int a = 1; a < k; ++a) {  // insertion sort: rows are short
+      const int v = seg[a];
+      int b = a - 1;
+      while (b >= 0 && seg[b] > v) {
+        seg[b + 1] = seg[b];
+        --b;
+      }
+      seg[b + 1] = v;
+    }
+    tcol[t] = t;
+    tsrc[t] = diag_w > 0 ? t * diag_w : -1;
+    for (int q = 0; q < wt - 1; ++q) {
+      const size_t at = (size_t)(q + 1) * n + t;
+      if (q < k) {
+        tcol[at] = seg[q] / w;
+        tsrc[at] = seg[q];
+      } else {
+        tcol[at] = t;
+        tsrc[at] = -1;
+      }
+    }
+  }
+}
+
+// values of the transposed ELL matrix: source flat i * w + s is entry (i, slot s) of the
+// slot-major source with leading dimension ld
+__global__ void tr_values(size_t count, int w, size_t ld, const int *__restrict__ tsrc, const double *__restrict__ val,
+                          double *__restrict__ tval) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < count; e += (size_t)gridDim.x * blockDim.x) {
+    const int f = tsrc[e];
+    tval[e] = f < 0 ? 0.0 : val[(size_t)(f % w) * ld + f / w];
+  }
+}
+
+// C[i, j] = c_field sum_k g[i, k] X_i[k, j] / h_i^(1 or 2): the cotangents of the
+// differences (phi_nbr - phi_i) of cell i's stencil (solver.cpp:315-358 transposed)
+__global__ void stencil_cot(int m, int lm, const double *__restrict__ gx, const double *__restrict__ h,
+                            const double *__restrict__ g, double c_field, double *__restrict__ cmat) {
+  const long long total = (long long)m * lm;
+  for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < total;
+       f += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(f / lm), j = (int)(f % lm);
+    const double *X = gx + (size_t)i * 9 * lm;
+    const double hi = h[i];
+    double s = 0.0;
+    for (int k = 0; k < 9; ++k) s += g[(size_t)i * 9 + k] * X[k * lm + j] / (k < 3 ? hi : hi * hi);
+    cmat[f] = c_field * s;
+  }
+}
+
+// phi_bar[t] = sum of C over the stencil entries naming t (sorted) - sum_j C[t, j]
+__global__ void stencil_gather(int m, int lm, int wt, const int *__restrict__ tsrc, const double *__restrict__ cmat,
+                               double *__restrict__ phib) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int q = 1; q < wt; ++q) {
+      const int f = tsrc[(size_t)q * m + t];
+      if (f >= 0) s += cmat[f];
+    }
+    double own = 0.0;
+    for (int j = 0; j < lm; ++j) own += cmat[(size_t)t * lm + j];
+    phib[t] = s - own;
+  }
+}
+
+// rho_bar = c_pot (r - w sum(r) / sum(w)), w = h^3: the transpose of rhs = c_pot (rho -
+// sum(rho h^3) / sum(h^3)) (solver.cpp:244-259)
+__global__ void mean_transpose(int m, const double *__restrict__ h, const double *__restrict__ r, double c_pot,
+                               double *__restrict__ out) {
+  __shared__ double sr[256], sw[256];
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    a += r[i];
+    b += h[i] * h[i] * h[i];
+  }
+  sr[threadIdx.x] = a;
+  sw[threadIdx.x] = b;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) {
+      sr[threadIdx.x] += sr[threadIdx.x + o];
+      sw[threadIdx.x] += sw[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  const double f = sr[0] / sw[0];
+  for (int i = threadIdx.x; i < m; i += blockDim.x) out[i] = c_pot * (r[i] - h[i] * h[i] * h[i] * f);
+}
+
 }  // namespace
+
+// Transpose the pattern of (n rows, w slots from s0) into c->tr_* / (tcol, tsrc); returns
+// the transposed width (1 + the largest column count).
+static int transpose_pattern(apc_context *c, int n, int w, int s0, size_t ss, size_t si, const int *col, int diag_w,
+                             int **tcol, int **tsrc, int *wt_out) {
+  APC_TRY(apc_ensure(c, &c->tr_cnt, (size_t)n + 1, nullptr));
+  APC_TRY(apc_ensure(c, &c->tr_off, (size_t)n + 1, nullptr));
+  APC_TRY(apc_ensure(c, &c->tr_cur, (size_t)n + 1, nullptr));
+  APC_TRY(apc_ensure(c, &c->tr_tmp, (size_t)n * w + 1, nullptr));
+  APC_CUDA_TRY(c, cudaMemsetAsync(c->tr_cnt, 0, sizeof(int) * (size_t)n, c->s));
+  const int G = grid_of((int)std::min<long long>((long long)n * w, 1 << 30));
+  tr_count<<<G, 256, 0, c->s>>>(n, w, s0, ss, si, col, c->tr_cnt);
+  APC_TRY(apc_exclusive_scan(c, c->tr_cnt, c->tr_off, n, nullptr));
+  APC_CUDA_TRY(c, cudaMemcpyAsync(c->tr_cur, c->tr_off, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, c->s));
+  tr_fill<<<G, 256, 0, c->s>>>(n, w, s0, ss, si, col, c->tr_cur, c->tr_tmp);
+  int *mx = c->counters + 110;
+  APC_CUDA_TRY(c, cudaMemsetAsync(mx, 0, sizeof(int), c->s));
+  max_count<<<grid_of(n), 256, 0, c->s>>>(n, c->tr_cnt, mx);
+  int h = 0;
+  APC_CUDA_TRY(c, cudaMemcpyAsync(&h, mx, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  const int wt = h + 1;
+  APC_TRY(apc_ensure(c, tcol, (size_t)n * wt, nullptr));
+  APC_TRY(apc_ensure(c, tsrc, (size_t)n * wt, nullptr));
+  tr_emit<<<grid_of(n), 256, 0, c->s>>>(n, w, wt, diag_w, c->tr_off, c->tr_cnt, c->tr_tmp, *tcol, *tsrc);
+  apc_count_launch(c, 4);
+  APC_CUDA_TRY(c, cudaGetLastError());
+  *wt_out = wt;
+  return APC_OK;
+}
 
 extern "C" {
 
@@ -103,6 +268,75 @@ int apc_vjp_kick_drift(int n, const double *const hess[6], double kdt, double dd
                                                 cot[0], cot[1], cot[2], cot[3], cot[4], cot[5]);
   if (cudaGetLastError() != cudaSuccess) return APC_ERR_CUDA;
   return cudaStreamSynchronize(s) == cudaSuccess ? APC_OK : APC_ERR_CUDA;
+}
+
+int apc_fields_from_rhs(apc_context *c, const double *rhs_dev) {
+  if (!c || !rhs_dev) return APC_ERR_INVALID_ARG;
+  if (!c->have_fields) {
+    c->err = "no solve on the current cells";
+    return APC_ERR_INVALID_ARG;
+  }
+  cudaSetDevice(c->dev);
+  const int M = c->nc + c->nv;
+  APC_CUDA_TRY(c, cudaMemcpyAsync(c->rhs, rhs_dev, sizeof(double) * M, cudaMemcpyDeviceToDevice, c->s));
+  apc_solve_stats &st = c->stats;
+  APC_TRY(apc_krylov_solve(c, 0, c->rhs, c->density, &st.density_its, &st.density_rnorm, &st.density_reason,
+                           &st.density_refinements));
+  APC_TRY(apc_potential_rhs(c, c->last_c_pot));
+  APC_TRY(apc_krylov_solve(c, 1, c->rhs, c->potential, &st.potential_its, &st.potential_rnorm,
+                           &st.potential_reason, &st.potential_refinements));
+  APC_TRY(apc_differentiate(c, c->last_c_field));
+  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  return APC_OK;
+}
+
+int apc_solve_vjp(apc_context *c, const double *g_deriv, double *g_rhs, double *g_rho, double *g_phi) {
+  if (!c || !g_deriv || !g_rhs) return APC_ERR_INVALID_ARG;
+  if (!c->have_fields) {
+    c->err = "no solve on the current cells";
+    return APC_ERR_INVALID_ARG;
+  }
+  if (c->cfg.bc != 1) return APC_ERR_UNSUPPORTED;
+  cudaSetDevice(c->dev);
+  const int M = c->nc + c->nv, lm = c->lm, w = c->ell_w;
+  const size_t ld = (size_t)c->m_cap;
+  APC_TRY(apc_ensure(c, &c->vjp_c, (size_t)M * lm + 1, nullptr));
+  APC_TRY(apc_ensure(c, &c->vjp_phi, (size_t)M + 1, nullptr));
+  APC_TRY(apc_ensure(c, &c->vjp_r2, (size_t)M + 1, nullptr));
+  APC_TRY(apc_ensure(c, &c->vjp_rho, (size_t)M + 1, nullptr));
+  // 1. the transposed differentiation stencil
+  int wtp = 0;
+  APC_TRY(transpose_pattern(c, M, lm, 0, 1, (size_t)lm, c->st_idx, 0, &c->tp_col, &c->tp_src, &wtp));
+  const int G = grid_of((int)std::min<long long>((long long)M * lm, 1 << 30));
+  stencil_cot<<<G, 256, 0, c->s>>>(M, lm, c->gfd_x, c->ch, g_deriv, c->last_c_field, c->vjp_c);
+  stencil_gather<<<grid_of(M), 256, 0, c->s>>>(M, lm, wtp, c->tp_src, c->vjp_c, c->vjp_phi);
+  apc_count_launch(c, 2);
+  // 2. A2^T r2 = phi_bar
+  int wt = 0, its = 0, reason = 0;
+  double rn = 0.0;
+  APC_TRY(transpose_pattern(c, M, w, 1, ld, 1, c->ell_col, w, &c->ta_col, &c->ta_src, &wt));
+  APC_TRY(apc_ensure(c, &c->ta_val, (size_t)M * wt, nullptr));
+  tr_values<<<grid_of(M * wt), 256, 0, c->s>>>((size_t)M * wt, w, ld, c->ta_src, c->a2, c->ta_val);
+  apc_count_launch(c);
+  APC_TRY(apc_gmres_fp64_ell(c, M, wt, (size_t)M, c->ta_col, c->ta_val, c->vjp_phi, c->vjp_r2, &its, &rn, &reason));
+  c->stats.adjoint_potential_its = its;
+  c->stats.adjoint_potential_reason = reason;
+  // 3. the mean subtraction, transposed
+  mean_transpose<<<1, 256, 0, c->s>>>(M, c->ch, c->vjp_r2, c->last_c_pot, c->vjp_rho);
+  apc_count_launch(c);
+  // 4. A1^T r1 = rho_bar (same pattern as A2)
+  tr_values<<<grid_of(M * wt), 256, 0, c->s>>>((size_t)M * wt, w, ld, c->ta_src, c->a1, c->ta_val);
+  apc_count_launch(c);
+  APC_TRY(apc_gmres_fp64_ell(c, M, wt, (size_t)M, c->ta_col, c->ta_val, c->vjp_rho, g_rhs, &its, &rn, &reason));
+  c->stats.adjoint_density_its = its;
+  c->stats.adjoint_density_reason = reason;
+  if (g_rho)
+    APC_CUDA_TRY(c, cudaMemcpyAsync(g_rho, c->vjp_rho, sizeof(double) * M, cudaMemcpyDeviceToDevice, c->s));
+  if (g_phi)
+    APC_CUDA_TRY(c, cudaMemcpyAsync(g_phi, c->vjp_phi, sizeof(double) * M, cudaMemcpyDeviceToDevice, c->s));
+  APC_CUDA_TRY(c, cudaGetLastError());
+  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  return APC_OK;
 }
 
 int apc_trajectory_vjp(apc_context *c, const apc_trajectory *t, const double *const state0[6],

@@ -107,6 +107,11 @@ struct apc_context {
   int *nnb = nullptr;    // Neigh24 count per cell
   int *cell_of = nullptr;  // sorted particle -> cell
   double *adj_ckpt = nullptr, *adj_tape = nullptr;  // trajectory VJP: checkpoints, Hessian tape
+  double last_c_pot = 0.0, last_c_field = 0.0;       // constants of the last apc_solve
+  // solve VJP: transposed stencil pattern and matrices (ELL, leading dimension M)
+  int *tr_cnt = nullptr, *tr_off = nullptr, *tr_cur = nullptr, *tr_tmp = nullptr;
+  int *tp_col = nullptr, *tp_src = nullptr, *ta_col = nullptr, *ta_src = nullptr;
+  double *ta_val = nullptr, *vjp_c = nullptr, *vjp_phi = nullptr, *vjp_r2 = nullptr, *vjp_rho = nullptr;
 
   // ---- GFD / solver ----
   int lm = 17;
@@ -153,6 +158,8 @@ int apc_gfd_assemble(apc_context *c, double c_dens);    // gfd.cu
 int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int *its,
                      double *rnorm, int *reason, int *refinements);  // krylov.cu
 void apc_krylov_free(apc_context *c);
+int apc_gmres_fp64_ell(apc_context *c, int n, int w, size_t ld, const int *col, const double *val,
+                       const double *b, double *x, int *its, double *rnorm, int *reason);  // krylov.cu
 void apc_mg_free(apc_context *c);
 // One solve of the mixed path (mg.cu): FP64 refinement with FP32 (F)GMRES corrections on
 // the Jacobi-scaled operator valf, run on the device as one CUDA graph; with use_mg the

@@ -86,7 +86,9 @@ void free_all(apc_context *c) {
                   c->d_err, c->scan_tmp, c->flags, c->cx, c->cy, c->cz, c->ch, c->cfirst, c->ccount,
                   c->ctype, c->ccode, c->nb24, c->nnb, c->cell_of, c->st_idx, c->st_dist, c->gfd_x,
                   c->ell_col, c->a1, c->a2, c->a1f, c->a2f, c->rhs, c->bcrhs, c->density, c->potential,
-                  c->deriv, c->adj_ckpt, c->adj_tape};
+                  c->deriv, c->adj_ckpt, c->adj_tape, c->tr_cnt, c->tr_off, c->tr_cur, c->tr_tmp,
+                  c->tp_col, c->tp_src, c->ta_col, c->ta_src, c->ta_val, c->vjp_c, c->vjp_phi, c->vjp_r2,
+                  c->vjp_rho};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -372,6 +374,8 @@ int apc_solve(apc_context *c, double c_dens, double c_pot, double c_field) {
                            &st.potential_reason, &st.potential_refinements));
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[7], c->s));
   APC_TRY(apc_differentiate(c, c_field));
+  c->last_c_pot = c_pot;
+  c->last_c_field = c_field;
   (void)M;
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[3], c->s));
   APC_CUDA_TRY(c, cudaEventSynchronize(c->ev[3]));

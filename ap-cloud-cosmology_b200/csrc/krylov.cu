@@ -477,7 +477,8 @@ void apc_krylov_free(apc_context *c) {
 
 template <class T, bool RE>
 static int launch_gmres(apc_context *c, int n, const T *val, const T *b, T *x, int restart, double rtol,
-                        double atol, double dtol, int max_it, int *its, double *rnorm, int *reason) {
+                        double atol, double dtol, int max_it, int *its, double *rnorm, int *reason,
+                        const int *col = nullptr, int w = 0, size_t ld = 0) {
   KrylovWork *k = c->kw;
   if (restart < 1 || restart > 31) {
     c->err = "GMRES restart must be in [1, 31]";
@@ -505,9 +506,9 @@ static int launch_gmres(apc_context *c, int n, const T *val, const T *b, T *x, i
   APC_CUDA_TRY(c, cudaMemsetAsync(k->bar, 0, sizeof(GridBar), c->s));
   GmresArgs<T> a;
   a.n = n;
-  a.w = c->ell_w;
-  a.ld = (size_t)c->m_cap;
-  a.col = c->ell_col;
+  a.w = col ? w : c->ell_w;
+  a.ld = col ? ld : (size_t)c->m_cap;
+  a.col = col ? col : c->ell_col;
   a.val = val;
   a.b = b;
   a.x = x;
@@ -582,6 +583,19 @@ static int ensure_work(apc_context *c, int n) {
     k->cap_n = cap;
   }
   return APC_OK;
+}
+
+// FP64 GMRES (the FP64 path's kernel and stopping test) on an ELL matrix of the caller's:
+// slot-major, leading dimension ld, width w, diagonal in slot 0; x starts from zero.
+int apc_gmres_fp64_ell(apc_context *c, int n, int w, size_t ld, const int *col, const double *val,
+                       const double *b, double *x, int *its, double *rnorm, int *reason) {
+  APC_TRY(ensure_work(c, n));
+  const int G = std::max(1, std::min((n + 255) / 256, 4096));
+  zero_f64<<<G, 256, 0, c->s>>>(n, x);
+  apc_count_launch(c);
+  const apc_config &cfg = c->cfg;
+  return launch_gmres<double, false>(c, n, val, b, x, cfg.gmres_restart, cfg.gmres_rtol, cfg.gmres_atol,
+                                     cfg.gmres_dtol, cfg.gmres_max_it, its, rnorm, reason, col, w, ld);
 }
 
 // Solve A_which x = b.  FP64: one PETSc-semantics GMRES.  Mixed: FP64 iterative

@@ -96,6 +96,8 @@ typedef struct apc_solve_stats {
   double density_rnorm, potential_rnorm;    /* final preconditioned residual norm */
   int density_refinements, potential_refinements; /* FP64 outer steps (mixed mode) */
   int mg_levels;                            /* multigrid levels of the last potential solve (0 = none) */
+  int adjoint_density_its, adjoint_potential_its;       /* transposed solves of the last apc_solve_vjp */
+  int adjoint_density_reason, adjoint_potential_reason;
 } apc_solve_stats;
 
 typedef struct apc_context apc_context;
@@ -251,6 +253,23 @@ int apc_get_hessians_device(apc_context *ctx, double *hxx, double *hyy, double *
  * kdt = C_vel dt, ddt = C_pos dt.  stream: cudaStream_t or NULL; returns when done. */
 int apc_vjp_kick_drift(int n_particles, const double *const hess[6], double kdt, double ddt,
                        double *const cot[6], void *stream);
+
+/* Re-solve the fields of the current cells for another density right-hand side
+ * rhs_dev (device, M = nc + nv values in cell order; the reference's is n_p / h^3 C_dens,
+ * solver.cpp:116-172), with the constants of the last apc_solve: density solve,
+ * potential rhs, potential solve and differentiation (solver.cpp:182-362).  The
+ * context's fields are replaced. */
+int apc_fields_from_rhs(apc_context *ctx, const double *rhs_dev);
+
+/* Vector-Jacobian product of the solve phase with respect to its density right-hand side:
+ * given g_deriv (device, M x 9, the cotangent of the 9 field derivatives per cell),
+ * write to g_rhs (device, M) the cotangent of the density rhs.  The transposed
+ * differentiation stencil is applied, then FP64 GMRES on A2^T, the transposed mean
+ * subtraction and FP64 GMRES on A1^T (the transposes are built from the current ELL
+ * matrices; GMRES settings from the config).  g_rho / g_phi (optional, device, M)
+ * receive the intermediate cotangents of the density and the potential.  Periodic boxes
+ * only. */
+int apc_solve_vjp(apc_context *ctx, const double *g_deriv, double *g_rhs, double *g_rho, double *g_phi);
 
 typedef struct apc_trajectory {
   int n_steps;                   /* Controller steps after the start */

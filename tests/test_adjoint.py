@@ -106,3 +106,43 @@ def test_gpu_vjp_finite_differences_mixed():
         errs.append(abs((lp - lm) / (2 * h) - grad[c]) / np.abs(grad).max())
     g.close()
     assert sorted(errs)[-2] < 1e-4, errs
+
+
+@pytest.mark.gpu
+def test_solve_vjp_dot_product():
+    """<g, J d> = <J^T g, d> for the linear map density rhs -> field derivatives, with J d
+    from two re-solves and J^T g from apc_solve_vjp (transposed stencil, GMRES on A2^T
+    and A1^T)."""
+    import torch
+
+    from apcloud import binding
+
+    psi, fac, gfd_c, sched = _case(side=12, steps=1)
+    parts = ics.particles_from_field(psi, fac)
+    g = binding.GpuPath(parts, 21, gfd_c, precision=binding.APC_PREC_FP64, rtol=1e-13)
+    _, _, steps = sched
+    dt, c_dens, c_pot, c_field, c_vel, c_pos = steps[0]
+    g.select()
+    g.solve(c_dens, c_pot, c_field)
+    nc, nv, _, _ = g.counts()
+    m = nc + nv
+    cells = g.cells()
+    rhs0 = cells.count[:m] / cells.h[:m] ** 3 * c_dens
+    rng = np.random.default_rng(9)
+    d = rng.standard_normal(m) * np.abs(rhs0).mean()
+    gbar = rng.standard_normal((m, 9))
+    out = []
+    for sign in (1.0, -1.0):
+        r = torch.tensor(rhs0 + sign * d, dtype=torch.float64, device="cuda")
+        g.fields_from_rhs(r.data_ptr())
+        out.append(g.fields().deriv.copy())
+    jd = 0.5 * (out[0] - out[1])
+    gb = torch.tensor(gbar, dtype=torch.float64, device="cuda")
+    gr = torch.empty(m, dtype=torch.float64, device="cuda")
+    g.solve_vjp(gb.data_ptr(), gr.data_ptr())
+    st = g.solve_stats()
+    g.close()
+    lhs = float(np.sum(gbar * jd))
+    rhs = float(np.dot(gr.cpu().numpy(), d))
+    assert st["adjoint_potential_reason"] > 0 and st["adjoint_density_reason"] > 0, st
+    assert abs(lhs - rhs) <= 1e-7 * abs(lhs), (lhs, rhs)
