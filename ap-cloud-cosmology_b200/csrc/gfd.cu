@@ -33,7 +33,8 @@
 
 namespace {
 
-constexpr int kWarps = 4;         // warps per block
+constexpr int kWarps = 4;         // warps per block of the least-squares phase
+constexpr int kSearchWarps = 4;   // warps per block of the search phase
 constexpr int kBucketCap = 48;    // entries per octant bucket
 constexpr int kListCap = 256;     // candidates entering the final sort
 constexpr int kMaxLm = 32;
@@ -175,12 +176,19 @@ __device__ void warp_aquicksort(double &key, int &idx, int n, int limit, int lan
   }
 }
 
+// neighbour search and sort, per warp
 struct WarpSmem {
   int soff[32], sp[32];  // expansion ring: item offset and cell of each candidate
   int bidx[8][kBucketCap];
   double bd2[8][kBucketCap];
   double ldist[kListCap];
   int lidx[kListCap];
+};
+
+// least squares, per warp
+struct LsqSmem {
+  double red[9][32];     // column reductions of the QR: one value per (column, lane)
+  double sums[9];
   double R[9][9];
 };
 
@@ -225,12 +233,38 @@ __device__ __forceinline__ bool append(WarpSmem &S, int (&nn)[8], bool valid, in
   return ok;
 }
 
-__global__ void __launch_bounds__(32 * kWarps) gfd_stencil(GfdParams P) {
-  __shared__ WarpSmem smem[kWarps];
+// sums[c] = sum over the lanes of val[c], c in [c0, 9).  Every lane stores its values;
+// then g lanes per column (4 for up to 8 columns, 2 for 9) each add a chunk of rows in
+// row order, and the chunks are combined by a fixed shuffle tree.  Fewer instructions
+// than one 5-step butterfly per column; the order is fixed, so results are reproducible.
+__device__ __forceinline__ void col_sums(LsqSmem &S, const double (&val)[9], int c0, int lane) {
+#pragma unroll
+  for (int c = 0; c < 9; ++c)
+    if (c >= c0) S.red[c][lane] = val[c];
+  __syncwarp();
+  const int ncol = 9 - c0;
+  const int g = ncol <= 8 ? 4 : 2;
+  const int rows = 32 / g;
+  const int col = c0 + lane / g, chunk = lane % g;
+  double t = 0.0;
+  if (col < 9) {
+    const double *r = &S.red[col][chunk * rows];
+    for (int q = 0; q < rows; ++q) t += r[q];
+  }
+  for (int o = 1; o < g; o <<= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if (col < 9 && chunk == 0) S.sums[col] = t;
+  __syncwarp();
+}
+
+// Phase 1, one warp per cell: the neighbour search and the reference's sort; the first lm
+// candidates go to st_idx.  A cell whose search fails raises its flag and gets its own
+// index in every slot, so that phase 2 stays in bounds (the step then fails).
+__global__ void __launch_bounds__(32 * kSearchWarps) gfd_search(GfdParams P) {
+  __shared__ WarpSmem smem[kSearchWarps];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   WarpSmem &S = smem[w];
   const int lm = P.lm;
-  for (int i0 = blockIdx.x * kWarps + w; i0 < P.m; i0 += gridDim.x * kWarps) {
+  for (int i0 = blockIdx.x * kSearchWarps + w; i0 < P.m; i0 += gridDim.x * kSearchWarps) {
     int nn[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     bool ok = true;   // false once a bucket overflowed
     bool few = false; // true when 5 expansions did not reach lm candidates
@@ -314,12 +348,10 @@ __global__ void __launch_bounds__(32 * kWarps) gfd_stencil(GfdParams P) {
 #pragma unroll
       for (int o = 0; o < 8; ++o) l += nn[o];
     }
-    if (few) {
-      if (lane == 0) atomicOr(P.err, DERR_STENCIL_FEW);
-      continue;
-    }
-    if (!ok || l > P.sort_cap) {
-      if (lane == 0) atomicOr(P.err, DERR_STENCIL_MANY);
+    if (few || !ok || l > P.sort_cap) {
+      if (lane == 0) atomicOr(P.err, few ? DERR_STENCIL_FEW : DERR_STENCIL_MANY);
+      if (lane < lm) P.st_idx[(size_t)i0 * lm + lane] = i0;
+      __syncwarp();
       continue;
     }
     // ---- sorting (solver.cpp:553-569) ----
@@ -368,9 +400,22 @@ __global__ void __launch_bounds__(32 * kWarps) gfd_stencil(GfdParams P) {
       aquicksort(S.ldist, S.lidx, 0, l - 1, lm);
     }
     __syncwarp();
+    if (lane < lm) P.st_idx[(size_t)i0 * lm + lane] = S.lidx[lane];
+    __syncwarp();
+  }
+}
+
+// Phase 2, one warp per cell: weights, the weighted monomial system, its FP64 Householder
+// QR, the operator X and the matrix rows, from the stencil of phase 1.
+__global__ void __launch_bounds__(32 * kWarps, 4) gfd_lsq(GfdParams P) {
+  __shared__ LsqSmem smem[kWarps];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  LsqSmem &S = smem[w];
+  const int lm = P.lm;
+  for (int i0 = blockIdx.x * kWarps + w; i0 < P.m; i0 += gridDim.x * kWarps) {
     // ---- weights and weighted monomials (solver.cpp:75-103) ----
     const bool act = lane < lm;
-    const int mj = act ? S.lidx[lane] : i0;
+    const int mj = act ? P.st_idx[(size_t)i0 * lm + lane] : i0;
     double wx, wy, wz;
     offset_of(P, mj, i0, wx, wy, wz);
     const double dist = act ? sqrt(sq3(wx, wy, wz)) : 0.0;
@@ -405,10 +450,15 @@ __global__ void __launch_bounds__(32 * kWarps) gfd_stencil(GfdParams P) {
       v[k] = lane >= k ? vr : 0.0;
       if (lane == k) b[k] = beta;
       if (beta == 0.0) rank_ok = false;
+      if (k < 8) {
+        double pv[9];
 #pragma unroll
-      for (int c = k + 1; c < 9; ++c) {
-        const double s = warp_sum(v[k] * b[c]);
-        if (lane >= k) b[c] = b[c] + v[k] * (-tk * s);
+        for (int c = 0; c < 9; ++c) pv[c] = c > k ? v[k] * b[c] : 0.0;
+        col_sums(S, pv, k + 1, lane);
+#pragma unroll
+        for (int c = k + 1; c < 9; ++c)
+          if (lane >= k) b[c] = b[c] + v[k] * (-tk * S.sums[c]);
+        __syncwarp();
       }
     }
     if (!rank_ok) {
@@ -425,11 +475,13 @@ __global__ void __launch_bounds__(32 * kWarps) gfd_stencil(GfdParams P) {
     for (int c = 0; c < 9; ++c) q[c] = (lane == c) ? 1.0 : 0.0;
 #pragma unroll
     for (int k = 8; k >= 0; --k) {
+      double pv[9];
 #pragma unroll
-      for (int c = k; c < 9; ++c) {
-        const double s = warp_sum(v[k] * q[c]);
-        q[c] = q[c] - tau[k] * v[k] * s;
-      }
+      for (int c = 0; c < 9; ++c) pv[c] = c >= k ? v[k] * q[c] : 0.0;
+      col_sums(S, pv, k, lane);
+#pragma unroll
+      for (int c = k; c < 9; ++c) q[c] = q[c] - tau[k] * v[k] * S.sums[c];
+      __syncwarp();
     }
     __syncwarp();
     // ---- X(:, j) = w_j R^-1 Q1(j, :)^T, lane j ----
@@ -445,7 +497,6 @@ __global__ void __launch_bounds__(32 * kWarps) gfd_stencil(GfdParams P) {
     if (act) {
 #pragma unroll
       for (int k = 0; k < 9; ++k) X[k * lm + lane] = weight * y[k];
-      P.st_idx[(size_t)i0 * lm + lane] = mj;
       P.st_dist[(size_t)i0 * lm + lane] = dist;
     }
     // ---- rows of A1, A2 and the density rhs (solver.cpp:116-172) ----
@@ -610,11 +661,13 @@ int apc_gfd_assemble(apc_context *c, double c_dens) {
   P.ell_col = c->ell_col; P.a1 = c->a1; P.a2 = c->a2; P.rhs = c->rhs;
   P.ld = ld;
   P.err = c->d_err;
+  const int sblocks = std::max(1, std::min((M + kSearchWarps - 1) / kSearchWarps, apc_sm_count(c) * 32));
   const int blocks = std::max(1, std::min((M + kWarps - 1) / kWarps, apc_sm_count(c) * 16));
   APC_CUDA_TRY(c, cudaEventRecord(c->gev[0], c->s));
-  gfd_stencil<<<blocks, 32 * kWarps, 0, c->s>>>(P);
+  gfd_search<<<sblocks, 32 * kSearchWarps, 0, c->s>>>(P);
+  gfd_lsq<<<blocks, 32 * kWarps, 0, c->s>>>(P);
   APC_CUDA_TRY(c, cudaEventRecord(c->gev[1], c->s));
-  apc_count_launch(c);
+  apc_count_launch(c, 2);
   APC_CUDA_TRY(c, cudaGetLastError());
   int derr = 0;
   APC_TRY(apc_read_errors(c, &derr));
