@@ -106,6 +106,8 @@ struct apc_context {
   int *nb24 = nullptr;   // 24 per cell
   int *nnb = nullptr;    // Neigh24 count per cell
   int *cell_of = nullptr;  // sorted particle -> cell
+  double *gfd_scr_d = nullptr;  // GFD search: per-warp sort lists longer than a warp
+  int *gfd_scr_i = nullptr;
   double *adj_ckpt = nullptr, *adj_tape = nullptr;  // trajectory VJP: checkpoints, Hessian tape
   double last_c_pot = 0.0, last_c_field = 0.0;       // constants of the last apc_solve
   // solve VJP: transposed stencil pattern and matrices (ELL, leading dimension M)

@@ -49,6 +49,8 @@ struct GfdParams {
   const int *count, *type, *nb24, *nnb;
   int *st_idx;
   double *st_dist, *gx;
+  double *scr_d;  // per search warp: kListCap sort keys and indices (lists over 32)
+  int *scr_i;
   int *ell_col;
   double *a1, *a2, *rhs;
   size_t ld;  // ELL leading dimension (row capacity)
@@ -181,8 +183,6 @@ struct WarpSmem {
   int soff[32], sp[32];  // expansion ring: item offset and cell of each candidate
   int bidx[8][kBucketCap];
   double bd2[8][kBucketCap];
-  double ldist[kListCap];
-  int lidx[kListCap];
 };
 
 // least squares, per warp
@@ -384,23 +384,27 @@ __global__ void __launch_bounds__(32 * kSearchWarps) gfd_search(GfdParams P) {
         idx = S.bidx[b][e];
       }
       warp_aquicksort(key, idx, l, lm, lane);
-      if (lane < l) S.lidx[lane] = idx;
+      if (lane < lm) P.st_idx[(size_t)i0 * lm + lane] = idx;
     } else if (lane == 0) {
+      // longer lists: the reference's sequential sort by lane 0, on this warp's slice of
+      // a global scratch list
+      const size_t gw = (size_t)blockIdx.x * kSearchWarps + w;
+      double *ldist = P.scr_d + gw * kListCap;
+      int *lidx = P.scr_i + gw * kListCap;
       aquicksort(S.bd2[0], S.bidx[0], 0, nn[0] - 1, nn[0]);
       int k = 0;
       for (int b = 0; b < 8; ++b) {
         double penalty = 1.0;
         for (int e = 0; e < nn[b]; ++e) {
-          S.lidx[k] = S.bidx[b][e];
-          S.ldist[k] = __dmul_rn(penalty, S.bd2[b][e]);
+          lidx[k] = S.bidx[b][e];
+          ldist[k] = __dmul_rn(penalty, S.bd2[b][e]);
           penalty = __dmul_rn(penalty, 10000.0);
           ++k;
         }
       }
-      aquicksort(S.ldist, S.lidx, 0, l - 1, lm);
+      aquicksort(ldist, lidx, 0, l - 1, lm);
+      for (int k = 0; k < lm; ++k) P.st_idx[(size_t)i0 * lm + k] = lidx[k];
     }
-    __syncwarp();
-    if (lane < lm) P.st_idx[(size_t)i0 * lm + lane] = S.lidx[lane];
     __syncwarp();
   }
 }
@@ -662,6 +666,10 @@ int apc_gfd_assemble(apc_context *c, double c_dens) {
   P.ld = ld;
   P.err = c->d_err;
   const int sblocks = std::max(1, std::min((M + kSearchWarps - 1) / kSearchWarps, apc_sm_count(c) * 32));
+  APC_TRY(apc_ensure(c, &c->gfd_scr_d, (size_t)sblocks * kSearchWarps * kListCap, nullptr));
+  APC_TRY(apc_ensure(c, &c->gfd_scr_i, (size_t)sblocks * kSearchWarps * kListCap, nullptr));
+  P.scr_d = c->gfd_scr_d;
+  P.scr_i = c->gfd_scr_i;
   const int blocks = std::max(1, std::min((M + kWarps - 1) / kWarps, apc_sm_count(c) * 16));
   APC_CUDA_TRY(c, cudaEventRecord(c->gev[0], c->s));
   gfd_search<<<sblocks, 32 * kSearchWarps, 0, c->s>>>(P);
