@@ -629,7 +629,10 @@ int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int 
   // cycles cheapest at 128^3), 30 without a preconditioner
   const bool use_mg = which == 1 && cfg.mixed_precond == APC_PRECOND_MULTIGRID;
   const int m32 = cfg.mixed_restart > 0 ? cfg.mixed_restart : (use_mg ? 16 : 30);
-  const double rtol_in = cfg.mixed_inner_rtol > 0 ? cfg.mixed_inner_rtol : 1e-5;
+  // inner tolerance: a correction gains only ~2-3 digits of the FP64 residual whatever its
+  // inner accuracy (the FP32 operator's rounding, ~cond(A) 6e-8, bounds it), so the
+  // multigrid cycles stop at 1e-3; the density solve keeps 1e-5
+  const double rtol_in = cfg.mixed_inner_rtol > 0 ? cfg.mixed_inner_rtol : (use_mg ? 1e-3 : 1e-5);
   int levels = 0;
   APC_TRY(apc_ir_solve(c, which, use_mg, val, af, b, x, k->r, m32, rtol_in, its, rnorm, reason, refinements,
                        &levels));

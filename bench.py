@@ -339,7 +339,7 @@ def run_ours(args) -> dict:
         "config": {"workload": workload_desc(cfg), "precision": "mixed", "parallelism": f"replicas x{ws}",
                    "l2": "flushed (512 MiB write) before every timed step",
                    "start_a": round(t_state, 6), "mixed_restart": args.mixed_restart or 16,
-                   "inner_rtol": args.inner_rtol or 1e-5},
+                   "inner_rtol": args.inner_rtol or 1e-3},
         "fp64": {"value": fp64_value, "ms_per_step": (fp64_ms / args.steps) if fp64_ms else None,
                  "speedup_mixed_over_fp64": (value / fp64_value) if fp64_value else None,
                  "potential_its": fp64_stats["potential_its"] if fp64_value else None,

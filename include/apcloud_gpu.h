@@ -78,7 +78,7 @@ typedef struct apc_config {
   int gmres_max_it;      /* -ksp_max_it */
   int precision;         /* apc_precision */
   int mixed_restart;     /* FP32 inner restart for APC_PREC_MIXED (0 = 16 with multigrid, 30 without) */
-  double mixed_inner_rtol; /* FP32 inner solve relative tolerance (0 = 1e-5) */
+  double mixed_inner_rtol; /* FP32 inner solve relative tolerance (0 = 1e-3 with multigrid, 1e-5 without) */
   int device;            /* CUDA device ordinal */
   int mixed_precond;     /* APC_PREC_MIXED potential solve: APC_PRECOND_JACOBI or APC_PRECOND_MULTIGRID */
   int mg_sweeps;         /* multigrid: Jacobi sweeps before and after each coarse correction (0 = 2) */
