@@ -130,15 +130,27 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist(const uint64_t *keys,
   hist[(size_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
-// stable scatter: within a tile, rank = (warp offset) + (earlier rows of the warp) +
-// (earlier lanes of the row with the same digit)
+// Stable scatter.  Within a tile, an item's rank among the tile's items of its digit is
+// (earlier warps' counts) + (earlier rows of its warp) + (earlier lanes of its row).  The
+// tile is first staged in shared memory in digit order, then written out by consecutive
+// threads, so each digit's run goes to consecutive global addresses (coalesced).
+struct ScatterSmem {
+  uint64_t key[kSortTile];
+  uint32_t val[kSortTile];
+  uint32_t wcount[kSortWarps][256];
+  uint32_t bstart[256];  // tile-local start of each digit
+  uint32_t goff[256];    // global start of each digit's run of this tile
+  uint32_t wsum[kSortWarps];
+};
+
 __global__ void __launch_bounds__(kSortThreads) radix_scatter(const uint64_t *keys_in,
                                                               const uint32_t *vals_in,
                                                               uint64_t *keys_out, uint32_t *vals_out,
                                                               int n, int shift, int nblocks,
                                                               const uint32_t *offsets) {
-  __shared__ uint32_t wcount[kSortWarps][256];
-  for (int k = threadIdx.x; k < kSortWarps * 256; k += kSortThreads) (&wcount[0][0])[k] = 0;
+  extern __shared__ __align__(16) unsigned char scatter_smem[];
+  ScatterSmem &S = *reinterpret_cast<ScatterSmem *>(scatter_smem);
+  for (int k = threadIdx.x; k < kSortWarps * 256; k += kSortThreads) (&S.wcount[0][0])[k] = 0;
   __syncthreads();
   const long long t0 = (long long)blockIdx.x * kSortTile;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -154,33 +166,55 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter(const uint64_t *ke
     vv[r] = ok ? vals_in[i] : 0u;
     unsigned d = ok ? (unsigned)((kk[r] >> shift) & 0xffu) : 256u;
     unsigned peers = __match_any_sync(0xffffffffu, d);
-    unsigned prior = ok ? wcount[warp][d] : 0u;
+    unsigned prior = ok ? S.wcount[warp][d] : 0u;
     rk[r] = prior + __popc(peers & lt);
     __syncwarp();
-    if (ok && lane == __ffs(peers) - 1) wcount[warp][d] = prior + __popc(peers);
+    if (ok && lane == __ffs(peers) - 1) S.wcount[warp][d] = prior + __popc(peers);
     __syncwarp();
   }
   __syncthreads();
   {
-    // per digit: global block offset, then the earlier warps of this block
+    // thread d: the tile's count of digit d and the earlier warps' counts; then the
+    // tile-local digit starts by a block exclusive scan over d
     const int d = threadIdx.x;
-    uint32_t run = offsets[(size_t)d * nblocks + blockIdx.x];
+    uint32_t run = 0;
     for (int w = 0; w < kSortWarps; ++w) {
-      uint32_t c = wcount[w][d];
-      wcount[w][d] = run;
+      const uint32_t c = S.wcount[w][d];
+      S.wcount[w][d] = run;
       run += c;
     }
+    uint32_t incl = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) S.wsum[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int w = 0; w < warp; ++w) before += S.wsum[w];
+    S.bstart[d] = before + incl - run;
+    S.goff[d] = offsets[(size_t)d * nblocks + blockIdx.x];
   }
   __syncthreads();
 #pragma unroll
   for (int r = 0; r < kSortRows; ++r) {
     long long i = t0 + (long long)warp * 32 * kSortRows + r * 32 + lane;
     if (i < n) {
-      unsigned d = (unsigned)((kk[r] >> shift) & 0xffu);
-      uint32_t pos = wcount[warp][d] + rk[r];
-      keys_out[pos] = kk[r];
-      vals_out[pos] = vv[r];
+      const unsigned d = (unsigned)((kk[r] >> shift) & 0xffu);
+      const uint32_t lp = S.bstart[d] + S.wcount[warp][d] + rk[r];
+      S.key[lp] = kk[r];
+      S.val[lp] = vv[r];
     }
+  }
+  __syncthreads();
+  const int cnt = (int)min((long long)kSortTile, (long long)n - t0);
+  for (int p = threadIdx.x; p < cnt; p += kSortThreads) {
+    const uint64_t k = S.key[p];
+    const unsigned d = (unsigned)((k >> shift) & 0xffu);
+    const uint32_t pos = S.goff[d] + ((uint32_t)p - S.bstart[d]);
+    keys_out[pos] = k;
+    vals_out[pos] = S.val[p];
   }
 }
 
@@ -210,10 +244,13 @@ int apc_radix_sort_u64(apc_context *c, uint64_t *keys, uint32_t *vals, uint64_t 
   APC_TRY(apc_ensure(c, &c->sort_hist, hn, nullptr));
   uint64_t *ki = keys, *ko = keys_alt;
   uint32_t *vi = vals, *vo = vals_alt;
+  APC_CUDA_TRY(c, cudaFuncSetAttribute(radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sizeof(ScatterSmem)));
   for (int shift = lo_bit; shift < hi_bit; shift += 8) {
     radix_hist<<<nblocks, kSortThreads, 0, c->s>>>(ki, n, shift, nblocks, c->sort_hist);
     APC_TRY(apc_exclusive_scan(c, (const int *)c->sort_hist, (int *)c->sort_hist, (int)hn, nullptr));
-    radix_scatter<<<nblocks, kSortThreads, 0, c->s>>>(ki, vi, ko, vo, n, shift, nblocks, c->sort_hist);
+    radix_scatter<<<nblocks, kSortThreads, sizeof(ScatterSmem), c->s>>>(ki, vi, ko, vo, n, shift, nblocks,
+                                                                        c->sort_hist);
     apc_count_launch(c, 2);
     APC_CUDA_TRY(c, cudaGetLastError());
     uint64_t *tk = ki; ki = ko; ko = tk;
