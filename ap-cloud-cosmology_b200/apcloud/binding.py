@@ -29,7 +29,7 @@ EXPORTED = [
     "apc_get_phase_times", "apc_get_profile", "apc_reset_profile", "apc_move_velocity_noalloc",
     "apc_batch_create", "apc_batch_destroy", "apc_batch_size", "apc_batch_context", "apc_batch_step",
     "apc_get_hessians_device", "apc_vjp_kick_drift", "apc_trajectory_vjp", "apc_fields_from_rhs",
-    "apc_solve_vjp",
+    "apc_solve_vjp", "apc_max_cell_density", "apc_adaptive_dt",
 ]
 
 
@@ -131,6 +131,8 @@ def load_library(path: str = LIB_PATH):
         "apc_batch_step": (C.c_int, [vp, C.POINTER(ApcStepParams), ip, vp, vp]),
         "apc_get_hessians_device": (C.c_int, [vp] + [vp] * 6),
         "apc_fields_from_rhs": (C.c_int, [vp, vp]),
+        "apc_max_cell_density": (C.c_int, [vp, C.POINTER(C.c_double)]),
+        "apc_adaptive_dt": (C.c_int, [vp, C.c_double, C.POINTER(C.c_double)]),
         "apc_solve_vjp": (C.c_int, [vp, vp, vp, vp, vp]),
         "apc_vjp_kick_drift": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.c_double, C.c_double,
                                          C.POINTER(C.c_void_p), vp]),
@@ -292,6 +294,16 @@ class GpuPath:
     def hessians_device(self, ptrs):
         self._check(self.lib.apc_get_hessians_device(self.h, *[C.c_void_p(p) for p in ptrs]),
                     "apc_get_hessians_device")
+
+    def max_cell_density(self) -> float:
+        v = C.c_double()
+        self._check(self.lib.apc_max_cell_density(self.h, C.byref(v)), "apc_max_cell_density")
+        return v.value
+
+    def adaptive_dt(self, delta_a: float) -> float:
+        v = C.c_double()
+        self._check(self.lib.apc_adaptive_dt(self.h, delta_a, C.byref(v)), "apc_adaptive_dt")
+        return v.value
 
     def fields_from_rhs(self, rhs_ptr: int):
         self._check(self.lib.apc_fields_from_rhs(self.h, C.c_void_p(rhs_ptr)), "apc_fields_from_rhs")

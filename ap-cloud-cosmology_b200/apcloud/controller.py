@@ -4,8 +4,8 @@ has the phase calls select / solve / move_velocity / move_position.
 The reference's call sequence is kept:
   - an initial select and a half drift;
   - per step: select, solve, kick(t), drift(t + dt/2), t += dt, with dt clipped to end_a;
-  - adaptive time stepping off (ADAPTIVE_TIME_STEP, apcloud_macro.h:25-27) and viewer
-    output off.
+  - adaptive time stepping (ADAPTIVE_TIME_STEP, apcloud_macro.h:25-27) off unless asked
+    for, and viewer output off.
 The constants follow the equations of the reference README (README.md:28-34):
   - drift F(a)/a^2 and kick F(a), F(a) = (Omega0/a + OmegaL a^2)^(-1/2);
   - C_pot = 3 Omega0 / (2a) and C_field = -1;
@@ -37,6 +37,7 @@ class Controller:
     end_a: float
     delta_a: float
     box_volume: float = 1.0
+    adaptive: bool = False  # ADAPTIVE_TIME_STEP (controller.cpp:146-164)
     t: float = field(init=False)
     log: list = field(default_factory=list)
 
@@ -58,12 +59,13 @@ class Controller:
         return not (self.t < self.end_a)
 
     def step(self) -> StepLog:
-        """One pass of controller.cpp:133-208."""
-        dt = self.delta_a
+        """One pass of controller.cpp:133-208: select, the step size (adaptive: from the
+        densest cell, controller.cpp:146-164), solve, kick, drift."""
+        m = self.backend.select()
+        dt = self.backend.adaptive_dt(self.delta_a) if self.adaptive else self.delta_a
         if self.t + dt > self.end_a:
             dt = self.end_a - self.t
         k = self.constants(self.t, dt)
-        m = self.backend.select()
         self.backend.solve(k["c_dens"], k["c_pot"], k["c_field"])
         dv = self.backend.move_velocity(dt, k["c_vel"])
         dx = self.backend.move_position(dt, k["c_pos"])
@@ -73,5 +75,6 @@ class Controller:
         return rec
 
 
-def for_config(backend, cfg: "ics.RunConfig") -> Controller:
-    return Controller(backend, cfg.n, cfg.omega0, cfg.omegal, cfg.a_start, cfg.a_end, cfg.delta_a)
+def for_config(backend, cfg: "ics.RunConfig", adaptive: bool = False) -> Controller:
+    return Controller(backend, cfg.n, cfg.omega0, cfg.omegal, cfg.a_start, cfg.a_end, cfg.delta_a,
+                      adaptive=adaptive)

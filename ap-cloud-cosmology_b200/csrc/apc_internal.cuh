@@ -174,6 +174,7 @@ int apc_potential_rhs(apc_context *c, double c_pot);    // gfd.cu
 int apc_differentiate(apc_context *c, double c_field);  // gfd.cu
 int apc_mover_velocity(apc_context *c, double dt, double c_vel, double *max_dv);  // mover.cu
 int apc_mover_position(apc_context *c, double dt, double c_pos, double *max_dx);  // mover.cu
+int apc_mover_max_density(apc_context *c, double *out);                           // mover.cu
 int apc_exclusive_scan(apc_context *c, const int *in, int *out, int n, int *total_dev);  // scan.cu
 int apc_radix_sort_u64(apc_context *c, uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
                        uint32_t *vals_alt, int n, int lo_bit, int hi_bit, bool *result_in_alt);

@@ -578,6 +578,26 @@ int apc_reset_profile(apc_context *c) {
   return APC_OK;
 }
 
+int apc_max_cell_density(apc_context *c, double *max_density) {
+  APC_TRY(check_ready(c, true, true, false));
+  if (!max_density) return APC_ERR_INVALID_ARG;
+  cudaSetDevice(c->dev);
+  return apc_mover_max_density(c, max_density);
+}
+
+int apc_adaptive_dt(apc_context *c, double delta_a, double *dt) {
+  if (!dt) return APC_ERR_INVALID_ARG;
+  double rho = 0.0;
+  APC_TRY(apc_max_cell_density(c, &rho));
+  // controller.cpp:157-162: dt = 0.05 Delta_A / max_density^(1/2), at most Delta_A
+  const double step = 0.05 * delta_a;
+  const double d = 1.0 / pow(rho, 1.0 / 2);
+  double v = step * d;
+  if (v > delta_a) v = delta_a;
+  *dt = v;
+  return APC_OK;
+}
+
 int apc_get_phase_times(apc_context *c, double *a, double *b, double *d) {
   if (!c) return APC_ERR_INVALID_ARG;
   if (a) *a = c->t_select_ms;

@@ -111,7 +111,35 @@ __global__ void __launch_bounds__(256) drift(int n, double *__restrict__ x, doub
   if (threadIdx.x == 0) atomic_max_nonneg(maxbits, mx);
 }
 
+// max over the cells of n_p / h / h / h, in the reference's operation order
+// (controller.cpp:150-156); values are non-negative, so atomicMax on the bits is exact
+__global__ void max_cell_density(int m, const int *__restrict__ count, const double *__restrict__ h,
+                                 unsigned long long *maxbits) {
+  double mx = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const double hi = h[i];
+    mx = fmax(mx, __ddiv_rn(__ddiv_rn(__ddiv_rn((double)count[i], hi), hi), hi));
+  }
+  mx = block_max(mx);
+  if (threadIdx.x == 0) atomic_max_nonneg(maxbits, mx);
+}
+
 }  // namespace
+
+int apc_mover_max_density(apc_context *c, double *out) {
+  const int m = c->nc + c->nv + c->nb;
+  unsigned long long *mb = (unsigned long long *)(c->counters + 104);
+  APC_CUDA_TRY(c, cudaMemsetAsync(mb, 0, sizeof(unsigned long long), c->s));
+  const int G = std::max(1, std::min((m + 255) / 256, apc_sm_count(c) * 8));
+  max_cell_density<<<G, 256, 0, c->s>>>(m, c->ccount, c->ch, mb);
+  apc_count_launch(c);
+  APC_CUDA_TRY(c, cudaGetLastError());
+  unsigned long long bits = 0;
+  APC_CUDA_TRY(c, cudaMemcpyAsync(&bits, mb, sizeof(bits), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  memcpy(out, &bits, sizeof(double));
+  return APC_OK;
+}
 
 int apc_mover_velocity(apc_context *c, double dt, double c_vel, double *max_dv) {
   const int n = c->n, M = c->nc + c->nv;

@@ -231,6 +231,13 @@ int apc_move_velocity_noalloc(int n_particles, int n_cells, const int *first, co
                               double *ay, double *az, double dt, double c_vel, double *max_dv,
                               void *stream);
 
+/* Adaptive time step (ADAPTIVE_TIME_STEP, controller.cpp:146-164), after apc_select:
+ * max_density = max over the cells of n_p / h^3, reduced on the device in the reference's
+ * operation order; dt = 0.05 delta_a / max_density^(1/2), at most delta_a (the caller
+ * still clips t + dt to the end time, controller.cpp:168-169). */
+int apc_max_cell_density(apc_context *ctx, double *max_density);
+int apc_adaptive_dt(apc_context *ctx, double delta_a, double *dt);
+
 /* Device time (ms) of the last select / solve / move phases, from CUDA events. */
 int apc_get_phase_times(apc_context *ctx, double *select_ms, double *solve_ms, double *move_ms);
 

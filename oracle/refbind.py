@@ -176,6 +176,18 @@ class CpuPath:
         self.f["last_matrix"](which, None, None, rp.ctypes.data, ci.ctypes.data, v.ctypes.data)
         return rp, ci, v
 
+    def max_cell_density(self) -> float:
+        """max n_p / h / h / h over the cells (controller.cpp:150-156), as the reference."""
+        c = self.cells()
+        return float(np.max(c.count.astype(np.float64) / c.h / c.h / c.h))
+
+    def adaptive_dt(self, delta_a: float) -> float:
+        """controller.cpp:157-162."""
+        import math
+
+        v = 0.05 * delta_a * (1.0 / math.pow(self.max_cell_density(), 1.0 / 2))
+        return delta_a if v > delta_a else v
+
     def move_velocity(self, dt: float, c_vel: float) -> float:
         return self.f["move_velocity"](self.h, dt, c_vel)
 

@@ -240,3 +240,30 @@ def test_full_size_lcdm128_properties(gpu_lib):
     assert res["fp64"][1] == res["mixed"][1] == res["ref"][1]
     assert np.all(np.isfinite(res["fp64"][0])) and np.all(np.isfinite(res["mixed"][0]))
     assert _acc_rms(list(res["mixed"][0]), list(res["ref"][0])) <= MIXED_ACC_RMS
+
+
+def test_adaptive_time_step_vs_oracle(gpu_lib, oracle_lib):
+    """ADAPTIVE_TIME_STEP (controller.cpp:146-164): the densest cell's n_p/h^3, reduced on
+    the device, equals the oracle's bit for bit, and so does dt; three adaptive steps keep
+    the trajectories together."""
+    import refbind
+
+    cfg = ics.config("ball32k", n=6000, seed=321, steps=20)
+    p = cfg.particles()
+    o = refbind.CpuPath("oracle", p, cfg.depth, cfg.gfd_c)
+    o.set_gmres(30, 1e-10)
+    gp = binding.GpuPath(p, cfg.depth, cfg.gfd_c)
+    co, cg = for_config(o, cfg, adaptive=True), for_config(gp, cfg, adaptive=True)
+    co.start()
+    cg.start()
+    for _ in range(3):
+        ro, rg = co.step(), cg.step()
+        assert gp.max_cell_density() == o.max_cell_density()
+        assert rg.dt == ro.dt and rg.dt < cfg.delta_a
+    po, pg = o.particles(), gp.particles()
+    for k in range(3):
+        d = pg[k] - po[k]
+        d -= np.round(d)
+        assert np.max(np.abs(d)) <= 1e-11
+    o.close()
+    gp.close()
