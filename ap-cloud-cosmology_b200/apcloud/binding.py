@@ -29,7 +29,7 @@ EXPORTED = [
     "apc_get_phase_times", "apc_get_profile", "apc_reset_profile", "apc_move_velocity_noalloc",
     "apc_batch_create", "apc_batch_destroy", "apc_batch_size", "apc_batch_context", "apc_batch_step",
     "apc_get_hessians_device", "apc_vjp_kick_drift", "apc_trajectory_vjp", "apc_fields_from_rhs",
-    "apc_solve_vjp", "apc_max_cell_density", "apc_adaptive_dt",
+    "apc_solve_vjp", "apc_max_cell_density", "apc_adaptive_dt", "apc_config_from_options",
 ]
 
 
@@ -132,6 +132,7 @@ def load_library(path: str = LIB_PATH):
         "apc_get_hessians_device": (C.c_int, [vp] + [vp] * 6),
         "apc_fields_from_rhs": (C.c_int, [vp, vp]),
         "apc_max_cell_density": (C.c_int, [vp, C.POINTER(C.c_double)]),
+        "apc_config_from_options": (C.c_int, [C.POINTER(ApcConfig), C.c_int, C.POINTER(C.c_char_p)]),
         "apc_adaptive_dt": (C.c_int, [vp, C.c_double, C.POINTER(C.c_double)]),
         "apc_solve_vjp": (C.c_int, [vp, vp, vp, vp, vp]),
         "apc_vjp_kick_drift": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.c_double, C.c_double,

@@ -38,6 +38,8 @@ class Controller:
     delta_a: float
     box_volume: float = 1.0
     adaptive: bool = False  # ADAPTIVE_TIME_STEP (controller.cpp:146-164)
+    output_dir: str | None = None  # VTK snapshots (viewer.cpp) every write_interval steps
+    write_interval: int = 0
     t: float = field(init=False)
     log: list = field(default_factory=list)
 
@@ -60,7 +62,11 @@ class Controller:
 
     def step(self) -> StepLog:
         """One pass of controller.cpp:133-208: select, the step size (adaptive: from the
-        densest cell, controller.cpp:146-164), solve, kick, drift."""
+        densest cell, controller.cpp:146-164), solve, kick, drift.  With an output
+        directory, snapshots are written first every write_interval steps
+        (controller.cpp:136-146)."""
+        if self.output_dir and self.write_interval > 0 and len(self.log) % self.write_interval == 0:
+            self.snapshot()
         m = self.backend.select()
         dt = self.backend.adaptive_dt(self.delta_a) if self.adaptive else self.delta_a
         if self.t + dt > self.end_a:
@@ -73,6 +79,16 @@ class Controller:
         self.log.append(rec)
         self.t += dt
         return rec
+
+
+    def snapshot(self) -> None:
+        """physical_<t>.vtk, and computational_<t>.vtk once a solve has run (viewer.cpp)."""
+        from . import vtk
+
+        p = self.backend.particles()
+        vtk.write_physical(self.output_dir, self.t, *p[:9])
+        if self.log:
+            vtk.write_computational(self.output_dir, self.t, self.backend.cells(), self.backend.fields())
 
 
 def for_config(backend, cfg: "ics.RunConfig", adaptive: bool = False) -> Controller:

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <unordered_map>
 #include <vector>
@@ -575,6 +576,45 @@ int apc_get_profile(apc_context *c, apc_profile *out) {
 int apc_reset_profile(apc_context *c) {
   if (!c) return APC_ERR_INVALID_ARG;
   c->prof = apc_profile{};
+  return APC_OK;
+}
+
+int apc_config_from_options(apc_config *cfg, int argc, const char *const *argv) {
+  // the KSP options of the reference's run lines (Makefile:30-32) reach both solves
+  // through KSPSetFromOptions (solver.cpp:202, 275)
+  if (!cfg || argc < 0 || (argc > 0 && !argv)) return APC_ERR_INVALID_ARG;
+  for (int i = 0; i < argc; ++i) {
+    const char *a = argv[i];
+    if (!a || a[0] != '-') continue;
+    const bool has = i + 1 < argc && argv[i + 1];
+    auto num = [&](double *out) {
+      if (!has) return false;
+      char *end = nullptr;
+      const double v = strtod(argv[i + 1], &end);
+      if (!end || *end != '\0') return false;
+      *out = v;
+      ++i;
+      return true;
+    };
+    double v = 0.0;
+    if (!strcmp(a, "-ksp_gmres_restart")) {
+      if (!num(&v) || v != (int)v) return APC_ERR_INVALID_ARG;
+      if (v < 1 || v > 31) return APC_ERR_UNSUPPORTED;  // the GMRES kernels hold <= 31 basis vectors
+      cfg->gmres_restart = (int)v;
+    } else if (!strcmp(a, "-ksp_rtol")) {
+      if (!num(&v)) return APC_ERR_INVALID_ARG;
+      cfg->gmres_rtol = v;
+    } else if (!strcmp(a, "-ksp_atol")) {
+      if (!num(&v)) return APC_ERR_INVALID_ARG;
+      cfg->gmres_atol = v;
+    } else if (!strcmp(a, "-ksp_divtol")) {
+      if (!num(&v)) return APC_ERR_INVALID_ARG;
+      cfg->gmres_dtol = v;
+    } else if (!strcmp(a, "-ksp_max_it")) {
+      if (!num(&v) || v != (int)v || v < 1) return APC_ERR_INVALID_ARG;
+      cfg->gmres_max_it = (int)v;
+    }
+  }
   return APC_OK;
 }
 

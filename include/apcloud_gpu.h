@@ -231,6 +231,13 @@ int apc_move_velocity_noalloc(int n_particles, int n_cells, const int *first, co
                               double *ay, double *az, double dt, double c_vel, double *max_dv,
                               void *stream);
 
+/* Apply the PETSc KSP command-line options that the reference's runs pass to both solves
+ * (KSPSetFromOptions, solver.cpp:202, 275; run lines in Makefile:30-32): -ksp_gmres_restart,
+ * -ksp_rtol, -ksp_atol, -ksp_divtol, -ksp_max_it.  Other arguments are ignored, as PETSc
+ * ignores options it does not use.  A restart above 31 returns APC_ERR_UNSUPPORTED (the
+ * GMRES kernels keep at most 31 basis vectors); a malformed value APC_ERR_INVALID_ARG. */
+int apc_config_from_options(apc_config *cfg, int argc, const char *const *argv);
+
 /* Adaptive time step (ADAPTIVE_TIME_STEP, controller.cpp:146-164), after apc_select:
  * max_density = max over the cells of n_p / h^3, reduced on the device in the reference's
  * operation order; dt = 0.05 delta_a / max_density^(1/2), at most delta_a (the caller

@@ -76,3 +76,24 @@ def test_library_is_built_for_sm100a(gpu_lib):
     if out.returncode != 0:
         pytest.skip("cuobjdump unavailable")
     assert "sm_100a" in out.stdout
+
+
+def test_petsc_ksp_options(gpu_lib):
+    """The reference's run-line options (Makefile:30-32) map onto the GMRES settings."""
+    from apcloud import binding
+
+    lib = binding.load_library(gpu_lib)
+    cfg = binding.ApcConfig()
+    lib.apc_config_default(C.byref(cfg))
+
+    def apply(*args):
+        arr = (C.c_char_p * len(args))(*[a.encode() for a in args])
+        return lib.apc_config_from_options(C.byref(cfg), len(args), arr)
+
+    assert apply("./run", "parameter.param", "-ksp_gmres_restart", "20", "-ksp_max_it", "1000",
+                 "-ksp_atol", "1.e-60", "-ksp_rtol", "1e-8", "-ksp_monitor") == 0
+    assert (cfg.gmres_restart, cfg.gmres_max_it) == (20, 1000)
+    assert cfg.gmres_atol == pytest.approx(1e-60) and cfg.gmres_rtol == pytest.approx(1e-8)
+    assert apply("-ksp_gmres_restart", "200") == -9  # APC_ERR_UNSUPPORTED
+    assert cfg.gmres_restart == 20
+    assert apply("-ksp_max_it", "abc") == -1
