@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libapcloud_gpu.so")
 SOURCES = ["capi.cu", "scan_sort.cu", "octree_build.cu", "selection.cu", "gfd.cu", "krylov.cu", "mover.cu",
-           "noalloc.cu", "mg.cu", "batch.cu", "adjoint.cu"]
+           "noalloc.cu", "mg.cu", "batch.cu", "adjoint.cu", "warmstart.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

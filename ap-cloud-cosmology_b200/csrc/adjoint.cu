@@ -346,6 +346,14 @@ int apc_trajectory_vjp(apc_context *c, const apc_trajectory *t, const double *co
   for (int k = 0; k < 6; ++k)
     if (!state0[k] || !cot[k]) return APC_ERR_INVALID_ARG;
   cudaSetDevice(c->dev);
+  // cold starts in both passes: a warm start would make each segment's rerun depend on
+  // the solve that ran before it, and the rerun must repeat the forward run exactly
+  struct WarmOff {
+    apc_context *c;
+    int saved;
+    ~WarmOff() { c->cfg.warm_start = saved; }
+  } warm_off{c, c->cfg.warm_start};
+  c->cfg.warm_start = 0;
   const int n = c->n, K = t->n_steps, every = std::min(std::max(1, t->checkpoint_every), std::max(1, K));
   const int nseg = K > 0 ? (K + every - 1) / every : 0;
   const size_t nn = (size_t)n;

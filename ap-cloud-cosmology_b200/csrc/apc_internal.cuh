@@ -110,6 +110,9 @@ struct apc_context {
   int *gfd_scr_i = nullptr;
   double *adj_ckpt = nullptr, *adj_tape = nullptr;  // trajectory VJP: checkpoints, Hessian tape
   double last_c_pot = 0.0, last_c_field = 0.0;       // constants of the last apc_solve
+  uint64_t *warm_keys = nullptr;      // warm start: codes of the previous step's cells (hash)
+  double *warm_rho = nullptr, *warm_phi = nullptr;
+  int warm_cap = 0;
   // solve VJP: transposed stencil pattern and matrices (ELL, leading dimension M)
   int *tr_cnt = nullptr, *tr_off = nullptr, *tr_cur = nullptr, *tr_tmp = nullptr;
   int *tp_col = nullptr, *tp_src = nullptr, *ta_col = nullptr, *ta_src = nullptr;
@@ -170,6 +173,8 @@ void apc_mg_free(apc_context *c);
 int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, const float *valf, const double *b,
                  double *x, double *r, int restart, double rtol_in, int *its, double *rnorm, int *reason,
                  int *refinements, int *levels);
+int apc_warm_save(apc_context *c);                       // warmstart.cu
+int apc_warm_guess(apc_context *c, int which, double *x);
 int apc_potential_rhs(apc_context *c, double c_pot);    // gfd.cu
 int apc_differentiate(apc_context *c, double c_field);  // gfd.cu
 int apc_mover_velocity(apc_context *c, double dt, double c_vel, double *max_dv);  // mover.cu

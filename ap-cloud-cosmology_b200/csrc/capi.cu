@@ -87,7 +87,8 @@ void free_all(apc_context *c) {
                   c->d_err, c->scan_tmp, c->flags, c->cx, c->cy, c->cz, c->ch, c->cfirst, c->ccount,
                   c->ctype, c->ccode, c->nb24, c->nnb, c->cell_of, c->st_idx, c->st_dist, c->gfd_x,
                   c->ell_col, c->a1, c->a2, c->a1f, c->a2f, c->rhs, c->bcrhs, c->density, c->potential,
-                  c->deriv, c->adj_ckpt, c->adj_tape, c->gfd_scr_d, c->gfd_scr_i, c->tr_cnt, c->tr_off, c->tr_cur, c->tr_tmp,
+                  c->deriv, c->adj_ckpt, c->adj_tape, c->gfd_scr_d, c->gfd_scr_i, c->warm_keys, c->warm_rho,
+                  c->warm_phi, c->tr_cnt, c->tr_off, c->tr_cur, c->tr_tmp,
                   c->tp_col, c->tp_src, c->ta_col, c->ta_src, c->ta_val, c->vjp_c, c->vjp_phi, c->vjp_r2,
                   c->vjp_rho};
   for (void *p : ptrs)
@@ -155,6 +156,7 @@ void apc_config_default(apc_config *cfg) {
   cfg->mg_omega = 0.0;
   cfg->mg_alpha = 0.0;
   cfg->mg_reorth = 0;
+  cfg->warm_start = 0;
 }
 
 const char *apc_status_string(int s) {
@@ -282,6 +284,7 @@ static int set_particles_impl(apc_context *c, const double *const *src, cudaMemc
   c->have_particles = true;
   c->have_cells = false;
   c->have_fields = false;
+  c->warm_cap = 0;  // a new particle set: no guess from the previous one
   return APC_OK;
 }
 
@@ -375,6 +378,7 @@ int apc_solve(apc_context *c, double c_dens, double c_pot, double c_field) {
                            &st.potential_reason, &st.potential_refinements));
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[7], c->s));
   APC_TRY(apc_differentiate(c, c_field));
+  if (c->cfg.precision == APC_PREC_MIXED && c->cfg.warm_start) APC_TRY(apc_warm_save(c));
   c->last_c_pot = c_pot;
   c->last_c_field = c_field;
   (void)M;

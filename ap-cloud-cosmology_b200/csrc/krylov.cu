@@ -623,8 +623,13 @@ int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int 
   const int G = std::max(1, std::min((n + 255) / 256, std::min(apc_sm_count(c) * 8, 4096)));
   ell_to_f32_scaled<<<std::min<size_t>((ell_count + 255) / 256, 8192), 256, 0, c->s>>>((size_t)c->m_cap, c->ell_w,
                                                                                        n, val, af);
-  zero_f64<<<G, 256, 0, c->s>>>(n, x);
-  apc_count_launch(c, 2);
+  apc_count_launch(c);
+  if (cfg.warm_start) {
+    APC_TRY(apc_warm_guess(c, which, x));
+  } else {
+    zero_f64<<<G, 256, 0, c->s>>>(n, x);
+    apc_count_launch(c);
+  }
   // inner restart: 16 for the multigrid FGMRES (a V-cycle per iteration makes short
   // cycles cheapest at 128^3), 30 without a preconditioner
   const bool use_mg = which == 1 && cfg.mixed_precond == APC_PRECOND_MULTIGRID;

@@ -302,6 +302,7 @@ struct IrState {
   int it;         // iteration of the current FGMRES cycle
   double rn;      // ||D^-1 (b - A x)|| of the current iterate
   double rn0, ttol;
+  double bnorm;   // ||D^-1 b||: the stopping test's scale, whatever the initial guess
   double rtol, atol, dtol, rtol_in;
   int max_it, max_outer, M, inner_max;
   double beta;    // ||v_0|| of the current cycle
@@ -594,12 +595,12 @@ __global__ void __launch_bounds__(kT) ir_residual(int n, int w, size_t ld, const
   if (threadIdx.x != 0) return;
   const double rn = sqrt(__ldcg(tmp));
   if (S->outer == 0) {
-    S->ttol = fmax(S->rtol * rn, S->atol);
-    S->rn0 = rn;
+    S->ttol = fmax(S->rtol * S->bnorm, S->atol);
+    S->rn0 = S->bnorm;
   }
   int reason = 0;
   bool stop = true;
-  if (S->outer == 0 && rn == 0.0) reason = kConvergedAtol;
+  if (S->outer == 0 && S->bnorm == 0.0) reason = kConvergedAtol;
   else if (!(rn == rn)) reason = kDivergedNanOrInf;
   else if (rn <= S->ttol) reason = rn < S->atol ? kConvergedAtol : kConvergedRtol;
   else if (rn >= S->dtol * S->rn0) reason = kDivergedDtol;
@@ -609,6 +610,22 @@ __global__ void __launch_bounds__(kT) ir_residual(int n, int w, size_t ld, const
   S->rn = rn;
   S->reason = reason;
   cudaGraphSetConditional(cond, stop ? 0u : 1u);
+}
+
+// ||D^-1 b|| into the state (last block)
+__global__ void __launch_bounds__(kT) ir_bnorm(int n, const double *__restrict__ val, const double *__restrict__ b,
+                                                IrState *S, double *partial, unsigned *counter, double *tmp) {
+  double nrm = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double d = val[i];
+    const double pb = (d == 0.0 ? 1.0 : 1.0 / d) * b[i];
+    nrm += pb * pb;
+  }
+  block_partial1(nrm, partial);
+  if (!last_block_arrived(counter)) return;
+  finish_sums(1, partial, counter, tmp);
+  __syncthreads();
+  if (threadIdx.x == 0) S->bnorm = sqrt(__ldcg(tmp));
 }
 
 // v_0 = D^-1 r / ||D^-1 r|| rounded to FP32, and beta = ||v_0||; the last block opens
@@ -819,8 +836,10 @@ void apc_mg_free(apc_context *c) {
 }
 
 static int read_int(apc_context *c, const int *dev, int *host) {
-  APC_CUDA_TRY(c, cudaMemcpyAsync(host, dev, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+  // through the context's pinned word: a pageable destination would be staged
+  APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 10, dev, sizeof(int), cudaMemcpyDeviceToHost, c->s));
   APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  *host = c->h_pinned[10];
   return APC_OK;
 }
 
@@ -896,9 +915,11 @@ static int mg_build(apc_context *c) {
                             m->uval, c->d_err);
     max_int<<<grid_for(nc, 256), kT, 0, c->s>>>(nc, m->rowstart, m->total);
     apc_count_launch(c, 2);
-    int wc = 0, derr = 0;
-    APC_TRY(read_int(c, m->total, &wc));
-    APC_TRY(apc_read_errors(c, &derr));
+    // the row width and the error flags in one round trip
+    APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 8, m->total, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+    APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 9, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+    APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+    const int wc = c->h_pinned[8], derr = c->h_pinned[9];
     if (derr & DERR_STENCIL_MANY) {
       c->err = "multigrid coarse row exceeds its buffers";
       return APC_ERR_UNSUPPORTED;
@@ -1129,6 +1150,7 @@ static int capture_solve(apc_context *c, const IrSolveArgs &a) {
   if (ok(cudaStreamGetCaptureInfo(s, &st, nullptr, &top, nullptr, nullptr)) &&
       ok(cudaGraphConditionalHandleCreate(&cond_out, top, 0, 0))) {
     ir_init<<<1, 1, 0, s>>>(m->state, a.rtol, a.atol, a.dtol, a.rtol_in, a.max_it, a.max_outer, a.M);
+    ir_bnorm<<<G, kT, 0, s>>>(n, a.val, a.b, m->state, m->partial, m->counter, tmp);
     ir_residual<<<G, kT, 0, s>>>(n, a.w, a.ld, a.col, a.val, a.b, a.x, a.r, m->state, m->partial, m->counter, tmp,
                                  cond_out);
     if (ok(cudaGetLastError()) && ok(add_while(s, cond_out, &body_out)) &&
@@ -1278,7 +1300,7 @@ int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, cons
   *refinements = S.outer;
   *levels = use_mg ? m->nlev : 0;
   const int per_it = (int)m->vcycle_nodes[which] + 3 + (cfg.mg_reorth != 0 ? 1 : 0);
-  apc_count_launch(c, 2 + 6 * S.outer + per_it * S.total_its);
+  apc_count_launch(c, 3 + 6 * S.outer + per_it * S.total_its);
   if (use_mg) {
     c->prof.mg_solve_ms += ms;
     c->prof.mg_iterations += S.total_its;

@@ -134,10 +134,10 @@ int apc_mover_max_density(apc_context *c, double *out) {
   max_cell_density<<<G, 256, 0, c->s>>>(m, c->ccount, c->ch, mb);
   apc_count_launch(c);
   APC_CUDA_TRY(c, cudaGetLastError());
-  unsigned long long bits = 0;
-  APC_CUDA_TRY(c, cudaMemcpyAsync(&bits, mb, sizeof(bits), cudaMemcpyDeviceToHost, c->s));
+  unsigned long long *hb = (unsigned long long *)(c->h_pinned + 12);  // pinned, 8-byte aligned
+  APC_CUDA_TRY(c, cudaMemcpyAsync(hb, mb, sizeof(*hb), cudaMemcpyDeviceToHost, c->s));
   APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
-  memcpy(out, &bits, sizeof(double));
+  memcpy(out, hb, sizeof(double));
   return APC_OK;
 }
 
@@ -163,11 +163,11 @@ int apc_mover_velocity(apc_context *c, double dt, double c_vel, double *max_dv) 
     return APC_ERR_CUDA;
   }
   if (max_dv) {
-    unsigned long long bits = 0;
-    APC_CUDA_TRY(c, cudaMemcpyAsync(&bits, mb, sizeof(bits), cudaMemcpyDeviceToHost, c->s));
+    unsigned long long *hb = (unsigned long long *)(c->h_pinned + 12);  // pinned, 8-byte aligned
+    APC_CUDA_TRY(c, cudaMemcpyAsync(hb, mb, sizeof(*hb), cudaMemcpyDeviceToHost, c->s));
     APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
     double v;
-    memcpy(&v, &bits, sizeof(v));
+    memcpy(&v, hb, sizeof(v));
     *max_dv = std::sqrt(v);
   }
   return APC_OK;
@@ -184,11 +184,11 @@ int apc_mover_position(apc_context *c, double dt, double c_pos, double *max_dx) 
   apc_count_launch(c);
   APC_CUDA_TRY(c, cudaGetLastError());
   if (max_dx) {
-    unsigned long long bits = 0;
-    APC_CUDA_TRY(c, cudaMemcpyAsync(&bits, mb, sizeof(bits), cudaMemcpyDeviceToHost, c->s));
+    unsigned long long *hb = (unsigned long long *)(c->h_pinned + 12);  // pinned, 8-byte aligned
+    APC_CUDA_TRY(c, cudaMemcpyAsync(hb, mb, sizeof(*hb), cudaMemcpyDeviceToHost, c->s));
     APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
     double v;
-    memcpy(&v, &bits, sizeof(v));
+    memcpy(&v, hb, sizeof(v));
     *max_dx = std::sqrt(v);
   }
   return APC_OK;

@@ -85,6 +85,9 @@ typedef struct apc_config {
   double mg_omega;       /* multigrid: Jacobi damping (0 = 0.95) */
   double mg_alpha;       /* multigrid: coarse-correction over-scaling (0 = 1.8) */
   int mg_reorth;         /* multigrid FGMRES: 1 = classical Gram-Schmidt twice, 0 = once (default) */
+  int warm_start;        /* mixed path: start both solves from the previous step's solution at the
+                            same octree cells (1) or from zero (0, default); the stopping test stays
+                            rtol ||D^-1 b||.  At 128^3 and a < 0.1 it saves ~1 of 20 iterations */
 } apc_config;
 
 enum { APC_PRECOND_JACOBI = 0, APC_PRECOND_MULTIGRID = 1 };
