@@ -211,52 +211,6 @@ __global__ void jacobi_first(int n, const float *__restrict__ dinv, const float 
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = omega * dinv[i] * b[i];
 }
 
-__global__ void jacobi_sweep(int n, int w, size_t ld, const int *__restrict__ col, const float *__restrict__ val,
-                             const float *__restrict__ dinv, const float *__restrict__ b,
-                             const float *__restrict__ xin, float omega, float *__restrict__ xout) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    float s = 0.f;
-#pragma unroll 6
-    for (int k = 0; k < w; ++k) {
-      const size_t at = (size_t)k * ld + i;
-      s += val[at] * xin[col[at]];
-    }
-    xout[i] = xin[i] + omega * dinv[i] * (b[i] - s);
-  }
-}
-
-// Two damped Jacobi sweeps from x = 0 in one pass: x1 = omega D^-1 b is formed on the fly
-// at the row and at its neighbours, x2 = x1 + omega D^-1 (b - A x1).
-__global__ void jacobi_first2(int n, int w, size_t ld, const int *__restrict__ col, const float *__restrict__ val,
-                              const float *__restrict__ dinv, const float *__restrict__ b, float omega,
-                              float *__restrict__ xout) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    float s = 0.f;
-#pragma unroll 6
-    for (int k = 0; k < w; ++k) {
-      const size_t at = (size_t)k * ld + i;
-      const int j = col[at];
-      s += val[at] * (omega * dinv[j] * b[j]);
-    }
-    const float x1 = omega * dinv[i] * b[i];
-    xout[i] = x1 + omega * dinv[i] * (b[i] - s);
-  }
-}
-
-// r = b - A x, one thread per row
-__global__ void residual_f32(int n, int w, size_t ld, const int *__restrict__ col, const float *__restrict__ val,
-                             const float *__restrict__ b, const float *__restrict__ x, float *__restrict__ r) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    float s = 0.f;
-#pragma unroll 6
-    for (int k = 0; k < w; ++k) {
-      const size_t at = (size_t)k * ld + i;
-      s += val[at] * x[col[at]];
-    }
-    r[i] = b[i] - s;
-  }
-}
-
 // b_c[I] = sum of r over the members of I, in member order
 __global__ void restrict_sum(int nc, const int *__restrict__ mptr, int nf, const int *__restrict__ mem,
                              const float *__restrict__ r, float *__restrict__ bc) {
@@ -268,22 +222,53 @@ __global__ void restrict_sum(int nc, const int *__restrict__ mptr, int nf, const
   }
 }
 
-// The first post-smoothing sweep with the coarse correction applied on the fly:
-// y = x + alpha P xc at the row and at its neighbours, out = y + omega D^-1 (b - A y).
-__global__ void prolong_sweep(int n, int w, size_t ld, const int *__restrict__ col, const float *__restrict__ val,
-                              const float *__restrict__ dinv, const float *__restrict__ b,
-                              const float *__restrict__ xin, const int *__restrict__ agg,
-                              const float *__restrict__ xc, float alpha, float omega, float *__restrict__ xout) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    float s = 0.f;
-#pragma unroll 6
-    for (int k = 0; k < w; ++k) {
-      const size_t at = (size_t)k * ld + i;
-      const int j = col[at];
-      s += val[at] * (xin[j] + alpha * xc[agg[j]]);
+// The row operations of the grid levels, with G lanes per row: coarse Galerkin rows are
+// 30-70 entries wide, and one thread per row would walk them serially.  The lanes of a
+// group take slots sub, sub + G, ... (the slot-major ELL keeps each slot's rows adjacent,
+// so a warp still reads whole sectors) and add their sums by a fixed shuffle tree.
+enum RowOp { kOpFirst2, kOpSweep, kOpResidual, kOpProlongSweep };
+
+template <int G, int OP>
+__global__ void __launch_bounds__(kT) row_op(int n, int w, size_t ld, const int *__restrict__ col,
+                                             const float *__restrict__ val, const float *__restrict__ dinv,
+                                             const float *__restrict__ b, const float *__restrict__ xin,
+                                             const int *__restrict__ agg, const float *__restrict__ xc, float alpha,
+                                             float omega, float *__restrict__ out) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int sub = (int)(tid % G);
+  const long long groups = ((long long)gridDim.x * blockDim.x) / G;
+  const long long rounds = (n + groups - 1) / groups;  // the same for every lane
+  for (long long rd = 0; rd < rounds; ++rd) {
+    const long long i = tid / G + rd * groups;
+    const bool act = i < n;
+    float sacc = 0.f;
+    if (act) {
+#pragma unroll 4
+      for (int k = sub; k < w; k += G) {
+        const size_t at = (size_t)k * ld + i;
+        const int j = col[at];
+        float xj;
+        if (OP == kOpFirst2) xj = omega * dinv[j] * b[j];
+        else if (OP == kOpProlongSweep) xj = xin[j] + alpha * xc[agg[j]];
+        else xj = xin[j];
+        sacc += val[at] * xj;
+      }
     }
-    const float y = xin[i] + alpha * xc[agg[i]];
-    xout[i] = y + omega * dinv[i] * (b[i] - s);
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
+    if (act && sub == 0) {
+      if (OP == kOpFirst2) {
+        const float x1 = omega * dinv[i] * b[i];
+        out[i] = x1 + omega * dinv[i] * (b[i] - sacc);
+      } else if (OP == kOpSweep) {
+        out[i] = xin[i] + omega * dinv[i] * (b[i] - sacc);
+      } else if (OP == kOpResidual) {
+        out[i] = b[i] - sacc;
+      } else {
+        const float y = xin[i] + alpha * xc[agg[i]];
+        out[i] = y + omega * dinv[i] * (b[i] - sacc);
+      }
+    }
   }
 }
 
@@ -670,7 +655,7 @@ constexpr int kTail = 1024;
 constexpr int kTailLevels = 12;
 
 struct TailLevel {
-  int n, w;
+  int n, w, g;  // g: lanes per row (power of two)
   size_t ld;
   const int *col;
   const float *val, *dinv;
@@ -686,15 +671,28 @@ struct TailArgs {
   float omega, alpha;
 };
 
-__device__ __forceinline__ void tail_sweep(const TailLevel &L, const float *xin, float *xout, float omega) {
-  for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
+// (A x)_i for every row of a tail level, L.g lanes per row; emit(i, sum) runs on the
+// group's first lane.  The trip count is the same for the whole block (shuffles).
+template <class F>
+__device__ __forceinline__ void tail_rows(const TailLevel &L, const float *xin, F emit) {
+  const int g = L.g, sub = threadIdx.x & (g - 1);
+  const int per = blockDim.x / g;
+  const int rounds = (L.n + per - 1) / per;
+  for (int rd = 0; rd < rounds; ++rd) {
+    const int i = (int)threadIdx.x / g + rd * per;
     float sacc = 0.f;
-    for (int k = 0; k < L.w; ++k) {
-      const size_t at = (size_t)k * L.ld + i;
-      sacc += L.val[at] * xin[L.col[at]];
-    }
-    xout[i] = xin[i] + omega * L.dinv[i] * (L.b[i] - sacc);
+    if (i < L.n)
+      for (int k = sub; k < L.w; k += g) {
+        const size_t at = (size_t)k * L.ld + i;
+        sacc += L.val[at] * xin[L.col[at]];
+      }
+    for (int o = g >> 1; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
+    if (i < L.n && sub == 0) emit(i, sacc);
   }
+}
+
+__device__ __forceinline__ void tail_sweep(const TailLevel &L, const float *xin, float *xout, float omega) {
+  tail_rows(L, xin, [&](int i, float sacc) { xout[i] = xin[i] + omega * L.dinv[i] * (L.b[i] - sacc); });
   __syncthreads();
 }
 
@@ -710,14 +708,7 @@ __global__ void __launch_bounds__(1024) vcycle_tail(TailArgs A) {
       float *t = c; c = o; o = t;
     }
     cur[l] = c;
-    for (int i = threadIdx.x; i < L.n; i += blockDim.x) {
-      float sacc = 0.f;
-      for (int k = 0; k < L.w; ++k) {
-        const size_t at = (size_t)k * L.ld + i;
-        sacc += L.val[at] * c[L.col[at]];
-      }
-      L.r[i] = L.b[i] - sacc;
-    }
+    tail_rows(L, c, [&](int i, float sacc) { L.r[i] = L.b[i] - sacc; });
     __syncthreads();
     const TailLevel &C = A.L[l + 1];
     for (int I = threadIdx.x; I < C.n; I += blockDim.x) {
@@ -1026,6 +1017,10 @@ static void vcycle(apc_context *c, cudaStream_t s, int l, const float *b, float 
       TailLevel &D = A.L[k];
       D.n = T.n;
       D.w = T.w;
+      // wide rows get several lanes while the block has lanes to spare
+      D.g = 1;
+      if (T.w > 24)
+        while (D.g < 8 && 2 * D.g * T.n <= 1024) D.g *= 2;
       D.ld = T.ld;
       D.col = T.col;
       D.val = T.val;
@@ -1043,36 +1038,65 @@ static void vcycle(apc_context *c, cudaStream_t s, int l, const float *b, float 
     return;
   }
   MgLevel &C = m->lv[l + 1];
-  const int G = grid_for(n);
+  // lanes per row from the width of this level's rows
+  const int g = L.w <= 24 ? 1 : (L.w <= 48 ? 4 : 8);
+  const int G = grid_for((long long)n * g);
+  auto op = [&](int kind, const float *xin, float *out) {
+#define APC_ROW_OP(GG)                                                                                            \
+  switch (kind) {                                                                                                 \
+    case kOpFirst2:                                                                                               \
+      row_op<GG, kOpFirst2><<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, xin, L.agg, C.x, alpha,       \
+                                            omega, out);                                                         \
+      break;                                                                                                      \
+    case kOpSweep:                                                                                                \
+      row_op<GG, kOpSweep><<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, xin, L.agg, C.x, alpha,        \
+                                           omega, out);                                                          \
+      break;                                                                                                      \
+    case kOpResidual:                                                                                             \
+      row_op<GG, kOpResidual><<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, xin, L.agg, C.x, alpha,     \
+                                              omega, out);                                                       \
+      break;                                                                                                      \
+    default:                                                                                                      \
+      row_op<GG, kOpProlongSweep><<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, xin, L.agg, C.x, alpha, \
+                                                  omega, out);                                                   \
+  }
+    if (g == 1) {
+      APC_ROW_OP(1)
+    } else if (g == 4) {
+      APC_ROW_OP(4)
+    } else {
+      APC_ROW_OP(8)
+    }
+#undef APC_ROW_OP
+    apc_count_launch(c);
+  };
   // Buffers alternate between x and L.x2.  The pre-smoothing result is placed so that the
   // `sweeps` post-smoothing sweeps, each flipping buffers, end in x.
   float *cur, *nxt;
   if (sweeps >= 2) {
-    jacobi_first2<<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, omega, x);
+    op(kOpFirst2, nullptr, x);
     cur = x;
     nxt = L.x2;
     for (int k = 2; k < sweeps; ++k) {
-      jacobi_sweep<<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, cur, omega, nxt);
+      op(kOpSweep, cur, nxt);
       std::swap(cur, nxt);
     }
-    apc_count_launch(c, sweeps - 1);
   } else {
-    jacobi_first<<<G, kT, 0, s>>>(n, L.dinv, b, omega, L.x2);
+    jacobi_first<<<grid_for(n), kT, 0, s>>>(n, L.dinv, b, omega, L.x2);
     cur = L.x2;
     nxt = x;
     apc_count_launch(c);
   }
-  residual_f32<<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, b, cur, L.r);
+  op(kOpResidual, cur, L.r);
   restrict_sum<<<grid_for(C.n), kT, 0, s>>>(C.n, C.mptr, n, C.mem, L.r, C.b);
-  apc_count_launch(c, 2);
+  apc_count_launch(c);
   vcycle(c, s, l + 1, C.b, C.x);
-  prolong_sweep<<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, cur, L.agg, C.x, alpha, omega, nxt);
+  op(kOpProlongSweep, cur, nxt);
   std::swap(cur, nxt);
   for (int k = 1; k < sweeps; ++k) {
-    jacobi_sweep<<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, cur, omega, nxt);
+    op(kOpSweep, cur, nxt);
     std::swap(cur, nxt);
   }
-  apc_count_launch(c, sweeps);
 }
 
 // Add a conditional WHILE node after the current capture dependencies of stream s and
