@@ -108,6 +108,7 @@ struct apc_context {
   int *cell_of = nullptr;  // sorted particle -> cell
   double *gfd_scr_d = nullptr;  // GFD search: per-warp sort lists longer than a warp
   int *gfd_scr_i = nullptr;
+  int *gfd_qr = nullptr;         // GFD: cells queued for the Householder pass
   double *adj_ckpt = nullptr, *adj_tape = nullptr;  // trajectory VJP: checkpoints, Hessian tape
   double last_c_pot = 0.0, last_c_field = 0.0;       // constants of the last apc_solve
   uint64_t *warm_keys = nullptr;      // warm start: codes of the previous step's cells (hash)

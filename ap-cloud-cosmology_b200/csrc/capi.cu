@@ -87,7 +87,7 @@ void free_all(apc_context *c) {
                   c->d_err, c->scan_tmp, c->flags, c->cx, c->cy, c->cz, c->ch, c->cfirst, c->ccount,
                   c->ctype, c->ccode, c->nb24, c->nnb, c->cell_of, c->st_idx, c->st_dist, c->gfd_x,
                   c->ell_col, c->a1, c->a2, c->a1f, c->a2f, c->rhs, c->bcrhs, c->density, c->potential,
-                  c->deriv, c->adj_ckpt, c->adj_tape, c->gfd_scr_d, c->gfd_scr_i, c->warm_keys, c->warm_rho,
+                  c->deriv, c->adj_ckpt, c->adj_tape, c->gfd_scr_d, c->gfd_scr_i, c->gfd_qr, c->warm_keys, c->warm_rho,
                   c->warm_phi, c->tr_cnt, c->tr_off, c->tr_cur, c->tr_tmp,
                   c->tp_col, c->tp_src, c->ta_col, c->ta_src, c->ta_val, c->vjp_c, c->vjp_phi, c->vjp_r2,
                   c->vjp_rho};

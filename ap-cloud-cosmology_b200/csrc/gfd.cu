@@ -51,6 +51,7 @@ struct GfdParams {
   double *st_dist, *gx;
   double *scr_d;  // per search warp: kListCap sort keys and indices (lists over 32)
   int *scr_i;
+  int *qr_list, *qr_count;  // cells for the Householder pass
   int *ell_col;
   double *a1, *a2, *rhs;
   size_t ld;  // ELL leading dimension (row capacity)
@@ -185,21 +186,31 @@ struct WarpSmem {
   double bd2[8][kBucketCap];
 };
 
-// least squares, per warp
-struct LsqSmem {
-  union {
-    double g45[45][32];  // Gram products b_r b_c (r <= c) of each row (fast path)
-    struct {
-      double red[9][32]; // column reductions of the QR: one value per (column, lane)
-      double sums[9];
-      double R[9][9];
-    };
-  };
-  double G[45];          // the Gram matrix B^T B (upper triangle, row-major)
-  double L[9][9];        // its Cholesky factor
-  double inv[9];         // 1 / L[k][k]
-  int chol_ok;
+// Least squares, per warp: a slice of the dynamic shared memory laid out as
+//   [0, A)            the Gram products b_r b_c (r <= c) of each row, 45 x lm (fast path),
+//                     or the QR's column reductions red (9 x 32), sums (9) and R (9 x 9);
+//   G (45), L (9 x 9), inv (9), the pivot flag.
+// A = max(45 lm, 378) doubles, so the slice is only as large as lm needs.
+struct LsqView {
+  double *g45, *red, *sums, *R, *G, *L, *inv;
+  int *chol_ok;
 };
+
+__host__ __device__ constexpr int lsq_area(int lm) { return 45 * lm > 378 ? 45 * lm : 378; }
+__host__ __device__ constexpr int lsq_doubles(int lm) { return (lsq_area(lm) + 45 + 81 + 9 + 1 + 1) & ~1; }
+
+__device__ __forceinline__ LsqView lsq_view(double *base, int lm) {
+  LsqView v;
+  v.g45 = base;
+  v.red = base;
+  v.sums = base + 9 * 32;
+  v.R = base + 9 * 32 + 9;
+  v.G = base + lsq_area(lm);
+  v.L = v.G + 45;
+  v.inv = v.L + 81;
+  v.chol_ok = reinterpret_cast<int *>(v.inv + 9);
+  return v;
+}
 
 // position of (r, c), r <= c, in the row-major upper triangle of a 9 x 9 matrix
 __host__ __device__ constexpr int tri(int r, int c) { return r * 9 - r * (r - 1) / 2 + (c - r); }
@@ -249,10 +260,10 @@ __device__ __forceinline__ bool append(WarpSmem &S, int (&nn)[8], bool valid, in
 // then g lanes per column (4 for up to 8 columns, 2 for 9) each add a chunk of rows in
 // row order, and the chunks are combined by a fixed shuffle tree.  Fewer instructions
 // than one 5-step butterfly per column; the order is fixed, so results are reproducible.
-__device__ __forceinline__ void col_sums(LsqSmem &S, const double (&val)[9], int c0, int lane) {
+__device__ __forceinline__ void col_sums(const LsqView &S, const double (&val)[9], int c0, int lane) {
 #pragma unroll
   for (int c = 0; c < 9; ++c)
-    if (c >= c0) S.red[c][lane] = val[c];
+    if (c >= c0) S.red[c * 32 + lane] = val[c];
   __syncwarp();
   const int ncol = 9 - c0;
   const int g = ncol <= 8 ? 4 : 2;
@@ -260,7 +271,7 @@ __device__ __forceinline__ void col_sums(LsqSmem &S, const double (&val)[9], int
   const int col = c0 + lane / g, chunk = lane % g;
   double t = 0.0;
   if (col < 9) {
-    const double *r = &S.red[col][chunk * rows];
+    const double *r = &S.red[col * 32 + chunk * rows];
     for (int q = 0; q < rows; ++q) t += r[q];
   }
   for (int o = 1; o < g; o <<= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
@@ -423,13 +434,18 @@ __global__ void __launch_bounds__(32 * kSearchWarps) gfd_search(GfdParams P) {
 
 // Phase 2, one warp per cell: weights, the weighted monomial system, its FP64 Householder
 // QR, the operator X and the matrix rows, from the stencil of phase 1.
-__global__ void __launch_bounds__(32 * kWarps, 4) gfd_lsq(GfdParams P) {
-  extern __shared__ __align__(16) unsigned char lsq_smem[];  // kWarps LsqSmem
-  LsqSmem *smem = reinterpret_cast<LsqSmem *>(lsq_smem);
+// QR = false: every cell by the Cholesky fast path; a cell that fails its pivot check is
+// queued.  QR = true: the queued cells by Householder QR.  The two instantiations keep
+// their register budgets apart, so the fast path runs at higher occupancy.
+template <bool QR>
+__global__ void __launch_bounds__(32 * kWarps, QR ? 4 : 6) gfd_lsq(GfdParams P) {
+  extern __shared__ __align__(16) double lsq_smem[];  // kWarps slices of lsq_doubles(lm)
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  LsqSmem &S = smem[w];
   const int lm = P.lm;
-  for (int i0 = blockIdx.x * kWarps + w; i0 < P.m; i0 += gridDim.x * kWarps) {
+  const LsqView S = lsq_view(lsq_smem + (size_t)w * lsq_doubles(lm), lm);
+  const int ncell = QR ? *P.qr_count : P.m;
+  for (int it = blockIdx.x * kWarps + w; it < ncell; it += gridDim.x * kWarps) {
+    const int i0 = QR ? P.qr_list[it] : it;
     // ---- weights and weighted monomials (solver.cpp:75-103) ----
     const bool act = lane < lm;
     const int mj = act ? P.st_idx[(size_t)i0 * lm + lane] : i0;
@@ -453,54 +469,58 @@ __global__ void __launch_bounds__(32 * kWarps, 4) gfd_lsq(GfdParams P) {
     //      cell whose Cholesky pivots fall below 1e-4 of the diagonal (cond(B) over ~100)
     //      takes the Householder path below. ----
     double y[9];
-    {
+    if (!QR) {
       int pidx = 0;
 #pragma unroll
       for (int r = 0; r < 9; ++r)
 #pragma unroll
-        for (int c = r; c < 9; ++c) S.g45[pidx++][lane] = b[r] * b[c];
+        for (int c = r; c < 9; ++c) S.g45[(pidx++) * lm + lane] = b[r] * b[c];
       __syncwarp();
       for (int t = lane; t < 45; t += 32) {
         double sacc = 0.0;
-        for (int q = 0; q < lm; ++q) sacc += S.g45[t][q];
+        for (int q = 0; q < lm; ++q) sacc += S.g45[t * lm + q];
         S.G[t] = sacc;
       }
-      if (lane == 0) S.chol_ok = 1;
+      if (lane == 0) *S.chol_ok = 1;
       __syncwarp();
       for (int k = 0; k < 9; ++k) {
         if (lane == 0) {
           double d = S.G[tri(k, k)];
-          for (int j = 0; j < k; ++j) d -= S.L[k][j] * S.L[k][j];
-          if (!(d > 1e-4 * S.G[tri(k, k)])) S.chol_ok = 0;
+          for (int j = 0; j < k; ++j) d -= S.L[k * 9 + j] * S.L[k * 9 + j];
+          if (!(d > 1e-4 * S.G[tri(k, k)])) *S.chol_ok = 0;
           const double lkk = sqrt(fmax(d, 1e-300));
-          S.L[k][k] = lkk;
+          S.L[k * 9 + k] = lkk;
           S.inv[k] = 1.0 / lkk;
         }
         __syncwarp();
         if (lane > k && lane < 9) {
           double t = S.G[tri(k, lane)];
-          for (int j = 0; j < k; ++j) t -= S.L[lane][j] * S.L[k][j];
-          S.L[lane][k] = t * S.inv[k];
+          for (int j = 0; j < k; ++j) t -= S.L[lane * 9 + j] * S.L[k * 9 + j];
+          S.L[lane * 9 + k] = t * S.inv[k];
         }
         __syncwarp();
       }
     }
-    const bool fast = S.chol_ok != 0;
-    if (fast) {
+    if (!QR && *S.chol_ok == 0) {
+      if (lane == 0) P.qr_list[atomicAdd(P.qr_count, 1)] = i0;
+      __syncwarp();
+      continue;
+    }
+    if (!QR) {
       // lane j: y = G^-1 b_j by the two triangular solves
       double t9[9];
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
         double t = b[k];
 #pragma unroll
-        for (int j = 0; j < k; ++j) t -= S.L[k][j] * t9[j];
+        for (int j = 0; j < k; ++j) t -= S.L[k * 9 + j] * t9[j];
         t9[k] = t * S.inv[k];
       }
 #pragma unroll
       for (int k = 8; k >= 0; --k) {
         double t = t9[k];
 #pragma unroll
-        for (int j = k + 1; j < 9; ++j) t -= S.L[j][k] * y[j];
+        for (int j = k + 1; j < 9; ++j) t -= S.L[j * 9 + k] * y[j];
         y[k] = t * S.inv[k];
       }
     } else {
@@ -541,7 +561,7 @@ __global__ void __launch_bounds__(32 * kWarps, 4) gfd_lsq(GfdParams P) {
     }
     if (lane < 9) {
 #pragma unroll
-      for (int c = 0; c < 9; ++c) S.R[lane][c] = c >= lane ? b[c] : 0.0;
+      for (int c = 0; c < 9; ++c) S.R[lane * 9 + c] = c >= lane ? b[c] : 0.0;
     }
     // ---- thin Q rows: Q1 = H0 H1 ... H8 [I; 0] (backward accumulation) ----
     double q[9];
@@ -563,8 +583,8 @@ __global__ void __launch_bounds__(32 * kWarps, 4) gfd_lsq(GfdParams P) {
     for (int k = 8; k >= 0; --k) {
       double t = q[k];
 #pragma unroll
-      for (int c = k + 1; c < 9; ++c) t -= S.R[k][c] * y[c];
-      y[k] = t / S.R[k][k];
+      for (int c = k + 1; c < 9; ++c) t -= S.R[k * 9 + c] * y[c];
+      y[k] = t / S.R[k * 9 + k];
     }
     }
     // ---- X(:, j) = w_j y ----
@@ -741,13 +761,22 @@ int apc_gfd_assemble(apc_context *c, double c_dens) {
   APC_TRY(apc_ensure(c, &c->gfd_scr_i, (size_t)sblocks * kSearchWarps * kListCap, nullptr));
   P.scr_d = c->gfd_scr_d;
   P.scr_i = c->gfd_scr_i;
+  APC_TRY(apc_ensure(c, &c->gfd_qr, (size_t)M + 1, nullptr));
+  P.qr_list = c->gfd_qr;
+  P.qr_count = c->counters + 112;
   const int blocks = std::max(1, std::min((M + kWarps - 1) / kWarps, apc_sm_count(c) * 16));
   APC_CUDA_TRY(c, cudaEventRecord(c->gev[0], c->s));
   gfd_search<<<sblocks, 32 * kSearchWarps, 0, c->s>>>(P);
-  const size_t lsq_bytes = sizeof(LsqSmem) * kWarps;
-  static_assert(sizeof(LsqSmem) * kWarps <= 227 * 1024, "least-squares shared memory");
-  APC_CUDA_TRY(c, cudaFuncSetAttribute(gfd_lsq, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsq_bytes));
-  gfd_lsq<<<blocks, 32 * kWarps, lsq_bytes, c->s>>>(P);
+  const size_t lsq_bytes = sizeof(double) * lsq_doubles(lm) * kWarps;
+  APC_CUDA_TRY(c, cudaFuncSetAttribute(gfd_lsq<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)lsq_bytes));
+  APC_CUDA_TRY(c, cudaFuncSetAttribute(gfd_lsq<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)lsq_bytes));
+  APC_CUDA_TRY(c, cudaMemsetAsync(P.qr_count, 0, sizeof(int), c->s));
+  gfd_lsq<false><<<blocks, 32 * kWarps, lsq_bytes, c->s>>>(P);
+  // the queued cells, whatever their number: the kernel reads the count itself
+  gfd_lsq<true><<<apc_sm_count(c) * 4, 32 * kWarps, lsq_bytes, c->s>>>(P);
+  apc_count_launch(c);
   APC_CUDA_TRY(c, cudaEventRecord(c->gev[1], c->s));
   apc_count_launch(c, 2);
   APC_CUDA_TRY(c, cudaGetLastError());
