@@ -59,6 +59,10 @@ struct apc_context {
   double *px = nullptr, *py = nullptr, *pz = nullptr, *pvx = nullptr, *pvy = nullptr, *pvz = nullptr;
   double *pax = nullptr, *pay = nullptr, *paz = nullptr;
   int *pid = nullptr;  // caller index of each sorted particle
+  // particles are sorted by the top 3 * sorted_levels bits of their keys (the selection
+  // needs no more than its deepest level); levels_hint = the last selection's deepest
+  // level, 0 = unknown (then the sort takes every bit)
+  int sorted_levels = 0, levels_hint = 0;
   double *qx = nullptr, *qy = nullptr, *qz = nullptr, *qvx = nullptr, *qvy = nullptr, *qvz = nullptr;
   int *qid = nullptr;
   uint64_t *keys = nullptr, *keys_alt = nullptr;
@@ -106,6 +110,8 @@ struct apc_context {
   int *nb24 = nullptr;   // 24 per cell
   int *nnb = nullptr;    // Neigh24 count per cell
   int *cell_of = nullptr;  // sorted particle -> cell
+  uint64_t *full_keys = nullptr, *full_keys_alt = nullptr;  // fully sorted key copies (diagnostics)
+  uint32_t *full_ids = nullptr, *full_ids_alt = nullptr;
   double *gfd_scr_d = nullptr;  // GFD search: per-warp sort lists longer than a warp
   int *gfd_scr_i = nullptr;
   int *gfd_qr = nullptr;         // GFD: cells queued for the Householder pass
@@ -160,6 +166,8 @@ inline void apc_count_launch(apc_context *c, int k = 1) { c->launches += k; }
 int apc_octree_build(apc_context *c);        // keys, sort, permute (octree_build.cu)
 int apc_octree_levels_count(apc_context *c); // numnodes per level (octree_build.cu)
 int apc_selection(apc_context *c);           // top-down + balance + cells (selection.cu)
+constexpr int APC_RETRY_FULL_SORT = -100;    // internal: the selection went deeper than the sort
+int apc_sorted_keys_copy(apc_context *c, uint64_t **keys, uint32_t **ids);  // octree_build.cu
 int apc_gfd_assemble(apc_context *c, double c_dens);    // gfd.cu
 int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int *its,
                      double *rnorm, int *reason, int *refinements);  // krylov.cu

@@ -87,7 +87,7 @@ void free_all(apc_context *c) {
                   c->d_err, c->scan_tmp, c->flags, c->cx, c->cy, c->cz, c->ch, c->cfirst, c->ccount,
                   c->ctype, c->ccode, c->nb24, c->nnb, c->cell_of, c->st_idx, c->st_dist, c->gfd_x,
                   c->ell_col, c->a1, c->a2, c->a1f, c->a2f, c->rhs, c->bcrhs, c->density, c->potential,
-                  c->deriv, c->adj_ckpt, c->adj_tape, c->gfd_scr_d, c->gfd_scr_i, c->gfd_qr, c->warm_keys, c->warm_rho,
+                  c->deriv, c->adj_ckpt, c->adj_tape, c->gfd_scr_d, c->gfd_scr_i, c->gfd_qr, c->full_keys, c->full_keys_alt, c->full_ids, c->full_ids_alt, c->warm_keys, c->warm_rho,
                   c->warm_phi, c->tr_cnt, c->tr_off, c->tr_cur, c->tr_tmp,
                   c->tp_col, c->tp_src, c->ta_col, c->ta_src, c->ta_val, c->vjp_c, c->vjp_phi, c->vjp_r2,
                   c->vjp_rho};
@@ -285,6 +285,7 @@ static int set_particles_impl(apc_context *c, const double *const *src, cudaMemc
   c->have_cells = false;
   c->have_fields = false;
   c->warm_cap = 0;  // a new particle set: no guess from the previous one
+  c->levels_hint = 0;  // and no depth hint for its sort
   return APC_OK;
 }
 
@@ -345,7 +346,14 @@ int apc_select(apc_context *c, int *n_cells) {
     c->err = "non-finite particle coordinates";
     return APC_ERR_NOT_FINITE;
   }
-  APC_TRY(apc_selection(c));
+  int rc = apc_selection(c);
+  if (rc == APC_RETRY_FULL_SORT) {
+    // the tree went deeper than the sort: sort by every bit and select again
+    c->levels_hint = 0;
+    APC_TRY(apc_octree_build(c));
+    rc = apc_selection(c);
+  }
+  APC_TRY(rc);
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[1], c->s));
   APC_CUDA_TRY(c, cudaEventSynchronize(c->ev[1]));
   c->t_select_ms = elapsed(c->ev[0], c->ev[1]);
@@ -491,8 +499,11 @@ int apc_get_cell_codes(apc_context *c, uint64_t *codes) {
 
 int apc_get_keys(apc_context *c, uint64_t *keys, int *index) {
   APC_TRY(check_ready(c, true, true, false));
-  if (keys) APC_CUDA_TRY(c, cudaMemcpy(keys, c->keys, sizeof(uint64_t) * c->n, cudaMemcpyDeviceToHost));
-  if (index) APC_CUDA_TRY(c, cudaMemcpy(index, c->pid, sizeof(int) * c->n, cudaMemcpyDeviceToHost));
+  uint64_t *k = nullptr;
+  uint32_t *id = nullptr;
+  APC_TRY(apc_sorted_keys_copy(c, &k, &id));
+  if (keys) APC_CUDA_TRY(c, cudaMemcpy(keys, k, sizeof(uint64_t) * c->n, cudaMemcpyDeviceToHost));
+  if (index) APC_CUDA_TRY(c, cudaMemcpy(index, id, sizeof(int) * c->n, cudaMemcpyDeviceToHost));
   return APC_OK;
 }
 

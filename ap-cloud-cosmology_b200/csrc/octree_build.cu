@@ -11,6 +11,8 @@
 // reads coalesced SoA arrays.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "apc_internal.cuh"
 
 namespace {
@@ -91,8 +93,12 @@ int apc_octree_build(apc_context *c) {
   apc_count_launch(c);
   APC_CUDA_TRY(c, cudaGetLastError());
   bool in_alt = false;
-  APC_TRY(apc_radix_sort_u64(c, c->keys, c->perm, c->keys_alt, c->perm_alt, n, 0, 3 * c->cfg.depth,
-                             &in_alt));
+  // Sort by the top bits the selection will read: two levels below the last selection's
+  // deepest, or all of them.  A selection that goes deeper asks for a full sort.
+  const int D = c->cfg.depth;
+  const int ls = c->levels_hint > 0 ? std::min(D, c->levels_hint + 2) : D;
+  APC_TRY(apc_radix_sort_u64(c, c->keys, c->perm, c->keys_alt, c->perm_alt, n, 3 * (D - ls), 3 * D, &in_alt));
+  c->sorted_levels = ls;
   if (in_alt) {
     uint64_t *tk = c->keys; c->keys = c->keys_alt; c->keys_alt = tk;
     uint32_t *tp = c->perm; c->perm = c->perm_alt; c->perm_alt = tp;
@@ -111,14 +117,39 @@ int apc_octree_build(apc_context *c) {
   return APC_OK;
 }
 
+// Copies of the keys and caller ids sorted by every key bit (the context's particles may
+// be sorted by the top bits only); for the key and octree-level accessors.
+int apc_sorted_keys_copy(apc_context *c, uint64_t **keys, uint32_t **ids) {
+  const int n = c->n;
+  APC_TRY(apc_ensure(c, &c->full_keys, (size_t)n + 1, nullptr));
+  APC_TRY(apc_ensure(c, &c->full_keys_alt, (size_t)n + 1, nullptr));
+  APC_TRY(apc_ensure(c, &c->full_ids, (size_t)n + 1, nullptr));
+  APC_TRY(apc_ensure(c, &c->full_ids_alt, (size_t)n + 1, nullptr));
+  APC_CUDA_TRY(c, cudaMemcpyAsync(c->full_keys, c->keys, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, c->s));
+  APC_CUDA_TRY(c, cudaMemcpyAsync(c->full_ids, c->pid, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, c->s));
+  bool alt = false;
+  // an LSD sort orders by its last digits, so the copy is sorted by every bit again
+  if (c->sorted_levels < c->cfg.depth)
+    APC_TRY(apc_radix_sort_u64(c, c->full_keys, c->full_ids, c->full_keys_alt, c->full_ids_alt, n, 0,
+                               3 * c->cfg.depth, &alt));
+  *keys = alt ? c->full_keys_alt : c->full_keys;
+  *ids = alt ? c->full_ids_alt : c->full_ids;
+  // callers read the copies with plain cudaMemcpy, which does not wait for this stream
+  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  return APC_OK;
+}
+
 int apc_octree_levels_count(apc_context *c) {
   const int D = c->cfg.depth, n = c->n;
   c->numnodes.assign(D + 1, 0);
   if (n <= 0) return APC_OK;
+  uint64_t *sorted = nullptr;
+  uint32_t *ids = nullptr;
+  APC_TRY(apc_sorted_keys_copy(c, &sorted, &ids));
   int *hist = c->counters + 64;  // 24 ints reserved
   APC_CUDA_TRY(c, cudaMemsetAsync(hist, 0, 24 * sizeof(int), c->s));
   int G = std::min((n + 255) / 256, apc_sm_count(c) * 8);
-  lcp_histogram<<<G, 256, 0, c->s>>>(c->keys, n, D, hist);
+  lcp_histogram<<<G, 256, 0, c->s>>>(sorted, n, D, hist);
   apc_count_launch(c);
   APC_CUDA_TRY(c, cudaGetLastError());
   int h[24];

@@ -400,6 +400,8 @@ static int select_once(apc_context *c, int *hash_full) {
   for (int L = 0; L < D; ++L) {
     const int off = c->td_level_off[L], cnt = c->td_level_off[L + 1] - off;
     if (cnt == 0) break;
+    // children at level L + 1 need the particles sorted by that many levels of key bits
+    if (L + 1 > c->sorted_levels) return APC_RETRY_FULL_SORT;
     maxlev = L + 1;
     const long long m8 = 8ll * cnt;
     APC_TRY(apc_ensure(c, &c->flags, (size_t)(3 * m8 + 1), nullptr));
@@ -428,6 +430,7 @@ static int select_once(apc_context *c, int *hash_full) {
   }
   const int n_open_td = c->td_level_off.back();
   c->n_open_td = n_open_td;
+  c->levels_hint = maxlev;
   n_open = n_open_td;
   const int child_base_bal = 1 + 8 * n_open_td;  // j after the top-down sweep
 
