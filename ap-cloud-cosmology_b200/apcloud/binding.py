@@ -62,7 +62,8 @@ class ApcProfile(C.Structure):
                 ("move_ms", C.c_double), ("steps", C.c_int64), ("step_ms", C.c_double),
                 ("gfd_ms", C.c_double), ("mg_build_ms", C.c_double), ("mg_solve_ms", C.c_double),
                 ("mg_iterations", C.c_int64), ("assemble_ms", C.c_double), ("density_ms", C.c_double),
-                ("potential_ms", C.c_double), ("graph_instantiations", C.c_int64), ("graph_updates", C.c_int64)]
+                ("potential_ms", C.c_double), ("graph_instantiations", C.c_int64), ("graph_updates", C.c_int64),
+                ("sort_retries", C.c_int64)]
 
 
 class ApcStepParams(C.Structure):
@@ -232,6 +233,13 @@ class GpuPath:
         h = C.c_void_p()
         self._check(self.lib.apc_create(C.byref(cfg), C.byref(h)), "apc_create", None)
         self.h = h
+        self.set_particles(parts)
+
+    def set_particles(self, parts: "ics.Particles") -> None:
+        """Replace the particle set (same count) from host arrays; cells and fields are
+        invalidated until the next select."""
+        if parts.n != self.n:
+            raise ValueError(f"particle count {parts.n} != {self.n}")
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in parts.as_tuple()]
         self._check(self.lib.apc_set_particles(self.h, *[_ptr(a) for a in arrs]), "apc_set_particles")
 

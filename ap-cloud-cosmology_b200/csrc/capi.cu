@@ -285,7 +285,7 @@ static int set_particles_impl(apc_context *c, const double *const *src, cudaMemc
   c->have_cells = false;
   c->have_fields = false;
   c->warm_cap = 0;  // a new particle set: no guess from the previous one
-  c->levels_hint = 0;  // and no depth hint for its sort
+  // levels_hint stays: a selection deeper than the hint redoes the sort over every bit
   return APC_OK;
 }
 
@@ -350,6 +350,7 @@ int apc_select(apc_context *c, int *n_cells) {
   if (rc == APC_RETRY_FULL_SORT) {
     // the tree went deeper than the sort: sort by every bit and select again
     c->levels_hint = 0;
+    c->prof.sort_retries++;
     APC_TRY(apc_octree_build(c));
     rc = apc_selection(c);
   }

@@ -114,18 +114,49 @@ class Dist:
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed region.
+
+    NVML is polled every 5 ms from a thread, so that a region of a few hundred ms still gets
+    dozens of samples; the device is found by its PCI bus id (CUDA and NVML may number GPUs
+    differently).  Without NVML, nvidia-smi is run at its 200 ms minimum.  Only reads."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, period_s: float = 0.005):
         self.device = device
+        self.period = period_s
         self.proc = None
+        self.nvml = None
+        self.stop = threading.Event()
+        self.samples: list[tuple[float, float, set]] = []
         self.lines: list[str] = []
 
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:
+            pr = torch.cuda.get_device_properties(self.device)
+            bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
     def __enter__(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.nvml = (nv, h, nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                         nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
@@ -136,11 +167,25 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def _poll(self):
+        nv, h, mx = self.nvml
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), float(mx), {n for n, b in zip(self.NAMES, self.bits) if r & b}))
+            except Exception:
+                return
+            self.stop.wait(self.period)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        self.stop.set()
+        if self.nvml:
+            self.thread.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             try:
@@ -150,7 +195,10 @@ class ClockSampler:
 
     def summary(self) -> dict:
         sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for f, m, r in self.samples:
+            sm.append(f)
+            mx = max(mx, m)
+            reasons |= r
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
@@ -160,11 +208,12 @@ class ClockSampler:
                 mx = max(mx, float(parts[2]))
             except ValueError:
                 continue
-            for k, nm in enumerate(names):
+            for k, nm in enumerate(self.NAMES):
                 if parts[5 + k].lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml 5 ms" if self.samples else "nvidia-smi 200 ms"}
 
 
 def measured_peaks() -> tuple[float, str]:

@@ -201,6 +201,8 @@ typedef struct apc_profile {
   double potential_ms;   /* ... of the potential solve (incl. hierarchy build and capture) */
   int64_t graph_instantiations;  /* solve graphs instantiated */
   int64_t graph_updates;         /* solve graphs updated in place from a new capture */
+  int64_t sort_retries;  /* selections that went deeper than the particle sort and were redone
+                            after a sort over every key bit */
 } apc_profile;
 int apc_get_profile(apc_context *ctx, apc_profile *out);
 int apc_reset_profile(apc_context *ctx);

@@ -148,6 +148,39 @@ def test_bitexact_cells_along_a_trajectory_vs_oracle(gpu_lib, oracle_lib):
     gp.close()
 
 
+def test_selection_deeper_than_the_sort_redoes_it(gpu_lib):
+    """The particle sort covers the previous selection's deepest level plus two.  After a
+    shallow particle set, a clustered one of the same size needs more: the selection must
+    redo the sort over every key bit and give the keys and cells of a fresh context."""
+    g = np.load(os.path.join(GOLDEN, "ball2k.npz"))
+    deep = _parts(g)
+    for a in (deep.x, deep.y, deep.z):
+        a[:] = 0.5 + (a - 0.5) / 64.0  # the same ball, six levels deeper
+    rng = np.random.default_rng(7)
+    shallow = ics.Particles(*(rng.uniform(0.0, 1.0, deep.n) for _ in range(3)),
+                            *(np.zeros(deep.n) for _ in range(3)))
+    gp = _gpu(shallow, g)
+    gp.select()
+    gp.reset_profile()
+    gp.set_particles(deep)
+    m = gp.select()
+    assert gp.profile()["sort_retries"] == 1
+    fresh = _gpu(deep, g)
+    assert fresh.select() == m
+    ka, ia = gp.keys()
+    kb, ib = fresh.keys()
+    assert np.array_equal(ka, kb) and np.all(ka[1:] >= ka[:-1])
+    assert np.array_equal(gp.octree_levels(), fresh.octree_levels())
+    a, b = gp.cells(), fresh.cells()
+    for f in ("x", "y", "z", "h", "count", "type", "first", "firstneigh", "numneigh", "neigh24"):
+        assert np.array_equal(getattr(a, f), getattr(b, f)), f
+    # the next selection of the same set starts from the deep hint: no second retry
+    gp.set_particles(deep)
+    assert gp.select() == m and gp.profile()["sort_retries"] == 1
+    gp.close()
+    fresh.close()
+
+
 @pytest.mark.parametrize("path", CASES, ids=IDS)
 def test_mixed_precision_equal_force_error(gpu_lib, path):
     g = np.load(path)
