@@ -183,7 +183,7 @@ int apc_create(const apc_config *cfg, apc_context **out) {
   *out = nullptr;
   if (cfg->n_particles < 1 || cfg->depth < 1 || cfg->depth > 21 || cfg->lm < 9 || cfg->lm > 32 ||
       (cfg->bc != 0 && cfg->bc != 1) || !(cfg->gfd_c >= 0.0) || cfg->gmres_restart < 1 ||
-      cfg->gmres_restart > 31 || cfg->mixed_restart < 0 || cfg->mixed_restart > 31 || cfg->mg_sweeps < 0 ||
+      cfg->gmres_restart > 255 || cfg->mixed_restart < 0 || cfg->mixed_restart > 31 || cfg->mg_sweeps < 0 ||
       (cfg->mixed_precond != APC_PRECOND_JACOBI && cfg->mixed_precond != APC_PRECOND_MULTIGRID) ||
       (cfg->precision != APC_PREC_FP64 && cfg->precision != APC_PREC_MIXED))
     return APC_ERR_INVALID_ARG;
@@ -615,7 +615,7 @@ int apc_config_from_options(apc_config *cfg, int argc, const char *const *argv) 
     double v = 0.0;
     if (!strcmp(a, "-ksp_gmres_restart")) {
       if (!num(&v) || v != (int)v) return APC_ERR_INVALID_ARG;
-      if (v < 1 || v > 31) return APC_ERR_UNSUPPORTED;  // the GMRES kernels hold <= 31 basis vectors
+      if (v < 1 || v > 255) return APC_ERR_UNSUPPORTED;  // the FP64 GMRES kernel holds <= 255 basis vectors
       cfg->gmres_restart = (int)v;
     } else if (!strcmp(a, "-ksp_rtol")) {
       if (!num(&v)) return APC_ERR_INVALID_ARG;

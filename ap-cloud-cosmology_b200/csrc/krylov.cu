@@ -37,7 +37,9 @@ namespace {
 constexpr int kThreads = 1024;              // one block per SM
 constexpr int kWarpsPB = kThreads / 32;
 constexpr int kMaxBlocks = 256;             // partial sums are laid out [slot][block]
-constexpr int kSlots = 48;                  // slots per partial-sum buffer
+constexpr int kMaxRestart = 255;            // basis vectors of the large instantiation, minus one
+constexpr int kSlots = kMaxRestart + 2;     // slots per partial-sum buffer: the dots, and one norm
+constexpr int kNormSlot = kSlots - 1;
 constexpr long long kSpinLimit = 1ll << 24;  // ~1-2 s of __nanosleep(64)
 
 struct GridBar {
@@ -100,6 +102,7 @@ struct GmresArgs {
   T *x;                 // solution (out)
   T *U;                 // (restart+1) x n basis, un-normalised
   size_t un;            // basis leading dimension
+  double *hh;           // per-block Hessenberg, (restart+1) x restart, when it exceeds shared memory
   double *part;         // 2 x kSlots x kMaxBlocks partial sums
   GridBar *bar;
   int *err;
@@ -176,44 +179,77 @@ __device__ __forceinline__ void block_dots(const T *a, const T *U, size_t un, in
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int per = (r1 - r0 + kWarpsPB - 1) / kWarpsPB;
   const int ws = r0 + warp * per, we = min(r1, ws + per);
-  for (int j0 = 0; j0 < nv; j0 += 4) {
-    double v[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int r = ws + lane; r < we; r += 32) {
-      const double ar = (double)ldcg(a + r);
+  // 32 basis vectors at a time through the [warp][32] staging array
+  for (int c0 = 0; c0 < nv; c0 += 32) {
+    const int cn = min(32, nv - c0);
+    for (int j0 = 0; j0 < cn; j0 += 4) {
+      double v[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int r = ws + lane; r < we; r += 32) {
+        const double ar = (double)ldcg(a + r);
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (j0 + q < nv) v[q] += ar * (double)ldcg(U + (size_t)(j0 + q) * un + r);
+        for (int q = 0; q < 4; ++q)
+          if (j0 + q < cn) v[q] += ar * (double)ldcg(U + (size_t)(c0 + j0 + q) * un + r);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        double t = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if (lane == 0 && j0 + q < cn) sm_red[warp * 33 + j0 + q] = t;
+      }
     }
+    __syncthreads();
+    if ((int)threadIdx.x < cn) {
+      double t = 0.0;
+      for (int wv = 0; wv < kWarpsPB; ++wv) t += sm_red[wv * 33 + threadIdx.x];
+      put_partial(part, c0 + threadIdx.x, t);
+    }
+    if (c0 + 32 < nv) __syncthreads();
+  }
+}
+
+// t -/+= sum_{j <= last} coef[j] u_j[i], one term at a time in j order.  Up to 32 vectors
+// the loop is unrolled with predicates (independent loads); above, a plain loop.
+template <int MAXV, bool SUB, class T>
+__device__ __forceinline__ double basis_axpy(double t, const T *U, size_t un, int i, const double *coef,
+                                             int last) {
+  if constexpr (MAXV <= 32) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      double t = v[q];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-      if (lane == 0 && j0 + q < nv) sm_red[warp * 33 + j0 + q] = t;
+    for (int j = 0; j < MAXV; ++j)
+      if (j <= last) {
+        const double u = (double)ldcg(U + (size_t)j * un + i);
+        t = SUB ? t - coef[j] * u : t + coef[j] * u;
+      }
+  } else {
+#pragma unroll 8
+    for (int j = 0; j <= last; ++j) {
+      const double u = (double)ldcg(U + (size_t)j * un + i);
+      t = SUB ? t - coef[j] * u : t + coef[j] * u;
     }
   }
-  __syncthreads();
-  if ((int)threadIdx.x < nv) {
-    double t = 0.0;
-    for (int wv = 0; wv < kWarpsPB; ++wv) t += sm_red[wv * 33 + threadIdx.x];
-    put_partial(part, threadIdx.x, t);
-  }
+  return t;
 }
 
 // Each block owns the contiguous rows [r0, r1); within a pass every thread takes rows
 // r0 + threadIdx.x + k * blockDim.x.
-template <class T, bool REORTH>
+//
+// MAXV bounds the basis (restart <= MAXV - 1).  Up to 32 vectors the Hessenberg matrix
+// lives in shared memory; above (PETSc production runs use restart 200), in the block's
+// own slice of global memory, written and read by thread 0 of that block only.
+template <class T, bool REORTH, int MAXV>
 __global__ void __launch_bounds__(kThreads, 1) gmres_kernel(GmresArgs<T> A) {
-  constexpr int MAXV = 32;  // restart <= 31
+  constexpr bool kSmemH = MAXV <= 32;
   __shared__ double sm_red[kWarpsPB * 33];
   __shared__ double sh[MAXV + 1];      // reduced dots / norms of this step
-  __shared__ double HH[(MAXV + 1) * MAXV];
+  __shared__ double HHs[kSmemH ? (MAXV + 1) * MAXV : 1];
   __shared__ double cc[MAXV], ss[MAXV], grs[MAXV + 1], scale[MAXV + 1], coef[MAXV + 1];
   __shared__ int s_flow[4];
   __shared__ double s_res;
 
   const int nb = gridDim.x;
   const int m = A.restart;
+  const int hld = kSmemH ? MAXV + 1 : m + 1;  // Hessenberg column stride
+  double *HH = kSmemH ? HHs : A.hh + (size_t)blockIdx.x * (size_t)hld * m;
   const int rpb = (A.n + nb - 1) / nb;
   const int r0 = min(A.n, (int)blockIdx.x * rpb), r1 = min(A.n, r0 + rpb);
   double *partA = A.part;
@@ -287,17 +323,14 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_kernel(GmresArgs<T> A) {
       __syncthreads();
       if ((int)threadIdx.x <= it) {
         const double h = sh[threadIdx.x] * scale[threadIdx.x];  // <v_j, w>
-        HH[it * (MAXV + 1) + threadIdx.x] = h;
+        HH[it * hld + threadIdx.x] = h;
         coef[threadIdx.x] = h * scale[threadIdx.x];              // weight on u_j
       }
       __syncthreads();
       // ---- pass B: w -= sum_j h_j v_j, then its norm (CGS) or a second sweep (CGS2) ----
       double nr = 0.0;
       for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
-        double t = (double)ldcg(w + i);
-#pragma unroll
-        for (int j = 0; j < MAXV; ++j)
-          if (j <= it) t -= coef[j] * (double)ldcg(A.U + (size_t)j * A.un + i);
+        const double t = basis_axpy<MAXV, true>((double)ldcg(w + i), A.U, A.un, i, coef, it);
         const T tv = T(t);
         w[i] = tv;
         nr += (double)tv * (double)tv;
@@ -310,24 +343,21 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_kernel(GmresArgs<T> A) {
         __syncthreads();
         if ((int)threadIdx.x <= it) {
           const double h2 = sh[threadIdx.x] * scale[threadIdx.x];
-          HH[it * (MAXV + 1) + threadIdx.x] += h2;
+          HH[it * hld + threadIdx.x] += h2;
           coef[threadIdx.x] = h2 * scale[threadIdx.x];
         }
         __syncthreads();
         nr = 0.0;
         for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
-          double t = (double)ldcg(w + i);
-#pragma unroll
-          for (int j = 0; j < MAXV; ++j)
-            if (j <= it) t -= coef[j] * (double)ldcg(A.U + (size_t)j * A.un + i);
+          const double t = basis_axpy<MAXV, true>((double)ldcg(w + i), A.U, A.un, i, coef, it);
           const T tv = T(t);
           w[i] = tv;
           nr += (double)tv * (double)tv;
         }
         const double v = block_sum(nr, sm_red);
-        if (threadIdx.x == 0) put_partial(partA, 40, v);
+        if (threadIdx.x == 0) put_partial(partA, kNormSlot, v);
         if (!grid_sync(A.bar, nb, A.err)) return;
-        gather_partials(partA + (size_t)40 * kMaxBlocks, nb, 1, sh);
+        gather_partials(partA + (size_t)kNormSlot * kMaxBlocks, nb, 1, sh);
         __syncthreads();
       } else {
         const double v = block_sum(nr, sm_red);
@@ -340,7 +370,7 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_kernel(GmresArgs<T> A) {
       if (threadIdx.x == 0) {
         const double tt = sqrt(sh[0]);
         scale[it + 1] = tt != 0.0 ? 1.0 / tt : 1.0;
-        double *hh = HH + it * (MAXV + 1);
+        double *hh = HH + it * hld;
         hh[it + 1] = tt;
         double hapbnd = fabs(tt / grs[it]);
         if (hapbnd > 1e-30) hapbnd = 1e-30;
@@ -391,23 +421,20 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_kernel(GmresArgs<T> A) {
     if (last >= 0) {
       if (threadIdx.x == 0) {
         double *y = sh;
-        const double hl = HH[last * (MAXV + 1) + last];
+        const double hl = HH[last * hld + last];
         y[last] = hl != 0.0 ? grs[last] / hl : 0.0;
         for (int ii = 1; ii <= last; ++ii) {
           const int k = last - ii;
           double t = grs[k];
-          for (int j = k + 1; j <= last; ++j) t -= HH[j * (MAXV + 1) + k] * y[j];
-          const double hkk = HH[k * (MAXV + 1) + k];
+          for (int j = k + 1; j <= last; ++j) t -= HH[j * hld + k] * y[j];
+          const double hkk = HH[k * hld + k];
           y[k] = hkk != 0.0 ? t / hkk : 0.0;
         }
         for (int j = 0; j <= last; ++j) coef[j] = y[j] * scale[j];
       }
       __syncthreads();
       for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
-        double t = 0.0;
-#pragma unroll
-        for (int j = 0; j < MAXV; ++j)
-          if (j <= last) t += coef[j] * (double)ldcg(A.U + (size_t)j * A.un + i);
+        const double t = basis_axpy<MAXV, false>(0.0, A.U, A.un, i, coef, last);
         A.x[i] = T((double)A.x[i] + t);
       }
     }
@@ -457,6 +484,8 @@ struct KrylovWork {
   double *dres = nullptr;  // rnorm
   double *r = nullptr;  // FP64 residual of the mixed path
   float *a32 = nullptr;
+  double *hh = nullptr;  // per-block Hessenberg slices of the large-restart kernel
+  size_t hh_bytes = 0;
   int cap_n = 0;
   int occ64[2] = {0, 0}, occ32[2] = {0, 0};
 };
@@ -471,6 +500,7 @@ void apc_krylov_free(apc_context *c) {
   cudaFree(k->dres);
   cudaFree(k->r);
   cudaFree(k->a32);
+  cudaFree(k->hh);
   delete k;
   c->kw = nullptr;
 }
@@ -480,10 +510,13 @@ static int launch_gmres(apc_context *c, int n, const T *val, const T *b, T *x, i
                         double atol, double dtol, int max_it, int *its, double *rnorm, int *reason,
                         const int *col = nullptr, int w = 0, size_t ld = 0) {
   KrylovWork *k = c->kw;
-  if (restart < 1 || restart > 31) {
-    c->err = "GMRES restart must be in [1, 31]";
+  if (restart < 1 || restart > kMaxRestart) {
+    c->err = "GMRES restart must be in [1, 255]";
     return APC_ERR_INVALID_ARG;
   }
+  const bool large = restart > 31;
+  const void *kern = large ? (const void *)gmres_kernel<T, RE, kMaxRestart + 1>
+                           : (const void *)gmres_kernel<T, RE, 32>;
   const size_t un = ((size_t)n + 31) & ~(size_t)31;
   const size_t need = un * (restart + 1) * sizeof(T);
   if (need > k->u_bytes) {
@@ -493,7 +526,7 @@ static int launch_gmres(apc_context *c, int n, const T *val, const T *b, T *x, i
     k->u_bytes = need;
   }
   int occ = 0;
-  APC_CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gmres_kernel<T, RE>, kThreads, 0));
+  APC_CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, 0));
   if (occ < 1) {
     c->err = "GMRES kernel does not fit on an SM";
     return APC_ERR_CUDA;
@@ -502,6 +535,15 @@ static int launch_gmres(apc_context *c, int n, const T *val, const T *b, T *x, i
   if (!k->part) {
     APC_TRY(apc_alloc(c, (void **)&k->part, sizeof(double) * 2 * kSlots * (size_t)kMaxBlocks));
     k->part_blocks = kMaxBlocks;
+  }
+  if (large) {
+    const size_t hb = sizeof(double) * (size_t)blocks * (restart + 1) * restart;
+    if (hb > k->hh_bytes) {
+      cudaFree(k->hh);
+      k->hh = nullptr;
+      APC_TRY(apc_alloc(c, (void **)&k->hh, hb));
+      k->hh_bytes = hb;
+    }
   }
   APC_CUDA_TRY(c, cudaMemsetAsync(k->bar, 0, sizeof(GridBar), c->s));
   GmresArgs<T> a;
@@ -514,6 +556,7 @@ static int launch_gmres(apc_context *c, int n, const T *val, const T *b, T *x, i
   a.x = x;
   a.U = (T *)k->U;
   a.un = un;
+  a.hh = large ? k->hh : nullptr;
   a.part = k->part;
   a.bar = k->bar;
   a.err = c->d_err;
@@ -527,8 +570,7 @@ static int launch_gmres(apc_context *c, int n, const T *val, const T *b, T *x, i
   a.out_rnorm = k->dres;
   void *args[] = {&a};
   APC_CUDA_TRY(c, cudaEventRecord(c->kev[0], c->s));
-  APC_CUDA_TRY(c, cudaLaunchCooperativeKernel((const void *)gmres_kernel<T, RE>, dim3(blocks), dim3(kThreads),
-                                              args, 0, c->s));
+  APC_CUDA_TRY(c, cudaLaunchCooperativeKernel(kern, dim3(blocks), dim3(kThreads), args, 0, c->s));
   APC_CUDA_TRY(c, cudaEventRecord(c->kev[1], c->s));
   apc_count_launch(c);
   int hi[2];

@@ -71,7 +71,7 @@ typedef struct apc_config {
   int maxnc;             /* first temp-node budget (Mover::Set_maxnc; controller sets 10000).
                             The budget doubles on failure while below nmax_cap. */
   int nmax_cap;          /* budget cap: 1000000 reproduces mover.cpp:20; 0 = no cap */
-  int gmres_restart;     /* -ksp_gmres_restart (PETSc default 30) */
+  int gmres_restart;     /* -ksp_gmres_restart (PETSc default 30), 1..255 */
   double gmres_rtol;     /* -ksp_rtol */
   double gmres_atol;     /* -ksp_atol */
   double gmres_dtol;     /* -ksp_divtol */
@@ -239,8 +239,9 @@ int apc_move_velocity_noalloc(int n_particles, int n_cells, const int *first, co
 /* Apply the PETSc KSP command-line options that the reference's runs pass to both solves
  * (KSPSetFromOptions, solver.cpp:202, 275; run lines in Makefile:30-32): -ksp_gmres_restart,
  * -ksp_rtol, -ksp_atol, -ksp_divtol, -ksp_max_it.  Other arguments are ignored, as PETSc
- * ignores options it does not use.  A restart above 31 returns APC_ERR_UNSUPPORTED (the
- * GMRES kernels keep at most 31 basis vectors); a malformed value APC_ERR_INVALID_ARG. */
+ * ignores options it does not use.  A restart above 255 returns APC_ERR_UNSUPPORTED (the
+ * FP64 GMRES kernel keeps at most 255 basis vectors; the reference's production runs use
+ * 200); a malformed value APC_ERR_INVALID_ARG. */
 int apc_config_from_options(apc_config *cfg, int argc, const char *const *argv);
 
 /* Adaptive time step (ADAPTIVE_TIME_STEP, controller.cpp:146-164), after apc_select:

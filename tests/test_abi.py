@@ -54,7 +54,7 @@ def test_library_loads_and_rejects_invalid_config(gpu_lib):
     h = C.c_void_p()
     assert lib.apc_create(None, C.byref(h)) == -1
     for field, bad in (("n_particles", 0), ("depth", 22), ("depth", 0), ("lm", 8), ("lm", 33),
-                       ("gmres_restart", 0), ("gmres_restart", 32), ("precision", 7), ("bc", 2)):
+                       ("gmres_restart", 0), ("gmres_restart", 256), ("mixed_restart", 32), ("precision", 7), ("bc", 2)):
         c2 = binding.ApcConfig()
         lib.apc_config_default(C.byref(c2))
         c2.n_particles = 100
@@ -94,6 +94,8 @@ def test_petsc_ksp_options(gpu_lib):
                  "-ksp_atol", "1.e-60", "-ksp_rtol", "1e-8", "-ksp_monitor") == 0
     assert (cfg.gmres_restart, cfg.gmres_max_it) == (20, 1000)
     assert cfg.gmres_atol == pytest.approx(1e-60) and cfg.gmres_rtol == pytest.approx(1e-8)
-    assert apply("-ksp_gmres_restart", "200") == -9  # APC_ERR_UNSUPPORTED
-    assert cfg.gmres_restart == 20
+    # the reference's production run line (restart 200) is accepted; above 255 is not
+    assert apply("-ksp_gmres_restart", "200") == 0 and cfg.gmres_restart == 200
+    assert apply("-ksp_gmres_restart", "256") == -9  # APC_ERR_UNSUPPORTED
+    assert cfg.gmres_restart == 200
     assert apply("-ksp_max_it", "abc") == -1

@@ -148,6 +148,35 @@ def test_bitexact_cells_along_a_trajectory_vs_oracle(gpu_lib, oracle_lib):
     gp.close()
 
 
+@pytest.mark.parametrize("restart", [64, 200])
+def test_fp64_gmres_long_restart_vs_oracle(gpu_lib, oracle_lib, restart):
+    """-ksp_gmres_restart above 31 (the reference's production runs use 200): the FP64
+    kernel keeps the Hessenberg matrix in global memory.  Both solves against the oracle's
+    GMRES with the same restart: iteration counts within +-1, fields within 1e-10."""
+    import refbind
+
+    g = np.load(os.path.join(GOLDEN, "zel16.npz"))
+    p = _parts(g)
+    o = refbind.CpuPath("oracle", p, int(g["depth"]), float(g["gfd_c"]), int(g["lm"]))
+    o.set_gmres(restart, float(g["rtol"]))
+    gp = binding.GpuPath(p, int(g["depth"]), float(g["gfd_c"]), int(g["lm"]), restart=restart,
+                         rtol=float(g["rtol"]))
+    assert o.select() == gp.select()
+    o.solve(float(g["c_dens"]), float(g["c_pot"]), -1.0)
+    gp.solve(float(g["c_dens"]), float(g["c_pot"]), -1.0)
+    (d_its, _, d_rs, _), (p_its, _, p_rs, _) = o.solve_stats()[-2:]
+    st = gp.solve_stats()
+    assert st["density_reason"] == d_rs == 2 and st["potential_reason"] == p_rs == 2
+    assert abs(st["density_its"] - d_its) <= 1 and abs(st["potential_its"] - p_its) <= 1
+    if restart == 64:
+        assert p_its > restart  # the potential solve restarts at least once
+    fo, fg = o.fields(), gp.fields()
+    for name in ("density", "potential", "deriv"):
+        assert _rel(getattr(fg, name), getattr(fo, name)) <= FIELD_RTOL, name
+    o.close()
+    gp.close()
+
+
 def test_selection_deeper_than_the_sort_redoes_it(gpu_lib):
     """The particle sort covers the previous selection's deepest level plus two.  After a
     shallow particle set, a clustered one of the same size needs more: the selection must
