@@ -229,7 +229,7 @@ static int transpose_pattern(apc_context *c, int n, int w, int s0, size_t ss, si
   max_count<<<grid_of(n), 256, 0, c->s>>>(n, c->tr_cnt, mx);
   int h = 0;
   APC_CUDA_TRY(c, cudaMemcpyAsync(&h, mx, sizeof(int), cudaMemcpyDeviceToHost, c->s));
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   const int wt = h + 1;
   APC_TRY(apc_ensure(c, tcol, (size_t)n * wt, nullptr));
   APC_TRY(apc_ensure(c, tsrc, (size_t)n * wt, nullptr));
@@ -254,7 +254,7 @@ int apc_get_hessians_device(apc_context *c, double *hxx, double *hyy, double *hz
   gather_hessians<<<grid_of(n), 256, 0, c->s>>>(n, m, c->cell_of, c->pid, c->deriv, hxx, hyy, hzz, hxy, hxz, hyz);
   apc_count_launch(c);
   APC_CUDA_TRY(c, cudaGetLastError());
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   return APC_OK;
 }
 
@@ -286,7 +286,7 @@ int apc_fields_from_rhs(apc_context *c, const double *rhs_dev) {
   APC_TRY(apc_krylov_solve(c, 1, c->rhs, c->potential, &st.potential_its, &st.potential_rnorm,
                            &st.potential_reason, &st.potential_refinements));
   APC_TRY(apc_differentiate(c, c->last_c_field));
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   return APC_OK;
 }
 
@@ -335,7 +335,7 @@ int apc_solve_vjp(apc_context *c, const double *g_deriv, double *g_rhs, double *
   if (g_phi)
     APC_CUDA_TRY(c, cudaMemcpyAsync(g_phi, c->vjp_phi, sizeof(double) * M, cudaMemcpyDeviceToDevice, c->s));
   APC_CUDA_TRY(c, cudaGetLastError());
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   return APC_OK;
 }
 
@@ -408,7 +408,7 @@ int apc_trajectory_vjp(apc_context *c, const apc_trajectory *t, const double *co
                                               cot[4], cot[5]);
   apc_count_launch(c);
   APC_CUDA_TRY(c, cudaGetLastError());
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   return APC_OK;
 }
 

@@ -50,6 +50,7 @@ struct apc_context {
   // owning pointer; per context, so contexts can be driven from different host threads
   std::unordered_map<const void *, size_t> caps;
   cudaStream_t s = nullptr;
+  cudaMemPool_t pool = nullptr;  // the device's stream-ordered pool (all device buffers)
   std::string err;
   int64_t launches = 0;
   bool have_particles = false, have_cells = false, have_fields = false;
@@ -146,6 +147,7 @@ struct apc_context {
   cudaEvent_t kev[2] = {};   // around each GMRES launch
   cudaEvent_t gev[2] = {};   // around the GFD stencil kernel
   cudaEvent_t sev[3] = {};   // solve phase: after assembly, after the density solve, after the potential rhs
+  cudaEvent_t wait_ev = nullptr;  // host waits of a context driven by a batch fiber
   double t_select_ms = 0, t_solve_ms = 0, t_move_ms = 0;
   apc_profile prof{};
   bool step_open = false;    // a select has started a step that move_position will close
@@ -155,9 +157,18 @@ struct apc_context {
 // ----------------------------------------------------------- helpers (host)
 
 int apc_alloc(apc_context *c, void **p, size_t bytes);
+void apc_free(apc_context *c, void *p);  // stream-ordered release of an apc_alloc buffer
+cudaMemPool_t apc_device_pool(int dev);
 template <class T>
 int apc_ensure(apc_context *c, T **p, size_t count, size_t *cap_elems_io = nullptr);
 int apc_read_errors(apc_context *c, int *flags);
+
+// Host waits for the context's stream (or one of its events).  On an ordinary thread they
+// block like cudaStreamSynchronize / cudaEventSynchronize.  Inside a batch fiber
+// (batch.cu) they poll the event and yield to the other boxes' fibers until it completes,
+// so one host thread keeps many boxes' GPU work in flight.
+cudaError_t apc_stream_wait(apc_context *c);
+cudaError_t apc_event_wait(cudaEvent_t e);
 
 // launch accounting
 inline void apc_count_launch(apc_context *c, int k = 1) { c->launches += k; }

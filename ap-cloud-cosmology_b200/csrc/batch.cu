@@ -1,26 +1,118 @@
 // Batches of independent boxes (a batch of contexts stepped together).
 //
 // The reference runs one box per process (test.cpp:16-80) and has no batched entry
-// point.  A batch is one context per box, each with its own CUDA stream.  apc_batch_step
-// hands the boxes to host worker threads through a shared queue ordered largest box
-// first (longest-processing-time order), and each worker runs the box's ordinary
-// apc_step.  The boxes' kernels then run concurrently on the GPU: the many small grids
-// of a 16^3 box leave most SMs idle, and other boxes fill them.  Every box runs the
-// single-context code path, so its results are exactly those of a lone context.
+// point.  A batch is one context per box, each with its own CUDA stream, and every box
+// runs the single-context code path, so its results are exactly those of a lone context.
+//
+// Scheduling.  A small box's step is a chain of short kernels broken by host round trips
+// (level sizes of the selection, hierarchy sizes of the multigrid, solver statistics).
+// Driven one box per blocking host thread, the GPU idles through each round trip and the
+// threads contend for the driver.  Here every box runs as a fiber (a user-space stack
+// switched with swapcontext) on a few host threads.  A host wait inside the library
+// (apc_stream_wait / apc_event_wait) records an event and yields to the next box instead
+// of blocking, so one thread keeps the kernels of many boxes in flight and the boxes'
+// small grids fill the SMs together.  Boxes are dealt to the threads in
+// longest-processing-time order (largest first, round robin).
 #include <cuda_runtime.h>
+#include <sys/mman.h>
+#include <ucontext.h>
 
 #include <algorithm>
-#include <atomic>
 #include <new>
 #include <thread>
 #include <vector>
 
 #include "apc_internal.cuh"
 
+namespace {
+
+constexpr size_t kStackBytes = 8u << 20;  // per box; pages are committed only when touched
+constexpr size_t kGuardBytes = 64u << 10; // no-access guard below each stack
+
+struct Fiber {
+  ucontext_t uc;
+  bool done = false;
+  apc_context *ctx = nullptr;
+  const apc_step_params *params = nullptr;
+  int status = APC_OK;
+  double dv = 0.0, dx = 0.0;
+};
+
+struct Sched {
+  ucontext_t main;
+  Fiber *cur = nullptr;
+};
+
+thread_local Sched *t_sched = nullptr;
+
+void fiber_main() {
+  Fiber *f = t_sched->cur;
+  f->status = apc_step(f->ctx, f->params, nullptr, &f->dv, &f->dx);
+  f->done = true;
+}  // returning resumes uc_link, the scheduler
+
+inline bool in_fiber() { return t_sched && t_sched->cur; }
+
+inline void yield() {
+  Fiber *f = t_sched->cur;
+  swapcontext(&f->uc, &t_sched->main);
+}
+
+// Run the fibers of one host thread until all have finished: each is resumed in turn and
+// runs until it waits on the GPU (yield) or its step ends.
+void run_fibers(std::vector<Fiber *> &fibers, std::vector<char *> &stacks) {
+  Sched sch;
+  t_sched = &sch;
+  for (size_t k = 0; k < fibers.size(); ++k) {
+    Fiber *f = fibers[k];
+    getcontext(&f->uc);
+    f->uc.uc_stack.ss_sp = stacks[k] + kGuardBytes;
+    f->uc.uc_stack.ss_size = kStackBytes - kGuardBytes;
+    f->uc.uc_link = &sch.main;
+    makecontext(&f->uc, fiber_main, 0);
+  }
+  size_t live = fibers.size();
+  while (live) {
+    for (Fiber *f : fibers) {
+      if (f->done) continue;
+      sch.cur = f;
+      swapcontext(&sch.main, &f->uc);
+      sch.cur = nullptr;
+      if (f->done) --live;
+    }
+  }
+  t_sched = nullptr;
+}
+
+}  // namespace
+
+cudaError_t apc_event_wait(cudaEvent_t e) {
+  if (!in_fiber()) return cudaEventSynchronize(e);
+  // every fiber leaves through here with no launch error pending, so the thread's last
+  // error can be cleared after each not-ready poll without losing another box's error
+  const cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess) return pending;
+  for (;;) {
+    const cudaError_t q = cudaEventQuery(e);
+    if (q != cudaErrorNotReady) return q;
+    cudaGetLastError();
+    yield();
+  }
+}
+
+cudaError_t apc_stream_wait(apc_context *c) {
+  if (!in_fiber()) return cudaStreamSynchronize(c->s);
+  const cudaError_t e = cudaEventRecord(c->wait_ev, c->s);
+  if (e != cudaSuccess) return e;
+  return apc_event_wait(c->wait_ev);
+}
+
 struct apc_batch {
   std::vector<apc_context *> ctx;
   std::vector<int> order;  // boxes by decreasing particle count
-  int workers = 1;
+  int threads = 1;
+  char *stack_base = nullptr;  // n_boxes stacks of kStackBytes, guard page first
+  size_t stack_bytes = 0;
 };
 
 extern "C" {
@@ -39,11 +131,21 @@ int apc_batch_create(const apc_config *cfgs, int n_boxes, int n_workers, apc_bat
       return rc;
     }
   }
+  b->stack_bytes = kStackBytes * (size_t)n_boxes;
+  void *m = mmap(nullptr, b->stack_bytes, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS | MAP_NORESERVE,
+                 -1, 0);
+  if (m == MAP_FAILED) {
+    b->stack_bytes = 0;
+    apc_batch_destroy(b);
+    return APC_ERR_OUT_OF_MEMORY;
+  }
+  b->stack_base = static_cast<char *>(m);
+  for (int i = 0; i < n_boxes; ++i) mprotect(b->stack_base + kStackBytes * (size_t)i, kGuardBytes, PROT_NONE);
   b->order.resize(n_boxes);
   for (int i = 0; i < n_boxes; ++i) b->order[i] = i;
   std::stable_sort(b->order.begin(), b->order.end(),
                    [&](int a, int c) { return cfgs[a].n_particles > cfgs[c].n_particles; });
-  b->workers = n_workers > 0 ? std::min(n_workers, n_boxes) : std::min(n_boxes, 8);
+  b->threads = n_workers > 0 ? std::min(n_workers, n_boxes) : std::min(n_boxes, 8);
   *out = b;
   return APC_OK;
 }
@@ -52,6 +154,7 @@ int apc_batch_destroy(apc_batch *b) {
   if (!b) return APC_ERR_INVALID_ARG;
   for (apc_context *c : b->ctx)
     if (c) apc_destroy(c);
+  if (b->stack_base) munmap(b->stack_base, b->stack_bytes);
   delete b;
   return APC_OK;
 }
@@ -66,32 +169,37 @@ apc_context *apc_batch_context(apc_batch *b, int box) {
 int apc_batch_step(apc_batch *b, const apc_step_params *params, int *status, double *max_dv, double *max_dx) {
   if (!b || !params) return APC_ERR_INVALID_ARG;
   const int n = (int)b->ctx.size();
-  std::vector<int> st(n, APC_OK);
-  std::atomic<int> next{0};
-  auto work = [&]() {
-    for (;;) {
-      const int k = next.fetch_add(1);
-      if (k >= n) return;
+  std::vector<Fiber> fib(n);
+  for (int i = 0; i < n; ++i) {
+    fib[i].ctx = b->ctx[i];
+    fib[i].params = &params[i];
+  }
+  const int T = b->threads;
+  auto work = [&](int t) {
+    std::vector<Fiber *> mine;
+    std::vector<char *> stacks;
+    for (int k = t; k < n; k += T) {
       const int i = b->order[k];
-      double dv = 0.0, dx = 0.0;
-      st[i] = apc_step(b->ctx[i], &params[i], nullptr, &dv, &dx);
-      if (max_dv) max_dv[i] = dv;
-      if (max_dx) max_dx[i] = dx;
+      mine.push_back(&fib[i]);
+      stacks.push_back(b->stack_base + kStackBytes * (size_t)i);
     }
+    run_fibers(mine, stacks);
   };
-  if (b->workers <= 1) {
-    work();
+  if (T <= 1) {
+    work(0);
   } else {
     std::vector<std::thread> pool;
-    pool.reserve(b->workers - 1);
-    for (int w = 1; w < b->workers; ++w) pool.emplace_back(work);
-    work();
-    for (std::thread &t : pool) t.join();
+    pool.reserve(T - 1);
+    for (int t = 1; t < T; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (std::thread &th : pool) th.join();
   }
   int first = APC_OK;
   for (int i = 0; i < n; ++i) {
-    if (status) status[i] = st[i];
-    if (first == APC_OK && st[i] != APC_OK) first = st[i];
+    if (status) status[i] = fib[i].status;
+    if (max_dv) max_dv[i] = fib[i].dv;
+    if (max_dx) max_dx[i] = fib[i].dx;
+    if (first == APC_OK && fib[i].status != APC_OK) first = fib[i].status;
   }
   return first;
 }

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <unordered_map>
 #include <vector>
 
@@ -14,15 +15,50 @@
 
 // --------------------------------------------------------------- allocation
 
+// Device buffers come from one stream-ordered memory pool per device: allocation and
+// release are ordered on the context's stream, so growing a buffer between steps never
+// synchronises the device (cudaFree would wait for every stream, stalling the other
+// boxes of a batch).  Freed blocks stay in the pool for reuse until a context is
+// destroyed, which trims the pool's unused memory.  Reuse across streams waits for the
+// free to complete instead of adding a cross-stream dependency.
+cudaMemPool_t apc_device_pool(int dev) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  if (dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps pr{};
+    pr.allocType = cudaMemAllocationTypePinned;
+    pr.location.type = cudaMemLocationTypeDevice;
+    pr.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &pr) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    uint64_t keep = UINT64_MAX;
+    int no = 0;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    cudaMemPoolSetAttribute(p, cudaMemPoolReuseAllowInternalDependencies, &no);
+    pools[dev] = p;
+  }
+  return pools[dev];
+}
+
 int apc_alloc(apc_context *c, void **p, size_t bytes) {
   *p = nullptr;
-  cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+  cudaError_t e = cudaMallocFromPoolAsync(p, std::max<size_t>(bytes, 16), c->pool, c->s);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    c->err = std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e);
+    *p = nullptr;
+    c->err = std::string("device allocation of ") + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e);
     return e == cudaErrorMemoryAllocation ? APC_ERR_OUT_OF_MEMORY : APC_ERR_CUDA;
   }
   return APC_OK;
+}
+
+void apc_free(apc_context *c, void *p) {
+  if (p) cudaFreeAsync(p, c->s);
 }
 
 template <class T>
@@ -30,8 +66,7 @@ int apc_ensure(apc_context *c, T **p, size_t count, size_t *) {
   size_t &cap = c->caps[(const void *)p];
   if (*p && cap >= count) return APC_OK;
   if (*p) {
-    cudaStreamSynchronize(c->s);
-    cudaFree(*p);
+    apc_free(c, *p);  // ordered after the work already queued on the stream
     *p = nullptr;
   }
   size_t want = std::max<size_t>(count + count / 4, 64);
@@ -47,7 +82,7 @@ template int apc_ensure<uint64_t>(apc_context *, uint64_t **, size_t, size_t *);
 
 int apc_read_errors(apc_context *c, int *flags) {
   APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 1, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->s));
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   *flags = c->h_pinned[1];
   return APC_OK;
 }
@@ -91,13 +126,17 @@ void free_all(apc_context *c) {
                   c->warm_phi, c->tr_cnt, c->tr_off, c->tr_cur, c->tr_tmp,
                   c->tp_col, c->tp_src, c->ta_col, c->ta_src, c->ta_val, c->vjp_c, c->vjp_phi, c->vjp_r2,
                   c->vjp_rho};
-  for (void *p : ptrs)
-    if (p) cudaFree(p);
+  if (c->s) {
+    for (void *p : ptrs) apc_free(c, p);
+    cudaStreamSynchronize(c->s);
+  }
+  if (c->pool) cudaMemPoolTrimTo(c->pool, 0);
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
   for (auto &e : c->kev)
     if (e) cudaEventDestroy(e);
+  if (c->wait_ev) cudaEventDestroy(c->wait_ev);
   for (auto &e : c->gev)
     if (e) cudaEventDestroy(e);
   for (auto &e : c->sev)
@@ -206,6 +245,8 @@ int apc_create(const apc_config *cfg, apc_context **out) {
     return fail(APC_ERR_CUDA);
   }
   if (cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking) != cudaSuccess) return fail(APC_ERR_CUDA);
+  c->pool = apc_device_pool(c->dev);
+  if (!c->pool) return fail(APC_ERR_CUDA);
   for (auto &e : c->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(APC_ERR_CUDA);
   for (auto &e : c->kev)
@@ -214,6 +255,7 @@ int apc_create(const apc_config *cfg, apc_context **out) {
     if (cudaEventCreate(&e) != cudaSuccess) return fail(APC_ERR_CUDA);
   for (auto &e : c->sev)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(APC_ERR_CUDA);
+  if (cudaEventCreateWithFlags(&c->wait_ev, cudaEventDisableTiming) != cudaSuccess) return fail(APC_ERR_CUDA);
   if (cudaMallocHost((void **)&c->h_pinned, 64 * sizeof(int)) != cudaSuccess) return fail(APC_ERR_CUDA);
   const size_t n = (size_t)c->n;
   double **dbl[] = {&c->px, &c->py, &c->pz, &c->pvx, &c->pvy, &c->pvz, &c->pax, &c->pay, &c->paz,
@@ -314,7 +356,7 @@ static int get_particles_impl(apc_context *c, double *const *dst, int count, cud
     apc_count_launch(c);
     APC_CUDA_TRY(c, cudaMemcpyAsync(dst[k], c->qx, bytes, kind, c->s));
   }
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   return APC_OK;
 }
 
@@ -356,7 +398,7 @@ int apc_select(apc_context *c, int *n_cells) {
   }
   APC_TRY(rc);
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[1], c->s));
-  APC_CUDA_TRY(c, cudaEventSynchronize(c->ev[1]));
+  APC_CUDA_TRY(c, apc_event_wait(c->ev[1]));
   c->t_select_ms = elapsed(c->ev[0], c->ev[1]);
   c->prof.select_ms += c->t_select_ms;
   c->numnodes.clear();
@@ -392,7 +434,7 @@ int apc_solve(apc_context *c, double c_dens, double c_pot, double c_field) {
   c->last_c_field = c_field;
   (void)M;
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[3], c->s));
-  APC_CUDA_TRY(c, cudaEventSynchronize(c->ev[3]));
+  APC_CUDA_TRY(c, apc_event_wait(c->ev[3]));
   c->t_solve_ms = elapsed(c->ev[2], c->ev[3]);
   c->prof.assemble_ms += elapsed(c->ev[2], c->sev[0]);
   c->prof.density_ms += elapsed(c->sev[0], c->sev[1]);
@@ -418,7 +460,7 @@ int apc_move_position(apc_context *c, double dt, double c_pos, double *max_dx) {
   cudaSetDevice(c->dev);
   APC_TRY(apc_mover_position(c, dt, c_pos, max_dx));
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[6], c->s));
-  APC_CUDA_TRY(c, cudaEventSynchronize(c->ev[6]));
+  APC_CUDA_TRY(c, apc_event_wait(c->ev[6]));
   if (c->kick_recorded) {
     c->t_move_ms = elapsed(c->ev[4], c->ev[6]);
     c->prof.move_ms += c->t_move_ms;
@@ -442,7 +484,7 @@ int apc_step(apc_context *c, const apc_step_params *p, int *n_cells, double *max
 
 int apc_synchronize(apc_context *c) {
   if (!c) return APC_ERR_INVALID_ARG;
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   return APC_OK;
 }
 

@@ -493,14 +493,14 @@ struct KrylovWork {
 void apc_krylov_free(apc_context *c) {
   KrylovWork *k = c->kw;
   if (!k) return;
-  cudaFree(k->U);
-  cudaFree(k->part);
-  cudaFree(k->bar);
-  cudaFree(k->ires);
-  cudaFree(k->dres);
-  cudaFree(k->r);
-  cudaFree(k->a32);
-  cudaFree(k->hh);
+  apc_free(c, k->U);
+  apc_free(c, k->part);
+  apc_free(c, k->bar);
+  apc_free(c, k->ires);
+  apc_free(c, k->dres);
+  apc_free(c, k->r);
+  apc_free(c, k->a32);
+  apc_free(c, k->hh);
   delete k;
   c->kw = nullptr;
 }
@@ -520,7 +520,7 @@ static int launch_gmres(apc_context *c, int n, const T *val, const T *b, T *x, i
   const size_t un = ((size_t)n + 31) & ~(size_t)31;
   const size_t need = un * (restart + 1) * sizeof(T);
   if (need > k->u_bytes) {
-    cudaFree(k->U);
+    apc_free(c, k->U);
     k->U = nullptr;
     APC_TRY(apc_alloc(c, &k->U, need));
     k->u_bytes = need;
@@ -539,7 +539,7 @@ static int launch_gmres(apc_context *c, int n, const T *val, const T *b, T *x, i
   if (large) {
     const size_t hb = sizeof(double) * (size_t)blocks * (restart + 1) * restart;
     if (hb > k->hh_bytes) {
-      cudaFree(k->hh);
+      apc_free(c, k->hh);
       k->hh = nullptr;
       APC_TRY(apc_alloc(c, (void **)&k->hh, hb));
       k->hh_bytes = hb;
@@ -577,7 +577,7 @@ static int launch_gmres(apc_context *c, int n, const T *val, const T *b, T *x, i
   double hd;
   APC_CUDA_TRY(c, cudaMemcpyAsync(hi, k->ires, sizeof(hi), cudaMemcpyDeviceToHost, c->s));
   APC_CUDA_TRY(c, cudaMemcpyAsync(&hd, k->dres, sizeof(hd), cudaMemcpyDeviceToHost, c->s));
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   int derr = 0;
   APC_TRY(apc_read_errors(c, &derr));
   if (derr & DERR_KRYLOV) {
@@ -618,7 +618,7 @@ static int ensure_work(apc_context *c, int n) {
   }
   KrylovWork *k = c->kw;
   if (n > k->cap_n) {
-    cudaFree(k->r);
+    apc_free(c, k->r);
     k->r = nullptr;
     const int cap = n + n / 4 + 1024;
     APC_TRY(apc_alloc(c, (void **)&k->r, sizeof(double) * cap));

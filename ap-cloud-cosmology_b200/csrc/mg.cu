@@ -805,23 +805,23 @@ void apc_mg_free(apc_context *c) {
   if (!m) return;
   for (auto &L : m->lv) {
     if (L.owns_matrix) {
-      cudaFree(L.col);
-      cudaFree(L.val);
+      apc_free(c, L.col);
+      apc_free(c, L.val);
     }
-    cudaFree(L.dinv);
-    cudaFree(L.code);
-    cudaFree(L.agg);
-    cudaFree(L.mptr);
-    cudaFree(L.mem);
-    cudaFree(L.x);
-    cudaFree(L.x2);
-    cudaFree(L.b);
-    cudaFree(L.r);
+    apc_free(c, L.dinv);
+    apc_free(c, L.code);
+    apc_free(c, L.agg);
+    apc_free(c, L.mptr);
+    apc_free(c, L.mem);
+    apc_free(c, L.x);
+    apc_free(c, L.x2);
+    apc_free(c, L.b);
+    apc_free(c, L.r);
   }
   void *p[] = {m->coarse_inv, m->pkey, m->pkey_alt, m->pidx, m->pidx_alt, m->eflag, m->epos, m->ucol,
                m->rowstart, m->uval, m->V, m->Z, m->vin, m->vout, m->dvec,
                m->partial, m->dots, m->counter, m->state, m->total};
-  for (void *q : p) cudaFree(q);
+  for (void *q : p) apc_free(c, q);
   if (m->host) cudaFreeHost(m->host);
   for (int k = 0; k < 2; ++k) {
     if (m->solve_exec[k]) cudaGraphExecDestroy(m->solve_exec[k]);
@@ -836,7 +836,7 @@ void apc_mg_free(apc_context *c) {
 static int read_int(apc_context *c, const int *dev, int *host) {
   // through the context's pinned word: a pageable destination would be staged
   APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 10, dev, sizeof(int), cudaMemcpyDeviceToHost, c->s));
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   *host = c->h_pinned[10];
   return APC_OK;
 }
@@ -916,7 +916,7 @@ static int mg_build(apc_context *c) {
     // the row width and the error flags in one round trip
     APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 8, m->total, sizeof(int), cudaMemcpyDeviceToHost, c->s));
     APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 9, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->s));
-    APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+    APC_CUDA_TRY(c, apc_stream_wait(c));
     const int wc = c->h_pinned[8], derr = c->h_pinned[9];
     if (derr & DERR_STENCIL_MANY) {
       c->err = "multigrid coarse row exceeds its buffers";
@@ -957,7 +957,7 @@ static int mg_build(apc_context *c) {
   std::vector<float> val(K.ld * K.w);
   APC_CUDA_TRY(c, cudaMemcpyAsync(col.data(), K.col, sizeof(int) * col.size(), cudaMemcpyDeviceToHost, c->s));
   APC_CUDA_TRY(c, cudaMemcpyAsync(val.data(), K.val, sizeof(float) * val.size(), cudaMemcpyDeviceToHost, c->s));
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   std::vector<double> a((size_t)n * n, 0.0), inv((size_t)n * n, 0.0);
   for (int i = 0; i < n; ++i) {
     for (int s = 0; s < K.w; ++s) a[(size_t)i * n + col[(size_t)s * K.ld + i]] += val[(size_t)s * K.ld + i];
@@ -995,7 +995,7 @@ static int mg_build(apc_context *c) {
   APC_TRY(apc_ensure(c, &m->coarse_inv, (size_t)n * n + 1));
   APC_CUDA_TRY(c, cudaMemcpyAsync(m->coarse_inv, invf.data(), sizeof(float) * invf.size(), cudaMemcpyHostToDevice,
                                   c->s));
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   m->coarse_n = n;
   return APC_OK;
 }
@@ -1289,7 +1289,7 @@ int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, cons
   const apc_config &cfg = c->cfg;
   const auto t0 = std::chrono::steady_clock::now();
   if (use_mg) {
-    APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+    APC_CUDA_TRY(c, apc_stream_wait(c));
     APC_TRY(mg_build(c));
   }
   IrSolveArgs a{};
@@ -1320,7 +1320,7 @@ int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, cons
   APC_CUDA_TRY(c, cudaGraphLaunch(m->solve_exec[which], c->s));
   APC_CUDA_TRY(c, cudaEventRecord(c->kev[1], c->s));
   APC_CUDA_TRY(c, cudaMemcpyAsync(m->host, m->state, sizeof(IrState), cudaMemcpyDeviceToHost, c->s));
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   APC_CUDA_TRY(c, cudaGetLastError());
   const IrState &S = *reinterpret_cast<const IrState *>(m->host);
   float ms = 0.f;

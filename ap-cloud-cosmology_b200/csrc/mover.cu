@@ -136,7 +136,7 @@ int apc_mover_max_density(apc_context *c, double *out) {
   APC_CUDA_TRY(c, cudaGetLastError());
   unsigned long long *hb = (unsigned long long *)(c->h_pinned + 12);  // pinned, 8-byte aligned
   APC_CUDA_TRY(c, cudaMemcpyAsync(hb, mb, sizeof(*hb), cudaMemcpyDeviceToHost, c->s));
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   memcpy(out, hb, sizeof(double));
   return APC_OK;
 }
@@ -165,7 +165,7 @@ int apc_mover_velocity(apc_context *c, double dt, double c_vel, double *max_dv) 
   if (max_dv) {
     unsigned long long *hb = (unsigned long long *)(c->h_pinned + 12);  // pinned, 8-byte aligned
     APC_CUDA_TRY(c, cudaMemcpyAsync(hb, mb, sizeof(*hb), cudaMemcpyDeviceToHost, c->s));
-    APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+    APC_CUDA_TRY(c, apc_stream_wait(c));
     double v;
     memcpy(&v, hb, sizeof(v));
     *max_dv = std::sqrt(v);
@@ -186,7 +186,7 @@ int apc_mover_position(apc_context *c, double dt, double c_pos, double *max_dx) 
   if (max_dx) {
     unsigned long long *hb = (unsigned long long *)(c->h_pinned + 12);  // pinned, 8-byte aligned
     APC_CUDA_TRY(c, cudaMemcpyAsync(hb, mb, sizeof(*hb), cudaMemcpyDeviceToHost, c->s));
-    APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+    APC_CUDA_TRY(c, apc_stream_wait(c));
     double v;
     memcpy(&v, hb, sizeof(v));
     *max_dx = std::sqrt(v);

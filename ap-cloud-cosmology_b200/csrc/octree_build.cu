@@ -135,7 +135,7 @@ int apc_sorted_keys_copy(apc_context *c, uint64_t **keys, uint32_t **ids) {
   *keys = alt ? c->full_keys_alt : c->full_keys;
   *ids = alt ? c->full_ids_alt : c->full_ids;
   // callers read the copies with plain cudaMemcpy, which does not wait for this stream
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   return APC_OK;
 }
 
@@ -154,7 +154,7 @@ int apc_octree_levels_count(apc_context *c) {
   APC_CUDA_TRY(c, cudaGetLastError());
   int h[24];
   APC_CUDA_TRY(c, cudaMemcpyAsync(h, hist, sizeof(h), cudaMemcpyDeviceToHost, c->s));
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   // keys first differing at level lev+1 create a new node on every level >= lev+1
   c->numnodes[0] = 1;
   for (int k = 1; k <= D; ++k) {

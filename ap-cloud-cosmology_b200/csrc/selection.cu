@@ -324,7 +324,7 @@ int grid_for(long long n) { return (int)std::max<long long>(1, (n + kT - 1) / kT
 
 static int read_int(apc_context *c, const int *dev, int *host) {
   APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned, dev, sizeof(int), cudaMemcpyDeviceToHost, c->s));
-  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   *host = c->h_pinned[0];
   return APC_OK;
 }
@@ -344,11 +344,10 @@ static int ensure_open_cap(apc_context *c, long long need) {
     APC_CUDA_TRY(c, cudaMemcpyAsync(nb, c->op_base, sizeof(int) * c->op_cap, cudaMemcpyDeviceToDevice, c->s));
     APC_CUDA_TRY(c, cudaMemcpyAsync(nf, c->op_first, sizeof(int) * c->op_cap, cudaMemcpyDeviceToDevice, c->s));
     APC_CUDA_TRY(c, cudaMemcpyAsync(nn, c->op_count, sizeof(int) * c->op_cap, cudaMemcpyDeviceToDevice, c->s));
-    APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
-    cudaFree(c->op_code);
-    cudaFree(c->op_base);
-    cudaFree(c->op_first);
-    cudaFree(c->op_count);
+    apc_free(c, c->op_code);
+    apc_free(c, c->op_base);
+    apc_free(c, c->op_first);
+    apc_free(c, c->op_count);
   }
   c->op_code = nc;
   c->op_base = nb;
@@ -360,8 +359,8 @@ static int ensure_open_cap(apc_context *c, long long need) {
 
 static int ensure_hash(apc_context *c, uint64_t **keys, void **vals, size_t val_size, int *cap, int want) {
   if (want > *cap) {
-    if (*keys) cudaFree(*keys);
-    if (*vals) cudaFree(*vals);
+    apc_free(c, *keys);
+    apc_free(c, *vals);
     *keys = nullptr;
     *vals = nullptr;
     APC_TRY(apc_alloc(c, (void **)keys, sizeof(uint64_t) * (size_t)want));

@@ -32,6 +32,11 @@ import sys
 import threading
 import time
 
+# 32 hardware work queues instead of CUDA's default 8, read when the CUDA context is
+# created: the batched workload keeps one stream per box in flight, and with 8 queues
+# streams share queues and wait on one another's kernels.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "ap-cloud-cosmology_b200")
 sys.path.insert(0, PKG)

@@ -311,14 +311,14 @@ int apc_trajectory_vjp(apc_context *ctx, const apc_trajectory *t, const double *
 /* ---- batches of independent boxes ----
  * The reference runs one box per process (test.cpp:16-80); it has no batched
  * interface.  A batch owns one context per box (each with its own stream) and steps
- * them together: host worker threads take boxes from a queue, largest first, and each
- * runs that box's apc_step (controller.cpp:133-197, the same code path as a single
- * context), so the GPU overlaps the kernels of many small boxes.  Per-box results are
- * those of the single-box path. */
+ * them together.  Each box's apc_step (controller.cpp:133-197, the same code path as a
+ * single context) runs as a fiber on one of a few host threads, boxes dealt largest
+ * first.  A fiber that waits on the GPU yields to the next box, so the GPU overlaps
+ * the kernels of many small boxes.  Per-box results are those of the single-box path. */
 typedef struct apc_batch apc_batch;
 
 /* Create n_boxes contexts from cfgs[0..n_boxes-1] (all on cfgs[i].device), stepped by
- * n_workers host threads (0 = min(n_boxes, 8)). */
+ * n_workers host threads (0 = min(n_boxes, 8)), each running its boxes as fibers. */
 int apc_batch_create(const apc_config *cfgs, int n_boxes, int n_workers, apc_batch **out);
 int apc_batch_destroy(apc_batch *b);
 int apc_batch_size(const apc_batch *b);

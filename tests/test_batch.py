@@ -84,16 +84,18 @@ def test_batch_shard_two_gloo_ranks(tmp_path):
 
 
 @pytest.mark.gpu
-def test_batch_matches_single_contexts():
+@pytest.mark.parametrize("workers", [1, 4])
+def test_batch_matches_single_contexts(workers):
     """Boxes stepped together through apc_batch_step end exactly where the same boxes end
-    when each runs alone through its own context."""
+    when each runs alone through its own context: with one host thread running all six
+    boxes as fibers, and with four threads."""
     from apcloud import binding
     from apcloud.batch import BatchRun
     from apcloud.controller import Controller
 
-    cfgs = [c for c in ics.batch_boxes(n_boxes=12, seed=11, sides=(16, 24)) ][:6]
+    cfgs = ics.batch_boxes(n_boxes=12, seed=11, sides=(16, 24))[:6]
     steps = 3
-    br = BatchRun(cfgs, precision=binding.APC_PREC_MIXED, n_workers=4)
+    br = BatchRun(cfgs, precision=binding.APC_PREC_MIXED, n_workers=workers)
     br.start()
     for _ in range(steps):
         br.step()
