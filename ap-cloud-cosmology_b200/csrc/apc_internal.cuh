@@ -180,8 +180,13 @@ int apc_selection(apc_context *c);           // top-down + balance + cells (sele
 constexpr int APC_RETRY_FULL_SORT = -100;    // internal: the selection went deeper than the sort
 int apc_sorted_keys_copy(apc_context *c, uint64_t **keys, uint32_t **ids);  // octree_build.cu
 int apc_gfd_assemble(apc_context *c, double c_dens);    // gfd.cu
+// during (optional): host work run while the mixed solve's graph runs on the GPU, before
+// the host waits for its outcome
 int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int *its,
-                     double *rnorm, int *reason, int *refinements);  // krylov.cu
+                     double *rnorm, int *reason, int *refinements,
+                     int (*during)(apc_context *) = nullptr);  // krylov.cu
+// the potential operator in FP32, Jacobi-scaled (c->a2 -> c->a2f), on stream s
+void apc_potential_to_f32(apc_context *c, cudaStream_t s);  // krylov.cu
 void apc_krylov_free(apc_context *c);
 int apc_gmres_fp64_ell(apc_context *c, int n, int w, size_t ld, const int *col, const double *val,
                        const double *b, double *x, int *its, double *rnorm, int *reason);  // krylov.cu
@@ -192,7 +197,16 @@ void apc_mg_free(apc_context *c);
 // is rebuilt from valf
 int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, const float *valf, const double *b,
                  double *x, double *r, int restart, double rtol_in, int *its, double *rnorm, int *reason,
-                 int *refinements, int *levels);
+                 int *refinements, int *levels, int (*during)(apc_context *) = nullptr);
+// Overlap of the potential solve's set-up with the density solve (mg.cu).  After the
+// assembly, apc_mg_mark_assembled records where the potential operator is ready;
+// apc_mg_prebuild, run while the density graph executes, converts that operator to FP32
+// and builds the multigrid hierarchy on a second stream, and makes the context's stream
+// wait for it; the potential solve then uses the prebuilt hierarchy (apc_mg_prebuilt)
+// instead of building its own.
+int apc_mg_mark_assembled(apc_context *c);
+int apc_mg_prebuild(apc_context *c);
+bool apc_mg_prebuilt(const apc_context *c);
 int apc_warm_save(apc_context *c);                       // warmstart.cu
 int apc_warm_guess(apc_context *c, int which, double *x);
 int apc_potential_rhs(apc_context *c, double c_pot);    // gfd.cu

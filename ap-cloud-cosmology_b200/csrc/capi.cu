@@ -419,9 +419,12 @@ int apc_solve(apc_context *c, double c_dens, double c_pot, double c_field) {
     APC_TRY(apc_ensure(c, &c->a2f, (size_t)c->m_cap * c->ell_w, nullptr));
   }
   apc_solve_stats &st = c->stats;
+  // mixed path with multigrid: the potential hierarchy is built while the density solve runs
+  const bool overlap = c->cfg.precision == APC_PREC_MIXED && c->cfg.mixed_precond == APC_PRECOND_MULTIGRID;
+  if (overlap) APC_TRY(apc_mg_mark_assembled(c));
   APC_CUDA_TRY(c, cudaEventRecord(c->sev[0], c->s));
   APC_TRY(apc_krylov_solve(c, 0, c->rhs, c->density, &st.density_its, &st.density_rnorm, &st.density_reason,
-                           &st.density_refinements));
+                           &st.density_refinements, overlap ? apc_mg_prebuild : nullptr));
   APC_CUDA_TRY(c, cudaEventRecord(c->sev[1], c->s));
   APC_TRY(apc_potential_rhs(c, c_pot));
   APC_CUDA_TRY(c, cudaEventRecord(c->sev[2], c->s));

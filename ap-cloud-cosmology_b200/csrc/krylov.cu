@@ -646,8 +646,16 @@ int apc_gmres_fp64_ell(apc_context *c, int n, int w, size_t ld, const int *col, 
 // Jacobi-scaled system (D^-1 A) d = D^-1 r / ||D^-1 r|| in FP32 to the inner tolerance,
 // by GMRES(CGS2) or, for the potential with the multigrid option, by FGMRES with the
 // octree-aggregation V-cycle.
+void apc_potential_to_f32(apc_context *c, cudaStream_t s) {
+  const int n = c->nc + c->nv;
+  const size_t ell_count = (size_t)c->m_cap * c->ell_w;
+  ell_to_f32_scaled<<<std::min<size_t>((ell_count + 255) / 256, 8192), 256, 0, s>>>((size_t)c->m_cap, c->ell_w, n,
+                                                                                    c->a2, c->a2f);
+  apc_count_launch(c);
+}
+
 int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int *its, double *rnorm,
-                     int *reason, int *refinements) {
+                     int *reason, int *refinements, int (*during)(apc_context *)) {
   const int n = c->nc + c->nv;
   APC_TRY(ensure_work(c, n));
   KrylovWork *k = c->kw;
@@ -663,9 +671,13 @@ int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int 
   const size_t ell_count = (size_t)c->m_cap * c->ell_w;
   float *af = which == 0 ? c->a1f : c->a2f;
   const int G = std::max(1, std::min((n + 255) / 256, std::min(apc_sm_count(c) * 8, 4096)));
-  ell_to_f32_scaled<<<std::min<size_t>((ell_count + 255) / 256, 8192), 256, 0, c->s>>>((size_t)c->m_cap, c->ell_w,
-                                                                                       n, val, af);
-  apc_count_launch(c);
+  // a prebuilt potential hierarchy (apc_mg_prebuild) came with its FP32 operator
+  const bool prebuilt = which == 1 && apc_mg_prebuilt(c);
+  if (!prebuilt) {
+    ell_to_f32_scaled<<<std::min<size_t>((ell_count + 255) / 256, 8192), 256, 0, c->s>>>((size_t)c->m_cap,
+                                                                                         c->ell_w, n, val, af);
+    apc_count_launch(c);
+  }
   if (cfg.warm_start) {
     APC_TRY(apc_warm_guess(c, which, x));
   } else {
@@ -682,7 +694,7 @@ int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int 
   const double rtol_in = cfg.mixed_inner_rtol > 0 ? cfg.mixed_inner_rtol : (use_mg ? 1e-3 : 1e-5);
   int levels = 0;
   APC_TRY(apc_ir_solve(c, which, use_mg, val, af, b, x, k->r, m32, rtol_in, its, rnorm, reason, refinements,
-                       &levels));
+                       &levels, during));
   if (use_mg) c->stats.mg_levels = levels;
   return APC_OK;
 }

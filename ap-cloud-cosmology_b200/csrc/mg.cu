@@ -793,6 +793,10 @@ struct MgWork {
   cudaGraph_t solve_graph[2] = {nullptr, nullptr};  // density, potential
   cudaGraphExec_t solve_exec[2] = {nullptr, nullptr};
   int64_t vcycle_nodes[2] = {0, 0};
+  // the hierarchy built while the density solve runs (apc_mg_prebuild)
+  cudaStream_t side = nullptr;
+  cudaEvent_t side_ev[2] = {nullptr, nullptr};  // operator assembled (main), hierarchy built (side)
+  bool prebuilt = false;
 };
 
 static MgWork *mg(apc_context *c) {
@@ -829,6 +833,9 @@ void apc_mg_free(apc_context *c) {
   }
   for (cudaStream_t q : m->cap)
     if (q) cudaStreamDestroy(q);
+  if (m->side) cudaStreamDestroy(m->side);
+  for (cudaEvent_t e : m->side_ev)
+    if (e) cudaEventDestroy(e);
   delete m;
   c->mg = nullptr;
 }
@@ -1263,7 +1270,7 @@ static int capture_solve(apc_context *c, const IrSolveArgs &a) {
 // one graph and run; the host reads the outcome once.
 int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, const float *valf, const double *b,
                  double *x, double *r, int restart, double rtol_in, int *its, double *rnorm, int *reason,
-                 int *refinements, int *levels) {
+                 int *refinements, int *levels, int (*during)(apc_context *)) {
   MgWork *m = mg(c);
   const int n = c->nc + c->nv;
   const size_t vn = ((size_t)n + 31) & ~(size_t)31;
@@ -1288,7 +1295,9 @@ int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, cons
     if (!m->cap[k]) APC_CUDA_TRY(c, cudaStreamCreateWithFlags(&m->cap[k], cudaStreamNonBlocking));
   const apc_config &cfg = c->cfg;
   const auto t0 = std::chrono::steady_clock::now();
-  if (use_mg) {
+  const bool prebuilt = use_mg && m->prebuilt;  // built during the density solve
+  m->prebuilt = false;
+  if (use_mg && !prebuilt) {
     APC_CUDA_TRY(c, apc_stream_wait(c));
     APC_TRY(mg_build(c));
   }
@@ -1320,6 +1329,7 @@ int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, cons
   APC_CUDA_TRY(c, cudaGraphLaunch(m->solve_exec[which], c->s));
   APC_CUDA_TRY(c, cudaEventRecord(c->kev[1], c->s));
   APC_CUDA_TRY(c, cudaMemcpyAsync(m->host, m->state, sizeof(IrState), cudaMemcpyDeviceToHost, c->s));
+  if (during) APC_TRY(during(c));
   APC_CUDA_TRY(c, apc_stream_wait(c));
   APC_CUDA_TRY(c, cudaGetLastError());
   const IrState &S = *reinterpret_cast<const IrState *>(m->host);
@@ -1338,3 +1348,39 @@ int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, cons
   }
   return APC_OK;
 }
+
+int apc_mg_mark_assembled(apc_context *c) {
+  MgWork *m = mg(c);
+  if (!m->side) {
+    APC_CUDA_TRY(c, cudaStreamCreateWithFlags(&m->side, cudaStreamNonBlocking));
+    for (cudaEvent_t &e : m->side_ev) APC_CUDA_TRY(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  m->prebuilt = false;
+  APC_CUDA_TRY(c, cudaEventRecord(m->side_ev[0], c->s));
+  return APC_OK;
+}
+
+// Runs while the density solve's graph executes on the context's stream: the potential
+// operator's FP32 copy and the multigrid hierarchy are built on the side stream, after
+// the assembly recorded by apc_mg_mark_assembled.  The buffers they touch are not used by
+// the density solve.  The library's helpers all work on c->s, so c->s names the side
+// stream for the duration; allocations and releases are then ordered on it.
+int apc_mg_prebuild(apc_context *c) {
+  MgWork *m = c->mg;
+  if (!m || !m->side) return APC_ERR_INVALID_ARG;
+  const auto t0 = std::chrono::steady_clock::now();
+  cudaStream_t main = c->s;
+  APC_CUDA_TRY(c, cudaStreamWaitEvent(m->side, m->side_ev[0], 0));
+  c->s = m->side;
+  apc_potential_to_f32(c, c->s);
+  int rc = mg_build(c);
+  if (rc == APC_OK && cudaEventRecord(m->side_ev[1], c->s) != cudaSuccess) rc = APC_ERR_CUDA;
+  c->s = main;
+  APC_TRY(rc);
+  APC_CUDA_TRY(c, cudaStreamWaitEvent(c->s, m->side_ev[1], 0));
+  m->prebuilt = true;
+  c->prof.mg_build_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return APC_OK;
+}
+
+bool apc_mg_prebuilt(const apc_context *c) { return c->mg && c->mg->prebuilt; }
