@@ -348,8 +348,12 @@ __global__ void __launch_bounds__(32 * kSearchWarps) gfd_search(GfdParams P) {
         int m = -1, oct = 0;
         double d2 = 0;
         if (v) {
+          // the snapshot candidate whose Neigh24 list holds item f: the last q with
+          // soff[q] <= f (soff is a non-decreasing exclusive scan, soff[0] = 0 <= f), by
+          // binary search
           int c = 0;
-          for (int q = 1; q < lsnap; ++q) c += (S.soff[q] <= f) ? 1 : 0;
+          for (int step = 16; step > 0; step >>= 1)
+            if (c + step < lsnap && S.soff[c + step] <= f) c += step;
           m = P.nb24[24 * (size_t)S.sp[c] + (f - S.soff[c])];
           double wx, wy, wz;
           offset_of(P, m, i0, wx, wy, wz);
