@@ -44,6 +44,7 @@ struct GfdParams {
   double L[3], halfL[3];
   double rot[9];
   double e4;       // exp(-4)
+  double inv_1me4;  // 1 / (1 - exp(-4))
   double c_dens;
   const double *cx, *cy, *cz, *ch;
   const int *count, *type, *nb24, *nnb;
@@ -458,9 +459,13 @@ __global__ void __launch_bounds__(32 * kWarps, QR ? 4 : 6) gfd_lsq(GfdParams P) 
     const double dist = act ? sqrt(sq3(wx, wy, wz)) : 0.0;
     const double maxdis = warp_max(dist) * 0.7;
     double weight = 0.0;
-    if (act) weight = (exp(-dist * dist / maxdis / maxdis) - P.e4) / (1 - P.e4);
+    // the reference's divisions (solver.cpp:75-103) as products with reciprocals taken once
+    // per cell: the same values to a few ulp, far inside the least squares' own rounding
+    const double inv_m2 = 1.0 / (maxdis * maxdis);
+    if (act) weight = (exp(-dist * dist * inv_m2) - P.e4) * P.inv_1me4;
     const double h = P.ch[i0];
-    const double p1 = wx / h, p2 = wy / h, p3 = wz / h;
+    const double ih = 1.0 / h;
+    const double p1 = wx * ih, p2 = wy * ih, p3 = wz * ih;
     double b[9];
     b[0] = p1; b[1] = p2; b[2] = p3;
     b[3] = p1 * p1 / 2.0; b[4] = p2 * p2 / 2.0; b[5] = p3 * p3 / 2.0;
@@ -492,9 +497,11 @@ __global__ void __launch_bounds__(32 * kWarps, QR ? 4 : 6) gfd_lsq(GfdParams P) 
           double d = S.G[tri(k, k)];
           for (int j = 0; j < k; ++j) d -= S.L[k * 9 + j] * S.L[k * 9 + j];
           if (!(d > 1e-4 * S.G[tri(k, k)])) *S.chol_ok = 0;
-          const double lkk = sqrt(fmax(d, 1e-300));
-          S.L[k * 9 + k] = lkk;
-          S.inv[k] = 1.0 / lkk;
+          // 1 / L_kk by one reciprocal square root, L_kk = d / sqrt(d)
+          const double dd = fmax(d, 1e-300);
+          const double inv = rsqrt(dd);
+          S.L[k * 9 + k] = dd * inv;
+          S.inv[k] = inv;
         }
         __syncwarp();
         if (lane > k && lane < 9) {
@@ -600,8 +607,8 @@ __global__ void __launch_bounds__(32 * kWarps, QR ? 4 : 6) gfd_lsq(GfdParams P) 
     }
     // ---- rows of A1, A2 and the density rhs (solver.cpp:116-172) ----
     const double lap = act ? (weight * y[3] + weight * y[4]) + weight * y[5] : 0.0;
-    const double l24 = lap / 24.0;
-    const double lh2 = lap / h / h;
+    const double l24 = lap * (1.0 / 24.0);
+    const double lh2 = lap * (ih * ih);
     const bool in1 = act && mj < P.nc_nv;
     const bool in2 = act && P.type[mj] < 1;
     const bool pin = (i0 == 0) && (P.bc == 1);
@@ -624,7 +631,7 @@ __global__ void __launch_bounds__(32 * kWarps, QR ? 4 : 6) gfd_lsq(GfdParams P) 
       P.ell_col[at] = i0;
       P.a1[at] = s1 + 1;
       P.a2[at] = pin ? 1.0 : s2;
-      P.rhs[i0] = 1.0 * P.count[i0] / h / h / h * P.c_dens;
+      P.rhs[i0] = P.count[i0] * (ih * ih * ih) * P.c_dens;
     }
     __syncwarp();
   }
@@ -753,6 +760,7 @@ int apc_gfd_assemble(apc_context *c, double c_dens) {
   }
   for (int k = 0; k < 9; ++k) P.rot[k] = c->rot[k];
   P.e4 = std::exp(-4.0);
+  P.inv_1me4 = 1.0 / (1.0 - P.e4);
   P.c_dens = c_dens;
   P.cx = c->cx; P.cy = c->cy; P.cz = c->cz; P.ch = c->ch;
   P.count = c->ccount; P.type = c->ctype; P.nb24 = c->nb24; P.nnb = c->nnb;
