@@ -145,7 +145,7 @@ int apc_batch_create(const apc_config *cfgs, int n_boxes, int n_workers, apc_bat
   for (int i = 0; i < n_boxes; ++i) b->order[i] = i;
   std::stable_sort(b->order.begin(), b->order.end(),
                    [&](int a, int c) { return cfgs[a].n_particles > cfgs[c].n_particles; });
-  b->threads = n_workers > 0 ? std::min(n_workers, n_boxes) : std::min(n_boxes, 8);
+  b->threads = n_workers > 0 ? std::min(n_workers, n_boxes) : std::min(n_boxes, 16);
   *out = b;
   return APC_OK;
 }

@@ -480,7 +480,7 @@ def run_batch(args) -> dict | None:
             "vs_baseline": None, "dtype": "f32 Krylov / f64 refinement, GFD moments and leapfrog",
             "data": "synthetic",
             "config": {"workload": f"batch96: {len(cfgs)} EdS boxes, {total} particles, a 0.05->0.5 in 32 steps",
-                       "parallelism": f"boxes sharded over {ws} ranks by LPT; {args.batch_workers or 8} "
+                       "parallelism": f"boxes sharded over {ws} ranks by LPT; {args.batch_workers or 16} "
                                       f"host workers per rank",
                        "timing": "host clock around whole batch steps, device synchronised, max over ranks"},
             "rank0": {"boxes": len(mine), "sum_of_box_device_ms_per_step": dev_ms / args.steps},

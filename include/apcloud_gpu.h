@@ -318,7 +318,7 @@ int apc_trajectory_vjp(apc_context *ctx, const apc_trajectory *t, const double *
 typedef struct apc_batch apc_batch;
 
 /* Create n_boxes contexts from cfgs[0..n_boxes-1] (all on cfgs[i].device), stepped by
- * n_workers host threads (0 = min(n_boxes, 8)), each running its boxes as fibers. */
+ * n_workers host threads (0 = min(n_boxes, 16)), each running its boxes as fibers. */
 int apc_batch_create(const apc_config *cfgs, int n_boxes, int n_workers, apc_batch **out);
 int apc_batch_destroy(apc_batch *b);
 int apc_batch_size(const apc_batch *b);
