@@ -181,7 +181,9 @@ __device__ void warp_aquicksort(double &key, int &idx, int n, int limit, int lan
 }
 
 // neighbour search and sort, per warp
-struct WarpSmem {
+// 16-byte aligned so that bucket rows (kBucketCap ints, a multiple of 4) can be read as int4
+static_assert(kBucketCap % 4 == 0, "bucket rows are scanned four entries at a time");
+struct __align__(16) WarpSmem {
   int soff[32], sp[32];  // expansion ring: item offset and cell of each candidate
   int bidx[8][kBucketCap];
   double bd2[8][kBucketCap];
@@ -235,22 +237,27 @@ __device__ __forceinline__ double sq3(double wx, double wy, double wz) {
   return __dadd_rn(__dadd_rn(__dmul_rn(wx, wx), __dmul_rn(wy, wy)), __dmul_rn(wz, wz));
 }
 
-// ordered append of the valid lanes' candidates to their octant buckets
+// ordered append of the valid lanes' candidates to their octant buckets: a lane's slot is
+// its bucket's fill plus the number of lower valid lanes of the same octant
 __device__ __forceinline__ bool append(WarpSmem &S, int (&nn)[8], bool valid, int m, int oct,
                                        double d2, int lane) {
   bool ok = true;
   const unsigned lt = (1u << lane) - 1u;
+  // invalid lanes get keys no octant has, so they match only themselves
+  const unsigned peers = __match_any_sync(0xffffffffu, valid ? oct : 8 + lane);
+  if (valid) {
+    int base = 0;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) base = (oct == o) ? nn[o] : base;
+    const int p = base + __popc(peers & lt);
+    if (p < kBucketCap) {
+      S.bidx[oct][p] = m;
+      S.bd2[oct][p] = d2;
+    }
+  }
 #pragma unroll
   for (int o = 0; o < 8; ++o) {
-    unsigned bal = __ballot_sync(0xffffffffu, valid && oct == o);
-    if (valid && oct == o) {
-      int p = nn[o] + __popc(bal & lt);
-      if (p < kBucketCap) {
-        S.bidx[o][p] = m;
-        S.bd2[o][p] = d2;
-      }
-    }
-    nn[o] += __popc(bal);
+    nn[o] += __popc(__ballot_sync(0xffffffffu, valid && oct == o));
     if (nn[o] > kBucketCap) ok = false;
   }
   __syncwarp();
@@ -362,7 +369,12 @@ __global__ void __launch_bounds__(32 * kSearchWarps) gfd_search(GfdParams P) {
           d2 = sq3(wx, wy, wz);
           bool dup = (m == i0);
           const int cap = min(nn[oct], kBucketCap);
-          for (int q = 0; q < cap && !dup; ++q) dup = (S.bidx[oct][q] == m);
+          // membership among the bucket's first cap entries, four per shared-memory load
+          for (int q = 0; q < cap && !dup; q += 4) {
+            const int4 e = *reinterpret_cast<const int4 *>(&S.bidx[oct][q]);
+            dup = (e.x == m) | ((q + 1 < cap) & (e.y == m)) | ((q + 2 < cap) & (e.z == m)) |
+                  ((q + 3 < cap) & (e.w == m));
+          }
           v = !dup;
         }
         // only the first lane holding a given index survives within the chunk
