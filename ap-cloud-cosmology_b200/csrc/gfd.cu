@@ -134,49 +134,61 @@ __device__ __forceinline__ int select_bit(unsigned mask, int k) {
 // position.  Each partition is the reference's: with pivot a[l], the i scan stops at the
 // elements > pivot in (l, r] (g_0 < g_1 < ...), the j scan at the elements <= pivot in
 // [l, r] (s_0 > s_1 > ...); the k-th swap exchanges g_k and s_k while g_k < s_k, and
-// the pivot goes to j = s_0 (no swap) or max(s_K, g_{K-1}) after K swaps.  A warp does
-// one partition in a few ballots and shuffles; sub-ranges are disjoint, so taking the
-// lowest unsorted one first ends in the reference's order, ties included.  Sub-ranges
-// starting at or beyond `limit` are left unsorted.
+// the pivot goes to j = s_0 (no swap) or max(s_K, g_{K-1}) after K swaps.
+// The result of a quicksort depends only on the partition applied to each sub-range, not
+// on the order in which disjoint sub-ranges are taken.  So every pass partitions all
+// unsorted sub-ranges at once: each lane finds its sub-range (the run of not-yet-final
+// positions around it) and takes its part in that sub-range's ballots and shuffles.  The
+// passes number the recursion depth, not the number of pivots.  Sub-ranges starting at
+// or beyond `limit` are left unsorted, as the reference leaves them; positions below the
+// limit end exactly as in the full sort, ties included.
 __device__ void warp_aquicksort(double &key, int &idx, int n, int limit, int lane) {
   constexpr unsigned kAll = 0xffffffffu;
   unsigned U = n >= 32 ? kAll : ((1u << n) - 1u);  // positions not yet final
-  while (U) {
-    const int l = __ffs(U) - 1;
-    if (l >= limit) break;
-    const unsigned run = ~(U >> l);
-    const int len = run ? __ffs(run) - 1 : 32 - l;
-    if (len == 1) {
-      U &= ~(1u << l);
-      continue;
+  const unsigned lim = limit >= 32 ? kAll : ((1u << limit) - 1u);
+  const unsigned below = (1u << lane) - 1u;       // positions < lane
+  const unsigned upto = (2u << lane) - 1u;        // positions <= lane (all bits for lane 31)
+  for (;;) {
+    unsigned R = U & ~(U << 1), E = U & ~(U >> 1);  // first and last positions of the runs
+    U &= ~(R & E & lim);                            // runs of one position are final
+    R = U & ~(U << 1);
+    E = U & ~(U >> 1);
+    const bool inU = (U >> lane) & 1u;
+    int start = 0, end = 0;
+    if (inU) {
+      start = 31 - __clz(R & upto);
+      end = __ffs(E & ~below) - 1;
     }
-    const int r = l + len - 1;
-    const double pivot = __shfl_sync(kAll, key, l);
-    const bool in = lane >= l && lane <= r;
-    const unsigned gt = __ballot_sync(kAll, in && lane > l && key > pivot);
-    const unsigned le = __ballot_sync(kAll, in && key <= pivot);
-    const int nle = __popc(le);
+    const bool active = inU && start < limit && start < end;
+    if (!__any_sync(kAll, active)) break;
+    const double pivot = __shfl_sync(kAll, key, active ? start : lane);
+    const unsigned gt = __ballot_sync(kAll, active && lane > start && key > pivot);
+    const unsigned le = __ballot_sync(kAll, active && key <= pivot);
+    const unsigned seg = active ? (((2u << end) - 1u) & ~((1u << start) - 1u)) : 0u;
+    const unsigned gts = gt & seg, les = le & seg;
+    const int nle = __popc(les);
     int partner = -1;
-    if ((gt >> lane) & 1u) {
-      const int k = __popc(gt & ((1u << lane) - 1u));
+    if ((gts >> lane) & 1u) {
+      const int k = __popc(gts & below);
       if (k < nle) {
-        const int sk = select_bit(le, nle - 1 - k);
+        const int sk = select_bit(les, nle - 1 - k);
         if (sk > lane) partner = sk;
       }
     }
-    const int K = __popc(__ballot_sync(kAll, partner >= 0));
-    if ((le >> lane) & 1u) {
-      const int k = nle - 1 - __popc(le & ((1u << lane) - 1u));
-      if (k < K) partner = select_bit(gt, k);
+    const int K = __popc(__ballot_sync(kAll, partner >= 0) & seg);
+    if ((les >> lane) & 1u) {
+      const int k = nle - 1 - __popc(les & below);
+      if (k < K) partner = select_bit(gts, k);
     }
     const int src = partner >= 0 ? partner : lane;
     key = __shfl_sync(kAll, key, src);
     idx = __shfl_sync(kAll, idx, src);
-    const int j = K == 0 ? 31 - __clz(le) : max(select_bit(le, nle - 1 - K), select_bit(gt, K - 1));
-    const int src2 = lane == l ? j : (lane == j ? l : lane);
+    int j = lane;
+    if (active) j = K == 0 ? 31 - __clz(les) : max(select_bit(les, nle - 1 - K), select_bit(gts, K - 1));
+    const int src2 = !active ? lane : (lane == start ? j : (lane == j ? start : lane));
     key = __shfl_sync(kAll, key, src2);
     idx = __shfl_sync(kAll, idx, src2);
-    U &= ~(1u << j);
+    U &= ~__ballot_sync(kAll, active && lane == j);
   }
 }
 
