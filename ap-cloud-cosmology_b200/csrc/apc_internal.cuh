@@ -207,6 +207,7 @@ int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, cons
 int apc_mg_mark_assembled(apc_context *c);
 int apc_mg_prebuild(apc_context *c);
 bool apc_mg_prebuilt(const apc_context *c);
+void apc_mg_clear_prebuilt(apc_context *c);  // a new assembly invalidates a prebuilt hierarchy
 int apc_warm_save(apc_context *c);                       // warmstart.cu
 int apc_warm_guess(apc_context *c, int which, double *x);
 int apc_potential_rhs(apc_context *c, double c_pot);    // gfd.cu

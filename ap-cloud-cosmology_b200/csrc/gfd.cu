@@ -754,6 +754,8 @@ int apc_gfd_assemble(apc_context *c, double c_dens) {
     return APC_ERR_INVALID_ARG;
   }
   const size_t mc = (size_t)M + 1;
+  // a hierarchy built beside an earlier density solve belongs to the old operator
+  apc_mg_clear_prebuilt(c);
   APC_TRY(apc_ensure(c, &c->st_idx, mc * lm, nullptr));
   APC_TRY(apc_ensure(c, &c->st_dist, mc * lm, nullptr));
   APC_TRY(apc_ensure(c, &c->gfd_x, mc * 9 * lm, nullptr));

@@ -1384,3 +1384,7 @@ int apc_mg_prebuild(apc_context *c) {
 }
 
 bool apc_mg_prebuilt(const apc_context *c) { return c->mg && c->mg->prebuilt; }
+
+void apc_mg_clear_prebuilt(apc_context *c) {
+  if (c->mg) c->mg->prebuilt = false;
+}
