@@ -88,6 +88,28 @@ __global__ void __launch_bounds__(kScanThreads) scan_sums(int *sums, int nsums, 
   if (threadIdx.x == 0 && total) *total = carry;
 }
 
+// the whole scan in one block, for short arrays: chunks of a tile in order with a carry.
+// Each chunk is read completely before it is written, so out may alias in.
+constexpr int kScanSingleMax = 2 * kScanTile;
+__global__ void __launch_bounds__(kScanThreads) scan_single(const int *in, int *out, int n, int *total) {
+  int carry = 0;
+  for (int c0 = 0; c0 < n; c0 += kScanTile) {
+    int v[kScanItems];
+    for (int k = 0; k < kScanItems; ++k) {
+      const int i = c0 + threadIdx.x * kScanItems + k;
+      v[k] = i < n ? in[i] : 0;
+    }
+    int t;
+    block_scan_tile(v, &t);
+    for (int k = 0; k < kScanItems; ++k) {
+      const int i = c0 + threadIdx.x * kScanItems + k;
+      if (i < n) out[i] = v[k] + carry;
+    }
+    carry += t;
+  }
+  if (threadIdx.x == 0 && total) *total = carry;
+}
+
 __global__ void __launch_bounds__(kScanThreads) scan_apply(const int *in, int *out, int n,
                                                           const int *sums) {
   const long long t0 = (long long)blockIdx.x * kScanTile;
@@ -223,6 +245,12 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter(const uint64_t *ke
 int apc_exclusive_scan(apc_context *c, const int *in, int *out, int n, int *total_dev) {
   if (n <= 0) {
     if (total_dev) APC_CUDA_TRY(c, cudaMemsetAsync(total_dev, 0, sizeof(int), c->s));
+    return APC_OK;
+  }
+  if (n <= kScanSingleMax) {
+    scan_single<<<1, kScanThreads, 0, c->s>>>(in, out, n, total_dev);
+    apc_count_launch(c);
+    APC_CUDA_TRY(c, cudaGetLastError());
     return APC_OK;
   }
   int tiles = (n + kScanTile - 1) / kScanTile;
