@@ -40,8 +40,6 @@ namespace {
 constexpr int kT = 256;
 constexpr int kMaxLevels = 24;
 constexpr int kCoarsest = 64;
-constexpr int kCoarseRows = 4 * kCoarsest;  // the coarsest level may stop above kCoarsest, up to this
-constexpr int kWcap = 256;                  // widest coarse row
 
 int grid_for(long long n, int cap = 4096) {
   return (int)std::max<long long>(1, std::min<long long>((n + kT - 1) / kT, cap));
@@ -792,10 +790,6 @@ struct MgWork {
   unsigned *counter = nullptr;
   IrState *state = nullptr;
   void *host = nullptr;  // pinned readback of the state
-  // pinned staging of the coarsest level: its rows (kCoarseRows x kWcap columns and values)
-  // and the FP32 inverse uploaded from it
-  int *h_ccol = nullptr;
-  float *h_cval = nullptr, *h_cinv = nullptr;
   int *total = nullptr;
   int *widths = nullptr;  // per-level ELL widths on the device (kMaxLevels), read once per build
   // each mixed solve of the step as one graph, captured on c->s with the loop bodies on
@@ -838,9 +832,6 @@ void apc_mg_free(apc_context *c) {
                m->partial, m->dots, m->counter, m->state, m->total, m->widths};
   for (void *q : p) apc_free(c, q);
   if (m->host) cudaFreeHost(m->host);
-  if (m->h_ccol) cudaFreeHost(m->h_ccol);
-  if (m->h_cval) cudaFreeHost(m->h_cval);
-  if (m->h_cinv) cudaFreeHost(m->h_cinv);
   for (int k = 0; k < 2; ++k) {
     if (m->solve_exec[k]) cudaGraphExecDestroy(m->solve_exec[k]);
     if (m->solve_graph[k]) cudaGraphDestroy(m->solve_graph[k]);
@@ -925,7 +916,7 @@ static int mg_build(apc_context *c) {
     aggregate_map<<<grid_for(nf), kT, 0, c->s>>>(nf, pk, pi, m->eflag, m->epos, F.agg, C.code, C.mptr, C.mem);
     apc_count_launch(c);
     // ---- Galerkin product, one warp per coarse row ----
-    const int wcap = kWcap;
+    const int wcap = 256;
     APC_TRY(apc_ensure(c, &m->rowstart, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &m->ucol, (size_t)nc * wcap));
     APC_TRY(apc_ensure(c, &m->uval, (size_t)nc * wcap));
@@ -954,25 +945,11 @@ static int mg_build(apc_context *c) {
     ++lev;
   }
   m->nlev = lev + 1;
-  if (!m->h_ccol) {
-    APC_CUDA_TRY(c, cudaMallocHost((void **)&m->h_ccol, sizeof(int) * kCoarseRows * kWcap));
-    APC_CUDA_TRY(c, cudaMallocHost((void **)&m->h_cval, sizeof(float) * kCoarseRows * kWcap));
-    APC_CUDA_TRY(c, cudaMallocHost((void **)&m->h_cinv, sizeof(float) * kCoarseRows * kCoarseRows));
-  }
-  bool coarse_read = false;  // the coarsest rows came with the widths
   if (lev > 0) {
-    // every coarse width, the error flags and the coarsest level's rows (all kWcap slots,
-    // slot-major with ld = its size) in one round trip
+    // every coarse width and the error flags in one round trip
     static_assert(16 + kMaxLevels <= 64, "widths fit the context's pinned words");
     APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 16, m->widths, sizeof(int) * m->nlev, cudaMemcpyDeviceToHost, c->s));
     APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 9, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->s));
-    const MgLevel &Kc = m->lv[lev];
-    if (Kc.n <= kCoarseRows) {
-      const size_t cnt = Kc.ld * (size_t)kWcap;
-      APC_CUDA_TRY(c, cudaMemcpyAsync(m->h_ccol, Kc.col, sizeof(int) * cnt, cudaMemcpyDeviceToHost, c->s));
-      APC_CUDA_TRY(c, cudaMemcpyAsync(m->h_cval, Kc.val, sizeof(float) * cnt, cudaMemcpyDeviceToHost, c->s));
-      coarse_read = true;
-    }
     APC_CUDA_TRY(c, apc_stream_wait(c));
     if (c->h_pinned[9] & DERR_STENCIL_MANY) {
       c->err = "multigrid coarse row exceeds its buffers";
@@ -980,7 +957,7 @@ static int mg_build(apc_context *c) {
     }
     for (int l = 1; l < m->nlev; ++l) {
       const int wc = c->h_pinned[16 + l];
-      if (wc > kWcap) {
+      if (wc > 256) {
         c->err = "multigrid coarse row exceeds its buffers";
         return APC_ERR_UNSUPPORTED;
       }
@@ -998,23 +975,15 @@ static int mg_build(apc_context *c) {
   // ---- coarsest level: explicit inverse in FP64 on the host ----
   MgLevel &K = m->lv[lev];
   const int n = K.n;
-  if (n > kCoarseRows) {
+  if (n > 4 * kCoarsest) {
     c->err = "multigrid coarsening stalled";
     return APC_ERR_UNSUPPORTED;
   }
-  std::vector<int> col0;
-  std::vector<float> val0;
-  const int *col = m->h_ccol;
-  const float *val = m->h_cval;
-  if (!coarse_read) {  // no coarsening: the level-0 operator itself, in its own layout
-    col0.resize(K.ld * K.w);
-    val0.resize(K.ld * K.w);
-    APC_CUDA_TRY(c, cudaMemcpyAsync(col0.data(), K.col, sizeof(int) * col0.size(), cudaMemcpyDeviceToHost, c->s));
-    APC_CUDA_TRY(c, cudaMemcpyAsync(val0.data(), K.val, sizeof(float) * val0.size(), cudaMemcpyDeviceToHost, c->s));
-    APC_CUDA_TRY(c, apc_stream_wait(c));
-    col = col0.data();
-    val = val0.data();
-  }
+  std::vector<int> col(K.ld * K.w);
+  std::vector<float> val(K.ld * K.w);
+  APC_CUDA_TRY(c, cudaMemcpyAsync(col.data(), K.col, sizeof(int) * col.size(), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, cudaMemcpyAsync(val.data(), K.val, sizeof(float) * val.size(), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   std::vector<double> a((size_t)n * n, 0.0), inv((size_t)n * n, 0.0);
   for (int i = 0; i < n; ++i) {
     for (int s = 0; s < K.w; ++s) a[(size_t)i * n + col[(size_t)s * K.ld + i]] += val[(size_t)s * K.ld + i];
@@ -1048,12 +1017,11 @@ static int mg_build(apc_context *c) {
       }
     }
   }
-  // uploaded from pinned staging without a wait: the staging is next written by the next
-  // build, after this step's solves have been waited for
-  for (size_t e = 0; e < (size_t)n * n; ++e) m->h_cinv[e] = (float)inv[e];
+  std::vector<float> invf(inv.begin(), inv.end());
   APC_TRY(apc_ensure(c, &m->coarse_inv, (size_t)n * n + 1));
-  APC_CUDA_TRY(c, cudaMemcpyAsync(m->coarse_inv, m->h_cinv, sizeof(float) * (size_t)n * n, cudaMemcpyHostToDevice,
+  APC_CUDA_TRY(c, cudaMemcpyAsync(m->coarse_inv, invf.data(), sizeof(float) * invf.size(), cudaMemcpyHostToDevice,
                                   c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
   m->coarse_n = n;
   return APC_OK;
 }
