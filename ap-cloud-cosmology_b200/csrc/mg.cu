@@ -94,8 +94,7 @@ constexpr int kGalTab = 512;   // hash slots per warp
 constexpr int kGalRows = 256;  // distinct coarse columns per row
 
 __global__ void __launch_bounds__(32 * kGalWarps) galerkin_rows(int nc, const int *__restrict__ mptr, int nf,
-                                                              const int *__restrict__ mem, int wf_host,
-                                                              const int *__restrict__ wf_dev, size_t ldf,
+                                                              const int *__restrict__ mem, int wf, size_t ldf,
                                                               const int *__restrict__ colf,
                                                               const float *__restrict__ valf,
                                                               const int *__restrict__ agg, int wcap,
@@ -107,8 +106,6 @@ __global__ void __launch_bounds__(32 * kGalWarps) galerkin_rows(int nc, const in
   __shared__ int dkey[kGalWarps][kGalRows];
   __shared__ double dval[kGalWarps][kGalRows];
   const int lane = threadIdx.x & 31, wv = threadIdx.x >> 5;
-  // a width above wcap is an overflow the host reports after the build; reads stay in bounds
-  const int wf = wf_dev ? min(*wf_dev, wcap) : wf_host;
   int *K = tkey[wv];
   double *T = tsum[wv];
   for (int I = blockIdx.x * kGalWarps + wv; I < nc; I += gridDim.x * kGalWarps) {
@@ -181,12 +178,11 @@ __global__ void __launch_bounds__(32 * kGalWarps) galerkin_rows(int nc, const in
   }
 }
 
-__global__ void rows_to_ell(int n, const int *__restrict__ wp, size_t ld, int wcap, const int *__restrict__ rowlen,
+__global__ void rows_to_ell(int n, int w, size_t ld, int wcap, const int *__restrict__ rowlen,
                             const int *__restrict__ tcol, const float *__restrict__ tval, int *__restrict__ col,
                             float *__restrict__ val, float *__restrict__ dinv) {
-  const int w = min(*wp, wcap);  // the level's width, from max_int on the device
   for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < n; I += gridDim.x * blockDim.x) {
-    const int len = min(rowlen[I], wcap);
+    const int len = rowlen[I];
     float d = 0.f;
     for (int s = 0; s < w; ++s) {
       const bool in = s < len;
@@ -791,7 +787,6 @@ struct MgWork {
   IrState *state = nullptr;
   void *host = nullptr;  // pinned readback of the state
   int *total = nullptr;
-  int *widths = nullptr;  // per-level ELL widths on the device (kMaxLevels), read once per build
   // each mixed solve of the step as one graph, captured on c->s with the loop bodies on
   // two side streams
   cudaStream_t cap[2] = {nullptr, nullptr};
@@ -829,7 +824,7 @@ void apc_mg_free(apc_context *c) {
   }
   void *p[] = {m->coarse_inv, m->pkey, m->pkey_alt, m->pidx, m->pidx_alt, m->eflag, m->epos, m->ucol,
                m->rowstart, m->uval, m->V, m->Z, m->vin, m->vout, m->dvec,
-               m->partial, m->dots, m->counter, m->state, m->total, m->widths};
+               m->partial, m->dots, m->counter, m->state, m->total};
   for (void *q : p) apc_free(c, q);
   if (m->host) cudaFreeHost(m->host);
   for (int k = 0; k < 2; ++k) {
@@ -874,8 +869,6 @@ static int mg_build(apc_context *c) {
   ell_f32_dinv<<<grid_for(n0), kT, 0, c->s>>>(n0, L0.ld, L0.val, L0.dinv);
   apc_count_launch(c);
   if (!m->total) APC_TRY(apc_alloc(c, (void **)&m->total, 4 * sizeof(int)));
-  if (!m->widths) APC_TRY(apc_alloc(c, (void **)&m->widths, kMaxLevels * sizeof(int)));
-  APC_CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->s));
   int lev = 0;
   while (m->lv[lev].n > kCoarsest && lev + 1 < kMaxLevels) {
     MgLevel &F = m->lv[lev];
@@ -920,50 +913,38 @@ static int mg_build(apc_context *c) {
     APC_TRY(apc_ensure(c, &m->rowstart, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &m->ucol, (size_t)nc * wcap));
     APC_TRY(apc_ensure(c, &m->uval, (size_t)nc * wcap));
-    // the coarse width stays on the device (m->widths) until the hierarchy is complete: the
-    // ELL arrays are sized for wcap slots, and the host reads every width in one round trip
-    int *wdev = m->widths + lev + 1;
-    APC_CUDA_TRY(c, cudaMemsetAsync(wdev, 0, sizeof(int), c->s));
+    APC_CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->s));
+    APC_CUDA_TRY(c, cudaMemsetAsync(m->total, 0, sizeof(int), c->s));
     galerkin_rows<<<std::max(1, std::min((nc + kGalWarps - 1) / kGalWarps, apc_sm_count(c) * 8)), 32 * kGalWarps, 0,
-                    c->s>>>(nc, C.mptr, nf, C.mem, F.w, lev == 0 ? nullptr : m->widths + lev, F.ld, F.col, F.val,
-                            F.agg, wcap, m->rowstart, m->ucol, m->uval, c->d_err);
-    max_int<<<grid_for(nc, 256), kT, 0, c->s>>>(nc, m->rowstart, wdev);
+                    c->s>>>(nc, C.mptr, nf, C.mem, F.w, F.ld, F.col, F.val, F.agg, wcap, m->rowstart, m->ucol,
+                            m->uval, c->d_err);
+    max_int<<<grid_for(nc, 256), kT, 0, c->s>>>(nc, m->rowstart, m->total);
     apc_count_launch(c, 2);
-    C.w = wcap;  // bound until the widths are read
+    // the row width and the error flags in one round trip
+    APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 8, m->total, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+    APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 9, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+    APC_CUDA_TRY(c, apc_stream_wait(c));
+    const int wc = c->h_pinned[8], derr = c->h_pinned[9];
+    if (derr & DERR_STENCIL_MANY) {
+      c->err = "multigrid coarse row exceeds its buffers";
+      return APC_ERR_UNSUPPORTED;
+    }
+    C.w = wc;
     C.ld = (size_t)nc;
-    APC_TRY(apc_ensure(c, &C.col, C.ld * wcap));
-    APC_TRY(apc_ensure(c, &C.val, C.ld * wcap));
+    APC_TRY(apc_ensure(c, &C.col, C.ld * wc));
+    APC_TRY(apc_ensure(c, &C.val, C.ld * wc));
     APC_TRY(apc_ensure(c, &C.dinv, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &C.x, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &C.x2, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &C.b, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &C.r, (size_t)nc + 1));
-    rows_to_ell<<<grid_for(nc), kT, 0, c->s>>>(nc, wdev, C.ld, wcap, m->rowstart, m->ucol, m->uval, C.col, C.val,
+    rows_to_ell<<<grid_for(nc), kT, 0, c->s>>>(nc, wc, C.ld, wcap, m->rowstart, m->ucol, m->uval, C.col, C.val,
                                               C.dinv);
     apc_count_launch(c);
     APC_CUDA_TRY(c, cudaGetLastError());
     ++lev;
   }
   m->nlev = lev + 1;
-  if (lev > 0) {
-    // every coarse width and the error flags in one round trip
-    static_assert(16 + kMaxLevels <= 64, "widths fit the context's pinned words");
-    APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 16, m->widths, sizeof(int) * m->nlev, cudaMemcpyDeviceToHost, c->s));
-    APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 9, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->s));
-    APC_CUDA_TRY(c, apc_stream_wait(c));
-    if (c->h_pinned[9] & DERR_STENCIL_MANY) {
-      c->err = "multigrid coarse row exceeds its buffers";
-      return APC_ERR_UNSUPPORTED;
-    }
-    for (int l = 1; l < m->nlev; ++l) {
-      const int wc = c->h_pinned[16 + l];
-      if (wc > 256) {
-        c->err = "multigrid coarse row exceeds its buffers";
-        return APC_ERR_UNSUPPORTED;
-      }
-      m->lv[l].w = wc;
-    }
-  }
   {
     int first_tail = 0;
     while (first_tail < m->nlev - 1 && m->lv[first_tail].n > kTail) ++first_tail;
