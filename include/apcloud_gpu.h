@@ -77,7 +77,8 @@ typedef struct apc_config {
   double gmres_dtol;     /* -ksp_divtol */
   int gmres_max_it;      /* -ksp_max_it */
   int precision;         /* apc_precision */
-  int mixed_restart;     /* FP32 inner restart for APC_PREC_MIXED (0 = 16 with multigrid, 30 without) */
+  int mixed_restart;     /* FP32 inner restart of both APC_PREC_MIXED solves (0 = 16 for the multigrid
+                            potential solve, 30 for the others), at most 31 */
   double mixed_inner_rtol; /* FP32 inner solve relative tolerance (0 = 1e-3 with multigrid, 1e-5 without) */
   int device;            /* CUDA device ordinal */
   int mixed_precond;     /* APC_PREC_MIXED potential solve: APC_PRECOND_JACOBI or APC_PRECOND_MULTIGRID */
