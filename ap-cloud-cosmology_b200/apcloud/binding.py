@@ -30,6 +30,7 @@ EXPORTED = [
     "apc_batch_create", "apc_batch_destroy", "apc_batch_size", "apc_batch_context", "apc_batch_step",
     "apc_get_hessians_device", "apc_vjp_kick_drift", "apc_trajectory_vjp", "apc_fields_from_rhs",
     "apc_solve_vjp", "apc_max_cell_density", "apc_adaptive_dt", "apc_config_from_options",
+    "apc_device_code_version", "apc_check_bounded_wait",
 ]
 
 
@@ -140,6 +141,8 @@ def load_library(path: str = LIB_PATH):
                                          C.POINTER(C.c_void_p), vp]),
         "apc_trajectory_vjp": (C.c_int, [vp, C.POINTER(ApcTrajectory), C.POINTER(C.c_void_p),
                                          C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+        "apc_device_code_version": (C.c_int, [C.c_int, ip, ip]),
+        "apc_check_bounded_wait": (C.c_int, [C.c_int, C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -699,6 +699,22 @@ int apc_adaptive_dt(apc_context *c, double delta_a, double *dt) {
   return APC_OK;
 }
 
+int apc_device_code_version(int device, int *binary_version, int *ptx_version) {
+  if (!binary_version && !ptx_version) return APC_ERR_INVALID_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    return APC_ERR_CUDA;
+  }
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, (const void *)iota_int) != cudaSuccess) {
+    cudaGetLastError();
+    return APC_ERR_CUDA;
+  }
+  if (binary_version) *binary_version = fa.binaryVersion;
+  if (ptx_version) *ptx_version = fa.ptxVersion;
+  return APC_OK;
+}
+
 int apc_get_phase_times(apc_context *c, double *a, double *b, double *d) {
   if (!c) return APC_ERR_INVALID_ARG;
   if (a) *a = c->t_select_ms;

@@ -59,8 +59,10 @@ enum {
   KSP_DIVERGED_NANORINF = -9,
 };
 
-// bounded sense-free generation barrier; returns false when the grid must abort
-__device__ __forceinline__ bool grid_sync(GridBar *bar, unsigned nblocks, int *err) {
+// bounded sense-free generation barrier; returns false when the grid must abort.  A block
+// that waits more than `limit` polls raises DERR_KRYLOV and the abort flag, which every
+// other waiting block sees at its next poll
+__device__ __forceinline__ bool grid_sync(GridBar *bar, unsigned nblocks, int *err, long long limit = kSpinLimit) {
   __syncthreads();
   __shared__ int s_abort;
   if (threadIdx.x == 0) {
@@ -76,7 +78,7 @@ __device__ __forceinline__ bool grid_sync(GridBar *bar, unsigned nblocks, int *e
     } else {
       long long spins = 0;
       while (*vgen == g && !*vab) {
-        if (++spins > kSpinLimit) {
+        if (++spins > limit) {
           atomicOr(err, DERR_KRYLOV);
           atomicExch(&bar->abort, 1);
           break;
@@ -472,6 +474,13 @@ __global__ void zero_f64(int n, double *x) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = 0.0;
 }
 
+// Self-check of the bounded wait: block 0 waits at the barrier for block 1, which
+// leaves without arriving (a flag that nothing sets), so the wait must run out.
+__global__ void bounded_wait_probe(GridBar *bar, int *err, long long limit) {
+  if (blockIdx.x == 1) return;
+  grid_sync(bar, 2u, err, limit);
+}
+
 }  // namespace
 
 struct KrylovWork {
@@ -697,4 +706,33 @@ int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int 
                        &levels, during));
   if (use_mg) c->stats.mg_levels = levels;
   return APC_OK;
+}
+
+extern "C" int apc_check_bounded_wait(int device, int spin_limit) {
+  if (spin_limit < 1 || spin_limit > (1 << 24)) return APC_ERR_INVALID_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    return APC_ERR_CUDA;
+  }
+  // the barrier word and the error flag
+  void *buf = nullptr;
+  if (cudaMalloc(&buf, sizeof(GridBar) + 16) != cudaSuccess) {
+    cudaGetLastError();
+    return APC_ERR_OUT_OF_MEMORY;
+  }
+  GridBar *bar = (GridBar *)buf;
+  int *err = (int *)((char *)buf + sizeof(GridBar));
+  int flag = 0;
+  cudaError_t e = cudaMemset(buf, 0, sizeof(GridBar) + 16);
+  if (e == cudaSuccess) {
+    bounded_wait_probe<<<2, 32>>>(bar, err, spin_limit);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(&flag, err, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(buf);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return APC_ERR_CUDA;
+  }
+  return (flag & DERR_KRYLOV) ? APC_ERR_TIMEOUT : APC_OK;
 }

@@ -26,14 +26,28 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 void *g_scratch_ptr[kMaxDevices] = {nullptr};
 
+// acc[1] error bits: a range that runs outside [0, n), ranges that overlap, a particle no
+// range covers
+enum : unsigned long long { kBadRange = 1, kOverlap = 2, kUncovered = 4 };
+
 __global__ void noalloc_cell_map(int m, const int *__restrict__ first, const int *__restrict__ count, int n,
-                                 int *__restrict__ cell_of) {
+                                 int *__restrict__ cell_of, unsigned long long *acc) {
   const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
   for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < m; i += gridDim.x * wpb) {
-    const int f = first[i], c = count[i];
-    for (int k = lane; k < c; k += 32)
-      if (f + k >= 0 && f + k < n) cell_of[f + k] = i;
+    const long long f = first[i], c = count[i];
+    if (c < 0 || (c > 0 && (f < 0 || f + c > n))) {
+      if (lane == 0) atomicOr(acc + 1, kBadRange);
+      continue;
+    }
+    for (long long k = lane; k < c; k += 32)
+      if (atomicCAS(cell_of + f + k, -1, i) != -1) atomicOr(acc + 1, kOverlap);
   }
+}
+
+__global__ void noalloc_coverage(int n, const int *__restrict__ cell_of, unsigned long long *acc) {
+  bool hole = false;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) hole |= cell_of[s] < 0;
+  if (__any_sync(0xffffffffu, hole) && (threadIdx.x & 31) == 0) atomicOr(acc + 1, kUncovered);
 }
 
 // same arithmetic, operand order and rounding as the kick of apc_move_velocity
@@ -47,13 +61,13 @@ __global__ void __launch_bounds__(256) noalloc_kick(int n, int m, const int *__r
                                                     double *__restrict__ az, double cv, double dt,
                                                     unsigned long long *acc) {
   __shared__ double sm[8];
+  // malformed cell ranges (found by the two kernels before this one on the stream) leave
+  // every output untouched
+  if (*(volatile unsigned long long *)(acc + 1) != 0ull) return;
   double mx = 0.0;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
     const int i = cell_of[s];
-    if (i < 0 || i >= m) {
-      atomicOr(acc + 1, 1ull);  // a particle outside every cell range
-      continue;
-    }
+    if (i < 0 || i >= m) continue;  // unreachable once the checks above passed
     const double *d = deriv + (size_t)i * 9;
     const double dx = __dsub_rn(x[s], cx[i]), dy = __dsub_rn(y[s], cy[i]), dz = __dsub_rn(z[s], cz[i]);
     const double a1 = __dadd_rn(__dadd_rn(__dadd_rn(d[0], __dmul_rn(dx, d[3])), __dmul_rn(dy, d[6])), __dmul_rn(dz, d[7]));
@@ -131,9 +145,11 @@ extern "C" int apc_move_velocity_noalloc(int n_particles, int n_cells, const int
   }
   int sms = 1;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int gp = std::max(1, std::min((n_particles + 255) / 256, sms * 8));
   noalloc_cell_map<<<std::max(1, std::min((n_cells + 7) / 8, sms * 16)), 256, 0, s>>>(n_cells, first, count,
-                                                                                      n_particles, cell_of);
-  noalloc_kick<<<std::max(1, std::min((n_particles + 255) / 256, sms * 8)), 256, 0, s>>>(
+                                                                                      n_particles, cell_of, acc);
+  noalloc_coverage<<<gp, 256, 0, s>>>(n_particles, cell_of, acc);
+  noalloc_kick<<<gp, 256, 0, s>>>(
       n_particles, n_cells, cell_of, deriv9, cx, cy, cz, x, y, z, vx, vy, vz, ax, ay, az, c_vel, dt, acc);
   if (cudaGetLastError() != cudaSuccess) return APC_ERR_CUDA;
   unsigned long long host[2] = {0, 0};
@@ -142,7 +158,9 @@ extern "C" int apc_move_velocity_noalloc(int n_particles, int n_cells, const int
     cudaGetLastError();
     return APC_ERR_CUDA;
   }
-  if (host[1]) return APC_ERR_INVALID_ARG;  // cell ranges do not cover every particle
+  // cell ranges outside [0, n), overlapping, or leaving a particle uncovered: caller input,
+  // so an invalid argument (the context path builds its ranges itself); nothing was written
+  if (host[1]) return APC_ERR_INVALID_ARG;
   if (max_dv) {
     double v;
     std::memcpy(&v, &host[0], sizeof(v));

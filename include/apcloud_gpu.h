@@ -219,14 +219,19 @@ int apc_reset_profile(apc_context *ctx);
  * the library keeps until the process exits, so n_particles may not exceed
  * APC_NOALLOC_MAX_PARTICLES (larger sizes return APC_ERR_INVALID_ARG).  The first call
  * on a device looks up the array's device address (once per device) and should come
- * before any stream capture.  All calls share the one array: calls whose work overlaps
- * on the GPU (other streams, other host threads) race and must be serialised by the
- * caller.  Each call resets the parts of the scratch that must start cleared.
+ * before any stream capture; that address is kept for the life of the process, so the
+ * call must not be used on a device again after cudaDeviceReset there.  All calls share
+ * the one array: calls whose work overlaps on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller.  Each call resets the parts of the
+ * scratch that must start cleared.
  *
  * Inputs, all device pointers on the current device: particles x, y, z in cell order
  * (cell i owns particles first[i] .. first[i]+count[i]-1); cell centres cx, cy, cz;
  * deriv9 = p_x p_y p_z p_xx p_yy p_zz p_xy p_xz p_yz per cell.  In/out: vx, vy, vz
  * (v += a c_vel dt).  Out: ax, ay, az; *max_dv (host, may be NULL) as apc_move_velocity.
+ * The cell ranges must cover every particle exactly once: a range outside
+ * [0, n_particles), overlapping ranges or an uncovered particle return
+ * APC_ERR_INVALID_ARG, and then vx..az are left as they were.
  * stream: a cudaStream_t, or NULL for the default stream; the call returns after the
  * stream has finished its work. */
 #define APC_NOALLOC_MAX_PARTICLES (1 << 20)
@@ -254,6 +259,20 @@ int apc_adaptive_dt(apc_context *ctx, double delta_a, double *dt);
 
 /* Device time (ms) of the last select / solve / move phases, from CUDA events. */
 int apc_get_phase_times(apc_context *ctx, double *select_ms, double *solve_ms, double *move_ms);
+
+/* ---- diagnostics (no counterpart in the reference, which has no GPU code) ---- */
+
+/* The compute capability the library's device code was built for, as the runtime loaded
+ * it on `device` (cudaFuncGetAttributes: 100 = sm_100) and the PTX version behind it. */
+int apc_device_code_version(int device, int *binary_version, int *ptx_version);
+
+/* Self-check of the library's bounded device waits (the grid barrier of the persistent
+ * GMRES kernel).  Two blocks are launched on `device`; one leaves without arriving at
+ * the barrier, so the other's wait runs out after spin_limit polls (each a ~64 ns sleep;
+ * 1 <= spin_limit <= 2^24) and it raises the error and abort flags and returns, as the
+ * solver kernels do.  Returns APC_ERR_TIMEOUT when the wait gave up (the designed
+ * outcome), APC_OK if the barrier completed.  The device stays usable either way. */
+int apc_check_bounded_wait(int device, int spin_limit);
 
 /* ---- derivatives ----
  * The reference computes no derivatives.  These entry points are the reverse mode of

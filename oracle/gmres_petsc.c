@@ -28,14 +28,22 @@
 #include <stdlib.h>
 #include <string.h>
 
-static double vdot(int n, const double *a, const double *b) {
+/* th > 1: the loop runs on th OpenMP threads (as PETSc runs it on MPI ranks); th <= 1:
+   serially, in index order */
+static double vdot(int n, const double *a, const double *b, int th) {
   double s = 0.0;
+  if (th > 1) {
+#pragma omp parallel for num_threads(th) reduction(+ : s) schedule(static)
+    for (int i = 0; i < n; ++i) s += a[i] * b[i];
+    return s;
+  }
   for (int i = 0; i < n; ++i) s += a[i] * b[i];
   return s;
 }
 
 static void csr_matvec(int n, const int *rp, const int *ci, const double *v, const double *x,
-                       double *y) {
+                       double *y, int th) {
+#pragma omp parallel for num_threads(th > 1 ? th : 1) if (th > 1) schedule(static)
   for (int i = 0; i < n; ++i) {
     double s = 0.0;
     for (int k = rp[i]; k < rp[i + 1]; ++k) s += v[k] * x[ci[k]];
@@ -52,6 +60,7 @@ void oracle_gmres_defaults(oracle_gmres_params *p) {
   p->its = 0;
   p->rnorm = 0.0;
   p->reason = 0;
+  p->threads = 1;
 }
 
 /* KSPConvergedDefault */
@@ -71,6 +80,7 @@ int oracle_gmres_csr(int n, const int *rp, const int *ci, const double *val, con
                      double *x, oracle_gmres_params *p) {
   const int m = p->restart > 0 ? p->restart : 30;
   const double haptol = 1e-30;
+  const int th = p->threads;
   double *dinv = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
   double *V = (double *)malloc(sizeof(double) * (size_t)n * (m + 1) + 8);
   double *tmp = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
@@ -102,11 +112,11 @@ int oracle_gmres_csr(int n, const int *rp, const int *ci, const double *val, con
     if (guess_zero) {
       for (int i = 0; i < n; ++i) v0[i] = dinv[i] * b[i];
     } else {
-      csr_matvec(n, rp, ci, val, x, tmp);
+      csr_matvec(n, rp, ci, val, x, tmp, th);
       for (int i = 0; i < n; ++i) v0[i] = dinv[i] * (b[i] - tmp[i]);
     }
     /* KSPGMRESCycle */
-    double res_norm = sqrt(vdot(n, v0, v0));
+    double res_norm = sqrt(vdot(n, v0, v0, th));
     if (res_norm != 0.0) {
       double s = 1.0 / res_norm;
       for (int i = 0; i < n; ++i) v0[i] *= s;
@@ -123,18 +133,19 @@ int oracle_gmres_csr(int n, const int *rp, const int *ci, const double *val, con
       double *vk = V + (size_t)it * n;
       double *w = V + (size_t)(it + 1) * n;
       /* KSP_PCApplyBAorAB: w = B A v_it */
-      csr_matvec(n, rp, ci, val, vk, tmp);
+      csr_matvec(n, rp, ci, val, vk, tmp, th);
       for (int i = 0; i < n; ++i) w[i] = dinv[i] * tmp[i];
       /* classical Gram-Schmidt, refinement never */
-      for (int j = 0; j <= it; ++j) lhh[j] = -vdot(n, w, V + (size_t)j * n);
+      for (int j = 0; j <= it; ++j) lhh[j] = -vdot(n, w, V + (size_t)j * n, th);
       for (int j = 0; j <= it; ++j) {
         const double *vj = V + (size_t)j * n;
         double a = lhh[j];
+#pragma omp parallel for num_threads(th > 1 ? th : 1) if (th > 1) schedule(static)
         for (int i = 0; i < n; ++i) w[i] += a * vj[i];
       }
       double *hcol = HH + (size_t)it * (m + 1);
       for (int j = 0; j <= it; ++j) hcol[j] = -lhh[j];
-      double tt = sqrt(vdot(n, w, w));
+      double tt = sqrt(vdot(n, w, w, th));
       if (tt != 0.0) {
         double s = 1.0 / tt;
         for (int i = 0; i < n; ++i) w[i] *= s;

@@ -26,6 +26,10 @@ typedef struct oracle_gmres_params {
   int its;
   double rnorm;
   int reason;
+  /* host threads of the vector and matrix loops: <= 1 runs them serially, in the order
+     the parity tests pin; more spread them over OpenMP threads as PETSc spreads them
+     over MPI ranks (sums then depend on the thread count) */
+  int threads;
 } oracle_gmres_params;
 
 void oracle_gmres_defaults(oracle_gmres_params *p);

@@ -290,6 +290,24 @@ int apcref_last_matrix(int which, int *n, int *nnz, int *rp, int *ci, double *v)
   return 0;
 }
 
+/* The GFD stencil of every cell of the last solve, lm indices per cell in search order:
+ * Build_Linear_System inserts row i of A1 as its lm neighbours in the order
+ * searchneighboroctant returned them, then the diagonal (solver.cpp:116-125), so the
+ * first lm columns of each row's insertion log are the reference's own stencil. */
+int apcref_get_stencils(int lm, int *idx) {
+  const int *rp, *ci;
+  int n, len;
+  if (petsc_shim_last_matrix_log(0, &n, &len, &rp, &ci)) return -1;
+  for (int i = 0; i < n; ++i) {
+    if (rp[i + 1] - rp[i] < lm) return -1;
+    for (int j = 0; j < lm; ++j) idx[(size_t)i * lm + j] = ci[rp[i] + j];
+  }
+  return n;
+}
+
+/* host threads of the GMRES shim (PETSc spreads its solves over MPI ranks) */
+void apcref_set_threads(int threads) { petsc_shim_set_threads(threads); }
+
 /* Mover::move_velocity (mover.cpp:51-89): interpolation + kick */
 double apcref_move_velocity(void *h, double dt, double c_vel) {
   Ref *r = static_cast<Ref *>(h);

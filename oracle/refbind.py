@@ -75,6 +75,7 @@ def _bind_common(lib, prefix):
         ("move_position", C.c_double, [C.c_void_p, C.c_double, C.c_double]),
         ("get_particles", C.c_int, [C.c_void_p] + [C.c_void_p] * 9),
         ("phase_times", None, [C.c_void_p, _dp]),
+        ("set_threads", None, [C.c_int]),
     ]:
         fn = getattr(lib, prefix + name, None)
         if fn is None:
@@ -83,6 +84,13 @@ def _bind_common(lib, prefix):
         fn.argtypes = args
         lib_dict[name] = fn
     lib_dict["create"] = f
+    if prefix == "apcref_":
+        fn = lib.apcref_get_stencils
+        fn.restype, fn.argtypes = C.c_int, [C.c_int, _ip]
+    else:
+        fn = lib.apcor_get_stencils
+        fn.restype, fn.argtypes = C.c_int, [C.c_void_p, _ip, _dp]
+    lib_dict["get_stencils"] = fn
     return lib_dict
 
 
@@ -104,6 +112,8 @@ class CpuPath:
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in parts.as_tuple()]
         self.h = self.f["create"](self.n, *arrs, depth, bc, np.asarray(box, dtype=np.float64), gfd_c, lm)
         self.depth = depth
+        self.lm = lm
+        self.which = which
 
     def close(self):
         if self.h:
@@ -155,6 +165,25 @@ class CpuPath:
         rho, phi, der = np.zeros(m), np.zeros(m), np.zeros(9 * m)
         self.f["get_fields"](self.h, rho, phi, der)
         return Fields(rho, phi, der.reshape(m, 9))
+
+    def stencils(self) -> np.ndarray:
+        """(M, lm) GFD neighbour indices of the last solve, in search order.  For the
+        reference they come from the order in which Build_Linear_System inserts row i of
+        A1 (solver.cpp:116-125), recorded by the PETSc shim."""
+        nc, nv, nb, nn = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        self.f["cell_counts"](self.h, C.byref(nc), C.byref(nv), C.byref(nb), C.byref(nn))
+        m = nc.value + nv.value
+        idx = np.zeros(m * self.lm, np.int32)
+        if self.which == "ref":
+            if self.f["get_stencils"](self.lm, idx) != m:
+                raise RuntimeError("reference stencils unavailable (no solve since the last select?)")
+        else:
+            self.f["get_stencils"](self.h, idx, np.zeros(m * self.lm))
+        return idx.reshape(m, self.lm)
+
+    def set_threads(self, threads: int):
+        """Host threads of the reference's GMRES shim (1 = serial, the pinned order)."""
+        self.f["set_threads"](threads)
 
     def solve_stats(self):
         out = []

@@ -22,6 +22,7 @@ struct _p_Vec {
 struct _p_Mat {
   int n = 0;
   std::vector<std::map<int, double>> rows;
+  std::vector<std::vector<int>> log;  /* columns of every MatSetValues per row, in call order */
   std::vector<int> rp, ci;
   std::vector<double> v;
 };
@@ -38,7 +39,7 @@ struct _p_VecScatter {
 };
 
 namespace {
-oracle_gmres_params g_opts = {30, 1e-5, 1e-50, 1e5, 10000, 0, 0.0, 0};
+oracle_gmres_params g_opts = {30, 1e-5, 1e-50, 1e5, 10000, 0, 0.0, 0, 1};
 struct SolveStat {
   int its;
   double rnorm;
@@ -51,6 +52,10 @@ int g_mat_counter = 0;
 std::vector<int> g_keep_rp[2], g_keep_ci[2];
 std::vector<double> g_keep_v[2];
 int g_keep_n[2] = {0, 0};
+/* insertion order of the kept matrices: Build_Linear_System sets A1's row i as the lm
+   stencil neighbours in search order, then the diagonal (solver.cpp:116-125), so the log
+   of A1 is the reference's own stencil of every cell */
+std::vector<int> g_keep_log_rp[2], g_keep_log_ci[2];
 }  // namespace
 
 extern "C" void petsc_shim_set_options(int restart, double rtol, double atol, double dtol, int max_it) {
@@ -60,6 +65,7 @@ extern "C" void petsc_shim_set_options(int restart, double rtol, double atol, do
   g_opts.dtol = dtol;
   g_opts.max_it = max_it;
 }
+extern "C" void petsc_shim_set_threads(int threads) { g_opts.threads = threads > 1 ? threads : 1; }
 extern "C" int petsc_shim_solve_count(void) { return (int)g_stats.size(); }
 extern "C" void petsc_shim_solve_stats(int k, int *its, double *rnorm, int *reason, double *sec) {
   if (k < 0 || k >= (int)g_stats.size()) return;
@@ -77,6 +83,14 @@ extern "C" int petsc_shim_last_matrix(int which, int *n, int *nnz, const int **r
   *rp = g_keep_rp[which].data();
   *ci = g_keep_ci[which].data();
   *v = g_keep_v[which].data();
+  return 0;
+}
+extern "C" int petsc_shim_last_matrix_log(int which, int *n, int *len, const int **rp, const int **ci) {
+  if (which < 0 || which > 1) return -1;
+  *n = g_keep_n[which];
+  *len = (int)g_keep_log_ci[which].size();
+  *rp = g_keep_log_rp[which].data();
+  *ci = g_keep_log_ci[which].data();
   return 0;
 }
 
@@ -124,6 +138,7 @@ PetscErrorCode MatCreate(MPI_Comm, Mat *m) { *m = new _p_Mat(); return 0; }
 PetscErrorCode MatSetSizes(Mat m, PetscInt, PetscInt, PetscInt M, PetscInt) {
   m->n = M;
   m->rows.assign(M, {});
+  m->log.assign(M, {});
   return 0;
 }
 PetscErrorCode MatSetFromOptions(Mat) { return 0; }
@@ -136,6 +151,7 @@ PetscErrorCode MatSetValues(Mat m, PetscInt nr, const PetscInt ir[], PetscInt nc
     for (int b = 0; b < nc; ++b) {
       if (ir[a] < 0 || ir[a] >= m->n || ic[b] < 0 || ic[b] >= m->n) return 63;
       m->rows[ir[a]][ic[b]] = v[a * nc + b];
+      m->log[ir[a]].push_back(ic[b]);
     }
   return 0;
 }
@@ -157,6 +173,12 @@ PetscErrorCode MatAssemblyEnd(Mat m, MatAssemblyType) {
   g_keep_rp[slot] = m->rp;
   g_keep_ci[slot] = m->ci;
   g_keep_v[slot] = m->v;
+  g_keep_log_rp[slot].assign(m->n + 1, 0);
+  g_keep_log_ci[slot].clear();
+  for (int i = 0; i < m->n; ++i) {
+    g_keep_log_ci[slot].insert(g_keep_log_ci[slot].end(), m->log[i].begin(), m->log[i].end());
+    g_keep_log_rp[slot][i + 1] = (int)g_keep_log_ci[slot].size();
+  }
   return 0;
 }
 PetscErrorCode MatDestroy(Mat *m) { delete *m; *m = nullptr; return 0; }
@@ -172,6 +194,7 @@ PetscErrorCode KSPSetFromOptions(KSP k) {
   k->prm.atol = g_opts.atol;
   k->prm.dtol = g_opts.dtol;
   k->prm.max_it = g_opts.max_it;
+  k->prm.threads = g_opts.threads;
   return 0;
 }
 PetscErrorCode KSPSetUp(KSP) { return 0; }

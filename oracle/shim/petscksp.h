@@ -99,6 +99,11 @@ void petsc_shim_reset_stats(void);
 /* the most recently assembled matrices in CSR form (for parity tests) */
 int petsc_shim_last_matrix(int which, int *n, int *nnz, const int **rowptr, const int **col,
                            const double **val);
+/* the columns of every MatSetValues call on those matrices, per row in call order */
+int petsc_shim_last_matrix_log(int which, int *n, int *len, const int **rowptr, const int **col);
+/* host threads of the GMRES shim's vector and matrix loops (1 = serial, the default; the
+   serial order is the one the parity tests pin) */
+void petsc_shim_set_threads(int threads);
 }
 
 #endif

@@ -94,6 +94,29 @@ def test_oracle_matches_reference_live(oracle_lib, reference_lib):
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("case", ["ball32k", "eds64"])
+def test_oracle_stencils_and_matrices_match_reference(oracle_lib, reference_lib, case):
+    """The GFD stencils (the reference's: the order in which Build_Linear_System inserts
+    row i of A1, solver.cpp:116-125) and both assembled matrices, bit for bit, on reduced
+    versions of the ball and the Zel'dovich box (uniform lattice ties included)."""
+    cfg = ics.config(case, n=3000 if case == "ball32k" else 16 ** 3, seed=11)
+    p = cfg.particles()
+    out = {}
+    for which in ("ref", "oracle"):
+        r = refbind.CpuPath(which, p, cfg.depth, cfg.gfd_c, cfg.lm)
+        r.set_gmres(30, 1e-10)
+        r.select()
+        t = cfg.a_start + 0.5 * cfg.delta_a
+        r.solve(1.0 / p.n, 1.5 * cfg.omega0 / t, -1.0)
+        out[which] = (r.stencils(), r.last_matrix(0), r.last_matrix(1))
+        r.close()
+    assert out["ref"][0].shape[1] == cfg.lm
+    assert np.array_equal(out["ref"][0], out["oracle"][0])
+    for k in (1, 2):
+        for a, b in zip(out["ref"][k], out["oracle"][k]):
+            assert np.array_equal(a, b)
+
+
 def test_key64_known_answers(oracle_lib):
     lib = C.CDLL(oracle_lib)
     lib.apcor_key64.restype = C.c_uint64

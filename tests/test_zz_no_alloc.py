@@ -16,6 +16,8 @@ from apcloud import binding, ics
 pytestmark = pytest.mark.gpu
 
 RTOL = 1e-12  # the two entry points share arithmetic and rounding; equality is expected
+NOALLOC_MAX_PARTICLES = 1 << 20  # APC_NOALLOC_MAX_PARTICLES
+APC_ERR_INVALID_ARG = -1
 
 
 def _rel(a, b):
@@ -68,13 +70,40 @@ def test_noalloc_kick_matches_move_velocity_on_two_calls(gpu_lib):
         return rc, d.value
 
     for k in range(2):
+        free_before = torch.cuda.mem_get_info(0)[0]
+        held_before = torch.cuda.memory_allocated(0)
         rc, dv = call(p.n)
         assert rc == 0
+        if k == 1:
+            # the first call loaded the library's module (and with it the fixed scratch
+            # array); from then on a call leaves the device's free memory unchanged
+            assert torch.cuda.mem_get_info(0)[0] == free_before
+        assert torch.cuda.memory_allocated(0) == held_before
         assert dv == pytest.approx(dv_ref[k], rel=RTOL)
         for j in range(3):
             assert _rel(v[j].cpu().numpy(), states[k][3 + j][order]) <= RTOL
             assert _rel(acc[j].cpu().numpy(), states[k][6 + j][order]) <= RTOL
 
+    # cell ranges that leave particles uncovered, overlap, or run past the particle count
+    # are refused, and the velocities and accelerations are left as they were
+    before = [t.clone() for t in v + acc]
+    good_first, good_count = first.clone(), count.clone()
+    last = int(np.nonzero(cells.count)[0][-1])
+    for case, (df, dc) in {"uncovered": (0, -1), "overlap or past the end": (0, 1),
+                           "outside [0, n)": (p.n, 0)}.items():
+        first.copy_(good_first)
+        count.copy_(good_count)
+        first[last] += df
+        count[last] += dc
+        rc, _ = call(p.n)
+        assert rc == APC_ERR_INVALID_ARG, case
+        for t0, t1 in zip(before, v + acc):
+            assert torch.equal(t0, t1), case
+    first.copy_(good_first)
+    count.copy_(good_count)
+    rc, _ = call(p.n)
+    assert rc == 0
+
     # sizes beyond the fixed scratch array are refused before any work is queued
-    rc, _ = call(binding.load_library() and (1 << 20) + 1)
-    assert rc == -1
+    rc, _ = call(NOALLOC_MAX_PARTICLES + 1)
+    assert rc == APC_ERR_INVALID_ARG
