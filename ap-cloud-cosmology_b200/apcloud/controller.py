@@ -40,6 +40,7 @@ class Controller:
     adaptive: bool = False  # ADAPTIVE_TIME_STEP (controller.cpp:146-164)
     output_dir: str | None = None  # VTK snapshots (viewer.cpp) every write_interval steps
     write_interval: int = 0
+    fused: bool = True  # use the backend's whole-step call when it has one (fixed dt)
     t: float = field(init=False)
     log: list = field(default_factory=list)
 
@@ -67,6 +68,17 @@ class Controller:
         (controller.cpp:136-146)."""
         if self.output_dir and self.write_interval > 0 and len(self.log) % self.write_interval == 0:
             self.snapshot()
+        if not self.adaptive and self.fused and hasattr(self.backend, "step"):
+            # the whole step in one library call, kick and drift fused (apc_step)
+            dt = self.delta_a
+            if self.t + dt > self.end_a:
+                dt = self.end_a - self.t
+            k = self.constants(self.t, dt)
+            m, dv, dx = self.backend.step(dt, k["c_dens"], k["c_pot"], k["c_field"], k["c_vel"], k["c_pos"])
+            rec = StepLog(self.t, dt, m, dv, dx)
+            self.log.append(rec)
+            self.t += dt
+            return rec
         m = self.backend.select()
         dt = self.backend.adaptive_dt(self.delta_a) if self.adaptive else self.delta_a
         if self.t + dt > self.end_a:

@@ -134,7 +134,8 @@ struct apc_context {
   int ell_w = 18;            // ELL width lm + 1
   int *ell_col = nullptr;    // [slot][row]
   double *a1 = nullptr, *a2 = nullptr;  // [slot][row]
-  float *a1f = nullptr, *a2f = nullptr;
+  float *a1f = nullptr, *a2f = nullptr;    // D^-1 A1, D^-1 A2 in FP32 (mixed path)
+  double *a1d = nullptr, *a2d = nullptr;   // the same in FP64 (FP64 multigrid path)
   double *rhs = nullptr, *bcrhs = nullptr;
   double *density = nullptr, *potential = nullptr, *deriv = nullptr;
   double rot[9] = {0};       // octant rotation (solver.cpp:464-475), host-computed
@@ -185,19 +186,20 @@ int apc_gfd_assemble(apc_context *c, double c_dens);    // gfd.cu
 int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int *its,
                      double *rnorm, int *reason, int *refinements,
                      int (*during)(apc_context *) = nullptr);  // krylov.cu
-// the potential operator in FP32, Jacobi-scaled (c->a2 -> c->a2f), on stream s
-void apc_potential_to_f32(apc_context *c, cudaStream_t s);  // krylov.cu
+// the potential operator Jacobi-scaled in the inner precision of the configured path
+// (c->a2 -> c->a2f, or c->a2d for the FP64 multigrid path), on stream s
+void apc_potential_scaled(apc_context *c, cudaStream_t s);  // krylov.cu
 void apc_krylov_free(apc_context *c);
 int apc_gmres_fp64_ell(apc_context *c, int n, int w, size_t ld, const int *col, const double *val,
                        const double *b, double *x, int *its, double *rnorm, int *reason);  // krylov.cu
 void apc_mg_free(apc_context *c);
-// One solve of the mixed path (mg.cu): FP64 refinement with FP32 (F)GMRES corrections on
-// the Jacobi-scaled operator valf, run on the device as one CUDA graph; with use_mg the
-// corrections are right-preconditioned by the octree-aggregation V-cycle, whose hierarchy
-// is rebuilt from valf
-int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, const float *valf, const double *b,
-                 double *x, double *r, int restart, double rtol_in, int *its, double *rnorm, int *reason,
-                 int *refinements, int *levels, int (*during)(apc_context *) = nullptr);
+// One solve of the mixed or FP64 multigrid path (mg.cu): FP64 refinement with (F)GMRES
+// corrections on the Jacobi-scaled operator (c->a1f/a2f in FP32, c->a1d/a2d in FP64), run
+// on the device as one CUDA graph; with use_mg the corrections are right-preconditioned by
+// the octree-aggregation V-cycle, whose hierarchy is rebuilt from the scaled operator
+int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, const double *b, double *x, double *r,
+                 int restart, double rtol_in, int *its, double *rnorm, int *reason, int *refinements, int *levels,
+                 int (*during)(apc_context *) = nullptr);
 // Overlap of the potential solve's set-up with the density solve (mg.cu).  After the
 // assembly, apc_mg_mark_assembled records where the potential operator is ready;
 // apc_mg_prebuild, run while the density graph executes, converts that operator to FP32
@@ -214,6 +216,8 @@ int apc_potential_rhs(apc_context *c, double c_pot);    // gfd.cu
 int apc_differentiate(apc_context *c, double c_field);  // gfd.cu
 int apc_mover_velocity(apc_context *c, double dt, double c_vel, double *max_dv);  // mover.cu
 int apc_mover_position(apc_context *c, double dt, double c_pos, double *max_dx);  // mover.cu
+int apc_mover_kick_drift(apc_context *c, double dt, double c_vel, double c_pos, double *max_dv,
+                         double *max_dx);                                          // mover.cu
 int apc_mover_max_density(apc_context *c, double *out);                           // mover.cu
 int apc_exclusive_scan(apc_context *c, const int *in, int *out, int n, int *total_dev);  // scan.cu
 int apc_radix_sort_u64(apc_context *c, uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,

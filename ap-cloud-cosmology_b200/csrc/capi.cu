@@ -121,7 +121,7 @@ void free_all(apc_context *c) {
                   c->req_key_alt, c->req_idx, c->req_idx_alt, c->req_code, c->req_pos, c->counters,
                   c->d_err, c->scan_tmp, c->flags, c->cx, c->cy, c->cz, c->ch, c->cfirst, c->ccount,
                   c->ctype, c->ccode, c->nb24, c->nnb, c->cell_of, c->st_idx, c->st_dist, c->gfd_x,
-                  c->ell_col, c->a1, c->a2, c->a1f, c->a2f, c->rhs, c->bcrhs, c->density, c->potential,
+                  c->ell_col, c->a1, c->a2, c->a1f, c->a2f, c->a1d, c->a2d, c->rhs, c->bcrhs, c->density, c->potential,
                   c->deriv, c->adj_ckpt, c->adj_tape, c->gfd_scr_d, c->gfd_scr_i, c->gfd_qr, c->full_keys, c->full_keys_alt, c->full_ids, c->full_ids_alt, c->warm_keys, c->warm_rho,
                   c->warm_phi, c->tr_cnt, c->tr_off, c->tr_cur, c->tr_tmp,
                   c->tp_col, c->tp_src, c->ta_col, c->ta_src, c->ta_val, c->vjp_c, c->vjp_phi, c->vjp_r2,
@@ -224,7 +224,8 @@ int apc_create(const apc_config *cfg, apc_context **out) {
       (cfg->bc != 0 && cfg->bc != 1) || !(cfg->gfd_c >= 0.0) || cfg->gmres_restart < 1 ||
       cfg->gmres_restart > 255 || cfg->mixed_restart < 0 || cfg->mixed_restart > 31 || cfg->mg_sweeps < 0 ||
       (cfg->mixed_precond != APC_PRECOND_JACOBI && cfg->mixed_precond != APC_PRECOND_MULTIGRID) ||
-      (cfg->precision != APC_PREC_FP64 && cfg->precision != APC_PREC_MIXED))
+      (cfg->precision != APC_PREC_FP64 && cfg->precision != APC_PREC_MIXED &&
+       cfg->precision != APC_PREC_FP64_MULTIGRID))
     return APC_ERR_INVALID_ARG;
   for (int d = 0; d < 3; ++d)
     if (!(cfg->box[2 * d + 1] > cfg->box[2 * d])) return APC_ERR_INVALID_ARG;
@@ -417,10 +418,13 @@ int apc_solve(apc_context *c, double c_dens, double c_pot, double c_field) {
   if (c->cfg.precision == APC_PREC_MIXED) {
     APC_TRY(apc_ensure(c, &c->a1f, (size_t)c->m_cap * c->ell_w, nullptr));
     APC_TRY(apc_ensure(c, &c->a2f, (size_t)c->m_cap * c->ell_w, nullptr));
+  } else if (c->cfg.precision == APC_PREC_FP64_MULTIGRID) {
+    APC_TRY(apc_ensure(c, &c->a1d, (size_t)c->m_cap * c->ell_w, nullptr));
+    APC_TRY(apc_ensure(c, &c->a2d, (size_t)c->m_cap * c->ell_w, nullptr));
   }
   apc_solve_stats &st = c->stats;
-  // mixed path with multigrid: the potential hierarchy is built while the density solve runs
-  const bool overlap = c->cfg.precision == APC_PREC_MIXED && c->cfg.mixed_precond == APC_PRECOND_MULTIGRID;
+  // multigrid paths: the potential hierarchy is built while the density solve runs
+  const bool overlap = c->cfg.precision != APC_PREC_FP64 && c->cfg.mixed_precond == APC_PRECOND_MULTIGRID;
   if (overlap) APC_TRY(apc_mg_mark_assembled(c));
   APC_CUDA_TRY(c, cudaEventRecord(c->sev[0], c->s));
   APC_TRY(apc_krylov_solve(c, 0, c->rhs, c->density, &st.density_its, &st.density_rnorm, &st.density_reason,
@@ -432,7 +436,7 @@ int apc_solve(apc_context *c, double c_dens, double c_pot, double c_field) {
                            &st.potential_reason, &st.potential_refinements));
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[7], c->s));
   APC_TRY(apc_differentiate(c, c_field));
-  if (c->cfg.precision == APC_PREC_MIXED && c->cfg.warm_start) APC_TRY(apc_warm_save(c));
+  if (c->cfg.precision != APC_PREC_FP64 && c->cfg.warm_start) APC_TRY(apc_warm_save(c));
   c->last_c_pot = c_pot;
   c->last_c_field = c_field;
   (void)M;
@@ -480,8 +484,18 @@ int apc_step(apc_context *c, const apc_step_params *p, int *n_cells, double *max
   if (!p) return APC_ERR_INVALID_ARG;
   APC_TRY(apc_select(c, n_cells));
   APC_TRY(apc_solve(c, p->c_dens, p->c_pot, p->c_field));
-  APC_TRY(apc_move_velocity(c, p->dt, p->c_vel, max_dv));
-  APC_TRY(apc_move_position(c, p->dt, p->c_pos, max_dx));
+  // move_velocity + move_position (mover.cpp:51-121) as one fused pass over the particles
+  APC_CUDA_TRY(c, cudaEventRecord(c->ev[4], c->s));
+  APC_TRY(apc_mover_kick_drift(c, p->dt, p->c_vel, p->c_pos, max_dv, max_dx));
+  APC_CUDA_TRY(c, cudaEventRecord(c->ev[6], c->s));
+  APC_CUDA_TRY(c, apc_event_wait(c->ev[6]));
+  c->t_move_ms = elapsed(c->ev[4], c->ev[6]);
+  c->prof.move_ms += c->t_move_ms;
+  c->kick_recorded = false;
+  if (c->step_open) {
+    c->prof.step_ms += elapsed(c->ev[0], c->ev[6]);
+    c->step_open = false;
+  }
   return APC_OK;
 }
 

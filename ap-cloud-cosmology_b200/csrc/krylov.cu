@@ -457,16 +457,18 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_kernel(GmresArgs<T> A) {
 
 // ------------------------------------------------------------ mixed-path helpers
 
-__global__ void ell_to_f32_scaled(size_t ld, int w, int n, const double *__restrict__ a, float *__restrict__ f) {
+// D^-1 A in the inner precision T (rows past n zeroed)
+template <class T>
+__global__ void ell_to_scaled(size_t ld, int w, int n, const double *__restrict__ a, T *__restrict__ f) {
   const size_t count = ld * (size_t)w;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < count; e += (size_t)gridDim.x * blockDim.x) {
     const size_t i = e % ld;
     if ((int)i >= n) {
-      f[e] = 0.f;
+      f[e] = T(0);
       continue;
     }
     const double d = a[i];
-    f[e] = (float)(d == 0.0 ? a[e] : a[e] / d);
+    f[e] = (T)(d == 0.0 ? a[e] : a[e] / d);
   }
 }
 
@@ -655,13 +657,19 @@ int apc_gmres_fp64_ell(apc_context *c, int n, int w, size_t ld, const int *col, 
 // Jacobi-scaled system (D^-1 A) d = D^-1 r / ||D^-1 r|| in FP32 to the inner tolerance,
 // by GMRES(CGS2) or, for the potential with the multigrid option, by FGMRES with the
 // octree-aggregation V-cycle.
-void apc_potential_to_f32(apc_context *c, cudaStream_t s) {
+static void to_scaled(apc_context *c, cudaStream_t s, int which) {
   const int n = c->nc + c->nv;
   const size_t ell_count = (size_t)c->m_cap * c->ell_w;
-  ell_to_f32_scaled<<<std::min<size_t>((ell_count + 255) / 256, 8192), 256, 0, s>>>((size_t)c->m_cap, c->ell_w, n,
-                                                                                    c->a2, c->a2f);
+  const int G = (int)std::min<size_t>((ell_count + 255) / 256, 8192);
+  const double *a = which == 0 ? c->a1 : c->a2;
+  if (c->cfg.precision == APC_PREC_FP64_MULTIGRID)
+    ell_to_scaled<double><<<G, 256, 0, s>>>((size_t)c->m_cap, c->ell_w, n, a, which == 0 ? c->a1d : c->a2d);
+  else
+    ell_to_scaled<float><<<G, 256, 0, s>>>((size_t)c->m_cap, c->ell_w, n, a, which == 0 ? c->a1f : c->a2f);
   apc_count_launch(c);
 }
+
+void apc_potential_scaled(apc_context *c, cudaStream_t s) { to_scaled(c, s, 1); }
 
 int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int *its, double *rnorm,
                      int *reason, int *refinements, int (*during)(apc_context *)) {
@@ -675,18 +683,12 @@ int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int 
     return launch_gmres<double, false>(c, n, val, b, x, cfg.gmres_restart, cfg.gmres_rtol, cfg.gmres_atol,
                                        cfg.gmres_dtol, cfg.gmres_max_it, its, rnorm, reason);
   }
-  // ---- mixed precision: the refinement loop and its FP32 corrections run on the device
-  //      as one graph per solve (mg.cu) ----
-  const size_t ell_count = (size_t)c->m_cap * c->ell_w;
-  float *af = which == 0 ? c->a1f : c->a2f;
+  // ---- mixed precision or FP64 multigrid: the refinement loop and its corrections run on
+  //      the device as one graph per solve (mg.cu) ----
   const int G = std::max(1, std::min((n + 255) / 256, std::min(apc_sm_count(c) * 8, 4096)));
-  // a prebuilt potential hierarchy (apc_mg_prebuild) came with its FP32 operator
+  // a prebuilt potential hierarchy (apc_mg_prebuild) came with its scaled operator
   const bool prebuilt = which == 1 && apc_mg_prebuilt(c);
-  if (!prebuilt) {
-    ell_to_f32_scaled<<<std::min<size_t>((ell_count + 255) / 256, 8192), 256, 0, c->s>>>((size_t)c->m_cap,
-                                                                                         c->ell_w, n, val, af);
-    apc_count_launch(c);
-  }
+  if (!prebuilt) to_scaled(c, c->s, which);
   if (cfg.warm_start) {
     APC_TRY(apc_warm_guess(c, which, x));
   } else {
@@ -702,8 +704,8 @@ int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int 
   // multigrid cycles stop at 1e-3; the density solve keeps 1e-5
   const double rtol_in = cfg.mixed_inner_rtol > 0 ? cfg.mixed_inner_rtol : (use_mg ? 1e-3 : 1e-5);
   int levels = 0;
-  APC_TRY(apc_ir_solve(c, which, use_mg, val, af, b, x, k->r, m32, rtol_in, its, rnorm, reason, refinements,
-                       &levels, during));
+  APC_TRY(apc_ir_solve(c, which, use_mg, val, b, x, k->r, m32, rtol_in, its, rnorm, reason, refinements, &levels,
+                       during));
   if (use_mg) c->stats.mg_levels = levels;
   return APC_OK;
 }

@@ -76,10 +76,11 @@ __global__ void aggregate_map(int n, const uint64_t *__restrict__ key, const uin
   }
 }
 
-__global__ void ell_f32_dinv(int n, size_t ld, const float *__restrict__ val, float *__restrict__ dinv) {
+template <class V>
+__global__ void ell_dinv(int n, size_t ld, const V *__restrict__ val, V *__restrict__ dinv) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const float d = val[i];
-    dinv[i] = d != 0.f ? 1.f / d : 1.f;
+    const V d = val[i];
+    dinv[i] = d != V(0) ? V(1) / d : V(1);
   }
 }
 
@@ -93,13 +94,14 @@ constexpr int kGalWarps = 4;
 constexpr int kGalTab = 512;   // hash slots per warp
 constexpr int kGalRows = 256;  // distinct coarse columns per row
 
+template <class V>
 __global__ void __launch_bounds__(32 * kGalWarps) galerkin_rows(int nc, const int *__restrict__ mptr, int nf,
                                                               const int *__restrict__ mem, int wf, size_t ldf,
                                                               const int *__restrict__ colf,
-                                                              const float *__restrict__ valf,
+                                                              const V *__restrict__ valf,
                                                               const int *__restrict__ agg, int wcap,
                                                               int *__restrict__ rowlen, int *__restrict__ tcol,
-                                                              float *__restrict__ tval, int *__restrict__ err) {
+                                                              V *__restrict__ tval, int *__restrict__ err) {
   __shared__ int tkey[kGalWarps][kGalTab];
   __shared__ double tsum[kGalWarps][kGalTab];
   __shared__ double stage[kGalWarps][32];
@@ -166,7 +168,7 @@ __global__ void __launch_bounds__(32 * kGalWarps) galerkin_rows(int nc, const in
       for (int u = 0; u < len; ++u) rank += dkey[wv][u] < key ? 1 : 0;
       if (rank < wcap) {
         tcol[(size_t)I * wcap + rank] = key;
-        tval[(size_t)I * wcap + rank] = (float)dval[wv][q];
+        tval[(size_t)I * wcap + rank] = (V)dval[wv][q];
       }
     }
     bad = __any_sync(0xffffffffu, bad);
@@ -178,21 +180,22 @@ __global__ void __launch_bounds__(32 * kGalWarps) galerkin_rows(int nc, const in
   }
 }
 
+template <class V>
 __global__ void rows_to_ell(int n, int w, size_t ld, int wcap, const int *__restrict__ rowlen,
-                            const int *__restrict__ tcol, const float *__restrict__ tval, int *__restrict__ col,
-                            float *__restrict__ val, float *__restrict__ dinv) {
+                            const int *__restrict__ tcol, const V *__restrict__ tval, int *__restrict__ col,
+                            V *__restrict__ val, V *__restrict__ dinv) {
   for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < n; I += gridDim.x * blockDim.x) {
     const int len = rowlen[I];
-    float d = 0.f;
+    V d = V(0);
     for (int s = 0; s < w; ++s) {
       const bool in = s < len;
       const int c = in ? tcol[(size_t)I * wcap + s] : I;
-      const float v = in ? tval[(size_t)I * wcap + s] : 0.f;
+      const V v = in ? tval[(size_t)I * wcap + s] : V(0);
       col[(size_t)s * ld + I] = c;
       val[(size_t)s * ld + I] = v;
       if (in && c == I) d += v;
     }
-    dinv[I] = d != 0.f ? 1.f / d : 1.f;
+    dinv[I] = d != V(0) ? V(1) / d : V(1);
   }
 }
 
@@ -206,17 +209,19 @@ __global__ void max_int(int n, const int *__restrict__ a, int *out) {
 
 // ------------------------------------------------------------------ V-cycle
 
-__global__ void jacobi_first(int n, const float *__restrict__ dinv, const float *__restrict__ b, float omega,
-                             float *__restrict__ x) {
+template <class V>
+__global__ void jacobi_first(int n, const V *__restrict__ dinv, const V *__restrict__ b, V omega,
+                             V *__restrict__ x) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = omega * dinv[i] * b[i];
 }
 
 // b_c[I] = sum of r over the members of I, in member order
+template <class V>
 __global__ void restrict_sum(int nc, const int *__restrict__ mptr, int nf, const int *__restrict__ mem,
-                             const float *__restrict__ r, float *__restrict__ bc) {
+                             const V *__restrict__ r, V *__restrict__ bc) {
   for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
     const int a = mptr[I], e = (I + 1 < nc) ? mptr[I + 1] : nf;
-    float s = 0.f;
+    V s = V(0);
     for (int k = a; k < e; ++k) s += r[mem[k]];
     bc[I] = s;
   }
@@ -228,12 +233,12 @@ __global__ void restrict_sum(int nc, const int *__restrict__ mptr, int nf, const
 // so a warp still reads whole sectors) and add their sums by a fixed shuffle tree.
 enum RowOp { kOpFirst2, kOpSweep, kOpResidual, kOpProlongSweep };
 
-template <int G, int OP>
+template <int G, int OP, class V>
 __global__ void __launch_bounds__(kT) row_op(int n, int w, size_t ld, const int *__restrict__ col,
-                                             const float *__restrict__ val, const float *__restrict__ dinv,
-                                             const float *__restrict__ b, const float *__restrict__ xin,
-                                             const int *__restrict__ agg, const float *__restrict__ xc, float alpha,
-                                             float omega, float *__restrict__ out) {
+                                             const V *__restrict__ val, const V *__restrict__ dinv,
+                                             const V *__restrict__ b, const V *__restrict__ xin,
+                                             const int *__restrict__ agg, const V *__restrict__ xc, V alpha,
+                                             V omega, V *__restrict__ out) {
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int sub = (int)(tid % G);
   const long long groups = ((long long)gridDim.x * blockDim.x) / G;
@@ -241,13 +246,13 @@ __global__ void __launch_bounds__(kT) row_op(int n, int w, size_t ld, const int 
   for (long long rd = 0; rd < rounds; ++rd) {
     const long long i = tid / G + rd * groups;
     const bool act = i < n;
-    float sacc = 0.f;
+    V sacc = V(0);
     if (act) {
 #pragma unroll 4
       for (int k = sub; k < w; k += G) {
         const size_t at = (size_t)k * ld + i;
         const int j = col[at];
-        float xj;
+        V xj;
         if (OP == kOpFirst2) xj = omega * dinv[j] * b[j];
         else if (OP == kOpProlongSweep) xj = xin[j] + alpha * xc[agg[j]];
         else xj = xin[j];
@@ -258,14 +263,14 @@ __global__ void __launch_bounds__(kT) row_op(int n, int w, size_t ld, const int 
     for (int o = G / 2; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
     if (act && sub == 0) {
       if (OP == kOpFirst2) {
-        const float x1 = omega * dinv[i] * b[i];
+        const V x1 = omega * dinv[i] * b[i];
         out[i] = x1 + omega * dinv[i] * (b[i] - sacc);
       } else if (OP == kOpSweep) {
         out[i] = xin[i] + omega * dinv[i] * (b[i] - sacc);
       } else if (OP == kOpResidual) {
         out[i] = b[i] - sacc;
       } else {
-        const float y = xin[i] + alpha * xc[agg[i]];
+        const V y = xin[i] + alpha * xc[agg[i]];
         out[i] = y + omega * dinv[i] * (b[i] - sacc);
       }
     }
@@ -291,6 +296,7 @@ struct IrState {
   double rtol, atol, dtol, rtol_in;
   double rtol_in_base;  // the configured inner tolerance; rtol_in adapts per correction
   int max_it, max_outer, M, inner_max;
+  int exact_inner;  // FP64 corrections: each cycle aims straight at the outer tolerance
   double beta;    // ||v_0|| of the current cycle
   double scale;   // factor that normalises the newest basis vector
   double H[(kMaxM + 1) * kMaxM];  // column j at H[j * (M + 1)]
@@ -409,14 +415,14 @@ __device__ void arnoldi_step(IrState *S, const double *h1, const double *h2, dou
 // (one per lane); a row's basis values stay in registers for the update and the dots.
 //   MODE 1: w -= V h_in; h = V^T w.   MODE 2: w -= V h_in; out[0] = ||w||^2.
 // MODE 2 also finishes the Arnoldi step in its last block (h1, h2 as arnoldi_step).
-template <int MODE>
-__global__ void __launch_bounds__(kT) cgs_pass(int n, IrState *S, float *V, size_t vn,
+template <int MODE, class T>
+__global__ void __launch_bounds__(kT) cgs_pass(int n, IrState *S, T *V, size_t vn,
                                                 const double *__restrict__ h_in, double *partial, unsigned *counter,
                                                 double *out, const double *h1, const double *h2,
                                                 cudaGraphConditionalHandle cond) {
   __shared__ double hsh[32];
   const int nv = S->it + 1;
-  float *w = V + (size_t)nv * vn;
+  T *w = V + (size_t)nv * vn;
   if ((int)threadIdx.x < nv) hsh[threadIdx.x] = h_in[threadIdx.x];
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -429,15 +435,15 @@ __global__ void __launch_bounds__(kT) cgs_pass(int n, IrState *S, float *V, size
     const int i = tile * 32 + lane;
     const bool ok = i < n;
     if (MODE == 1) {
-      float vj[32];
+      T vj[32];
 #pragma unroll
-      for (int j = 0; j < 32; ++j) vj[j] = (j < nv && ok) ? V[(size_t)j * vn + i] : 0.f;
+      for (int j = 0; j < 32; ++j) vj[j] = (j < nv && ok) ? V[(size_t)j * vn + i] : T(0);
       double wi = ok ? (double)w[i] : 0.0;
 #pragma unroll
       for (int j = 0; j < 32; ++j)
         if (j < nv) wi -= hsh[j] * (double)vj[j];
-      if (ok) w[i] = (float)wi;
-      wi = (double)(float)wi;
+      if (ok) w[i] = (T)wi;
+      wi = (double)(T)wi;
 #pragma unroll
       for (int j = 0; j < 32; ++j)
         if (j < nv) acc[j] += wi * (double)vj[j];
@@ -446,8 +452,8 @@ __global__ void __launch_bounds__(kT) cgs_pass(int n, IrState *S, float *V, size
 #pragma unroll
       for (int j = 0; j < 32; ++j)
         if (j < nv) wi -= hsh[j] * (double)V[(size_t)j * vn + i];
-      w[i] = (float)wi;
-      wi = (double)(float)wi;
+      w[i] = (T)wi;
+      wi = (double)(T)wi;
       acc1 += wi * wi;
     }
   }
@@ -467,14 +473,15 @@ __global__ void __launch_bounds__(kT) cgs_pass(int n, IrState *S, float *V, size
 // V_{it+1} = A z and the dots <V_{it+1}, V_j>, j <= it, in the same warp-tile pass.
 // With a preconditioner z is its output, kept as Z_it for the solution; without one
 // (Z == nullptr) z is V_it itself.
+template <class T>
 __global__ void __launch_bounds__(kT) spmv_dots(int n, int ew, size_t ld, const int *__restrict__ col,
-                                                 const float *__restrict__ val, const float *zin, float *Z,
-                                                 float *V, size_t vn, const IrState *__restrict__ S, double *partial,
+                                                 const T *__restrict__ val, const T *zin, T *Z,
+                                                 T *V, size_t vn, const IrState *__restrict__ S, double *partial,
                                                  unsigned *counter, double *out) {
   const int it = S->it, nv = it + 1;
-  const float *z = Z ? zin : V + (size_t)it * vn;
-  float *zk = Z ? Z + (size_t)it * vn : nullptr;
-  float *w = V + (size_t)nv * vn;
+  const T *z = Z ? zin : V + (size_t)it * vn;
+  T *zk = Z ? Z + (size_t)it * vn : nullptr;
+  T *w = V + (size_t)nv * vn;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   double acc[32];
 #pragma unroll
@@ -483,7 +490,7 @@ __global__ void __launch_bounds__(kT) spmv_dots(int n, int ew, size_t ld, const 
   for (int tile = blockIdx.x * nw + warp; tile < ntiles; tile += gridDim.x * nw) {
     const int i = tile * 32 + lane;
     if (i >= n) continue;
-    float sacc = 0.f;
+    T sacc = T(0);
     for (int k = 0; k < ew; ++k) {
       const size_t at = (size_t)k * ld + i;
       sacc += val[at] * z[col[at]];
@@ -500,12 +507,13 @@ __global__ void __launch_bounds__(kT) spmv_dots(int n, int ew, size_t ld, const 
 }
 
 // V_it *= scale (the newest basis vector), and the same into the V-cycle's input if any
-__global__ void scale_next(int n, const IrState *__restrict__ S, float *__restrict__ V, size_t vn,
-                           float *__restrict__ vin) {
-  const float f = (float)S->scale;
-  float *v = V + (size_t)S->it * vn;
+template <class T>
+__global__ void scale_next(int n, const IrState *__restrict__ S, T *__restrict__ V, size_t vn,
+                           T *__restrict__ vin) {
+  const T f = (T)S->scale;
+  T *v = V + (size_t)S->it * vn;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const float u = v[i] * f;
+    const T u = v[i] * f;
     v[i] = u;
     if (vin) vin[i] = u;
   }
@@ -525,20 +533,21 @@ __global__ void fg_finish(IrState *S) {
 }
 
 // d = Z y
-__global__ void combine(int n, const float *__restrict__ Z, size_t vn, const IrState *__restrict__ S,
-                        float *__restrict__ d) {
+template <class T>
+__global__ void combine(int n, const T *__restrict__ Z, size_t vn, const IrState *__restrict__ S,
+                        T *__restrict__ d) {
   const int nv = S->it;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double t = 0.0;
     for (int j = 0; j < nv; ++j) t += S->y[j] * (double)Z[(size_t)j * vn + i];
-    d[i] = (float)t;
+    d[i] = (T)t;
   }
 }
 
 // ---- the FP64 refinement loop ----
 
 __global__ void ir_init(IrState *S, double rtol, double atol, double dtol, double rtol_in, int max_it, int max_outer,
-                        int M) {
+                        int M, int exact_inner) {
   S->outer = 0;
   S->total_its = 0;
   S->reason = 0;
@@ -552,6 +561,7 @@ __global__ void ir_init(IrState *S, double rtol, double atol, double dtol, doubl
   S->max_it = max_it;
   S->max_outer = max_outer;
   S->M = M;
+  S->exact_inner = exact_inner;
 }
 
 // r = b - A x in FP64 and ||D^-1 r||; the last block applies the stopping test of the
@@ -598,7 +608,13 @@ __global__ void __launch_bounds__(kT) ir_residual(int n, int w, size_t ld, const
   // (~cond(A) 6e-8, which grows as the tree deepens); solving the next correction much
   // further than the last one's achieved reduction is wasted.  So the next inner
   // tolerance is half the last reduction, never tighter than the configured one.
-  if (S->outer >= 1 && S->rn > 0.0) S->rtol_in = fmin(0.1, fmax(S->rtol_in_base, 0.5 * (rn / S->rn)));
+  if (S->exact_inner) {
+    // FP64 corrections carry no operator rounding to stop at: each cycle is asked for
+    // the whole remaining reduction, with a factor 2 of margin
+    if (rn > 0.0) S->rtol_in = fmin(0.1, fmax(0.5 * S->ttol / rn, 1e-15));
+  } else if (S->outer >= 1 && S->rn > 0.0) {
+    S->rtol_in = fmin(0.1, fmax(S->rtol_in_base, 0.5 * (rn / S->rn)));
+  }
   S->rn = rn;
   S->reason = reason;
   cudaGraphSetConditional(cond, stop ? 0u : 1u);
@@ -620,16 +636,17 @@ __global__ void __launch_bounds__(kT) ir_bnorm(int n, const double *__restrict__
   if (threadIdx.x == 0) S->bnorm = sqrt(__ldcg(tmp));
 }
 
-// v_0 = D^-1 r / ||D^-1 r|| rounded to FP32, and beta = ||v_0||; the last block opens
-// the FGMRES cycle (sets the inner loop's condition)
-__global__ void __launch_bounds__(kT) ir_to_f32(int n, const double *__restrict__ r, const double *__restrict__ diag,
-                                                 IrState *S, float *__restrict__ v0, double *partial,
-                                                 unsigned *counter, double *tmp, cudaGraphConditionalHandle cond) {
+// v_0 = D^-1 r / ||D^-1 r|| rounded to the inner precision, and beta = ||v_0||; the last
+// block opens the (F)GMRES cycle (sets the inner loop's condition)
+template <class T>
+__global__ void __launch_bounds__(kT) ir_to_inner(int n, const double *__restrict__ r, const double *__restrict__ diag,
+                                                   IrState *S, T *__restrict__ v0, double *partial,
+                                                   unsigned *counter, double *tmp, cudaGraphConditionalHandle cond) {
   const double inv_s = 1.0 / S->rn;
   double nrm = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double d = diag[i];
-    const float v = (float)((d == 0.0 ? r[i] : r[i] / d) * inv_s);
+    const T v = (T)((d == 0.0 ? r[i] : r[i] / d) * inv_s);
     v0[i] = v;
     nrm += (double)v * (double)v;
   }
@@ -648,7 +665,8 @@ __global__ void __launch_bounds__(kT) ir_to_f32(int n, const double *__restrict_
 }
 
 // x += ||D^-1 r|| d: apply the correction of the scaled system
-__global__ void ir_axpy(int n, IrState *S, const float *__restrict__ d, double *__restrict__ x) {
+template <class T>
+__global__ void ir_axpy(int n, IrState *S, const T *__restrict__ d, double *__restrict__ x) {
   const double s = S->rn;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] += s * (double)d[i];
   if (blockIdx.x == 0 && threadIdx.x == 0) S->outer += 1;
@@ -661,33 +679,35 @@ __global__ void ir_axpy(int n, IrState *S, const float *__restrict__ d, double *
 constexpr int kTail = 1024;
 constexpr int kTailLevels = 12;
 
+template <class V>
 struct TailLevel {
   int n, w, g;  // g: lanes per row (power of two)
   size_t ld;
   const int *col;
-  const float *val, *dinv;
+  const V *val, *dinv;
   const int *agg;             // node -> next coarser node
   const int *mptr, *mem;      // members of this level's nodes on the finer level
-  float *x, *x2, *b, *r;
+  V *x, *x2, *b, *r;
 };
+template <class V>
 struct TailArgs {
   int nl;                     // levels in the tail, the last one solved densely
-  TailLevel L[kTailLevels];
-  const float *inv;
+  TailLevel<V> L[kTailLevels];
+  const V *inv;
   int sweeps;
-  float omega, alpha;
+  V omega, alpha;
 };
 
 // (A x)_i for every row of a tail level, L.g lanes per row; emit(i, sum) runs on the
 // group's first lane.  The trip count is the same for the whole block (shuffles).
-template <class F>
-__device__ __forceinline__ void tail_rows(const TailLevel &L, const float *xin, F emit) {
+template <class V, class F>
+__device__ __forceinline__ void tail_rows(const TailLevel<V> &L, const V *xin, F emit) {
   const int g = L.g, sub = threadIdx.x & (g - 1);
   const int per = blockDim.x / g;
   const int rounds = (L.n + per - 1) / per;
   for (int rd = 0; rd < rounds; ++rd) {
     const int i = (int)threadIdx.x / g + rd * per;
-    float sacc = 0.f;
+    V sacc = V(0);
     if (i < L.n)
       for (int k = sub; k < L.w; k += g) {
         const size_t at = (size_t)k * L.ld + i;
@@ -698,38 +718,40 @@ __device__ __forceinline__ void tail_rows(const TailLevel &L, const float *xin, 
   }
 }
 
-__device__ __forceinline__ void tail_sweep(const TailLevel &L, const float *xin, float *xout, float omega) {
-  tail_rows(L, xin, [&](int i, float sacc) { xout[i] = xin[i] + omega * L.dinv[i] * (L.b[i] - sacc); });
+template <class V>
+__device__ __forceinline__ void tail_sweep(const TailLevel<V> &L, const V *xin, V *xout, V omega) {
+  tail_rows(L, xin, [&](int i, V sacc) { xout[i] = xin[i] + omega * L.dinv[i] * (L.b[i] - sacc); });
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(1024) vcycle_tail(TailArgs A) {
-  float *cur[kTailLevels];
+template <class V>
+__global__ void __launch_bounds__(1024) vcycle_tail(TailArgs<V> A) {
+  V *cur[kTailLevels];
   for (int l = 0; l < A.nl - 1; ++l) {
-    const TailLevel &L = A.L[l];
+    const TailLevel<V> &L = A.L[l];
     for (int i = threadIdx.x; i < L.n; i += blockDim.x) L.x[i] = A.omega * L.dinv[i] * L.b[i];
     __syncthreads();
-    float *c = L.x, *o = L.x2;
+    V *c = L.x, *o = L.x2;
     for (int k = 1; k < A.sweeps; ++k) {
       tail_sweep(L, c, o, A.omega);
-      float *t = c; c = o; o = t;
+      V *t = c; c = o; o = t;
     }
     cur[l] = c;
-    tail_rows(L, c, [&](int i, float sacc) { L.r[i] = L.b[i] - sacc; });
+    tail_rows(L, c, [&](int i, V sacc) { L.r[i] = L.b[i] - sacc; });
     __syncthreads();
-    const TailLevel &C = A.L[l + 1];
+    const TailLevel<V> &C = A.L[l + 1];
     for (int I = threadIdx.x; I < C.n; I += blockDim.x) {
       const int a = C.mptr[I], e = (I + 1 < C.n) ? C.mptr[I + 1] : L.n;
-      float sacc = 0.f;
+      V sacc = V(0);
       for (int q = a; q < e; ++q) sacc += L.r[C.mem[q]];
       C.b[I] = sacc;
     }
     __syncthreads();
   }
   {
-    const TailLevel &K = A.L[A.nl - 1];
+    const TailLevel<V> &K = A.L[A.nl - 1];
     for (int i = threadIdx.x; i < K.n; i += blockDim.x) {
-      float sacc = 0.f;
+      V sacc = V(0);
       for (int j = 0; j < K.n; ++j) sacc += A.inv[(size_t)i * K.n + j] * K.b[j];
       K.x[i] = sacc;
     }
@@ -737,15 +759,15 @@ __global__ void __launch_bounds__(1024) vcycle_tail(TailArgs A) {
     cur[A.nl - 1] = K.x;
   }
   for (int l = A.nl - 2; l >= 0; --l) {
-    const TailLevel &L = A.L[l];
-    float *c = cur[l];
-    float *o = (c == L.x) ? L.x2 : L.x;
-    const float *xc = cur[l + 1];
+    const TailLevel<V> &L = A.L[l];
+    V *c = cur[l];
+    V *o = (c == L.x) ? L.x2 : L.x;
+    const V *xc = cur[l + 1];
     for (int i = threadIdx.x; i < L.n; i += blockDim.x) c[i] += A.alpha * xc[L.agg[i]];
     __syncthreads();
     for (int k = 0; k < A.sweeps; ++k) {
       tail_sweep(L, c, o, A.omega);
-      float *t = c; c = o; o = t;
+      V *t = c; c = o; o = t;
     }
     if (c != L.x) {
       for (int i = threadIdx.x; i < L.n; i += blockDim.x) L.x[i] = c[i];
@@ -757,30 +779,39 @@ __global__ void __launch_bounds__(1024) vcycle_tail(TailArgs A) {
 
 }  // namespace
 
+// The hierarchy and Krylov vectors of one inner precision T: float for the mixed path,
+// double for the FP64 multigrid path.
+template <class T>
 struct MgLevel {
   int n = 0, w = 0;
   size_t ld = 0;
   int *col = nullptr;
-  float *val = nullptr, *dinv = nullptr;
+  T *val = nullptr, *dinv = nullptr;
   uint64_t *code = nullptr;
   int *agg = nullptr;                   // node -> coarser node
   int *mptr = nullptr, *mem = nullptr;  // members on the finer level (levels >= 1)
-  float *x = nullptr, *x2 = nullptr, *b = nullptr, *r = nullptr;
+  T *x = nullptr, *x2 = nullptr, *b = nullptr, *r = nullptr;
   bool owns_matrix = true;
 };
 
-struct MgWork {
-  MgLevel lv[kMaxLevels];
+template <class T>
+struct MgHier {
+  MgLevel<T> lv[kMaxLevels];
   int nlev = 0;
-  float *coarse_inv = nullptr;
+  T *coarse_inv = nullptr;
   int coarse_n = 0;
+  T *uval = nullptr;  // coarse rows before the ELL transpose
+  // FGMRES: basis V, preconditioned vectors Z, V-cycle in/out, correction
+  T *V = nullptr, *Z = nullptr, *vin = nullptr, *vout = nullptr, *dvec = nullptr;
+};
+
+struct MgWork {
+  MgHier<float> h32;
+  MgHier<double> h64;
   // hierarchy temporaries: parent-code sort, flags, coarse rows before the ELL transpose
   uint64_t *pkey = nullptr, *pkey_alt = nullptr;
   uint32_t *pidx = nullptr, *pidx_alt = nullptr;
   int *eflag = nullptr, *epos = nullptr, *ucol = nullptr, *rowstart = nullptr;
-  float *uval = nullptr;
-  // FGMRES: basis V, preconditioned vectors Z, V-cycle in/out, correction
-  float *V = nullptr, *Z = nullptr, *vin = nullptr, *vout = nullptr, *dvec = nullptr;
   size_t vn = 0;
   double *partial = nullptr, *dots = nullptr;
   unsigned *counter = nullptr;
@@ -804,10 +835,20 @@ static MgWork *mg(apc_context *c) {
   return c->mg;
 }
 
-void apc_mg_free(apc_context *c) {
-  MgWork *m = c->mg;
-  if (!m) return;
-  for (auto &L : m->lv) {
+template <class T>
+MgHier<T> &hier(MgWork *m);
+template <>
+MgHier<float> &hier<float>(MgWork *m) {
+  return m->h32;
+}
+template <>
+MgHier<double> &hier<double>(MgWork *m) {
+  return m->h64;
+}
+
+template <class T>
+static void free_hier(apc_context *c, MgHier<T> &H) {
+  for (auto &L : H.lv) {
     if (L.owns_matrix) {
       apc_free(c, L.col);
       apc_free(c, L.val);
@@ -822,9 +863,17 @@ void apc_mg_free(apc_context *c) {
     apc_free(c, L.b);
     apc_free(c, L.r);
   }
-  void *p[] = {m->coarse_inv, m->pkey, m->pkey_alt, m->pidx, m->pidx_alt, m->eflag, m->epos, m->ucol,
-               m->rowstart, m->uval, m->V, m->Z, m->vin, m->vout, m->dvec,
-               m->partial, m->dots, m->counter, m->state, m->total};
+  void *p[] = {H.coarse_inv, H.uval, H.V, H.Z, H.vin, H.vout, H.dvec};
+  for (void *q : p) apc_free(c, q);
+}
+
+void apc_mg_free(apc_context *c) {
+  MgWork *m = c->mg;
+  if (!m) return;
+  free_hier(c, m->h32);
+  free_hier(c, m->h64);
+  void *p[] = {m->pkey, m->pkey_alt, m->pidx, m->pidx_alt, m->eflag, m->epos, m->ucol,
+               m->rowstart, m->partial, m->dots, m->counter, m->state, m->total};
   for (void *q : p) apc_free(c, q);
   if (m->host) cudaFreeHost(m->host);
   for (int k = 0; k < 2; ++k) {
@@ -848,16 +897,30 @@ static int read_int(apc_context *c, const int *dev, int *host) {
   return APC_OK;
 }
 
-// Build the hierarchy over the current f32 potential operator (c->a2f) and cell codes.
+// Build the hierarchy over the current Jacobi-scaled potential operator in precision T
+// (c->a2f or c->a2d) and the cell codes.
+template <class T>
+static const T *scaled_potential(const apc_context *c);
+template <>
+const float *scaled_potential<float>(const apc_context *c) {
+  return c->a2f;
+}
+template <>
+const double *scaled_potential<double>(const apc_context *c) {
+  return c->a2d;
+}
+
+template <class T>
 static int mg_build(apc_context *c) {
   MgWork *m = mg(c);
+  MgHier<T> &H = hier<T>(m);
   const int n0 = c->nc + c->nv;
-  MgLevel &L0 = m->lv[0];
+  MgLevel<T> &L0 = H.lv[0];
   L0.n = n0;
   L0.w = c->ell_w;
   L0.ld = (size_t)c->m_cap;
   L0.col = c->ell_col;
-  L0.val = c->a2f;
+  L0.val = const_cast<T *>(scaled_potential<T>(c));
   L0.owns_matrix = false;
   APC_TRY(apc_ensure(c, &L0.dinv, (size_t)n0 + 1));
   APC_TRY(apc_ensure(c, &L0.code, (size_t)n0 + 1));
@@ -866,13 +929,13 @@ static int mg_build(apc_context *c) {
   APC_TRY(apc_ensure(c, &L0.b, (size_t)n0 + 1));
   APC_TRY(apc_ensure(c, &L0.r, (size_t)n0 + 1));
   APC_CUDA_TRY(c, cudaMemcpyAsync(L0.code, c->ccode, sizeof(uint64_t) * n0, cudaMemcpyDeviceToDevice, c->s));
-  ell_f32_dinv<<<grid_for(n0), kT, 0, c->s>>>(n0, L0.ld, L0.val, L0.dinv);
+  ell_dinv<T><<<grid_for(n0), kT, 0, c->s>>>(n0, L0.ld, L0.val, L0.dinv);
   apc_count_launch(c);
   if (!m->total) APC_TRY(apc_alloc(c, (void **)&m->total, 4 * sizeof(int)));
   int lev = 0;
-  while (m->lv[lev].n > kCoarsest && lev + 1 < kMaxLevels) {
-    MgLevel &F = m->lv[lev];
-    MgLevel &C = m->lv[lev + 1];
+  while (H.lv[lev].n > kCoarsest && lev + 1 < kMaxLevels) {
+    MgLevel<T> &F = H.lv[lev];
+    MgLevel<T> &C = H.lv[lev + 1];
     const int nf = F.n;
     // ---- aggregates: parents of this level's nodes ----
     APC_TRY(apc_ensure(c, &m->pkey, (size_t)nf));
@@ -912,12 +975,12 @@ static int mg_build(apc_context *c) {
     const int wcap = 256;
     APC_TRY(apc_ensure(c, &m->rowstart, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &m->ucol, (size_t)nc * wcap));
-    APC_TRY(apc_ensure(c, &m->uval, (size_t)nc * wcap));
+    APC_TRY(apc_ensure(c, &H.uval, (size_t)nc * wcap));
     APC_CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->s));
     APC_CUDA_TRY(c, cudaMemsetAsync(m->total, 0, sizeof(int), c->s));
     galerkin_rows<<<std::max(1, std::min((nc + kGalWarps - 1) / kGalWarps, apc_sm_count(c) * 8)), 32 * kGalWarps, 0,
                     c->s>>>(nc, C.mptr, nf, C.mem, F.w, F.ld, F.col, F.val, F.agg, wcap, m->rowstart, m->ucol,
-                            m->uval, c->d_err);
+                            H.uval, c->d_err);
     max_int<<<grid_for(nc, 256), kT, 0, c->s>>>(nc, m->rowstart, m->total);
     apc_count_launch(c, 2);
     // the row width and the error flags in one round trip
@@ -938,32 +1001,32 @@ static int mg_build(apc_context *c) {
     APC_TRY(apc_ensure(c, &C.x2, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &C.b, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &C.r, (size_t)nc + 1));
-    rows_to_ell<<<grid_for(nc), kT, 0, c->s>>>(nc, wc, C.ld, wcap, m->rowstart, m->ucol, m->uval, C.col, C.val,
-                                              C.dinv);
+    rows_to_ell<T><<<grid_for(nc), kT, 0, c->s>>>(nc, wc, C.ld, wcap, m->rowstart, m->ucol, H.uval, C.col, C.val,
+                                                 C.dinv);
     apc_count_launch(c);
     APC_CUDA_TRY(c, cudaGetLastError());
     ++lev;
   }
-  m->nlev = lev + 1;
+  H.nlev = lev + 1;
   {
     int first_tail = 0;
-    while (first_tail < m->nlev - 1 && m->lv[first_tail].n > kTail) ++first_tail;
-    if (m->nlev - first_tail > kTailLevels) {
+    while (first_tail < H.nlev - 1 && H.lv[first_tail].n > kTail) ++first_tail;
+    if (H.nlev - first_tail > kTailLevels) {
       c->err = "multigrid hierarchy deeper than the single-block tail supports";
       return APC_ERR_UNSUPPORTED;
     }
   }
   // ---- coarsest level: explicit inverse in FP64 on the host ----
-  MgLevel &K = m->lv[lev];
+  MgLevel<T> &K = H.lv[lev];
   const int n = K.n;
   if (n > 4 * kCoarsest) {
     c->err = "multigrid coarsening stalled";
     return APC_ERR_UNSUPPORTED;
   }
   std::vector<int> col(K.ld * K.w);
-  std::vector<float> val(K.ld * K.w);
+  std::vector<T> val(K.ld * K.w);
   APC_CUDA_TRY(c, cudaMemcpyAsync(col.data(), K.col, sizeof(int) * col.size(), cudaMemcpyDeviceToHost, c->s));
-  APC_CUDA_TRY(c, cudaMemcpyAsync(val.data(), K.val, sizeof(float) * val.size(), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, cudaMemcpyAsync(val.data(), K.val, sizeof(T) * val.size(), cudaMemcpyDeviceToHost, c->s));
   APC_CUDA_TRY(c, apc_stream_wait(c));
   std::vector<double> a((size_t)n * n, 0.0), inv((size_t)n * n, 0.0);
   for (int i = 0; i < n; ++i) {
@@ -998,80 +1061,81 @@ static int mg_build(apc_context *c) {
       }
     }
   }
-  std::vector<float> invf(inv.begin(), inv.end());
-  APC_TRY(apc_ensure(c, &m->coarse_inv, (size_t)n * n + 1));
-  APC_CUDA_TRY(c, cudaMemcpyAsync(m->coarse_inv, invf.data(), sizeof(float) * invf.size(), cudaMemcpyHostToDevice,
+  std::vector<T> invf(inv.begin(), inv.end());
+  APC_TRY(apc_ensure(c, &H.coarse_inv, (size_t)n * n + 1));
+  APC_CUDA_TRY(c, cudaMemcpyAsync(H.coarse_inv, invf.data(), sizeof(T) * invf.size(), cudaMemcpyHostToDevice,
                                   c->s));
   APC_CUDA_TRY(c, apc_stream_wait(c));
-  m->coarse_n = n;
+  H.coarse_n = n;
   return APC_OK;
 }
 
 // x = V-cycle(b) on level l, launched on stream s; b and x are that level's buffers
-static void vcycle(apc_context *c, cudaStream_t s, int l, const float *b, float *x) {
-  MgWork *m = c->mg;
-  MgLevel &L = m->lv[l];
+template <class T>
+static void vcycle(apc_context *c, cudaStream_t s, int l, const T *b, T *x) {
+  MgHier<T> &H = hier<T>(c->mg);
+  MgLevel<T> &L = H.lv[l];
   const int n = L.n;
   const int sweeps = c->cfg.mg_sweeps > 0 ? c->cfg.mg_sweeps : 2;
   // piecewise-constant prolongation under-corrects smooth errors; over-scaling the
   // coarse correction (1.8) with lightly damped Jacobi (0.95) took the 128^3 potential
   // solve from 48 to 29 FGMRES iterations
-  const float omega = (float)(c->cfg.mg_omega > 0 ? c->cfg.mg_omega : 0.95);
-  const float alpha = (float)(c->cfg.mg_alpha > 0 ? c->cfg.mg_alpha : 1.8);
-  if (n <= kTail || l == m->nlev - 1) {
+  const T omega = (T)(c->cfg.mg_omega > 0 ? c->cfg.mg_omega : 0.95);
+  const T alpha = (T)(c->cfg.mg_alpha > 0 ? c->cfg.mg_alpha : 1.8);
+  if (n <= kTail || l == H.nlev - 1) {
     // this level and every coarser one in a single block
-    TailArgs A{};
-    A.nl = std::min(m->nlev - l, kTailLevels);
-    A.inv = m->coarse_inv;
+    TailArgs<T> A{};
+    A.nl = std::min(H.nlev - l, kTailLevels);
+    A.inv = H.coarse_inv;
     A.sweeps = sweeps;
     A.omega = omega;
     A.alpha = alpha;
     for (int k = 0; k < A.nl; ++k) {
-      MgLevel &T = m->lv[l + k];
-      TailLevel &D = A.L[k];
-      D.n = T.n;
-      D.w = T.w;
+      MgLevel<T> &Q = H.lv[l + k];
+      TailLevel<T> &D = A.L[k];
+      D.n = Q.n;
+      D.w = Q.w;
       // wide rows get several lanes while the block has lanes to spare
       D.g = 1;
-      if (T.w > 24)
-        while (D.g < 8 && 2 * D.g * T.n <= 1024) D.g *= 2;
-      D.ld = T.ld;
-      D.col = T.col;
-      D.val = T.val;
-      D.dinv = T.dinv;
-      D.agg = T.agg;
-      D.mptr = T.mptr;
-      D.mem = T.mem;
-      D.x = k == 0 ? x : T.x;
-      D.b = k == 0 ? const_cast<float *>(b) : T.b;
-      D.x2 = T.x2;
-      D.r = T.r;
+      if (Q.w > 24)
+        while (D.g < 8 && 2 * D.g * Q.n <= 1024) D.g *= 2;
+      D.ld = Q.ld;
+      D.col = Q.col;
+      D.val = Q.val;
+      D.dinv = Q.dinv;
+      D.agg = Q.agg;
+      D.mptr = Q.mptr;
+      D.mem = Q.mem;
+      D.x = k == 0 ? x : Q.x;
+      D.b = k == 0 ? const_cast<T *>(b) : Q.b;
+      D.x2 = Q.x2;
+      D.r = Q.r;
     }
-    vcycle_tail<<<1, 1024, 0, s>>>(A);
+    vcycle_tail<T><<<1, 1024, 0, s>>>(A);
     apc_count_launch(c);
     return;
   }
-  MgLevel &C = m->lv[l + 1];
+  MgLevel<T> &C = H.lv[l + 1];
   // lanes per row from the width of this level's rows
   const int g = L.w <= 24 ? 1 : (L.w <= 48 ? 4 : 8);
   const int G = grid_for((long long)n * g);
-  auto op = [&](int kind, const float *xin, float *out) {
+  auto op = [&](int kind, const T *xin, T *out) {
 #define APC_ROW_OP(GG)                                                                                            \
   switch (kind) {                                                                                                 \
     case kOpFirst2:                                                                                               \
-      row_op<GG, kOpFirst2><<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, xin, L.agg, C.x, alpha,       \
+      row_op<GG, kOpFirst2, T><<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, xin, L.agg, C.x, alpha,       \
                                             omega, out);                                                         \
       break;                                                                                                      \
     case kOpSweep:                                                                                                \
-      row_op<GG, kOpSweep><<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, xin, L.agg, C.x, alpha,        \
+      row_op<GG, kOpSweep, T><<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, xin, L.agg, C.x, alpha,        \
                                            omega, out);                                                          \
       break;                                                                                                      \
     case kOpResidual:                                                                                             \
-      row_op<GG, kOpResidual><<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, xin, L.agg, C.x, alpha,     \
+      row_op<GG, kOpResidual, T><<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, xin, L.agg, C.x, alpha,     \
                                               omega, out);                                                       \
       break;                                                                                                      \
     default:                                                                                                      \
-      row_op<GG, kOpProlongSweep><<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, xin, L.agg, C.x, alpha, \
+      row_op<GG, kOpProlongSweep, T><<<G, kT, 0, s>>>(n, L.w, L.ld, L.col, L.val, L.dinv, b, xin, L.agg, C.x, alpha, \
                                                   omega, out);                                                   \
   }
     if (g == 1) {
@@ -1086,7 +1150,7 @@ static void vcycle(apc_context *c, cudaStream_t s, int l, const float *b, float 
   };
   // Buffers alternate between x and L.x2.  The pre-smoothing result is placed so that the
   // `sweeps` post-smoothing sweeps, each flipping buffers, end in x.
-  float *cur, *nxt;
+  T *cur, *nxt;
   if (sweeps >= 2) {
     op(kOpFirst2, nullptr, x);
     cur = x;
@@ -1096,15 +1160,15 @@ static void vcycle(apc_context *c, cudaStream_t s, int l, const float *b, float 
       std::swap(cur, nxt);
     }
   } else {
-    jacobi_first<<<grid_for(n), kT, 0, s>>>(n, L.dinv, b, omega, L.x2);
+    jacobi_first<T><<<grid_for(n), kT, 0, s>>>(n, L.dinv, b, omega, L.x2);
     cur = L.x2;
     nxt = x;
     apc_count_launch(c);
   }
   op(kOpResidual, cur, L.r);
-  restrict_sum<<<grid_for(C.n), kT, 0, s>>>(C.n, C.mptr, n, C.mem, L.r, C.b);
+  restrict_sum<T><<<grid_for(C.n), kT, 0, s>>>(C.n, C.mptr, n, C.mem, L.r, C.b);
   apc_count_launch(c);
-  vcycle(c, s, l + 1, C.b, C.x);
+  vcycle<T>(c, s, l + 1, C.b, C.x);
   op(kOpProlongSweep, cur, nxt);
   std::swap(cur, nxt);
   for (int k = 1; k < sweeps; ++k) {
@@ -1135,13 +1199,14 @@ static cudaError_t add_while(cudaStream_t s, cudaGraphConditionalHandle h, cudaG
   return cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
 }
 
+template <class T>
 struct IrSolveArgs {
   int which;               // 0 density, 1 potential
   bool mg;                 // V-cycle preconditioner (else none: GMRES on the scaled system)
   int n, w;
   size_t ld;
   const int *col;          // ELL columns shared by both operators
-  const float *valf;       // Jacobi-scaled FP32 operator D^-1 A
+  const T *valf;           // Jacobi-scaled operator D^-1 A in the inner precision
   const double *val, *b;   // FP64 operator (diagonal in slot 0) and rhs
   double *x, *r;           // solution, FP64 residual
   double rtol, atol, dtol, rtol_in;
@@ -1160,16 +1225,18 @@ struct IrSolveArgs {
 //   }
 // Both loops end by counters the kernels advance: at most max_outer corrections, M
 // iterations per cycle, max_it iterations in all.
-static int capture_solve(apc_context *c, const IrSolveArgs &a) {
+template <class T>
+static int capture_solve(apc_context *c, const IrSolveArgs<T> &a) {
   MgWork *m = c->mg;
+  MgHier<T> &H = hier<T>(m);
   const int n = a.n, slot = a.which;
   const size_t vn = m->vn;
   const int G = std::min(kRedBlocks, grid_for(n));
   const int Gs = grid_for(n, 1184);
   const bool reorth = c->cfg.mg_reorth != 0;
   double *h1 = m->dots, *h2 = m->dots + 34, *nr = m->dots + 68, *tmp = m->dots + 70;
-  float *Z = a.mg ? m->Z : nullptr;
-  float *vin = a.mg ? m->vin : nullptr;
+  T *Z = a.mg ? H.Z : nullptr;
+  T *vin = a.mg ? H.vin : nullptr;
   const int64_t l0 = c->launches;
   cudaStream_t s = c->s, s1 = m->cap[0], s2 = m->cap[1];
   cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
@@ -1187,7 +1254,8 @@ static int capture_solve(apc_context *c, const IrSolveArgs &a) {
   bool cap1 = false, cap2 = false;
   if (ok(cudaStreamGetCaptureInfo(s, &st, nullptr, &top, nullptr, nullptr)) &&
       ok(cudaGraphConditionalHandleCreate(&cond_out, top, 0, 0))) {
-    ir_init<<<1, 1, 0, s>>>(m->state, a.rtol, a.atol, a.dtol, a.rtol_in, a.max_it, a.max_outer, a.M);
+    ir_init<<<1, 1, 0, s>>>(m->state, a.rtol, a.atol, a.dtol, a.rtol_in, a.max_it, a.max_outer, a.M,
+                            sizeof(T) == sizeof(double) ? 1 : 0);
     ir_bnorm<<<G, kT, 0, s>>>(n, a.val, a.b, m->state, m->partial, m->counter, tmp);
     ir_residual<<<G, kT, 0, s>>>(n, a.w, a.ld, a.col, a.val, a.b, a.x, a.r, m->state, m->partial, m->counter, tmp,
                                  cond_out);
@@ -1195,25 +1263,25 @@ static int capture_solve(apc_context *c, const IrSolveArgs &a) {
         ok(cudaStreamBeginCaptureToGraph(s1, body_out, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal))) {
       cap1 = true;
       if (ok(cudaGraphConditionalHandleCreate(&cond_in, body_out, 0, 0))) {
-        ir_to_f32<<<G, kT, 0, s1>>>(n, a.r, a.val, m->state, m->V, m->partial, m->counter, tmp, cond_in);
-        scale_next<<<Gs, kT, 0, s1>>>(n, m->state, m->V, vn, vin);
+        ir_to_inner<T><<<G, kT, 0, s1>>>(n, a.r, a.val, m->state, H.V, m->partial, m->counter, tmp, cond_in);
+        scale_next<T><<<Gs, kT, 0, s1>>>(n, m->state, H.V, vn, vin);
         if (ok(cudaGetLastError()) && ok(add_while(s1, cond_in, &body_in)) &&
             ok(cudaStreamBeginCaptureToGraph(s2, body_in, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal))) {
           cap2 = true;
           const int64_t v0 = c->launches;
-          if (a.mg) vcycle(c, s2, 0, m->vin, m->vout);
+          if (a.mg) vcycle<T>(c, s2, 0, H.vin, H.vout);
           m->vcycle_nodes[slot] = c->launches - v0;
-          spmv_dots<<<G, kT, 0, s2>>>(n, a.w, a.ld, a.col, a.valf, a.mg ? m->vout : nullptr, Z, m->V, vn, m->state,
-                                      m->partial, m->counter, h1);
+          spmv_dots<T><<<G, kT, 0, s2>>>(n, a.w, a.ld, a.col, a.valf, a.mg ? H.vout : nullptr, Z, H.V, vn, m->state,
+                                         m->partial, m->counter, h1);
           if (reorth) {
-            cgs_pass<1><<<G, kT, 0, s2>>>(n, m->state, m->V, vn, h1, m->partial, m->counter, h2, nullptr, nullptr,
-                                          cond_in);
-            cgs_pass<2><<<G, kT, 0, s2>>>(n, m->state, m->V, vn, h2, m->partial, m->counter, nr, h1, h2, cond_in);
+            cgs_pass<1, T><<<G, kT, 0, s2>>>(n, m->state, H.V, vn, h1, m->partial, m->counter, h2, nullptr, nullptr,
+                                             cond_in);
+            cgs_pass<2, T><<<G, kT, 0, s2>>>(n, m->state, H.V, vn, h2, m->partial, m->counter, nr, h1, h2, cond_in);
           } else {
-            cgs_pass<2><<<G, kT, 0, s2>>>(n, m->state, m->V, vn, h1, m->partial, m->counter, nr, h1, nullptr,
-                                          cond_in);
+            cgs_pass<2, T><<<G, kT, 0, s2>>>(n, m->state, H.V, vn, h1, m->partial, m->counter, nr, h1, nullptr,
+                                             cond_in);
           }
-          scale_next<<<Gs, kT, 0, s2>>>(n, m->state, m->V, vn, vin);
+          scale_next<T><<<Gs, kT, 0, s2>>>(n, m->state, H.V, vn, vin);
           ok(cudaGetLastError());
         }
         if (cap2) {
@@ -1221,8 +1289,8 @@ static int capture_solve(apc_context *c, const IrSolveArgs &a) {
           ok(cudaStreamEndCapture(s2, &g2));
         }
         fg_finish<<<1, 32, 0, s1>>>(m->state);
-        combine<<<Gs, kT, 0, s1>>>(n, a.mg ? m->Z : m->V, vn, m->state, m->dvec);
-        ir_axpy<<<Gs, kT, 0, s1>>>(n, m->state, m->dvec, a.x);
+        combine<T><<<Gs, kT, 0, s1>>>(n, a.mg ? H.Z : H.V, vn, m->state, H.dvec);
+        ir_axpy<T><<<Gs, kT, 0, s1>>>(n, m->state, H.dvec, a.x);
         ir_residual<<<G, kT, 0, s1>>>(n, a.w, a.ld, a.col, a.val, a.b, a.x, a.r, m->state, m->partial, m->counter,
                                       tmp, cond_out);
         ok(cudaGetLastError());
@@ -1268,20 +1336,22 @@ static int capture_solve(apc_context *c, const IrSolveArgs &a) {
 // system.  For the potential with the multigrid option, builds the hierarchy over the
 // current operator and right-preconditions with its V-cycle.  The solve is captured as
 // one graph and run; the host reads the outcome once.
-int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, const float *valf, const double *b,
-                 double *x, double *r, int restart, double rtol_in, int *its, double *rnorm, int *reason,
-                 int *refinements, int *levels, int (*during)(apc_context *)) {
+template <class T>
+static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, const T *valf, const double *b,
+                    double *x, double *r, int restart, double rtol_in, int *its, double *rnorm, int *reason,
+                    int *refinements, int *levels, int (*during)(apc_context *)) {
   MgWork *m = mg(c);
+  MgHier<T> &H = hier<T>(m);
   const int n = c->nc + c->nv;
   const size_t vn = ((size_t)n + 31) & ~(size_t)31;
   const int M = std::max(1, std::min(restart, kMaxM));
-  APC_TRY(apc_ensure(c, &m->V, vn * (M + 1)));
+  APC_TRY(apc_ensure(c, &H.V, vn * (M + 1)));
   if (use_mg) {
-    APC_TRY(apc_ensure(c, &m->Z, vn * M));
-    APC_TRY(apc_ensure(c, &m->vin, vn));
-    APC_TRY(apc_ensure(c, &m->vout, vn));
+    APC_TRY(apc_ensure(c, &H.Z, vn * M));
+    APC_TRY(apc_ensure(c, &H.vin, vn));
+    APC_TRY(apc_ensure(c, &H.vout, vn));
   }
-  APC_TRY(apc_ensure(c, &m->dvec, vn));
+  APC_TRY(apc_ensure(c, &H.dvec, vn));
   APC_TRY(apc_ensure(c, &m->partial, (size_t)kRedBlocks * 34));
   APC_TRY(apc_ensure(c, &m->dots, (size_t)4 * 34));
   m->vn = vn;
@@ -1299,9 +1369,9 @@ int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, cons
   m->prebuilt = false;
   if (use_mg && !prebuilt) {
     APC_CUDA_TRY(c, apc_stream_wait(c));
-    APC_TRY(mg_build(c));
+    APC_TRY(mg_build<T>(c));
   }
-  IrSolveArgs a{};
+  IrSolveArgs<T> a{};
   a.which = which;
   a.mg = use_mg;
   a.n = n;
@@ -1318,9 +1388,10 @@ int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, cons
   a.dtol = cfg.gmres_dtol;
   a.rtol_in = rtol_in;
   a.max_it = cfg.gmres_max_it;
-  // the multigrid corrections gain ~5 digits each; without a preconditioner a correction
-  // may gain little, and max_it bounds the loop
-  a.max_outer = use_mg ? 40 : std::max(40, cfg.gmres_max_it);
+  // the FP32 multigrid corrections gain ~5 digits each; an FP64 correction is one
+  // restart cycle of FGMRES; without a preconditioner a correction may gain little.  max_it
+  // bounds the loop in every case
+  a.max_outer = use_mg && sizeof(T) == sizeof(float) ? 40 : std::max(40, cfg.gmres_max_it);
   a.M = M;
   APC_TRY(capture_solve(c, a));
   if (use_mg)
@@ -1339,7 +1410,7 @@ int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, cons
   *rnorm = S.rn;
   *reason = S.reason;
   *refinements = S.outer;
-  *levels = use_mg ? m->nlev : 0;
+  *levels = use_mg ? H.nlev : 0;
   const int per_it = (int)m->vcycle_nodes[which] + 3 + (cfg.mg_reorth != 0 ? 1 : 0);
   apc_count_launch(c, 3 + 6 * S.outer + per_it * S.total_its);
   if (use_mg) {
@@ -1347,6 +1418,16 @@ int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, cons
     c->prof.mg_iterations += S.total_its;
   }
   return APC_OK;
+}
+
+int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, const double *b, double *x, double *r,
+                 int restart, double rtol_in, int *its, double *rnorm, int *reason, int *refinements, int *levels,
+                 int (*during)(apc_context *)) {
+  if (c->cfg.precision == APC_PREC_FP64_MULTIGRID)
+    return ir_solve<double>(c, which, use_mg, val, which == 0 ? c->a1d : c->a2d, b, x, r, restart, rtol_in, its,
+                            rnorm, reason, refinements, levels, during);
+  return ir_solve<float>(c, which, use_mg, val, which == 0 ? c->a1f : c->a2f, b, x, r, restart, rtol_in, its, rnorm,
+                         reason, refinements, levels, during);
 }
 
 int apc_mg_mark_assembled(apc_context *c) {
@@ -1372,8 +1453,8 @@ int apc_mg_prebuild(apc_context *c) {
   cudaStream_t main = c->s;
   APC_CUDA_TRY(c, cudaStreamWaitEvent(m->side, m->side_ev[0], 0));
   c->s = m->side;
-  apc_potential_to_f32(c, c->s);
-  int rc = mg_build(c);
+  apc_potential_scaled(c, c->s);
+  int rc = c->cfg.precision == APC_PREC_FP64_MULTIGRID ? mg_build<double>(c) : mg_build<float>(c);
   if (rc == APC_OK && cudaEventRecord(m->side_ev[1], c->s) != cudaSuccess) rc = APC_ERR_CUDA;
   c->s = main;
   APC_TRY(rc);

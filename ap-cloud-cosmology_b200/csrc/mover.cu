@@ -111,6 +111,58 @@ __global__ void __launch_bounds__(256) drift(int n, double *__restrict__ x, doub
   if (threadIdx.x == 0) atomic_max_nonneg(maxbits, mx);
 }
 
+// Kick then drift in one pass (apc_step): the same operations as `kick` followed by
+// `drift`, so the results are bit-identical, with x and v read once and written once.
+__global__ void __launch_bounds__(256) kick_drift(int n, int m, const int *__restrict__ cell_of,
+                                                  const double *__restrict__ deriv, const double *__restrict__ cx,
+                                                  const double *__restrict__ cy, const double *__restrict__ cz,
+                                                  double *__restrict__ x, double *__restrict__ y,
+                                                  double *__restrict__ z, double *__restrict__ vx,
+                                                  double *__restrict__ vy, double *__restrict__ vz,
+                                                  double *__restrict__ ax, double *__restrict__ ay,
+                                                  double *__restrict__ az, double cv, double cp, double dt,
+                                                  double x0, double x1, double y0, double y1, double z0, double z1,
+                                                  int bc, unsigned long long *maxbits_v,
+                                                  unsigned long long *maxbits_x, int *err) {
+  double mv = 0.0, mxx = 0.0;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const int i = cell_of[s];
+    if (i < 0 || i >= m) {
+      atomicOr(err, DERR_NEIGH);
+      continue;
+    }
+    const double *d = deriv + (size_t)i * 9;
+    const double px = x[s], py = y[s], pz = z[s];
+    const double dx = __dsub_rn(px, cx[i]), dy = __dsub_rn(py, cy[i]), dz = __dsub_rn(pz, cz[i]);
+    const double a1 = __dadd_rn(__dadd_rn(__dadd_rn(d[0], __dmul_rn(dx, d[3])), __dmul_rn(dy, d[6])), __dmul_rn(dz, d[7]));
+    const double a2 = __dadd_rn(__dadd_rn(__dadd_rn(d[1], __dmul_rn(dx, d[6])), __dmul_rn(dy, d[4])), __dmul_rn(dz, d[8]));
+    const double a3 = __dadd_rn(__dadd_rn(__dadd_rn(d[2], __dmul_rn(dx, d[7])), __dmul_rn(dy, d[8])), __dmul_rn(dz, d[5]));
+    ax[s] = a1;
+    ay[s] = a2;
+    az[s] = a3;
+    const double u = __dadd_rn(vx[s], __dmul_rn(__dmul_rn(a1, cv), dt));
+    const double v = __dadd_rn(vy[s], __dmul_rn(__dmul_rn(a2, cv), dt));
+    const double w = __dadd_rn(vz[s], __dmul_rn(__dmul_rn(a3, cv), dt));
+    vx[s] = u;
+    vy[s] = v;
+    vz[s] = w;
+    const double sa = __dadd_rn(__dadd_rn(__dmul_rn(a1, a1), __dmul_rn(a2, a2)), __dmul_rn(a3, a3));
+    mv = fmax(mv, __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(sa, cv), cv), dt), dt));
+    x[s] = mwrap(__dadd_rn(px, __dmul_rn(__dmul_rn(u, cp), dt)), x0, x1, bc);
+    y[s] = mwrap(__dadd_rn(py, __dmul_rn(__dmul_rn(v, cp), dt)), y0, y1, bc);
+    z[s] = mwrap(__dadd_rn(pz, __dmul_rn(__dmul_rn(w, cp), dt)), z0, z1, bc);
+    const double sv = __dadd_rn(__dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v)), __dmul_rn(w, w));
+    mxx = fmax(mxx, __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(sv, cp), cp), dt), dt));
+  }
+  mv = block_max(mv);
+  __syncthreads();  // block_max's shared scratch is reused below
+  mxx = block_max(mxx);
+  if (threadIdx.x == 0) {
+    atomic_max_nonneg(maxbits_v, mv);
+    atomic_max_nonneg(maxbits_x, mxx);
+  }
+}
+
 // max over the cells of n_p / h / h / h, in the reference's operation order
 // (controller.cpp:150-156); values are non-negative, so atomicMax on the bits is exact
 __global__ void max_cell_density(int m, const int *__restrict__ count, const double *__restrict__ h,
@@ -191,5 +243,40 @@ int apc_mover_position(apc_context *c, double dt, double c_pos, double *max_dx) 
     memcpy(&v, hb, sizeof(v));
     *max_dx = std::sqrt(v);
   }
+  return APC_OK;
+}
+
+// Interpolation + kick + drift in one pass (apc_step); one readback for both maxima and
+// the error flag.
+int apc_mover_kick_drift(apc_context *c, double dt, double c_vel, double c_pos, double *max_dv, double *max_dx) {
+  const int n = c->n, M = c->nc + c->nv;
+  APC_TRY(apc_ensure(c, &c->cell_of, (size_t)n + 1, nullptr));
+  APC_CUDA_TRY(c, cudaMemsetAsync(c->cell_of, 0xff, sizeof(int) * (size_t)n, c->s));
+  APC_CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->s));
+  const int sms = apc_sm_count(c);
+  cell_of_particles<<<std::max(1, std::min((M + 7) / 8, sms * 16)), 256, 0, c->s>>>(M, c->cfirst, c->ccount,
+                                                                                   c->cell_of);
+  // counters + 96 .. + 99: the two maxima (8 bytes each)
+  unsigned long long *mb = (unsigned long long *)(c->counters + 96);
+  APC_CUDA_TRY(c, cudaMemsetAsync(mb, 0, 2 * sizeof(unsigned long long), c->s));
+  const int G = std::max(1, std::min((n + 255) / 256, sms * 8));
+  const double *b = c->cfg.box;
+  kick_drift<<<G, 256, 0, c->s>>>(n, M, c->cell_of, c->deriv, c->cx, c->cy, c->cz, c->px, c->py, c->pz, c->pvx,
+                                  c->pvy, c->pvz, c->pax, c->pay, c->paz, c_vel, c_pos, dt, b[0], b[1], b[2], b[3],
+                                  b[4], b[5], c->cfg.bc, mb, mb + 1, c->d_err);
+  apc_count_launch(c, 2);
+  APC_CUDA_TRY(c, cudaGetLastError());
+  unsigned long long *hb = (unsigned long long *)(c->h_pinned + 12);  // pinned, 8-byte aligned: 2 maxima
+  APC_CUDA_TRY(c, cudaMemcpyAsync(hb, mb, 2 * sizeof(*hb), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 16, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
+  if (c->h_pinned[16] & DERR_NEIGH) {
+    c->err = "a particle lies in no selected cell";
+    return APC_ERR_CUDA;
+  }
+  double v[2];
+  memcpy(v, hb, sizeof(v));
+  if (max_dv) *max_dv = std::sqrt(v[0]);
+  if (max_dx) *max_dx = std::sqrt(v[1]);
   return APC_OK;
 }

@@ -10,8 +10,12 @@ Workload (default): the 128^3 LambdaCDM Zel'dovich box.
   - GMRES(30), rtol 1e-10, max_it 10000.
 A step is one pass of the Controller sequence (select; solve; kick; drift) over the
 whole particle set.  The timed arm is the mixed-precision path: FP32 Krylov inside FP64
-iterative refinement, FP64 GFD moments and FP64 leapfrog.  The plain FP64 GPU path is
-timed beside it from the same state, and the force error between the two is reported.
+iterative refinement, FP64 GFD moments and FP64 leapfrog.  The plain FP64 GPU path (the
+same multigrid FGMRES solver with FP64 vectors and operators) is timed beside it from the
+same state.  Both arms' force errors are measured against one FP64 solve converged to
+rtol 1e-13, together with that of the reference-semantics FP64 GMRES(30)+Jacobi, which at
+this size stops at max_it.  `full_run` times the whole configured run (every step to
+a = 1) on a fresh context.
 
 Timing: W warm-up steps, then K steps.
   - Each step is timed on the device with the library's CUDA events, on its own stream.
@@ -48,7 +52,6 @@ from apcloud import ics  # noqa: E402
 METRIC = "particle-steps/s at 128^3: mixed-prec vs FP64 GPU path at equal force error"
 UNIT = "particle-steps/s"
 WORKLOAD = "lcdm128"
-REF_GMRES_SAMPLE_ITS = 200
 
 
 def workload_desc(cfg) -> str:
@@ -293,29 +296,37 @@ def run_ours(args) -> dict:
     state_parts = ics.Particles(*state[:6])
     t_state = ctl.t
 
-    # ---- force error of the two paths on the same state, against a solve converged
-    #      to 1e-13 (the FP64 GMRES(30)+Jacobi path stops at max_it at this size) ----
+    # ---- force error on the same state.  Arms: the mixed path (timed headline), the plain
+    #      FP64 GPU path (the same multigrid FGMRES solver with every vector and operator in
+    #      FP64), and the reference-semantics FP64 GMRES(30)+Jacobi, all to rtol 1e-10.  Each
+    #      is measured against one independent FP64 solve converged to rtol 1e-13 ----
+    arms = (("mixed", binding.APC_PREC_MIXED, cfg.rtol), ("fp64", binding.APC_PREC_FP64_MULTIGRID, cfg.rtol),
+            ("fp64_gmres", binding.APC_PREC_FP64, cfg.rtol), ("converged", binding.APC_PREC_FP64_MULTIGRID, 1e-13))
     acc = {}
-    for prec, name in ((binding.APC_PREC_FP64, "fp64"), (binding.APC_PREC_MIXED, "mixed"),
-                       (binding.APC_PREC_MIXED, "converged")):
-        g = make(prec, state_parts) if name != "converged" else binding.GpuPath(
-            state_parts, cfg.depth, cfg.gfd_c, cfg.lm, restart=cfg.restart, rtol=1e-13,
-            precision=prec, device=dev)
+    for name, prec, rtol in arms:
+        g = binding.GpuPath(state_parts, cfg.depth, cfg.gfd_c, cfg.lm, restart=cfg.restart, rtol=rtol,
+                            precision=prec, device=dev, mixed_restart=args.mixed_restart,
+                            mixed_inner_rtol=args.inner_rtol)
         c2 = for_config(g, cfg)
         c2.t = t_state
         k = c2.constants(c2.t, cfg.delta_a)
         g.select()
         g.solve(k["c_dens"], k["c_pot"], k["c_field"])
         g.move_velocity(cfg.delta_a, k["c_vel"])
-        acc[name] = (np.stack(g.particles()[6:9]), g.solve_stats())
+        acc[name] = (np.stack(g.particles()[6:9]), g.solve_stats(), g.fields().potential)
         g.close()
-    a64, amx, aref = acc["fp64"][0], acc["mixed"][0], acc["converged"][0]
 
     def rms(a, b):
         return float(np.sqrt(np.mean(np.sum((a - b) ** 2, 0)) / np.mean(np.sum(b ** 2, 0))))
 
-    force_err = rms(amx, a64)
-    err_mixed, err_fp64 = rms(amx, aref), rms(a64, aref)
+    aref, pref = acc["converged"][0], acc["converged"][2]
+    force = {name: {"acc_rms_vs_converged": rms(acc[name][0], aref),
+                    "potential_rms_vs_converged": float(np.sqrt(np.mean((acc[name][2] - pref) ** 2) /
+                                                                np.mean(pref ** 2))),
+                    "potential_its": acc[name][1]["potential_its"],
+                    "potential_reason": acc[name][1]["potential_reason"],
+                    "potential_refinements": acc[name][1]["potential_refinements"]}
+             for name in ("mixed", "fp64", "fp64_gmres")}
 
     def timed(g, c):
         dist.barrier()
@@ -335,17 +346,51 @@ def run_ours(args) -> dict:
     step_ms = dist.max(prof["step_ms"])
     value = ws * cfg.n * args.steps / (step_ms / 1e3)
 
-    fp64_value = None
-    fp64_ms = None
+    # ---- the whole configured run: a fresh context from the initial state through every
+    #      step to a_end, each step timed on the device (no L2 flush: a real run) ----
+    full = None
+    if not args.no_full_run:
+        gf = make(binding.APC_PREC_MIXED, parts)
+        cf = for_config(gf, cfg)
+        dist.barrier()
+        t0 = time.perf_counter()
+        cf.start()
+        per = []
+        while not cf.done():
+            gf.reset_profile()
+            cf.step()
+            per.append(gf.profile()["step_ms"])
+        wall = time.perf_counter() - t0
+        gf.close()
+        dev_s = dist.max(sum(per) / 1e3)
+        wall = dist.max(wall)
+        q = len(per) // 4
+        full = {"steps": len(per), "a_end": round(cf.t, 6), "value": ws * cfg.n * len(per) / dev_s,
+                "unit": UNIT, "seconds_device": dev_s, "seconds_wall": wall,
+                "value_wall": ws * cfg.n * len(per) / wall,
+                "ms_first_quarter": statistics.mean(per[:q]), "ms_last_quarter": statistics.mean(per[-q:]),
+                "ms_max": max(per), "ms_min": min(per),
+                "timing": "device events per step (select to drift), summed; seconds_wall = host clock around "
+                          "the whole run incl. the initial select + half drift"}
+
+    # ---- the plain FP64 GPU path from the same state, timed the same way ----
+    fp64 = None
     if not args.no_fp64:
-        g64 = make(binding.APC_PREC_FP64, state_parts)
+        g64 = make(binding.APC_PREC_FP64_MULTIGRID, state_parts)
         c64 = for_config(g64, cfg)
         c64.t = t_state
-        p64, _, _ = timed(g64, c64)
+        p64, l64, clk64 = timed(g64, c64)
         fp64_ms = dist.max(p64["step_ms"])
-        fp64_value = ws * cfg.n * args.steps / (fp64_ms / 1e3)
-        fp64_stats = g64.solve_stats()
+        st64 = g64.solve_stats()
         g64.close()
+        fv = ws * cfg.n * args.steps / (fp64_ms / 1e3)
+        fp64 = {"value": fv, "ms_per_step": fp64_ms / args.steps, "speedup_mixed_over_fp64": value / fv,
+                "solver": "FP64 multigrid FGMRES (APC_PREC_FP64_MULTIGRID): the mixed path's solver with FP64 "
+                          "vectors and operators, restarted from the true FP64 residual, rtol 1e-10",
+                "phases_ms_per_step": {k2: p64[k2 + "_ms"] / args.steps for k2 in
+                                       ("select", "solve", "assemble", "gfd", "density", "potential", "move")},
+                "potential_iterations_per_step": p64["mg_iterations"] / args.steps,
+                "potential_reason": st64["potential_reason"], "gpu_launches": l64, "clocks": clk64}
 
     # ---- end to end through the public API with host buffers ----
     e2e = None
@@ -392,20 +437,17 @@ def run_ours(args) -> dict:
         "dtype": "f32 Krylov / f64 refinement, GFD moments and leapfrog", "data": "synthetic",
         "config": {"workload": workload_desc(cfg), "precision": "mixed", "parallelism": f"replicas x{ws}",
                    "l2": "flushed (512 MiB write) before every timed step",
-                   "start_a": round(t_state, 6), "mixed_restart": args.mixed_restart or 16,
+                   "start_a": round(t_state, 6),
+                   "timed_steps": f"steps {args.warmup + 1}-{args.warmup + args.steps} of {cfg.steps} "
+                                  f"(a = {t_state:.4f} onwards); the whole run is in full_run",
+                   "mixed_restart": args.mixed_restart or 16,
                    "inner_rtol": args.inner_rtol or 1e-3},
-        "fp64": {"value": fp64_value, "ms_per_step": (fp64_ms / args.steps) if fp64_ms else None,
-                 "speedup_mixed_over_fp64": (value / fp64_value) if fp64_value else None,
-                 "potential_its": fp64_stats["potential_its"] if fp64_value else None,
-                 "potential_reason": fp64_stats["potential_reason"] if fp64_value else None},
-        "force_error": {"mixed_vs_converged": err_mixed, "fp64_vs_converged": err_fp64,
-                        "mixed_vs_fp64": force_err, "bound": 1e-6,
-                        "measure": "acceleration RMS relative error on the same state; 'converged' = potential "
-                                   "solved to rtol 1e-13",
-                        "fp64_potential_reason": acc["fp64"][1]["potential_reason"],
-                        "fp64_potential_its": acc["fp64"][1]["potential_its"],
-                        "mixed_potential_reason": acc["mixed"][1]["potential_reason"],
-                        "mixed_potential_its": acc["mixed"][1]["potential_its"]},
+        "fp64": fp64,
+        "force_error": dict(force, bound=1e-6,
+                            measure="RMS relative error of the accelerations (and potentials) of one step on the "
+                                    "same state, against an FP64 multigrid solve converged to rtol 1e-13",
+                            equal_force_error=bool(force["mixed"]["acc_rms_vs_converged"] <= 1e-6 and
+                                                   force["fp64"]["acc_rms_vs_converged"] <= 1e-6)),
         "phases_ms_per_step": {k: prof[k + "_ms"] / args.steps for k in
                                ("select", "solve", "assemble", "gfd", "density", "potential", "mg_build",
                                 "mg_solve", "move")},
@@ -425,6 +467,7 @@ def run_ours(args) -> dict:
                              "kernels"},
         "step_roofline": {"algorithmic_bytes": step_bytes, "achieved_gbs": step_bytes / (step_ms / args.steps / 1e3) / 1e9,
                           "frac": step_bytes / (step_ms / args.steps / 1e3) / 1e9 / peak},
+        "full_run": full,
         "gpu_launches": launches,
         "clocks": clocks,
         "e2e": e2e,
@@ -491,47 +534,68 @@ def run_batch(args) -> dict | None:
 
 # ------------------------------------------------------------- CPU reference
 
-def reference_sample(cfg, parts_state, t, fp64_its: int | None, args):
-    """One bounded sample of a step through the reference's own code (oracle/_ref).
-    Select, GFD assembly, differentiation and mover run in full.  The potential GMRES
-    is timed for REF_GMRES_SAMPLE_ITS iterations and its time scaled per iteration to
-    the full step's iteration count: the FP64 path's count when known, else max_it,
-    which the reference reaches at this size.  GMRES(30) iterations cost the same
-    throughout a solve, so the scaling is linear."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import refbind  # test infrastructure: only the CPU baseline leg loads it
+# The reference's own run lines cap GMRES at 1000 iterations (-ksp_max_it 1000,
+# Makefile:30-32).  At 128^3 GMRES(30)+Jacobi reaches neither 1000 nor 10000 iterations'
+# worth of rtol 1e-10, and a 10000-iteration step (~20-110 s on the host) cannot be
+# repeated K + W times within minutes, so the CPU arms run the reference's production cap.
+REF_MAX_IT = 1000
 
-    r = refbind.CpuPath("ref", parts_state, cfg.depth, cfg.gfd_c, cfg.lm)
-    r.set_gmres(cfg.restart, cfg.rtol, 1e-50, 1e5, REF_GMRES_SAMPLE_ITS)
-    r.reset_solve_stats()
-    t0 = time.perf_counter()
-    r.select()
-    t1 = time.perf_counter()
-    k = dict(c_dens=1.0 / cfg.n, c_pot=1.5 * cfg.omega0 / t)
-    r.solve(k["c_dens"], k["c_pot"], -1.0)
-    t2 = time.perf_counter()
-    r.move_velocity(cfg.delta_a, ics.kick_factor(t, cfg.omega0, cfg.omegal))
-    r.move_position(cfg.delta_a, ics.drift_factor(t + cfg.delta_a / 2, cfg.omega0, cfg.omegal))
-    t3 = time.perf_counter()
-    st = r.solve_stats()
-    r.close()
-    its_s, sec_s = st[-1][0], st[-1][3]
-    full_its = fp64_its if fp64_its else 10000
-    per_it = sec_s / max(its_s, 1)
-    est = (t1 - t0) + (t2 - t1 - sec_s) + per_it * full_its + (t3 - t2)
-    return est, (t3 - t0), its_s, full_its, per_it
+
+def reference_threads() -> int:
+    """All the host cores this process may use (OpenMP regions of the reference and the
+    GMRES shim, which spreads its loops as PETSc spreads them over MPI ranks)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+class ReferenceRun:
+    """The reference's own code (oracle/_ref: octree.cpp, mover.cpp, particle.cpp,
+    solver.cpp) driven through the Controller step sequence from the workload's initial
+    state: select + half drift, then whole steps (select; solve; kick; drift), each timed
+    in full on the host clock."""
+
+    def __init__(self, cfg, threads: int):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import refbind  # test infrastructure: only the CPU arms of the bench load it
+
+        from apcloud.controller import for_config
+
+        self.r = refbind.CpuPath("ref", cfg.particles(), cfg.depth, cfg.gfd_c, cfg.lm)
+        self.r.set_gmres(cfg.restart, cfg.rtol, 1e-50, 1e5, REF_MAX_IT)
+        self.r.set_threads(threads)
+        self.ctl = for_config(self.r, cfg)
+        self.ctl.start()
+
+    def step(self) -> tuple[float, list]:
+        self.r.reset_solve_stats()
+        t0 = time.perf_counter()
+        self.ctl.step()
+        dt = time.perf_counter() - t0
+        return dt, [(s[0], s[2]) for s in self.r.solve_stats()]
+
+    def close(self):
+        self.r.close()
+
+
+def ref_sample_text(cfg, threads: int, k: int, first_step: int, its) -> str:
+    return (f"{k} whole 128^3 step(s) of the reference code (oracle/_ref), steps {first_step}-{first_step + k - 1} "
+            f"of the run from its initial state: select, GFD assembly, density and potential GMRES({cfg.restart}) "
+            f"rtol {cfg.rtol} capped at {REF_MAX_IT} iterations as in the reference's run lines (Makefile:30-32), "
+            f"differentiation, kick, drift; each timed in full (no scaling); OpenMP regions and the GMRES loops on "
+            f"{threads} host threads, selection and assembly serial as in the reference; (its, reason) of the "
+            f"last step's solves {its}")
 
 
 def cpu_baseline(cfg, args) -> dict:
-    parts = cfg.particles()
-    t = cfg.a_start + 0.5 * cfg.delta_a
-    est, measured, its_s, full_its, per_it = reference_sample(cfg, parts, t, None, args)
-    return {"value": cfg.n / est, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-            "sample": (f"one 128^3 step through the reference code (oracle/_ref): select, GFD assembly, "
-                       f"differentiation and mover timed in full; potential GMRES timed for {its_s} iterations "
-                       f"({per_it * 1e3:.1f} ms each) and scaled to {full_its} iterations; {measured:.1f} s measured, "
-                       f"{est:.1f} s per step estimated; OpenMP regions on all cores, GMRES on one"),
-            "seconds_per_step": est}
+    """The reference on the host, bounded: the first whole step of the run."""
+    th = reference_threads()
+    rr = ReferenceRun(cfg, th)
+    sec, its = rr.step()
+    rr.close()
+    return {"value": cfg.n / sec, "unit": UNIT, "cores": th, "kind": "reference",
+            "sample": ref_sample_text(cfg, th, 1, 1, its), "seconds_per_step": sec}
 
 
 def run_reference(args) -> dict | None:
@@ -542,27 +606,28 @@ def run_reference(args) -> dict | None:
     ref_so = os.path.join(ROOT, "oracle", "_ref", "libapcref.so")
     if not os.path.exists(ref_so):
         return {"impl": "reference", "unavailable": "oracle/_ref/libapcref.so not built (make -C oracle ref)"}
-    parts = cfg.particles()
-    t = cfg.a_start + 0.5 * cfg.delta_a
+    th = reference_threads()
+    rr = ReferenceRun(cfg, th)
     for _ in range(args.warmup):
-        reference_sample(cfg, parts, t, None, args)
-    ests = []
-    meas = 0.0
+        rr.step()
+    secs = []
+    its = None
     for _ in range(args.steps):
-        est, measured, its_s, full_its, per_it = reference_sample(cfg, parts, t, None, args)
-        ests.append(est)
-        meas += measured
-    total = sum(ests)
+        sec, its = rr.step()
+        secs.append(sec)
+    rr.close()
+    total = sum(secs)
     value = cfg.n * args.steps / total
+    sample = ref_sample_text(cfg, th, args.steps, args.warmup + 1, its)
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_desc(cfg), "precision": "fp64 (reference CPU path)"},
+            "config": {"workload": workload_desc(cfg), "precision": "fp64 (reference CPU path)",
+                       "gmres_max_it": REF_MAX_IT, "timed_steps": f"{args.warmup + 1}-{args.warmup + args.steps}",
+                       "timing": "host clock around each whole step"},
             "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                             "sample": (f"each step: one 128^3 step of the reference code with the potential "
-                                        f"GMRES timed for {REF_GMRES_SAMPLE_ITS} iterations and scaled to "
-                                        f"{full_its}; {meas:.1f} s measured in total")},
+            "seconds_per_step": [round(x, 3) for x in secs],
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": th, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -578,6 +643,7 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-full-run", action="store_true")
     ap.add_argument("--batch-workers", type=int, default=0, help="host worker threads per rank (batch96)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -57,8 +57,12 @@ typedef enum apc_status {
 } apc_status;
 
 typedef enum apc_precision {
-  APC_PREC_FP64 = 0,  /* FP64 GMRES with the reference's semantics (the plain FP64 path) */
-  APC_PREC_MIXED = 1  /* FP32 SpMV/Krylov inside an FP64 iterative-refinement loop */
+  APC_PREC_FP64 = 0,  /* FP64 GMRES with the reference's semantics: GMRES(restart) + Jacobi */
+  APC_PREC_MIXED = 1, /* FP32 SpMV/Krylov inside an FP64 iterative-refinement loop */
+  APC_PREC_FP64_MULTIGRID = 2 /* the mixed path's solver with every vector and operator in FP64:
+                                 restarted (F)GMRES on the Jacobi-scaled systems, the potential
+                                 right-preconditioned by the same octree multigrid, each cycle
+                                 restarted from the true FP64 residual; same stopping test */
 } apc_precision;
 
 typedef struct apc_config {
@@ -77,11 +81,12 @@ typedef struct apc_config {
   double gmres_dtol;     /* -ksp_divtol */
   int gmres_max_it;      /* -ksp_max_it */
   int precision;         /* apc_precision */
-  int mixed_restart;     /* FP32 inner restart of both APC_PREC_MIXED solves (0 = 16 for the multigrid
-                            potential solve, 30 for the others), at most 31 */
+  int mixed_restart;     /* inner restart of both APC_PREC_MIXED / APC_PREC_FP64_MULTIGRID solves (0 = 16
+                            for the multigrid potential solve, 30 for the others), at most 31 */
   double mixed_inner_rtol; /* FP32 inner solve relative tolerance (0 = 1e-3 with multigrid, 1e-5 without) */
   int device;            /* CUDA device ordinal */
-  int mixed_precond;     /* APC_PREC_MIXED potential solve: APC_PRECOND_JACOBI or APC_PRECOND_MULTIGRID */
+  int mixed_precond;     /* APC_PREC_MIXED / APC_PREC_FP64_MULTIGRID potential solve: APC_PRECOND_JACOBI
+                            or APC_PRECOND_MULTIGRID */
   int mg_sweeps;         /* multigrid: Jacobi sweeps before and after each coarse correction (0 = 2) */
   double mg_omega;       /* multigrid: Jacobi damping (0 = 0.95) */
   double mg_alpha;       /* multigrid: coarse-correction over-scaling (0 = 1.8) */
@@ -143,7 +148,9 @@ int apc_move_velocity(apc_context *ctx, double dt, double c_vel, double *max_dv)
 int apc_move_position(apc_context *ctx, double dt, double c_pos, double *max_dx);
 
 /* One whole step {select; solve; move_velocity; move_position} with the constants of
- * controller.cpp:182-186 for time t and step dt.  Outputs may be NULL. */
+ * controller.cpp:182-186 for time t and step dt.  The interpolation, kick and drift run
+ * as one fused pass over the particles, bit-identical to apc_move_velocity followed by
+ * apc_move_position.  Outputs may be NULL. */
 typedef struct apc_step_params {
   double dt, c_dens, c_pot, c_field, c_vel, c_pos;
 } apc_step_params;

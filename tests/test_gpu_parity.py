@@ -225,6 +225,17 @@ def test_mixed_precision_equal_force_error(gpu_lib, path):
     assert _acc_rms(pmx[6:9], p64[6:9]) <= MIXED_ACC_RMS
     assert _rel(fmx.potential, f64.potential) <= 1e-7
     assert smx["potential_reason"] == 2 and smx["potential_refinements"] >= 1
+    # the FP64 multigrid path (the mixed path's solver in FP64 throughout) meets the same
+    # rtol 1e-10 as the FP64 GMRES; two such solutions differ by up to cond(A) 1e-10
+    gp = _gpu(_parts(g), g, precision=binding.APC_PREC_FP64_MULTIGRID)
+    gp.select()
+    gp.solve(float(g["c_dens"]), float(g["c_pot"]), -1.0)
+    gp.move_velocity(float(g["delta_a"]), float(g["c_vel"]))
+    pmg, fmg, smg = gp.particles(), gp.fields(), gp.solve_stats()
+    gp.close()
+    assert smg["potential_reason"] == 2 and smg["density_reason"] == 2 and smg["mg_levels"] >= 2
+    assert _acc_rms(pmg[6:9], p64[6:9]) <= 1e-7
+    assert _rel(fmg.potential, f64.potential) <= 1e-7
 
 
 def test_phase_order_and_invalid_input_errors(gpu_lib):
@@ -329,3 +340,24 @@ def test_adaptive_time_step_vs_oracle(gpu_lib, oracle_lib):
         assert np.max(np.abs(d)) <= 1e-11
     o.close()
     gp.close()
+
+
+def test_fused_step_equals_phase_calls(gpu_lib):
+    """apc_step runs the interpolation, kick and drift as one fused pass; it must give
+    the particles, accelerations and maxima of apc_move_velocity + apc_move_position bit
+    for bit, step after step."""
+    cfg = ics.config("ball32k", n=6000, seed=77, steps=20)
+    p = cfg.particles()
+    runs = []
+    for fused in (False, True):
+        gp = binding.GpuPath(p, cfg.depth, cfg.gfd_c)
+        ctl = for_config(gp, cfg)
+        ctl.fused = fused
+        ctl.start()
+        recs = [ctl.step() for _ in range(3)]
+        runs.append(([(r.n_cells, r.max_dv, r.max_dx) for r in recs], gp.particles()))
+        gp.close()
+    (ra, pa), (rb, pb) = runs
+    assert ra == rb
+    for a, b in zip(pa, pb):
+        assert np.array_equal(a, b)

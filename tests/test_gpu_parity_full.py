@@ -7,6 +7,7 @@ runs beside the CUDA path on the same particle sets:
   * eds64   - the 64^3 EdS Zel'dovich box: the first step;
   * lcdm128 - the 128^3 LambdaCDM Zel'dovich box: the first step, and a late state
               (the particles after 100 steps of a GPU run, 8 octree levels deep).
+Both multigrid paths (mixed precision, and FP64 throughout) are checked at 128^3.
 
 Bars:
   * bit-exact - Morton keys (index sets per key, std::sort is not stable), octree level
@@ -241,15 +242,19 @@ def _lcdm128_state_vs_reference(cfg, parts, t):
     ref = _ref(cfg, parts, max_it=30, threads=THREADS)
     m_ref = ref.select()
     ref.solve(k["c_dens"], k["c_pot"], k["c_field"])
-    gm = _gpu(cfg, parts, binding.APC_PREC_MIXED)
-    cells = _assert_selection_equal(gm, ref, gm.select(), m_ref)
-    gm.solve(k["c_dens"], k["c_pot"], k["c_field"])
-    st = gm.solve_stats()
-    assert st["density_reason"] == 2 and st["potential_reason"] == 2
-    report = {"cells": m_ref, "levels": int(np.max(np.round(np.log2(1.0 / cells.h))))}
-    report["matrix_err"] = _assert_assembly_equal(gm, ref)
-    report["residuals"] = _residuals_vs_reference_matrices(gm, ref, cells, k["c_dens"], k["c_pot"])
-    gm.close()
+    report = {}
+    for name, prec in (("mixed", binding.APC_PREC_MIXED), ("fp64_multigrid", binding.APC_PREC_FP64_MULTIGRID)):
+        gm = _gpu(cfg, parts, prec)
+        cells = _assert_selection_equal(gm, ref, gm.select(), m_ref)
+        gm.solve(k["c_dens"], k["c_pot"], k["c_field"])
+        st = gm.solve_stats()
+        assert st["density_reason"] == 2 and st["potential_reason"] == 2, (name, st)
+        if name == "mixed":
+            report.update(cells=m_ref, levels=int(np.max(np.round(np.log2(1.0 / cells.h)))))
+            report["matrix_err"] = _assert_assembly_equal(gm, ref)
+        report[name + "_residuals"] = _residuals_vs_reference_matrices(gm, ref, cells, k["c_dens"], k["c_pot"])
+        report[name + "_potential_its"] = st["potential_its"]
+        gm.close()
     ref.close()
     return report
 
