@@ -97,6 +97,7 @@ extern "C" int petsc_shim_last_matrix_log(int which, int *n, int *len, const int
 int MPI_Comm_rank(MPI_Comm, int *rank) { *rank = 0; return 0; }
 int MPI_Comm_size(MPI_Comm, int *size) { *size = 1; return 0; }
 int MPI_Barrier(MPI_Comm) { return 0; }
+int MPI_Bcast(void *, int, MPI_Datatype, int, MPI_Comm) { return 0; }
 
 PetscErrorCode VecCreate(MPI_Comm, Vec *v) { *v = new _p_Vec(); return 0; }
 PetscErrorCode VecSetSizes(Vec v, PetscInt, PetscInt N) { v->a.assign(N, 0.0); return 0; }

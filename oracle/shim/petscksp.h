@@ -18,6 +18,7 @@ typedef int PetscErrorCode;
 typedef int PetscInt;
 typedef double PetscScalar;
 typedef int MPI_Comm;
+typedef int MPI_Datatype;
 typedef int InsertMode;
 typedef int ScatterMode;
 typedef int MatAssemblyType;
@@ -26,6 +27,8 @@ typedef const char *PCType;
 
 #define PETSC_COMM_WORLD 0
 #define MPI_COMM_WORLD 0
+#define MPI_INT 1
+#define MPI_DOUBLE 2
 #define PETSC_DECIDE (-1)
 #define PETSC_TRUE 1
 #define PETSC_FALSE 0
@@ -50,6 +53,7 @@ typedef _p_VecScatter *VecScatter;
 int MPI_Comm_rank(MPI_Comm, int *rank);
 int MPI_Comm_size(MPI_Comm, int *size);
 int MPI_Barrier(MPI_Comm);
+int MPI_Bcast(void *buf, int count, MPI_Datatype type, int root, MPI_Comm);
 
 PetscErrorCode VecCreate(MPI_Comm, Vec *);
 PetscErrorCode VecSetSizes(Vec, PetscInt n, PetscInt N);
