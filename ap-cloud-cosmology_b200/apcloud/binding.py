@@ -43,7 +43,7 @@ class ApcConfig(C.Structure):
         ("gmres_dtol", C.c_double), ("gmres_max_it", C.c_int), ("precision", C.c_int),
         ("mixed_restart", C.c_int), ("mixed_inner_rtol", C.c_double), ("device", C.c_int),
         ("mixed_precond", C.c_int), ("mg_sweeps", C.c_int), ("mg_omega", C.c_double), ("mg_alpha", C.c_double),
-        ("mg_reorth", C.c_int), ("warm_start", C.c_int),
+        ("mg_reorth", C.c_int), ("warm_start", C.c_int), ("mixed_solve_graphs", C.c_int),
     ]
 
 
@@ -191,7 +191,7 @@ def make_config(n: int, depth: int, gfd_c: float, lm: int = 17,
                 max_it: int = 10000, mixed_restart: int = 0, mixed_inner_rtol: float = 0.0,
                 device: int = 0, maxnc: int = 10000, nmax_cap: int = 0, precond: int = APC_PRECOND_MULTIGRID,
                 mg_sweeps: int = 0, mg_omega: float = 0.0, mg_alpha: float = 0.0, mg_reorth: int = 0,
-                warm_start: int = 0) -> "ApcConfig":
+                warm_start: int = 0, solve_graphs: int = 0) -> "ApcConfig":
     """An apc_config: the library defaults with the given fields set."""
     lib = load_library()
     cfg = ApcConfig()
@@ -220,6 +220,7 @@ def make_config(n: int, depth: int, gfd_c: float, lm: int = 17,
     cfg.mg_alpha = mg_alpha
     cfg.mg_reorth = mg_reorth
     cfg.warm_start = warm_start
+    cfg.mixed_solve_graphs = solve_graphs
     return cfg
 
 

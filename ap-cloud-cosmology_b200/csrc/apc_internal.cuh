@@ -226,6 +226,55 @@ int apc_radix_sort_u64(apc_context *c, uint64_t *keys, uint32_t *vals, uint64_t 
 // grid sizing: a multiple of the SM count
 int apc_sm_count(apc_context *c);
 
+// ------------------------------------------------------- grid barrier (persistent kernels)
+
+// Generation barrier of a cooperative (persistent) kernel, in device memory zeroed before
+// the launch.
+struct GridBar {
+  unsigned count;
+  unsigned gen;
+  int abort;
+  int pad;
+};
+
+#ifdef __CUDACC__
+constexpr long long kSpinLimit = 1ll << 24;  // ~1-2 s of __nanosleep(64)
+
+// bounded sense-free generation barrier; returns false when the grid must abort.  A block
+// that waits more than `limit` polls raises DERR_KRYLOV and the abort flag, which every
+// other waiting block sees at its next poll
+__device__ __forceinline__ bool grid_sync(GridBar *bar, unsigned nblocks, int *err, long long limit = kSpinLimit) {
+  __syncthreads();
+  __shared__ int s_abort;
+  if (threadIdx.x == 0) {
+    volatile unsigned *vgen = &bar->gen;
+    volatile int *vab = &bar->abort;
+    const unsigned g = *vgen;
+    __threadfence();
+    const unsigned a = atomicAdd(&bar->count, 1u);
+    if (a == nblocks - 1) {
+      atomicExch(&bar->count, 0u);
+      __threadfence();
+      atomicAdd(&bar->gen, 1u);
+    } else {
+      long long spins = 0;
+      while (*vgen == g && !*vab) {
+        if (++spins > limit) {
+          atomicOr(err, DERR_KRYLOV);
+          atomicExch(&bar->abort, 1);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_abort = *vab;
+  }
+  __syncthreads();
+  return s_abort == 0;
+}
+#endif
+
 // ------------------------------------------------------- device helpers
 
 #ifdef __CUDACC__

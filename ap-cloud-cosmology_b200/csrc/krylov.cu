@@ -40,14 +40,7 @@ constexpr int kMaxBlocks = 256;             // partial sums are laid out [slot][
 constexpr int kMaxRestart = 255;            // basis vectors of the large instantiation, minus one
 constexpr int kSlots = kMaxRestart + 2;     // slots per partial-sum buffer: the dots, and one norm
 constexpr int kNormSlot = kSlots - 1;
-constexpr long long kSpinLimit = 1ll << 24;  // ~1-2 s of __nanosleep(64)
 
-struct GridBar {
-  unsigned count;
-  unsigned gen;
-  int abort;
-  int pad;
-};
 
 enum {
   KSP_CONVERGED_RTOL = 2,
@@ -58,40 +51,6 @@ enum {
   KSP_DIVERGED_BREAKDOWN = -5,
   KSP_DIVERGED_NANORINF = -9,
 };
-
-// bounded sense-free generation barrier; returns false when the grid must abort.  A block
-// that waits more than `limit` polls raises DERR_KRYLOV and the abort flag, which every
-// other waiting block sees at its next poll
-__device__ __forceinline__ bool grid_sync(GridBar *bar, unsigned nblocks, int *err, long long limit = kSpinLimit) {
-  __syncthreads();
-  __shared__ int s_abort;
-  if (threadIdx.x == 0) {
-    volatile unsigned *vgen = &bar->gen;
-    volatile int *vab = &bar->abort;
-    const unsigned g = *vgen;
-    __threadfence();
-    const unsigned a = atomicAdd(&bar->count, 1u);
-    if (a == nblocks - 1) {
-      atomicExch(&bar->count, 0u);
-      __threadfence();
-      atomicAdd(&bar->gen, 1u);
-    } else {
-      long long spins = 0;
-      while (*vgen == g && !*vab) {
-        if (++spins > limit) {
-          atomicOr(err, DERR_KRYLOV);
-          atomicExch(&bar->abort, 1);
-          break;
-        }
-        __nanosleep(64);
-      }
-    }
-    __threadfence();
-    s_abort = *vab;
-  }
-  __syncthreads();
-  return s_abort == 0;
-}
 
 template <class T>
 struct GmresArgs {

@@ -724,8 +724,10 @@ __device__ __forceinline__ void tail_sweep(const TailLevel<V> &L, const V *xin, 
   __syncthreads();
 }
 
+// The tail's levels in one block (every thread of the block takes part; the block
+// barriers separate the phases).
 template <class V>
-__global__ void __launch_bounds__(1024) vcycle_tail(TailArgs<V> A) {
+__device__ __forceinline__ void tail_body(const TailArgs<V> &A) {
   V *cur[kTailLevels];
   for (int l = 0; l < A.nl - 1; ++l) {
     const TailLevel<V> &L = A.L[l];
@@ -774,6 +776,492 @@ __global__ void __launch_bounds__(1024) vcycle_tail(TailArgs<V> A) {
       __syncthreads();
     }
     cur[l] = L.x;
+  }
+}
+
+
+template <class V>
+__global__ void __launch_bounds__(1024) vcycle_tail(TailArgs<V> A) {
+  tail_body(A);
+}
+// ---------------------------------------------- the whole solve as one persistent kernel
+//
+// One cooperative launch runs a complete solve: the FP64 refinement loop, each
+// correction's (F)GMRES cycle and, for the potential, the V-cycle of every iteration.
+// The phases are separated by the bounded grid barrier instead of kernel launches: per
+// iteration 4 barriers per grid level of the V-cycle plus one after the single-block
+// tail, one after the SpMV + dot products and one after the Gram-Schmidt update.
+//   * Reductions are deterministic: each block publishes its partial sums, and after the
+//     barrier every block adds all partials in block order, so every block holds the
+//     same Hessenberg column, Givens rotations and stopping decisions without another
+//     barrier, and takes the same branches.
+//   * Krylov vectors are kept un-normalised with a per-vector scale in shared memory, so
+//     normalisation costs no pass.
+//   * The V-cycle's residual and restriction are one phase: each coarse row sums its
+//     members' residuals directly.
+//   * Levels of <= kTail nodes run in block 0 (the same code as the graph path's tail
+//     kernel) while the other blocks wait at the next barrier.
+constexpr int kPT = 1024;         // threads per block, one block per SM
+constexpr int kPMaxBlocks = 256;  // partial sums are laid out [slot][block]
+constexpr int kPSlots = kMaxM + 2;
+
+template <class T>
+struct PLevel {
+  int n, w, g;                // rows, ELL width, lanes per row (power of two <= 8)
+  size_t ld;
+  const int *col;
+  const T *val, *dinv;
+  const int *agg;             // node -> next coarser node
+  const int *mptr, *mem;      // members (on the finer level) of this level's nodes
+  T *x, *x2, *b;
+};
+
+struct PResult {
+  int outer, total_its, reason, pad;
+  double rn;
+};
+
+template <class T>
+struct PSolveArgs {
+  int n, w;
+  size_t ld;
+  const int *col;
+  const T *valf;              // D^-1 A in the inner precision
+  const double *val, *b;      // FP64 operator (diagonal in slot 0) and rhs
+  double *x, *r;
+  T *V, *Z;                   // basis (M + 1 vectors), preconditioned vectors (M)
+  size_t vn;
+  int M, use_mg;
+  int nlev, tail;             // levels; first level of the single-block tail
+  PLevel<T> L[kMaxLevels];
+  TailArgs<T> ta;             // the tail levels (first = L[tail])
+  int sweeps;
+  T omega, alpha;
+  double rtol, atol, dtol, rtol_in;
+  int max_it, max_outer, exact_inner;
+  double *part;
+  GridBar *bar;
+  int *err;
+  PResult *out;
+};
+
+struct PShared {
+  double H[(kMaxM + 1) * kMaxM];  // column j at H[j * (M + 1)]
+  double cs[kMaxM], sn[kMaxM], g[kMaxM + 1], y[kMaxM], scale[kMaxM + 1], h[kPSlots];
+  double red[32];
+  double wdots[32][kPSlots];      // per-warp dot products of one Arnoldi step
+  double rn, rn0, ttol, bnorm, rtol_in, beta;
+  int outer, total_its, reason, it, inner_max, more;
+};
+
+__device__ __forceinline__ double p_block_sum(double v, double *red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (warp == 0) r = warp_sum(lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0);
+  return r;  // valid in warp 0
+}
+
+// all blocks: out[j] = sum over blocks of part[j][b], b in block order, for j < nv
+__device__ __forceinline__ void p_gather(const double *part, int nv, double *out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5, nb = gridDim.x;
+  for (int j = warp; j < nv; j += nw) {
+    double v = 0.0;
+#pragma unroll
+    for (int k = 0; k < kPMaxBlocks / 32; ++k) {
+      const int b = lane + 32 * k;
+      if (b < nb) v += __ldcg(part + (size_t)j * kPMaxBlocks + b);
+    }
+    v = warp_sum(v);
+    if (lane == 0) out[j] = v;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void p_put(double *part, int j, double v) {
+  if (threadIdx.x == 0) part[(size_t)j * kPMaxBlocks + blockIdx.x] = v;
+}
+
+template <class T>
+__device__ __forceinline__ T group_sum(T s, int G) {
+  for (int o = G >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+// f(i, sub, G, active) for every row of L, G lanes per row, over the whole grid; the trip
+// count is the same for every lane (the group sums shuffle)
+template <class T, class F>
+__device__ __forceinline__ void grid_rows(const PLevel<T> &L, F f) {
+  const int G = L.g;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int sub = (int)(tid & (G - 1));
+  const long long groups = ((long long)gridDim.x * blockDim.x) / G;
+  const long long rounds = (L.n + groups - 1) / groups;
+  for (long long rd = 0; rd < rounds; ++rd) {
+    const long long i = tid / G + rd * groups;
+    f((int)i, sub, G, i < L.n);
+  }
+}
+
+// two damped Jacobi sweeps from x = 0 in one pass: x1 = w D^-1 b, out = x1 + w D^-1 (b - A x1);
+// b = bs * bsrc
+template <class T>
+__device__ void p_first2(const PLevel<T> &L, const T *bsrc, T bs, T omega, T *out) {
+  grid_rows(L, [&](int i, int sub, int G, bool act) {
+    T s = T(0);
+    if (act)
+      for (int k = sub; k < L.w; k += G) {
+        const size_t at = (size_t)k * L.ld + i;
+        const int j = L.col[at];
+        s += L.val[at] * (omega * L.dinv[j] * (bs * bsrc[j]));
+      }
+    s = group_sum(s, G);
+    if (act && sub == 0) {
+      const T bi = bs * bsrc[i];
+      const T x1 = omega * L.dinv[i] * bi;
+      out[i] = x1 + omega * L.dinv[i] * (bi - s);
+    }
+  });
+}
+
+// x = w D^-1 b (one sweep from zero)
+template <class T>
+__device__ void p_first1(const PLevel<T> &L, const T *bsrc, T bs, T omega, T *out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n; i += gridDim.x * blockDim.x)
+    out[i] = omega * L.dinv[i] * (bs * bsrc[i]);
+}
+
+// out = y + w D^-1 (b - A y), y = xin (+ alpha xc[agg] when xc is given)
+template <class T>
+__device__ void p_sweep(const PLevel<T> &L, const T *bsrc, T bs, T omega, const T *xin, const T *xc, T alpha,
+                        T *out) {
+  grid_rows(L, [&](int i, int sub, int G, bool act) {
+    T s = T(0);
+    if (act)
+      for (int k = sub; k < L.w; k += G) {
+        const size_t at = (size_t)k * L.ld + i;
+        const int j = L.col[at];
+        const T yj = xc ? xin[j] + alpha * xc[L.agg[j]] : xin[j];
+        s += L.val[at] * yj;
+      }
+    s = group_sum(s, G);
+    if (act && sub == 0) {
+      const T yi = xc ? xin[i] + alpha * xc[L.agg[i]] : xin[i];
+      out[i] = yi + omega * L.dinv[i] * (bs * bsrc[i] - s);
+    }
+  });
+}
+
+// the coarse right-hand side: bc[I] = sum over the members i of I of (b - A x)_i, one
+// warp per coarse row, members' entries taken 32 at a time in member-then-slot order
+template <class T>
+__device__ void p_residual_restrict(const PLevel<T> &F, const T *bsrc, T bs, const T *x, const PLevel<T> &C) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int I = gw; I < C.n; I += nwarps) {
+    const int a = C.mptr[I], e = (I + 1 < C.n) ? C.mptr[I + 1] : F.n;
+    const int cnt = (e - a) * F.w;
+    T s = T(0);
+    for (int t = lane; t < cnt; t += 32) {
+      const int i = C.mem[a + t / F.w], k = t % F.w;
+      const size_t at = (size_t)k * F.ld + i;
+      s -= F.val[at] * x[F.col[at]];
+    }
+    for (int t = lane; t < e - a; t += 32) s += bs * bsrc[C.mem[a + t]];
+    s = warp_sum(s);
+    if (lane == 0) C.b[I] = s;
+  }
+}
+
+// z = V-cycle(bs * bsrc) into zout.  Every block calls it; all barriers are common.
+template <class T>
+__device__ bool p_vcycle(const PSolveArgs<T> &A, const T *bsrc, T bs, T *zout) {
+  const int S = A.sweeps;
+  T *pre[kMaxLevels];
+  // ---- down: pre-smoothing, then the coarse rhs from the residual ----
+  for (int l = 0; l < A.tail; ++l) {
+    const PLevel<T> &L = A.L[l];
+    const T *bl = l == 0 ? bsrc : L.b;
+    const T bsl = l == 0 ? bs : T(1);
+    // the post-smoothing's S sweeps alternate between two buffers and must end in the
+    // level's output (zout on level 0, L.x above it); so the pre-smoothing result, which
+    // the first post sweep reads, lies in the output buffer when S is even
+    T *outb = l == 0 ? zout : L.x;
+    T *altb = L.x2;
+    T *cur = (S % 2 == 0) ? outb : altb;
+    T *oth = cur == outb ? altb : outb;
+    // pre-smoothing: S sweeps from zero; the result must land in cur
+    if (S >= 2) {
+      T *tgt = (S % 2 == 0) ? cur : oth;  // S - 2 more sweeps each flip the buffer
+      p_first2(L, bl, bsl, A.omega, tgt);
+      if (!grid_sync(A.bar, gridDim.x, A.err)) return false;
+      for (int k = 2; k < S; ++k) {
+        T *nx = tgt == cur ? oth : cur;
+        p_sweep(L, bl, bsl, A.omega, tgt, (const T *)nullptr, A.alpha, nx);
+        if (!grid_sync(A.bar, gridDim.x, A.err)) return false;
+        tgt = nx;
+      }
+    } else {
+      p_first1(L, bl, bsl, A.omega, cur);
+      if (!grid_sync(A.bar, gridDim.x, A.err)) return false;
+    }
+    pre[l] = cur;
+    p_residual_restrict(L, bl, bsl, cur, A.L[l + 1]);
+    if (!grid_sync(A.bar, gridDim.x, A.err)) return false;
+  }
+  // ---- the tail in block 0 ----
+  if (blockIdx.x == 0) {
+    if (A.tail == 0) {  // the whole cycle is the tail: its rhs is the scaled input
+      const PLevel<T> &L = A.L[0];
+      for (int i = threadIdx.x; i < L.n; i += blockDim.x) L.b[i] = bs * bsrc[i];
+      __syncthreads();
+    }
+    tail_body(A.ta);
+    if (A.tail == 0) {
+      const PLevel<T> &L = A.L[0];
+      for (int i = threadIdx.x; i < L.n; i += blockDim.x) zout[i] = L.x[i];
+    }
+  }
+  if (!grid_sync(A.bar, gridDim.x, A.err)) return false;
+  // ---- up: coarse correction inside the first post sweep, then plain sweeps ----
+  for (int l = A.tail - 1; l >= 0; --l) {
+    const PLevel<T> &L = A.L[l];
+    const T *bl = l == 0 ? bsrc : L.b;
+    const T bsl = l == 0 ? bs : T(1);
+    T *outb = l == 0 ? zout : L.x;
+    T *altb = L.x2;
+    T *cur = pre[l];
+    T *nx = cur == outb ? altb : outb;
+    p_sweep(L, bl, bsl, A.omega, cur, (const T *)A.L[l + 1].x, A.alpha, nx);
+    if (!grid_sync(A.bar, gridDim.x, A.err)) return false;
+    for (int k = 1; k < S; ++k) {
+      cur = nx;
+      nx = cur == outb ? altb : outb;
+      p_sweep(L, bl, bsl, A.omega, cur, (const T *)nullptr, A.alpha, nx);
+      if (!grid_sync(A.bar, gridDim.x, A.err)) return false;
+    }
+  }
+  return true;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kPT, 1) ir_solve_persistent(PSolveArgs<T> A) {
+  __shared__ PShared sh;
+  const int nb = gridDim.x, n = A.n, M1 = A.M + 1;
+  const int rpb = (n + nb - 1) / nb;
+  const int r0 = min(n, (int)blockIdx.x * rpb), r1 = min(n, r0 + rpb);
+  // ---- ||D^-1 b||: the stopping test's scale ----
+  {
+    double s = 0.0;
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      const double d = A.val[i];
+      const double pb = (d == 0.0 ? 1.0 : 1.0 / d) * A.b[i];
+      s += pb * pb;
+    }
+    s = p_block_sum(s, sh.red);
+    p_put(A.part, 0, s);
+  }
+  if (threadIdx.x == 0) {
+    sh.outer = 0;
+    sh.total_its = 0;
+    sh.reason = 0;
+    sh.rn = 0.0;
+    sh.rtol_in = A.rtol_in;
+  }
+  if (!grid_sync(A.bar, nb, A.err)) return;
+  p_gather(A.part, 1, sh.h);
+  if (threadIdx.x == 0) sh.bnorm = sqrt(sh.h[0]);
+  __syncthreads();
+  for (;;) {
+    // ---- r = b - A x in FP64 and ||D^-1 r||; the reference's stopping test ----
+    if (!grid_sync(A.bar, nb, A.err)) return;  // x is complete
+    {
+      double s = 0.0;
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        double ax = 0.0;
+        for (int k = 0; k < A.w; ++k) {
+          const size_t at = (size_t)k * A.ld + i;
+          ax += A.val[at] * __ldcg(A.x + A.col[at]);
+        }
+        const double ri = A.b[i] - ax;
+        A.r[i] = ri;
+        const double d = A.val[i];
+        const double pr = (d == 0.0 ? 1.0 : 1.0 / d) * ri;
+        s += pr * pr;
+      }
+      s = p_block_sum(s, sh.red);
+      p_put(A.part, 0, s);
+    }
+    if (!grid_sync(A.bar, nb, A.err)) return;
+    p_gather(A.part, 1, sh.h);
+    if (threadIdx.x == 0) {
+      const double rn = sqrt(sh.h[0]);
+      if (sh.outer == 0) {
+        sh.ttol = fmax(A.rtol * sh.bnorm, A.atol);
+        sh.rn0 = sh.bnorm;
+      }
+      int reason = 0;
+      bool stop = true;
+      if (sh.outer == 0 && sh.bnorm == 0.0) reason = kConvergedAtol;
+      else if (!(rn == rn)) reason = kDivergedNanOrInf;
+      else if (rn <= sh.ttol) reason = rn < A.atol ? kConvergedAtol : kConvergedRtol;
+      else if (rn >= A.dtol * sh.rn0) reason = kDivergedDtol;
+      else if (sh.total_its >= A.max_it) reason = kDivergedIts;
+      else if (sh.outer >= A.max_outer) reason = 0;
+      else stop = false;
+      if (A.exact_inner) {
+        if (rn > 0.0) sh.rtol_in = fmin(0.1, fmax(0.5 * sh.ttol / rn, 1e-15));
+      } else if (sh.outer >= 1 && sh.rn > 0.0) {
+        sh.rtol_in = fmin(0.1, fmax(A.rtol_in, 0.5 * (rn / sh.rn)));
+      }
+      sh.rn = rn;
+      sh.reason = reason;
+      sh.more = stop ? 0 : 1;
+    }
+    __syncthreads();
+    if (!sh.more) break;
+    // ---- v_0 = D^-1 r / ||D^-1 r|| in the inner precision, beta = ||v_0|| ----
+    {
+      const double inv_s = 1.0 / sh.rn;
+      double s = 0.0;
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        const double d = A.val[i];
+        const T v = (T)((d == 0.0 ? A.r[i] : A.r[i] / d) * inv_s);
+        A.V[i] = v;
+        s += (double)v * (double)v;
+      }
+      s = p_block_sum(s, sh.red);
+      p_put(A.part, 0, s);
+    }
+    if (!grid_sync(A.bar, nb, A.err)) return;
+    p_gather(A.part, 1, sh.h);
+    if (threadIdx.x == 0) {
+      const double beta = sqrt(sh.h[0]);
+      sh.beta = beta;
+      sh.it = 0;
+      sh.g[0] = beta;
+      sh.scale[0] = beta > 0.0 ? 1.0 / beta : 0.0;
+      sh.inner_max = min(A.M, max(1, A.max_it - sh.total_its));
+      sh.more = beta > 0.0 ? 1 : 0;
+    }
+    __syncthreads();
+    // ---- the (F)GMRES cycle ----
+    while (sh.more) {
+      const int it = sh.it;
+      const T s_it = (T)sh.scale[it];
+      const T *vit = A.V + (size_t)it * A.vn;
+      T *zit = A.use_mg ? A.Z + (size_t)it * A.vn : nullptr;
+      if (A.use_mg && !p_vcycle(A, vit, s_it, zit)) return;
+      // w = A z; V_{it+1} = w; partial dots <w, V_j>, j <= it
+      T *w = A.V + (size_t)(it + 1) * A.vn;
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        T acc = T(0);
+        for (int k = 0; k < A.w; ++k) {
+          const size_t at = (size_t)k * A.ld + i;
+          const int j = A.col[at];
+          acc += A.valf[at] * (A.use_mg ? __ldcg(zit + j) : s_it * __ldcg(vit + j));
+        }
+        w[i] = acc;
+      }
+      __syncthreads();
+      {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        for (int j = 0; j <= it; ++j) {
+          const T *vj = A.V + (size_t)j * A.vn;
+          double s = 0.0;
+          for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) s += (double)w[i] * (double)vj[i];
+          s = warp_sum(s);
+          if (lane == 0) sh.wdots[warp][j] = s;
+        }
+        __syncthreads();
+        if ((int)threadIdx.x <= it) {
+          double s = 0.0;
+          for (int q = 0; q < nw; ++q) s += sh.wdots[q][threadIdx.x];
+          A.part[(size_t)threadIdx.x * kPMaxBlocks + blockIdx.x] = s;
+        }
+      }
+      if (!grid_sync(A.bar, nb, A.err)) return;
+      p_gather(A.part, it + 1, sh.h);
+      // w -= sum_j h_j v_j with v_j = scale_j V_j (h_j = scale_j <w, V_j>); ||w||^2
+      {
+        double s = 0.0;
+        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+          double wi = (double)w[i];
+          for (int j = 0; j <= it; ++j) {
+            const double sj = sh.scale[j];
+            wi -= (sh.h[j] * sj) * (sj * (double)A.V[(size_t)j * A.vn + i]);
+          }
+          const T wt = (T)wi;
+          w[i] = wt;
+          s += (double)wt * (double)wt;
+        }
+        s = p_block_sum(s, sh.red);
+        p_put(A.part, kPSlots - 1, s);
+      }
+      if (!grid_sync(A.bar, nb, A.err)) return;
+      p_gather(A.part + (size_t)(kPSlots - 1) * kPMaxBlocks, 1, sh.h + kPSlots - 1);
+      // Arnoldi scalars, the same in every block
+      if (threadIdx.x == 0) {
+        const double tt = sqrt(sh.h[kPSlots - 1]);
+        double *hc = sh.H + (size_t)it * M1;
+        for (int j = 0; j <= it; ++j) hc[j] = sh.h[j] * sh.scale[j];
+        hc[it + 1] = tt;
+        for (int j = 1; j <= it; ++j) {
+          const double t0 = hc[j - 1];
+          hc[j - 1] = sh.cs[j - 1] * t0 + sh.sn[j - 1] * hc[j];
+          hc[j] = sh.cs[j - 1] * hc[j] - sh.sn[j - 1] * t0;
+        }
+        const double t = sqrt(hc[it] * hc[it] + hc[it + 1] * hc[it + 1]);
+        bool more = false;
+        if (t != 0.0 && t == t) {
+          const double cs = hc[it] / t, sn = hc[it + 1] / t;
+          sh.cs[it] = cs;
+          sh.sn[it] = sn;
+          sh.g[it + 1] = -sn * sh.g[it];
+          sh.g[it] = cs * sh.g[it];
+          hc[it] = cs * hc[it] + sn * hc[it + 1];
+          more = !(fabs(sh.g[it + 1]) <= sh.rtol_in * sh.beta) && tt != 0.0;
+        }
+        sh.it = it + 1;
+        sh.more = (more && sh.it < sh.inner_max) ? 1 : 0;
+        sh.scale[it + 1] = tt > 0.0 ? 1.0 / tt : 0.0;
+      }
+      __syncthreads();
+    }
+    // ---- y = H^-1 g; x += ||D^-1 r|| sum_j y_j z_j ----
+    if (threadIdx.x == 0) {
+      const int it = sh.it;
+      for (int k = it - 1; k >= 0; --k) {
+        double s = sh.g[k];
+        for (int j = k + 1; j < it; ++j) s -= sh.H[(size_t)j * M1 + k] * sh.y[j];
+        const double hkk = sh.H[(size_t)k * M1 + k];
+        sh.y[k] = hkk != 0.0 ? s / hkk : 0.0;
+      }
+      sh.total_its += it;
+      sh.outer += 1;
+    }
+    __syncthreads();
+    {
+      const int nv = sh.it;
+      const double rn = sh.rn;
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        double t = 0.0;
+        if (A.use_mg)
+          for (int j = 0; j < nv; ++j) t += sh.y[j] * (double)A.Z[(size_t)j * A.vn + i];
+        else
+          for (int j = 0; j < nv; ++j) t += sh.y[j] * (sh.scale[j] * (double)A.V[(size_t)j * A.vn + i]);
+        A.x[i] += rn * (double)(T)t;
+      }
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    A.out->outer = sh.outer;
+    A.out->total_its = sh.total_its;
+    A.out->reason = sh.reason;
+    A.out->rn = sh.rn;
   }
 }
 
@@ -828,6 +1316,11 @@ struct MgWork {
   cudaStream_t side = nullptr;
   cudaEvent_t side_ev[2] = {nullptr, nullptr};  // operator assembled (main), hierarchy built (side)
   bool prebuilt = false;
+  // the persistent solve kernel: partial sums, grid barrier, outcome (+ its pinned copy)
+  double *ppart = nullptr;
+  GridBar *pbar = nullptr;
+  PResult *pres = nullptr;
+  PResult *pres_host = nullptr;
 };
 
 static MgWork *mg(apc_context *c) {
@@ -873,9 +1366,10 @@ void apc_mg_free(apc_context *c) {
   free_hier(c, m->h32);
   free_hier(c, m->h64);
   void *p[] = {m->pkey, m->pkey_alt, m->pidx, m->pidx_alt, m->eflag, m->epos, m->ucol,
-               m->rowstart, m->partial, m->dots, m->counter, m->state, m->total};
+               m->rowstart, m->partial, m->dots, m->counter, m->state, m->total, m->ppart, m->pbar, m->pres};
   for (void *q : p) apc_free(c, q);
   if (m->host) cudaFreeHost(m->host);
+  if (m->pres_host) cudaFreeHost(m->pres_host);
   for (int k = 0; k < 2; ++k) {
     if (m->solve_exec[k]) cudaGraphExecDestroy(m->solve_exec[k]);
     if (m->solve_graph[k]) cudaGraphDestroy(m->solve_graph[k]);
@@ -1336,6 +1830,110 @@ static int capture_solve(apc_context *c, const IrSolveArgs<T> &a) {
 // system.  For the potential with the multigrid option, builds the hierarchy over the
 // current operator and right-preconditions with its V-cycle.  The solve is captured as
 // one graph and run; the host reads the outcome once.
+// Run one solve as the persistent kernel (ir_solve_persistent): the arguments carry the
+// hierarchy's levels and the tail; `blocks` blocks of kPT threads, co-resident by the
+// cooperative launch.  Returns APC_ERR_UNSUPPORTED when the kernel cannot be launched
+// co-resident (the caller then uses the graph path).
+template <class T>
+static int persistent_solve(apc_context *c, const IrSolveArgs<T> &a, int blocks) {
+  MgWork *m = c->mg;
+  MgHier<T> &H = hier<T>(m);
+  const void *kern = (const void *)ir_solve_persistent<T>;
+  int occ = 0;
+  APC_CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kPT, 0));
+  if (occ < 1) return APC_ERR_UNSUPPORTED;
+  blocks = std::max(1, std::min(blocks, std::min(kPMaxBlocks, apc_sm_count(c) * occ)));
+  if (!m->ppart) {
+    APC_TRY(apc_alloc(c, (void **)&m->ppart, sizeof(double) * (size_t)kPSlots * kPMaxBlocks));
+    APC_TRY(apc_alloc(c, (void **)&m->pbar, sizeof(GridBar)));
+    APC_TRY(apc_alloc(c, (void **)&m->pres, sizeof(PResult)));
+  }
+  if (!m->pres_host) APC_CUDA_TRY(c, cudaMallocHost((void **)&m->pres_host, sizeof(PResult)));
+  PSolveArgs<T> P{};
+  P.n = a.n;
+  P.w = a.w;
+  P.ld = a.ld;
+  P.col = a.col;
+  P.valf = a.valf;
+  P.val = a.val;
+  P.b = a.b;
+  P.x = a.x;
+  P.r = a.r;
+  P.V = H.V;
+  P.Z = H.Z;
+  P.vn = m->vn;
+  P.M = a.M;
+  P.use_mg = a.mg ? 1 : 0;
+  P.sweeps = c->cfg.mg_sweeps > 0 ? c->cfg.mg_sweeps : 2;
+  P.omega = (T)(c->cfg.mg_omega > 0 ? c->cfg.mg_omega : 0.95);
+  P.alpha = (T)(c->cfg.mg_alpha > 0 ? c->cfg.mg_alpha : 1.8);
+  if (a.mg) {
+    P.nlev = H.nlev;
+    P.tail = 0;
+    while (P.tail < H.nlev - 1 && H.lv[P.tail].n > kTail) ++P.tail;
+    for (int l = 0; l < H.nlev; ++l) {
+      const MgLevel<T> &Q = H.lv[l];
+      PLevel<T> &D = P.L[l];
+      D.n = Q.n;
+      D.w = Q.w;
+      D.g = Q.w <= 24 ? 1 : (Q.w <= 48 ? 4 : 8);
+      D.ld = Q.ld;
+      D.col = Q.col;
+      D.val = Q.val;
+      D.dinv = Q.dinv;
+      D.agg = Q.agg;
+      D.mptr = Q.mptr;
+      D.mem = Q.mem;
+      D.x = Q.x;
+      D.x2 = Q.x2;
+      D.b = Q.b;
+    }
+    TailArgs<T> &TA = P.ta;
+    TA.nl = std::min(H.nlev - P.tail, kTailLevels);
+    TA.inv = H.coarse_inv;
+    TA.sweeps = P.sweeps;
+    TA.omega = P.omega;
+    TA.alpha = P.alpha;
+    for (int k = 0; k < TA.nl; ++k) {
+      const MgLevel<T> &Q = H.lv[P.tail + k];
+      TailLevel<T> &D = TA.L[k];
+      D.n = Q.n;
+      D.w = Q.w;
+      D.g = 1;
+      if (Q.w > 24)
+        while (D.g < 8 && 2 * D.g * Q.n <= kPT) D.g *= 2;
+      D.ld = Q.ld;
+      D.col = Q.col;
+      D.val = Q.val;
+      D.dinv = Q.dinv;
+      D.agg = Q.agg;
+      D.mptr = Q.mptr;
+      D.mem = Q.mem;
+      D.x = Q.x;
+      D.b = Q.b;
+      D.x2 = Q.x2;
+      D.r = Q.r;
+    }
+  }
+  P.rtol = a.rtol;
+  P.atol = a.atol;
+  P.dtol = a.dtol;
+  P.rtol_in = a.rtol_in;
+  P.max_it = a.max_it;
+  P.max_outer = a.max_outer;
+  P.exact_inner = sizeof(T) == sizeof(double) ? 1 : 0;
+  P.part = m->ppart;
+  P.bar = m->pbar;
+  P.err = c->d_err;
+  P.out = m->pres;
+  APC_CUDA_TRY(c, cudaMemsetAsync(m->pbar, 0, sizeof(GridBar), c->s));
+  APC_CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->s));
+  void *args[] = {&P};
+  APC_CUDA_TRY(c, cudaLaunchCooperativeKernel(kern, dim3(blocks), dim3(kPT), args, 0, c->s));
+  apc_count_launch(c);
+  return APC_OK;
+}
+
 template <class T>
 static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, const T *valf, const double *b,
                     double *x, double *r, int restart, double rtol_in, int *its, double *rnorm, int *reason,
@@ -1393,6 +1991,48 @@ static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, c
   // bounds the loop in every case
   a.max_outer = use_mg && sizeof(T) == sizeof(float) ? 40 : std::max(40, cfg.gmres_max_it);
   a.M = M;
+  // one persistent kernel per solve unless the graph path is asked for (or needed: the
+  // re-orthogonalising Gram-Schmidt runs only there)
+  bool persistent = !cfg.mixed_solve_graphs && !cfg.mg_reorth;
+  if (persistent) {
+    // a density solve overlapped with the potential's hierarchy build keeps half of the
+    // SMs free for it
+    const int sms = apc_sm_count(c);
+    const int want = std::max(1, (n + kPT - 1) / kPT);
+    const int blocks = during ? std::max(1, std::min(want, sms / 2)) : want;
+    if (use_mg)
+      c->prof.mg_build_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    APC_CUDA_TRY(c, cudaEventRecord(c->kev[0], c->s));
+    const int rc = persistent_solve<T>(c, a, blocks);
+    if (rc == APC_ERR_UNSUPPORTED) {
+      persistent = false;
+    } else {
+      APC_TRY(rc);
+      APC_CUDA_TRY(c, cudaEventRecord(c->kev[1], c->s));
+      APC_CUDA_TRY(c, cudaMemcpyAsync(m->pres_host, m->pres, sizeof(PResult), cudaMemcpyDeviceToHost, c->s));
+      APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 2, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+      if (during) APC_TRY(during(c));
+      APC_CUDA_TRY(c, apc_stream_wait(c));
+      APC_CUDA_TRY(c, cudaGetLastError());
+      if (c->h_pinned[2] & DERR_KRYLOV) {
+        c->err = "solve kernel grid barrier timed out";
+        return APC_ERR_TIMEOUT;
+      }
+      const PResult &R = *m->pres_host;
+      float ms = 0.f;
+      APC_CUDA_TRY(c, cudaEventElapsedTime(&ms, c->kev[0], c->kev[1]));
+      *its = R.total_its;
+      *rnorm = R.rn;
+      *reason = R.reason;
+      *refinements = R.outer;
+      *levels = use_mg ? H.nlev : 0;
+      if (use_mg) {
+        c->prof.mg_solve_ms += ms;
+        c->prof.mg_iterations += R.total_its;
+      }
+      return APC_OK;
+    }
+  }
   APC_TRY(capture_solve(c, a));
   if (use_mg)
     c->prof.mg_build_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

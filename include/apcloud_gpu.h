@@ -94,6 +94,10 @@ typedef struct apc_config {
   int warm_start;        /* mixed path: start both solves from the previous step's solution at the
                             same octree cells (1) or from zero (0, default); the stopping test stays
                             rtol ||D^-1 b||.  At 128^3 and a < 0.1 it saves ~1 of 20 iterations */
+  int mixed_solve_graphs; /* APC_PREC_MIXED / APC_PREC_FP64_MULTIGRID solves: 0 (default) = each solve
+                            is one persistent cooperative kernel (refinement loop, (F)GMRES cycles and
+                            V-cycles separated by grid barriers); 1 = a CUDA graph of per-phase
+                            kernels with conditional loop nodes (always used with mg_reorth) */
 } apc_config;
 
 enum { APC_PRECOND_JACOBI = 0, APC_PRECOND_MULTIGRID = 1 };
