@@ -7,13 +7,13 @@ fields of a step are constants of the step and the Jacobian of a particle's
 acceleration is its cell's Hessian.  The C ABI keeps the state every k steps and
 reruns each segment in the backward pass.
 
-    python -m apcloud.adjoint [--side 64] [--steps 32] [--every 8] [--fd 64] [--cpu-ref]
+    python -m apcloud.adjoint [--side 64] [--steps 32] [--every 8] [--fd 64]
 
 runs the adjoint workload (64^3 EdS Zel'dovich box, 32 steps from a = 0.05 to 0.5,
 checkpoints every 8 steps, loss = mean squared distance to a target perturbed from the
 forward result by N(0, 0.01 spacing)) and checks the gradient with respect to the FP32
-displacement field against central finite differences on random components, and
-optionally against the FP64 CPU adjoint of the oracle.
+displacement field against central finite differences on random components
+(tests/adjoint_c5_cpu_check.py adds the comparison with the FP64 CPU adjoint).
 """
 from __future__ import annotations
 
@@ -121,7 +121,7 @@ def fd_loss(g, psi64, fac, target, sched) -> float:
     return float(np.mean(np.sum(d * d, axis=0)))
 
 
-def main():
+def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--side", type=int, default=64)
     ap.add_argument("--steps", type=int, default=32)
@@ -130,8 +130,7 @@ def main():
     ap.add_argument("--h", type=float, default=1e-4)
     ap.add_argument("--seed", type=int, default=5)
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="mixed")
-    ap.add_argument("--cpu-ref", action="store_true")
-    args = ap.parse_args()
+    args = ap.parse_args(argv)
     side = args.side
     a0, a1 = 0.05, 0.5
     psi, fac = ics.zeldovich_field(side, -2.0, 0.2, a0, 1.0, 0.0, seed=args.seed)
@@ -178,26 +177,9 @@ def main():
            "fd_max_err_rel_to_max_grad": float(err.max()), "fd_median_err_rel_to_max_grad": float(np.median(err)),
            "fd_within_1e-3": int(np.sum(err < 1e-3)), "fd_redone_with_h_over_100": redo,
            "grad_norm": float(np.linalg.norm(grad))}
-    if args.cpu_ref:
-        import sys
-        import os
-
-        sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(
-            os.path.abspath(__file__)))), "oracle"))
-        import adjoint_ref  # the FP64 CPU adjoint (test infrastructure)
-
-        t1 = time.perf_counter()
-        parts = ics.particles_from_field(psi32.astype(np.float64), fac)
-        cot = np.zeros((6, n))
-        xf, _ = adjoint_ref.forward_state(parts, 21, gfd_c, sched)
-        d = wrap(xf[:3] - target)
-        cot[:3] = 2.0 * d / n
-        _, c0 = adjoint_ref.trajectory_vjp(parts, 21, gfd_c, sched, cot)
-        gref = (c0[:3] + fac * c0[3:]).reshape(3, side, side, side)
-        out["cpu_ref_seconds"] = time.perf_counter() - t1
-        out["cpu_ref_max_rel_err"] = float(np.max(np.abs(gref - grad)) / np.max(np.abs(gref)))
     g.close()
     print(json.dumps(out))
+    return out, grad, (psi32, fac, gfd_c, sched, target)
 
 
 if __name__ == "__main__":

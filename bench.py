@@ -284,7 +284,7 @@ def run_ours(args) -> dict:
     def make(prec, p):
         return binding.GpuPath(p, cfg.depth, cfg.gfd_c, cfg.lm, restart=cfg.restart, rtol=cfg.rtol,
                                precision=prec, device=dev, mixed_restart=args.mixed_restart,
-                               mixed_inner_rtol=args.inner_rtol)
+                               mixed_inner_rtol=args.inner_rtol, solve_graphs=int(args.solve_graphs))
 
     # ---- warm-up on the mixed path ----
     mx = make(binding.APC_PREC_MIXED, parts)
@@ -306,7 +306,7 @@ def run_ours(args) -> dict:
     for name, prec, rtol in arms:
         g = binding.GpuPath(state_parts, cfg.depth, cfg.gfd_c, cfg.lm, restart=cfg.restart, rtol=rtol,
                             precision=prec, device=dev, mixed_restart=args.mixed_restart,
-                            mixed_inner_rtol=args.inner_rtol)
+                            mixed_inner_rtol=args.inner_rtol, solve_graphs=int(args.solve_graphs))
         c2 = for_config(g, cfg)
         c2.t = t_state
         k = c2.constants(c2.t, cfg.delta_a)
@@ -441,7 +441,9 @@ def run_ours(args) -> dict:
                    "timed_steps": f"steps {args.warmup + 1}-{args.warmup + args.steps} of {cfg.steps} "
                                   f"(a = {t_state:.4f} onwards); the whole run is in full_run",
                    "mixed_restart": args.mixed_restart or 16,
-                   "inner_rtol": args.inner_rtol or 1e-3},
+                   "inner_rtol": args.inner_rtol or 1e-3,
+                   "solve": "CUDA graphs of per-phase kernels" if args.solve_graphs else
+                            "one persistent cooperative kernel per solve"},
         "fp64": fp64,
         "force_error": dict(force, bound=1e-6,
                             measure="RMS relative error of the accelerations (and potentials) of one step on the "
@@ -644,6 +646,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-full-run", action="store_true")
+    ap.add_argument("--solve-graphs", action="store_true",
+                    help="run the multigrid solves as CUDA graphs of per-phase kernels instead of one "
+                         "persistent kernel each")
     ap.add_argument("--batch-workers", type=int, default=0, help="host worker threads per rank (batch96)")
     args = ap.parse_args()
     if args.warmup < 3:

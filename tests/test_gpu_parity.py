@@ -361,3 +361,31 @@ def test_fused_step_equals_phase_calls(gpu_lib):
     assert ra == rb
     for a, b in zip(pa, pb):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("prec", [binding.APC_PREC_MIXED, binding.APC_PREC_FP64_MULTIGRID], ids=["mixed", "fp64mg"])
+@pytest.mark.parametrize("case", ["ball32k", "eds64"])
+def test_persistent_solve_matches_graph_solve(gpu_lib, prec, case):
+    """The solves run as one persistent kernel by default; the CUDA-graph path of per-phase
+    kernels is the same algorithm.  Both must meet the stopping test, and their fields
+    agree to the accuracy of the solves (eds64's first step has 32,768 cells: two grid
+    levels above the single-block tail)."""
+    cfg = ics.config(case)
+    p = cfg.particles()
+    t = cfg.a_start + 0.5 * cfg.delta_a
+    out = []
+    for graphs in (0, 1):
+        gp = binding.GpuPath(p, cfg.depth, cfg.gfd_c, precision=prec, solve_graphs=graphs)
+        gp.select()
+        gp.solve(1.0 / p.n, 1.5 * cfg.omega0 / t, -1.0)
+        gp.move_velocity(cfg.delta_a, ics.kick_factor(t, cfg.omega0, cfg.omegal))
+        st = gp.solve_stats()
+        assert st["density_reason"] == 2 and st["potential_reason"] == 2, st
+        out.append((gp.particles()[6:9], gp.fields(), st))
+        gp.close()
+    (pa, fa, sa), (pb, fb, sb) = out
+    print(case, prec, "persistent its", sa["potential_its"], sa["potential_refinements"], "graph its",
+          sb["potential_its"], sb["potential_refinements"], "acc rms", _acc_rms(pa, pb))
+    assert _acc_rms(pa, pb) <= 1e-7
+    assert _rel(fa.potential, fb.potential) <= 1e-7
+    assert abs(sa["potential_its"] - sb["potential_its"]) <= max(3, sb["potential_its"] // 5)
