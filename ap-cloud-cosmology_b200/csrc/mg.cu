@@ -854,6 +854,16 @@ struct PShared {
   int outer, total_its, reason, it, inner_max, more;
 };
 
+// The blocks that run one solve together: the whole grid for a single solve, or one group
+// of a batched launch.  Every phase indexes blocks by rank / size.
+struct Grp {
+  int rank, size;
+  GridBar *bar;
+  int *err;
+};
+
+__device__ __forceinline__ bool gsync(const Grp &g) { return grid_sync(g.bar, (unsigned)g.size, g.err); }
+
 __device__ __forceinline__ double p_block_sum(double v, double *red) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   v = warp_sum(v);
@@ -866,8 +876,8 @@ __device__ __forceinline__ double p_block_sum(double v, double *red) {
 }
 
 // all blocks: out[j] = sum over blocks of part[j][b], b in block order, for j < nv
-__device__ __forceinline__ void p_gather(const double *part, int nv, double *out) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5, nb = gridDim.x;
+__device__ __forceinline__ void p_gather(const Grp &g, const double *part, int nv, double *out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5, nb = g.size;
   for (int j = warp; j < nv; j += nw) {
     double v = 0.0;
 #pragma unroll
@@ -881,8 +891,8 @@ __device__ __forceinline__ void p_gather(const double *part, int nv, double *out
   __syncthreads();
 }
 
-__device__ __forceinline__ void p_put(double *part, int j, double v) {
-  if (threadIdx.x == 0) part[(size_t)j * kPMaxBlocks + blockIdx.x] = v;
+__device__ __forceinline__ void p_put(const Grp &g, double *part, int j, double v) {
+  if (threadIdx.x == 0) part[(size_t)j * kPMaxBlocks + g.rank] = v;
 }
 
 template <class T>
@@ -894,11 +904,11 @@ __device__ __forceinline__ T group_sum(T s, int G) {
 // f(i, sub, G, active) for every row of L, G lanes per row, over the whole grid; the trip
 // count is the same for every lane (the group sums shuffle)
 template <class T, class F>
-__device__ __forceinline__ void grid_rows(const PLevel<T> &L, F f) {
+__device__ __forceinline__ void grid_rows(const Grp &g, const PLevel<T> &L, F f) {
   const int G = L.g;
-  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long tid = (long long)g.rank * blockDim.x + threadIdx.x;
   const int sub = (int)(tid & (G - 1));
-  const long long groups = ((long long)gridDim.x * blockDim.x) / G;
+  const long long groups = ((long long)g.size * blockDim.x) / G;
   const long long rounds = (L.n + groups - 1) / groups;
   for (long long rd = 0; rd < rounds; ++rd) {
     const long long i = tid / G + rd * groups;
@@ -909,8 +919,8 @@ __device__ __forceinline__ void grid_rows(const PLevel<T> &L, F f) {
 // two damped Jacobi sweeps from x = 0 in one pass: x1 = w D^-1 b, out = x1 + w D^-1 (b - A x1);
 // b = bs * bsrc
 template <class T>
-__device__ void p_first2(const PLevel<T> &L, const T *bsrc, T bs, T omega, T *out) {
-  grid_rows(L, [&](int i, int sub, int G, bool act) {
+__device__ void p_first2(const Grp &g, const PLevel<T> &L, const T *bsrc, T bs, T omega, T *out) {
+  grid_rows(g, L, [&](int i, int sub, int G, bool act) {
     T s = T(0);
     if (act)
       for (int k = sub; k < L.w; k += G) {
@@ -929,16 +939,16 @@ __device__ void p_first2(const PLevel<T> &L, const T *bsrc, T bs, T omega, T *ou
 
 // x = w D^-1 b (one sweep from zero)
 template <class T>
-__device__ void p_first1(const PLevel<T> &L, const T *bsrc, T bs, T omega, T *out) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.n; i += gridDim.x * blockDim.x)
+__device__ void p_first1(const Grp &g, const PLevel<T> &L, const T *bsrc, T bs, T omega, T *out) {
+  for (int i = g.rank * blockDim.x + threadIdx.x; i < L.n; i += g.size * blockDim.x)
     out[i] = omega * L.dinv[i] * (bs * bsrc[i]);
 }
 
 // out = y + w D^-1 (b - A y), y = xin (+ alpha xc[agg] when xc is given)
 template <class T>
-__device__ void p_sweep(const PLevel<T> &L, const T *bsrc, T bs, T omega, const T *xin, const T *xc, T alpha,
+__device__ void p_sweep(const Grp &g, const PLevel<T> &L, const T *bsrc, T bs, T omega, const T *xin, const T *xc, T alpha,
                         T *out) {
-  grid_rows(L, [&](int i, int sub, int G, bool act) {
+  grid_rows(g, L, [&](int i, int sub, int G, bool act) {
     T s = T(0);
     if (act)
       for (int k = sub; k < L.w; k += G) {
@@ -958,9 +968,10 @@ __device__ void p_sweep(const PLevel<T> &L, const T *bsrc, T bs, T omega, const 
 // the coarse right-hand side: bc[I] = sum over the members i of I of (b - A x)_i, one
 // warp per coarse row, members' entries taken 32 at a time in member-then-slot order
 template <class T>
-__device__ void p_residual_restrict(const PLevel<T> &F, const T *bsrc, T bs, const T *x, const PLevel<T> &C) {
+__device__ void p_residual_restrict(const Grp &g, const PLevel<T> &F, const T *bsrc, T bs, const T *x,
+                                    const PLevel<T> &C) {
   const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int gw = (g.rank * blockDim.x + threadIdx.x) >> 5, nwarps = (g.size * blockDim.x) >> 5;
   for (int I = gw; I < C.n; I += nwarps) {
     const int a = C.mptr[I], e = (I + 1 < C.n) ? C.mptr[I + 1] : F.n;
     const int cnt = (e - a) * F.w;
@@ -978,7 +989,7 @@ __device__ void p_residual_restrict(const PLevel<T> &F, const T *bsrc, T bs, con
 
 // z = V-cycle(bs * bsrc) into zout.  Every block calls it; all barriers are common.
 template <class T>
-__device__ bool p_vcycle(const PSolveArgs<T> &A, const T *bsrc, T bs, T *zout) {
+__device__ bool p_vcycle(const Grp &g, const PSolveArgs<T> &A, const T *bsrc, T bs, T *zout) {
   const int S = A.sweeps;
   T *pre[kMaxLevels];
   // ---- down: pre-smoothing, then the coarse rhs from the residual ----
@@ -996,24 +1007,24 @@ __device__ bool p_vcycle(const PSolveArgs<T> &A, const T *bsrc, T bs, T *zout) {
     // pre-smoothing: S sweeps from zero; the result must land in cur
     if (S >= 2) {
       T *tgt = (S % 2 == 0) ? cur : oth;  // S - 2 more sweeps each flip the buffer
-      p_first2(L, bl, bsl, A.omega, tgt);
-      if (!grid_sync(A.bar, gridDim.x, A.err)) return false;
+      p_first2(g, L, bl, bsl, A.omega, tgt);
+      if (!gsync(g)) return false;
       for (int k = 2; k < S; ++k) {
         T *nx = tgt == cur ? oth : cur;
-        p_sweep(L, bl, bsl, A.omega, tgt, (const T *)nullptr, A.alpha, nx);
-        if (!grid_sync(A.bar, gridDim.x, A.err)) return false;
+        p_sweep(g, L, bl, bsl, A.omega, tgt, (const T *)nullptr, A.alpha, nx);
+        if (!gsync(g)) return false;
         tgt = nx;
       }
     } else {
-      p_first1(L, bl, bsl, A.omega, cur);
-      if (!grid_sync(A.bar, gridDim.x, A.err)) return false;
+      p_first1(g, L, bl, bsl, A.omega, cur);
+      if (!gsync(g)) return false;
     }
     pre[l] = cur;
-    p_residual_restrict(L, bl, bsl, cur, A.L[l + 1]);
-    if (!grid_sync(A.bar, gridDim.x, A.err)) return false;
+    p_residual_restrict(g, L, bl, bsl, cur, A.L[l + 1]);
+    if (!gsync(g)) return false;
   }
   // ---- the tail in block 0 ----
-  if (blockIdx.x == 0) {
+  if (g.rank == 0) {
     if (A.tail == 0) {  // the whole cycle is the tail: its rhs is the scaled input
       const PLevel<T> &L = A.L[0];
       for (int i = threadIdx.x; i < L.n; i += blockDim.x) L.b[i] = bs * bsrc[i];
@@ -1025,7 +1036,7 @@ __device__ bool p_vcycle(const PSolveArgs<T> &A, const T *bsrc, T bs, T *zout) {
       for (int i = threadIdx.x; i < L.n; i += blockDim.x) zout[i] = L.x[i];
     }
   }
-  if (!grid_sync(A.bar, gridDim.x, A.err)) return false;
+  if (!gsync(g)) return false;
   // ---- up: coarse correction inside the first post sweep, then plain sweeps ----
   for (int l = A.tail - 1; l >= 0; --l) {
     const PLevel<T> &L = A.L[l];
@@ -1035,24 +1046,25 @@ __device__ bool p_vcycle(const PSolveArgs<T> &A, const T *bsrc, T bs, T *zout) {
     T *altb = L.x2;
     T *cur = pre[l];
     T *nx = cur == outb ? altb : outb;
-    p_sweep(L, bl, bsl, A.omega, cur, (const T *)A.L[l + 1].x, A.alpha, nx);
-    if (!grid_sync(A.bar, gridDim.x, A.err)) return false;
+    p_sweep(g, L, bl, bsl, A.omega, cur, (const T *)A.L[l + 1].x, A.alpha, nx);
+    if (!gsync(g)) return false;
     for (int k = 1; k < S; ++k) {
       cur = nx;
       nx = cur == outb ? altb : outb;
-      p_sweep(L, bl, bsl, A.omega, cur, (const T *)nullptr, A.alpha, nx);
-      if (!grid_sync(A.bar, gridDim.x, A.err)) return false;
+      p_sweep(g, L, bl, bsl, A.omega, cur, (const T *)nullptr, A.alpha, nx);
+      if (!gsync(g)) return false;
     }
   }
   return true;
 }
 
+// One whole solve by the group g (all of its blocks call it); part holds the group's
+// [slot][block] partial sums.  Returns false when a barrier gave up.
 template <class T>
-__global__ void __launch_bounds__(kPT, 1) ir_solve_persistent(PSolveArgs<T> A) {
-  __shared__ PShared sh;
-  const int nb = gridDim.x, n = A.n, M1 = A.M + 1;
+__device__ bool solve_body(const PSolveArgs<T> &A, const Grp &g, PShared &sh, double *part) {
+  const int nb = g.size, n = A.n, M1 = A.M + 1;
   const int rpb = (n + nb - 1) / nb;
-  const int r0 = min(n, (int)blockIdx.x * rpb), r1 = min(n, r0 + rpb);
+  const int r0 = min(n, g.rank * rpb), r1 = min(n, r0 + rpb);
   // ---- ||D^-1 b||: the stopping test's scale ----
   {
     double s = 0.0;
@@ -1062,7 +1074,7 @@ __global__ void __launch_bounds__(kPT, 1) ir_solve_persistent(PSolveArgs<T> A) {
       s += pb * pb;
     }
     s = p_block_sum(s, sh.red);
-    p_put(A.part, 0, s);
+    p_put(g, part, 0, s);
   }
   if (threadIdx.x == 0) {
     sh.outer = 0;
@@ -1071,13 +1083,13 @@ __global__ void __launch_bounds__(kPT, 1) ir_solve_persistent(PSolveArgs<T> A) {
     sh.rn = 0.0;
     sh.rtol_in = A.rtol_in;
   }
-  if (!grid_sync(A.bar, nb, A.err)) return;
-  p_gather(A.part, 1, sh.h);
+  if (!gsync(g)) return false;
+  p_gather(g, part, 1, sh.h);
   if (threadIdx.x == 0) sh.bnorm = sqrt(sh.h[0]);
   __syncthreads();
   for (;;) {
     // ---- r = b - A x in FP64 and ||D^-1 r||; the reference's stopping test ----
-    if (!grid_sync(A.bar, nb, A.err)) return;  // x is complete
+    if (!gsync(g)) return false;  // x is complete
     {
       double s = 0.0;
       for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
@@ -1093,10 +1105,10 @@ __global__ void __launch_bounds__(kPT, 1) ir_solve_persistent(PSolveArgs<T> A) {
         s += pr * pr;
       }
       s = p_block_sum(s, sh.red);
-      p_put(A.part, 0, s);
+      p_put(g, part, 0, s);
     }
-    if (!grid_sync(A.bar, nb, A.err)) return;
-    p_gather(A.part, 1, sh.h);
+    if (!gsync(g)) return false;
+    p_gather(g, part, 1, sh.h);
     if (threadIdx.x == 0) {
       const double rn = sqrt(sh.h[0]);
       if (sh.outer == 0) {
@@ -1134,10 +1146,10 @@ __global__ void __launch_bounds__(kPT, 1) ir_solve_persistent(PSolveArgs<T> A) {
         s += (double)v * (double)v;
       }
       s = p_block_sum(s, sh.red);
-      p_put(A.part, 0, s);
+      p_put(g, part, 0, s);
     }
-    if (!grid_sync(A.bar, nb, A.err)) return;
-    p_gather(A.part, 1, sh.h);
+    if (!gsync(g)) return false;
+    p_gather(g, part, 1, sh.h);
     if (threadIdx.x == 0) {
       const double beta = sqrt(sh.h[0]);
       sh.beta = beta;
@@ -1154,7 +1166,7 @@ __global__ void __launch_bounds__(kPT, 1) ir_solve_persistent(PSolveArgs<T> A) {
       const T s_it = (T)sh.scale[it];
       const T *vit = A.V + (size_t)it * A.vn;
       T *zit = A.use_mg ? A.Z + (size_t)it * A.vn : nullptr;
-      if (A.use_mg && !p_vcycle(A, vit, s_it, zit)) return;
+      if (A.use_mg && !p_vcycle(g, A, vit, s_it, zit)) return false;
       // w = A z; V_{it+1} = w; partial dots <w, V_j>, j <= it
       T *w = A.V + (size_t)(it + 1) * A.vn;
       for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
@@ -1180,11 +1192,11 @@ __global__ void __launch_bounds__(kPT, 1) ir_solve_persistent(PSolveArgs<T> A) {
         if ((int)threadIdx.x <= it) {
           double s = 0.0;
           for (int q = 0; q < nw; ++q) s += sh.wdots[q][threadIdx.x];
-          A.part[(size_t)threadIdx.x * kPMaxBlocks + blockIdx.x] = s;
+          part[(size_t)threadIdx.x * kPMaxBlocks + g.rank] = s;
         }
       }
-      if (!grid_sync(A.bar, nb, A.err)) return;
-      p_gather(A.part, it + 1, sh.h);
+      if (!gsync(g)) return false;
+      p_gather(g, part, it + 1, sh.h);
       // w -= sum_j h_j v_j with v_j = scale_j V_j (h_j = scale_j <w, V_j>); ||w||^2
       {
         double s = 0.0;
@@ -1199,10 +1211,10 @@ __global__ void __launch_bounds__(kPT, 1) ir_solve_persistent(PSolveArgs<T> A) {
           s += (double)wt * (double)wt;
         }
         s = p_block_sum(s, sh.red);
-        p_put(A.part, kPSlots - 1, s);
+        p_put(g, part, kPSlots - 1, s);
       }
-      if (!grid_sync(A.bar, nb, A.err)) return;
-      p_gather(A.part + (size_t)(kPSlots - 1) * kPMaxBlocks, 1, sh.h + kPSlots - 1);
+      if (!gsync(g)) return false;
+      p_gather(g, part + (size_t)(kPSlots - 1) * kPMaxBlocks, 1, sh.h + kPSlots - 1);
       // Arnoldi scalars, the same in every block
       if (threadIdx.x == 0) {
         const double tt = sqrt(sh.h[kPSlots - 1]);
@@ -1257,12 +1269,20 @@ __global__ void __launch_bounds__(kPT, 1) ir_solve_persistent(PSolveArgs<T> A) {
       }
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (g.rank == 0 && threadIdx.x == 0) {
     A.out->outer = sh.outer;
     A.out->total_its = sh.total_its;
     A.out->reason = sh.reason;
     A.out->rn = sh.rn;
   }
+  return true;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kPT, 1) ir_solve_persistent(PSolveArgs<T> A) {
+  __shared__ PShared sh;
+  const Grp g{(int)blockIdx.x, (int)gridDim.x, A.bar, A.err};
+  solve_body(A, g, sh, A.part);
 }
 
 }  // namespace
