@@ -65,7 +65,7 @@ class ApcProfile(C.Structure):
                 ("gfd_ms", C.c_double), ("mg_build_ms", C.c_double), ("mg_solve_ms", C.c_double),
                 ("mg_iterations", C.c_int64), ("assemble_ms", C.c_double), ("density_ms", C.c_double),
                 ("potential_ms", C.c_double), ("graph_instantiations", C.c_int64), ("graph_updates", C.c_int64),
-                ("sort_retries", C.c_int64)]
+                ("sort_retries", C.c_int64), ("mg_bytes", C.c_double)]
 
 
 class ApcStepParams(C.Structure):

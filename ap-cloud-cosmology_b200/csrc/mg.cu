@@ -1954,6 +1954,41 @@ static int persistent_solve(apc_context *c, const IrSolveArgs<T> &a, int blocks)
   return APC_OK;
 }
 
+// Algorithmic bytes of one multigrid solve (apc_profile.mg_bytes): every array a phase
+// reads or writes, counted once per phase; S = sizeof(T), ELL rows cost w (S + 4).
+//   refinement step: FP64 residual (w 12 + b, x, r), v_0 (r, D, v_0), solution update
+//     (the cycle's basis vectors + x read and written);
+//   Arnoldi step with j earlier basis vectors (j averaged over the cycles): SpMV (ELL, z,
+//     w written), dots (w + j + 1 vectors), Gram-Schmidt update (w, j + 1 vectors, w);
+//   V-cycle, per grid level of n rows: two-sweep pre-smoothing (ELL, b, D^-1, x written),
+//     residual + restriction (ELL, x, b, coarse b written), prolongation + sweep (ELL, x,
+//     b, D^-1, aggregate map, coarse x, out), each further sweep (ELL, x, b, D^-1, out);
+//   the single-block tail: the same per level, from L2.
+template <class T>
+static double solve_bytes(const MgHier<T> &H, bool use_mg, int n, int w, int sweeps, int total_its, int outer) {
+  const double S = sizeof(T), N = n;
+  const double cyc = outer > 0 ? (double)total_its / outer : 0.0;
+  const double jbar = cyc > 0 ? 0.5 * (cyc - 1.0) : 0.0;
+  const double per_outer = N * (w * 12.0 + 24.0) + N * (16.0 + S) + N * (cyc * S + 16.0);
+  double per_it = N * (w * (S + 4) + 2 * S) + N * (jbar + 2) * S + N * (jbar + 3) * S;
+  if (use_mg) {
+    for (int l = 0; l < H.nlev; ++l) {
+      const MgLevel<T> &L = H.lv[l];
+      const double nl = L.n, ell = L.w * (S + 4);
+      const double nc = l + 1 < H.nlev ? H.lv[l + 1].n : 0.0;
+      if (l + 1 < H.nlev) {
+        per_it += nl * (ell + 3 * S);                   // pre-smoothing
+        per_it += nl * (ell + 2 * S) + nc * S;          // residual + restriction
+        per_it += nl * (ell + 4 * S + 4) + nc * S;      // prolongation + sweep
+        per_it += (sweeps - 1) * nl * (ell + 3 * S);    // further sweeps
+      } else {
+        per_it += 2.0 * nl * nl * S;                    // dense coarsest solve (inverse, b, x)
+      }
+    }
+  }
+  return outer * per_outer + total_its * per_it;
+}
+
 template <class T>
 static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, const T *valf, const double *b,
                     double *x, double *r, int restart, double rtol_in, int *its, double *rnorm, int *reason,
@@ -2049,6 +2084,8 @@ static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, c
       if (use_mg) {
         c->prof.mg_solve_ms += ms;
         c->prof.mg_iterations += R.total_its;
+        c->prof.mg_bytes += solve_bytes<T>(H, true, n, c->ell_w, c->cfg.mg_sweeps > 0 ? c->cfg.mg_sweeps : 2,
+                                           R.total_its, R.outer);
       }
       return APC_OK;
     }
@@ -2076,6 +2113,8 @@ static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, c
   if (use_mg) {
     c->prof.mg_solve_ms += ms;
     c->prof.mg_iterations += S.total_its;
+    c->prof.mg_bytes += solve_bytes<T>(H, true, n, c->ell_w, c->cfg.mg_sweeps > 0 ? c->cfg.mg_sweeps : 2,
+                                       S.total_its, S.outer);
   }
   return APC_OK;
 }

@@ -215,6 +215,10 @@ typedef struct apc_profile {
   int64_t graph_updates;         /* solve graphs updated in place from a new capture */
   int64_t sort_retries;  /* selections that went deeper than the particle sort and were redone
                             after a sort over every key bit */
+  double mg_bytes;       /* algorithmic bytes of the multigrid-preconditioned solves counted in
+                            mg_solve_ms: every array a phase must read or write, once per phase
+                            (ELL values + columns, vectors, aggregation maps), summed over the
+                            V-cycles, Arnoldi steps and FP64 refinement steps that ran */
 } apc_profile;
 int apc_get_profile(apc_context *ctx, apc_profile *out);
 int apc_reset_profile(apc_context *ctx);
