@@ -28,8 +28,10 @@ def load_tuned(path: str = TUNED_PATH) -> dict | None:
 class BatchRun:
     """A set of RunConfigs stepped together through binding.BatchPath."""
 
-    def __init__(self, cfgs, precision: int = binding.APC_PREC_MIXED, n_workers: int = 0, tuned=None, **kw):
-        """tuned: optional {n_particles: dict of make_config keywords} from autotune()."""
+    def __init__(self, cfgs, precision: int = binding.APC_PREC_MIXED, n_workers: int = 0, tuned=None,
+                 solve_mode: int = binding.APC_BATCH_SOLVE_PER_BOX, **kw):
+        """tuned: optional {n_particles: dict of make_config keywords} from autotune();
+        solve_mode: per-box solves, or one queued launch per solve phase for all boxes."""
         self.cfgs = list(cfgs)
         boxes = []
         for c in self.cfgs:
@@ -38,7 +40,7 @@ class BatchRun:
             if tuned and c.n in tuned:
                 opts.update(tuned[c.n])
             boxes.append((c.particles(), opts))
-        self.path = binding.BatchPath(boxes, n_workers=n_workers)
+        self.path = binding.BatchPath(boxes, n_workers=n_workers, solve_mode=solve_mode)
         self.ctl = [Controller(g, c.n, c.omega0, c.omegal, c.a_start, c.a_end, c.delta_a)
                     for g, c in zip(self.path.boxes, self.cfgs)]
 

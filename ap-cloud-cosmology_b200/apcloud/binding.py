@@ -20,6 +20,8 @@ APC_PREC_MIXED = 1
 APC_PREC_FP64_MULTIGRID = 2
 APC_PRECOND_JACOBI = 0
 APC_PRECOND_MULTIGRID = 1
+APC_BATCH_SOLVE_PER_BOX = 0
+APC_BATCH_SOLVE_QUEUED = 1
 
 EXPORTED = [
     "apc_config_default", "apc_status_string", "apc_last_error", "apc_create", "apc_destroy",
@@ -31,7 +33,7 @@ EXPORTED = [
     "apc_batch_create", "apc_batch_destroy", "apc_batch_size", "apc_batch_context", "apc_batch_step",
     "apc_get_hessians_device", "apc_vjp_kick_drift", "apc_trajectory_vjp", "apc_fields_from_rhs",
     "apc_solve_vjp", "apc_max_cell_density", "apc_adaptive_dt", "apc_config_from_options",
-    "apc_device_code_version", "apc_check_bounded_wait",
+    "apc_device_code_version", "apc_check_bounded_wait", "apc_batch_set_solve_mode", "apc_batch_solve_ms",
 ]
 
 
@@ -144,6 +146,8 @@ def load_library(path: str = LIB_PATH):
                                          C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
         "apc_device_code_version": (C.c_int, [C.c_int, ip, ip]),
         "apc_check_bounded_wait": (C.c_int, [C.c_int, C.c_int]),
+        "apc_batch_set_solve_mode": (C.c_int, [vp, C.c_int]),
+        "apc_batch_solve_ms": (C.c_float, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -431,8 +435,9 @@ class GpuPath:
 class BatchPath:
     """Independent boxes stepped together through apc_batch_step (one context each)."""
 
-    def __init__(self, boxes, n_workers: int = 0):
-        """boxes: sequence of (Particles, dict of make_config keywords incl. depth, gfd_c)."""
+    def __init__(self, boxes, n_workers: int = 0, solve_mode: int = APC_BATCH_SOLVE_PER_BOX):
+        """boxes: sequence of (Particles, dict of make_config keywords incl. depth, gfd_c);
+        solve_mode: APC_BATCH_SOLVE_PER_BOX or APC_BATCH_SOLVE_QUEUED (apc_batch_set_solve_mode)."""
         self.lib = load_library()
         n = len(boxes)
         cfgs = (ApcConfig * n)()
@@ -445,6 +450,9 @@ class BatchPath:
             raise ApcError(rc, "apc_batch_create", self.lib.apc_status_string(rc).decode())
         self.h = h
         self.cfgs = cfgs
+        rc = self.lib.apc_batch_set_solve_mode(h, solve_mode)
+        if rc != 0:
+            raise ApcError(rc, "apc_batch_set_solve_mode", self.lib.apc_status_string(rc).decode())
         self.boxes = [GpuPath.view(self.lib, C.c_void_p(self.lib.apc_batch_context(h, i)), cfgs[i]) for i in range(n)]
         for g, (parts, _) in zip(self.boxes, boxes):
             arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in parts.as_tuple()]
@@ -452,6 +460,10 @@ class BatchPath:
 
     def __len__(self) -> int:
         return len(self.boxes)
+
+    def solve_ms(self) -> float:
+        """Device time of the last step's queued solve launches (0 in per-box mode)."""
+        return float(self.lib.apc_batch_solve_ms(self.h))
 
     def step(self, params):
         """params: one (dt, c_dens, c_pot, c_field, c_vel, c_pos) per box."""

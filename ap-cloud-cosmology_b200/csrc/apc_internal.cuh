@@ -141,6 +141,10 @@ struct apc_context {
   double rot[9] = {0};       // octant rotation (solver.cpp:464-475), host-computed
   KrylovWork *kw = nullptr;
   MgWork *mg = nullptr;
+  // batched solves (apc_batch_step): the mixed solves are prepared here and run in one
+  // launch with the other boxes' (defer_solve); batch_ev marks the prepared state
+  bool defer_solve = false;
+  cudaEvent_t batch_ev = nullptr;
   apc_solve_stats stats{};
 
   // ---- timing ----
@@ -206,6 +210,22 @@ int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, cons
 // and builds the multigrid hierarchy on a second stream, and makes the context's stream
 // wait for it; the potential solve then uses the prebuilt hierarchy (apc_mg_prebuilt)
 // instead of building its own.
+// Solves of many contexts in one persistent launch (mg.cu): each context, with
+// defer_solve set, prepares its solve in apc_krylov_solve and records batch_ev; one
+// cooperative kernel then runs every prepared solve, its block groups pulling boxes from a
+// device work queue, largest first; apc_ir_finish reads each context's outcome.
+struct BatchSolveBuf;
+BatchSolveBuf *apc_batch_solve_buf_create(int device);
+void apc_batch_solve_buf_free(BatchSolveBuf *b);
+int apc_mg_batched_solve(apc_context *const *ctx, int n, BatchSolveBuf *buf, cudaStream_t s, float *ms);
+int apc_ir_finish(apc_context *c, int *its, double *rnorm, int *reason, int *refinements);
+// apc_solve in three parts (capi.cu): assembly + density solve; potential rhs + potential
+// solve; differentiation + bookkeeping.  With defer_solve the solves are only prepared and
+// each following part starts by reading the prepared solve's outcome.
+int apc_solve_part_density(apc_context *c, double c_dens);
+int apc_solve_part_potential(apc_context *c, double c_pot);
+int apc_solve_part_fields(apc_context *c, double c_field);
+int apc_step_move(apc_context *c, const apc_step_params *p, double *max_dv, double *max_dx);
 int apc_mg_mark_assembled(apc_context *c);
 int apc_mg_prebuild(apc_context *c);
 bool apc_mg_prebuilt(const apc_context *c);

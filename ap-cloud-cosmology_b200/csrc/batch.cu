@@ -29,14 +29,38 @@ namespace {
 constexpr size_t kStackBytes = 8u << 20;  // per box; pages are committed only when touched
 constexpr size_t kGuardBytes = 64u << 10; // no-access guard below each stack
 
+struct Fiber;
+using FiberFn = int (*)(Fiber *);
+
 struct Fiber {
   ucontext_t uc;
   bool done = false;
   apc_context *ctx = nullptr;
   const apc_step_params *params = nullptr;
+  FiberFn fn = nullptr;  // the work this fiber runs (a whole step, or one part of it)
   int status = APC_OK;
+  int n_cells = 0;
   double dv = 0.0, dx = 0.0;
 };
+
+int whole_step(Fiber *f) { return apc_step(f->ctx, f->params, &f->n_cells, &f->dv, &f->dx); }
+
+// the three parts of a step around the two batched solve launches
+int part_select_density(Fiber *f) {
+  f->ctx->defer_solve = true;
+  APC_TRY(apc_select(f->ctx, &f->n_cells));
+  APC_TRY(apc_solve_part_density(f->ctx, f->params->c_dens));
+  return cudaEventRecord(f->ctx->batch_ev, f->ctx->s) == cudaSuccess ? APC_OK : APC_ERR_CUDA;
+}
+int part_potential(Fiber *f) {
+  APC_TRY(apc_solve_part_potential(f->ctx, f->params->c_pot));
+  return cudaEventRecord(f->ctx->batch_ev, f->ctx->s) == cudaSuccess ? APC_OK : APC_ERR_CUDA;
+}
+int part_fields_move(Fiber *f) {
+  APC_TRY(apc_solve_part_fields(f->ctx, f->params->c_field));
+  f->ctx->defer_solve = false;
+  return apc_step_move(f->ctx, f->params, &f->dv, &f->dx);
+}
 
 struct Sched {
   ucontext_t main;
@@ -47,7 +71,7 @@ thread_local Sched *t_sched = nullptr;
 
 void fiber_main() {
   Fiber *f = t_sched->cur;
-  f->status = apc_step(f->ctx, f->params, nullptr, &f->dv, &f->dx);
+  f->status = f->fn(f);
   f->done = true;
 }  // returning resumes uc_link, the scheduler
 
@@ -113,7 +137,64 @@ struct apc_batch {
   int threads = 1;
   char *stack_base = nullptr;  // n_boxes stacks of kStackBytes, guard page first
   size_t stack_bytes = 0;
+  int solve_mode = APC_BATCH_SOLVE_PER_BOX;
+  BatchSolveBuf *sbuf = nullptr;  // the batched solves' queue, barriers and partial sums
+  cudaStream_t bstream = nullptr;
+  float last_solve_ms = 0.f;      // device time of the last step's two batched launches
 };
+
+namespace {
+
+// every box runs fn as a fiber, boxes dealt to the host threads largest first
+void run_all(apc_batch *b, std::vector<Fiber> &fib, FiberFn fn) {
+  const int n = (int)b->ctx.size();
+  for (int i = 0; i < n; ++i) {
+    fib[i].done = false;
+    fib[i].fn = fn;
+  }
+  const int T = b->threads;
+  auto work = [&](int t) {
+    std::vector<Fiber *> mine;
+    std::vector<char *> stacks;
+    for (int k = t; k < n; k += T) {
+      const int i = b->order[k];
+      if (fib[i].status != APC_OK) continue;  // a box that failed sits out the rest of the step
+      mine.push_back(&fib[i]);
+      stacks.push_back(b->stack_base + kStackBytes * (size_t)i);
+    }
+    run_fibers(mine, stacks);
+  };
+  if (T <= 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> pool;
+    pool.reserve(T - 1);
+    for (int t = 1; t < T; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (std::thread &th : pool) th.join();
+  }
+}
+
+// one launch for the prepared solves of every box still running
+void batched_solve(apc_batch *b, std::vector<Fiber> &fib, float *ms) {
+  std::vector<apc_context *> live;
+  for (size_t i = 0; i < fib.size(); ++i)
+    if (fib[i].status == APC_OK) live.push_back(b->ctx[i]);
+  if (live.empty()) return;
+  cudaSetDevice(live[0]->dev);
+  float t = 0.f;
+  const int rc = apc_mg_batched_solve(live.data(), (int)live.size(), b->sbuf, b->bstream, &t);
+  *ms += t;
+  if (rc != APC_OK)
+    for (size_t i = 0; i < fib.size(); ++i)
+      if (fib[i].status == APC_OK) {
+        fib[i].status = rc;
+        b->ctx[i]->defer_solve = false;
+        b->ctx[i]->err = "batched solve launch failed";
+      }
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -146,6 +227,12 @@ int apc_batch_create(const apc_config *cfgs, int n_boxes, int n_workers, apc_bat
   std::stable_sort(b->order.begin(), b->order.end(),
                    [&](int a, int c) { return cfgs[a].n_particles > cfgs[c].n_particles; });
   b->threads = n_workers > 0 ? std::min(n_workers, n_boxes) : std::min(n_boxes, 16);
+  for (apc_context *c : b->ctx)
+    if (cudaEventCreateWithFlags(&c->batch_ev, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      apc_batch_destroy(b);
+      return APC_ERR_CUDA;
+    }
   *out = b;
   return APC_OK;
 }
@@ -154,6 +241,8 @@ int apc_batch_destroy(apc_batch *b) {
   if (!b) return APC_ERR_INVALID_ARG;
   for (apc_context *c : b->ctx)
     if (c) apc_destroy(c);
+  if (b->bstream) cudaStreamDestroy(b->bstream);
+  apc_batch_solve_buf_free(b->sbuf);
   if (b->stack_base) munmap(b->stack_base, b->stack_bytes);
   delete b;
   return APC_OK;
@@ -166,6 +255,24 @@ apc_context *apc_batch_context(apc_batch *b, int box) {
   return b->ctx[box];
 }
 
+int apc_batch_set_solve_mode(apc_batch *b, int mode) {
+  if (!b || (mode != APC_BATCH_SOLVE_PER_BOX && mode != APC_BATCH_SOLVE_QUEUED)) return APC_ERR_INVALID_ARG;
+  if (mode == APC_BATCH_SOLVE_QUEUED && !b->sbuf) {
+    const int dev = b->ctx[0]->dev;
+    cudaSetDevice(dev);
+    b->sbuf = apc_batch_solve_buf_create(dev);
+    if (!b->sbuf) return APC_ERR_OUT_OF_MEMORY;
+    if (cudaStreamCreateWithFlags(&b->bstream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      return APC_ERR_CUDA;
+    }
+  }
+  b->solve_mode = mode;
+  return APC_OK;
+}
+
+float apc_batch_solve_ms(const apc_batch *b) { return b ? b->last_solve_ms : 0.f; }
+
 int apc_batch_step(apc_batch *b, const apc_step_params *params, int *status, double *max_dv, double *max_dx) {
   if (!b || !params) return APC_ERR_INVALID_ARG;
   const int n = (int)b->ctx.size();
@@ -174,25 +281,19 @@ int apc_batch_step(apc_batch *b, const apc_step_params *params, int *status, dou
     fib[i].ctx = b->ctx[i];
     fib[i].params = &params[i];
   }
-  const int T = b->threads;
-  auto work = [&](int t) {
-    std::vector<Fiber *> mine;
-    std::vector<char *> stacks;
-    for (int k = t; k < n; k += T) {
-      const int i = b->order[k];
-      mine.push_back(&fib[i]);
-      stacks.push_back(b->stack_base + kStackBytes * (size_t)i);
-    }
-    run_fibers(mine, stacks);
-  };
-  if (T <= 1) {
-    work(0);
+  if (b->solve_mode == APC_BATCH_SOLVE_QUEUED) {
+    // select + assembly + density solve prepared; one launch; potential rhs + potential
+    // solve prepared; one launch; differentiation + kick + drift
+    float ms = 0.f;
+    run_all(b, fib, part_select_density);
+    batched_solve(b, fib, &ms);
+    run_all(b, fib, part_potential);
+    batched_solve(b, fib, &ms);
+    run_all(b, fib, part_fields_move);
+    b->last_solve_ms = ms;
+    for (int i = 0; i < n; ++i) b->ctx[i]->defer_solve = false;
   } else {
-    std::vector<std::thread> pool;
-    pool.reserve(T - 1);
-    for (int t = 1; t < T; ++t) pool.emplace_back(work, t);
-    work(0);
-    for (std::thread &th : pool) th.join();
+    run_all(b, fib, whole_step);
   }
   int first = APC_OK;
   for (int i = 0; i < n; ++i) {

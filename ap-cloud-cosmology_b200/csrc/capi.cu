@@ -137,6 +137,7 @@ void free_all(apc_context *c) {
   for (auto &e : c->kev)
     if (e) cudaEventDestroy(e);
   if (c->wait_ev) cudaEventDestroy(c->wait_ev);
+  if (c->batch_ev) cudaEventDestroy(c->batch_ev);
   for (auto &e : c->gev)
     if (e) cudaEventDestroy(e);
   for (auto &e : c->sev)
@@ -408,13 +409,17 @@ int apc_select(apc_context *c, int *n_cells) {
   return APC_OK;
 }
 
-int apc_solve(apc_context *c, double c_dens, double c_pot, double c_field) {
+}  // extern "C"
+
+// The solve phase in three parts, so that a batch can run every box's density solve, and
+// then every potential solve, in one launch (batch.cu).  With ctx->defer_solve the mixed
+// solves are only prepared by apc_krylov_solve, and the next part reads their outcome.
+int apc_solve_part_density(apc_context *c, double c_dens) {
   APC_TRY(check_ready(c, true, true, false));
   cudaSetDevice(c->dev);
   c->err.clear();
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[2], c->s));
   APC_TRY(apc_gfd_assemble(c, c_dens));
-  const int M = c->nc + c->nv;
   if (c->cfg.precision == APC_PREC_MIXED) {
     APC_TRY(apc_ensure(c, &c->a1f, (size_t)c->m_cap * c->ell_w, nullptr));
     APC_TRY(apc_ensure(c, &c->a2f, (size_t)c->m_cap * c->ell_w, nullptr));
@@ -429,17 +434,31 @@ int apc_solve(apc_context *c, double c_dens, double c_pot, double c_field) {
   APC_CUDA_TRY(c, cudaEventRecord(c->sev[0], c->s));
   APC_TRY(apc_krylov_solve(c, 0, c->rhs, c->density, &st.density_its, &st.density_rnorm, &st.density_reason,
                            &st.density_refinements, overlap ? apc_mg_prebuild : nullptr));
+  return APC_OK;
+}
+
+int apc_solve_part_potential(apc_context *c, double c_pot) {
+  apc_solve_stats &st = c->stats;
+  if (c->defer_solve)
+    APC_TRY(apc_ir_finish(c, &st.density_its, &st.density_rnorm, &st.density_reason, &st.density_refinements));
   APC_CUDA_TRY(c, cudaEventRecord(c->sev[1], c->s));
   APC_TRY(apc_potential_rhs(c, c_pot));
   APC_CUDA_TRY(c, cudaEventRecord(c->sev[2], c->s));
   APC_TRY(apc_krylov_solve(c, 1, c->rhs, c->potential, &st.potential_its, &st.potential_rnorm,
                            &st.potential_reason, &st.potential_refinements));
+  c->last_c_pot = c_pot;
+  return APC_OK;
+}
+
+int apc_solve_part_fields(apc_context *c, double c_field) {
+  apc_solve_stats &st = c->stats;
+  if (c->defer_solve)
+    APC_TRY(apc_ir_finish(c, &st.potential_its, &st.potential_rnorm, &st.potential_reason,
+                          &st.potential_refinements));
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[7], c->s));
   APC_TRY(apc_differentiate(c, c_field));
   if (c->cfg.precision != APC_PREC_FP64 && c->cfg.warm_start) APC_TRY(apc_warm_save(c));
-  c->last_c_pot = c_pot;
   c->last_c_field = c_field;
-  (void)M;
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[3], c->s));
   APC_CUDA_TRY(c, apc_event_wait(c->ev[3]));
   c->t_solve_ms = elapsed(c->ev[2], c->ev[3]);
@@ -450,6 +469,30 @@ int apc_solve(apc_context *c, double c_dens, double c_pot, double c_field) {
   c->prof.steps += 1;
   c->have_fields = true;
   return APC_OK;
+}
+
+// move_velocity + move_position (mover.cpp:51-121) as one fused pass over the particles
+int apc_step_move(apc_context *c, const apc_step_params *p, double *max_dv, double *max_dx) {
+  APC_CUDA_TRY(c, cudaEventRecord(c->ev[4], c->s));
+  APC_TRY(apc_mover_kick_drift(c, p->dt, p->c_vel, p->c_pos, max_dv, max_dx));
+  APC_CUDA_TRY(c, cudaEventRecord(c->ev[6], c->s));
+  APC_CUDA_TRY(c, apc_event_wait(c->ev[6]));
+  c->t_move_ms = elapsed(c->ev[4], c->ev[6]);
+  c->prof.move_ms += c->t_move_ms;
+  c->kick_recorded = false;
+  if (c->step_open) {
+    c->prof.step_ms += elapsed(c->ev[0], c->ev[6]);
+    c->step_open = false;
+  }
+  return APC_OK;
+}
+
+extern "C" {
+
+int apc_solve(apc_context *c, double c_dens, double c_pot, double c_field) {
+  APC_TRY(apc_solve_part_density(c, c_dens));
+  APC_TRY(apc_solve_part_potential(c, c_pot));
+  return apc_solve_part_fields(c, c_field);
 }
 
 int apc_move_velocity(apc_context *c, double dt, double c_vel, double *max_dv) {
@@ -484,19 +527,7 @@ int apc_step(apc_context *c, const apc_step_params *p, int *n_cells, double *max
   if (!p) return APC_ERR_INVALID_ARG;
   APC_TRY(apc_select(c, n_cells));
   APC_TRY(apc_solve(c, p->c_dens, p->c_pot, p->c_field));
-  // move_velocity + move_position (mover.cpp:51-121) as one fused pass over the particles
-  APC_CUDA_TRY(c, cudaEventRecord(c->ev[4], c->s));
-  APC_TRY(apc_mover_kick_drift(c, p->dt, p->c_vel, p->c_pos, max_dv, max_dx));
-  APC_CUDA_TRY(c, cudaEventRecord(c->ev[6], c->s));
-  APC_CUDA_TRY(c, apc_event_wait(c->ev[6]));
-  c->t_move_ms = elapsed(c->ev[4], c->ev[6]);
-  c->prof.move_ms += c->t_move_ms;
-  c->kick_recorded = false;
-  if (c->step_open) {
-    c->prof.step_ms += elapsed(c->ev[0], c->ev[6]);
-    c->step_open = false;
-  }
-  return APC_OK;
+  return apc_step_move(c, p, max_dv, max_dx);
 }
 
 int apc_synchronize(apc_context *c) {

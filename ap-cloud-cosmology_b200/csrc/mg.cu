@@ -1285,6 +1285,34 @@ __global__ void __launch_bounds__(kPT, 1) ir_solve_persistent(PSolveArgs<T> A) {
   solve_body(A, g, sh, A.part);
 }
 
+// The solves of a batch of boxes in one cooperative launch.  The blocks form groups of
+// gsize blocks; each group takes the next box from a device work queue (the boxes are
+// queued largest first), copies its arguments to shared memory, runs its whole solve with
+// the group's own barrier and partial sums, and takes the next box until none is left.
+template <class T>
+__global__ void __launch_bounds__(kPT, 1) ir_solve_batched(const PSolveArgs<T> *__restrict__ boxes, int nbox,
+                                                          int gsize, int *queue, int *slot, GridBar *bars,
+                                                          double *parts, int *err) {
+  __shared__ PShared sh;
+  __shared__ PSolveArgs<T> A;
+  const int grp = blockIdx.x / gsize;
+  const Grp g{(int)(blockIdx.x % gsize), gsize, bars + grp, err};
+  double *part = parts + (size_t)grp * kPSlots * kPMaxBlocks;
+  for (;;) {
+    if (g.rank == 0 && threadIdx.x == 0) slot[grp] = atomicAdd(queue, 1);
+    if (!gsync(g)) return;  // publishes the slot to the group
+    const int b = __ldcg(slot + grp);
+    if (b >= nbox) return;
+    static_assert(sizeof(PSolveArgs<T>) % sizeof(int) == 0, "argument block copied as words");
+    const int *src = reinterpret_cast<const int *>(boxes + b);
+    int *dst = reinterpret_cast<int *>(&A);
+    for (int k = threadIdx.x; k < (int)(sizeof(PSolveArgs<T>) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
+    __syncthreads();
+    if (!solve_body(A, g, sh, part)) return;
+    __syncthreads();  // the next box's arguments overwrite A
+  }
+}
+
 }  // namespace
 
 // The hierarchy and Krylov vectors of one inner precision T: float for the mixed path,
@@ -1341,6 +1369,12 @@ struct MgWork {
   GridBar *pbar = nullptr;
   PResult *pres = nullptr;
   PResult *pres_host = nullptr;
+  // a solve prepared for a batched launch (apc_mg_batched_solve): its arguments, which
+  // solve it is, and whether it is multigrid-preconditioned
+  PSolveArgs<float> deferred32{};
+  PSolveArgs<double> deferred64{};
+  int deferred_which = -1;
+  bool deferred_mg = false;
 };
 
 static MgWork *mg(apc_context *c) {
@@ -1357,6 +1391,17 @@ MgHier<float> &hier<float>(MgWork *m) {
 template <>
 MgHier<double> &hier<double>(MgWork *m) {
   return m->h64;
+}
+
+template <class T>
+PSolveArgs<T> &deferred(MgWork *m);
+template <>
+PSolveArgs<float> &deferred<float>(MgWork *m) {
+  return m->deferred32;
+}
+template <>
+PSolveArgs<double> &deferred<double>(MgWork *m) {
+  return m->deferred64;
 }
 
 template <class T>
@@ -1854,22 +1899,18 @@ static int capture_solve(apc_context *c, const IrSolveArgs<T> &a) {
 // hierarchy's levels and the tail; `blocks` blocks of kPT threads, co-resident by the
 // cooperative launch.  Returns APC_ERR_UNSUPPORTED when the kernel cannot be launched
 // co-resident (the caller then uses the graph path).
+// The persistent kernel's arguments for one prepared solve (buffers of the context).
 template <class T>
-static int persistent_solve(apc_context *c, const IrSolveArgs<T> &a, int blocks) {
+static int fill_psolve(apc_context *c, const IrSolveArgs<T> &a, PSolveArgs<T> &P) {
   MgWork *m = c->mg;
   MgHier<T> &H = hier<T>(m);
-  const void *kern = (const void *)ir_solve_persistent<T>;
-  int occ = 0;
-  APC_CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kPT, 0));
-  if (occ < 1) return APC_ERR_UNSUPPORTED;
-  blocks = std::max(1, std::min(blocks, std::min(kPMaxBlocks, apc_sm_count(c) * occ)));
   if (!m->ppart) {
     APC_TRY(apc_alloc(c, (void **)&m->ppart, sizeof(double) * (size_t)kPSlots * kPMaxBlocks));
     APC_TRY(apc_alloc(c, (void **)&m->pbar, sizeof(GridBar)));
     APC_TRY(apc_alloc(c, (void **)&m->pres, sizeof(PResult)));
   }
   if (!m->pres_host) APC_CUDA_TRY(c, cudaMallocHost((void **)&m->pres_host, sizeof(PResult)));
-  PSolveArgs<T> P{};
+  P = PSolveArgs<T>{};
   P.n = a.n;
   P.w = a.w;
   P.ld = a.ld;
@@ -1946,6 +1987,19 @@ static int persistent_solve(apc_context *c, const IrSolveArgs<T> &a, int blocks)
   P.bar = m->pbar;
   P.err = c->d_err;
   P.out = m->pres;
+  return APC_OK;
+}
+
+template <class T>
+static int persistent_solve(apc_context *c, const IrSolveArgs<T> &a, int blocks) {
+  MgWork *m = c->mg;
+  const void *kern = (const void *)ir_solve_persistent<T>;
+  int occ = 0;
+  APC_CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kPT, 0));
+  if (occ < 1) return APC_ERR_UNSUPPORTED;
+  blocks = std::max(1, std::min(blocks, std::min(kPMaxBlocks, apc_sm_count(c) * occ)));
+  PSolveArgs<T> P;
+  APC_TRY(fill_psolve<T>(c, a, P));
   APC_CUDA_TRY(c, cudaMemsetAsync(m->pbar, 0, sizeof(GridBar), c->s));
   APC_CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->s));
   void *args[] = {&P};
@@ -2049,6 +2103,22 @@ static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, c
   // one persistent kernel per solve unless the graph path is asked for (or needed: the
   // re-orthogonalising Gram-Schmidt runs only there)
   bool persistent = !cfg.mixed_solve_graphs && !cfg.mg_reorth;
+  if (persistent && c->defer_solve) {
+    // prepared for a batched launch with other boxes' solves (apc_mg_batched_solve);
+    // apc_ir_finish reads the outcome
+    if (use_mg)
+      c->prof.mg_build_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    APC_TRY(fill_psolve<T>(c, a, deferred<T>(m)));
+    m->deferred_which = which;
+    m->deferred_mg = use_mg;
+    if (during) APC_TRY(during(c));
+    *its = 0;
+    *rnorm = 0.0;
+    *reason = 0;
+    *refinements = 0;
+    *levels = use_mg ? H.nlev : 0;
+    return APC_OK;
+  }
   if (persistent) {
     // a density solve overlapped with the potential's hierarchy build keeps half of the
     // SMs free for it
@@ -2167,4 +2237,173 @@ bool apc_mg_prebuilt(const apc_context *c) { return c->mg && c->mg->prebuilt; }
 
 void apc_mg_clear_prebuilt(apc_context *c) {
   if (c->mg) c->mg->prebuilt = false;
+}
+
+// ------------------------------------------------ batched solves across boxes (C4)
+
+struct BatchSolveBuf {
+  int dev = 0;
+  void *args = nullptr;        // device copy of the boxes' PSolveArgs, queue order
+  void *args_host = nullptr;   // pinned staging
+  size_t args_bytes = 0;
+  int *queue = nullptr;        // [0] next box; [1..] the groups' current slots
+  GridBar *bars = nullptr;     // one barrier per group
+  double *parts = nullptr;     // one [slot][block] partial-sum area per group
+  int *err = nullptr;          // barrier time-out flag of the launch
+  int *err_host = nullptr;
+  int max_groups = 0;
+  cudaEvent_t ev[2] = {nullptr, nullptr};  // around the launch (timing)
+};
+
+BatchSolveBuf *apc_batch_solve_buf_create(int device) {
+  BatchSolveBuf *b = new BatchSolveBuf();
+  b->dev = device;
+  int sms = 1;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  b->max_groups = std::max(1, sms);
+  bool ok = cudaMalloc((void **)&b->queue, sizeof(int) * (b->max_groups + 1)) == cudaSuccess &&
+            cudaMalloc((void **)&b->bars, sizeof(GridBar) * b->max_groups) == cudaSuccess &&
+            cudaMalloc((void **)&b->parts, sizeof(double) * (size_t)kPSlots * kPMaxBlocks * b->max_groups) ==
+                cudaSuccess &&
+            cudaMalloc((void **)&b->err, sizeof(int)) == cudaSuccess &&
+            cudaMallocHost((void **)&b->err_host, sizeof(int)) == cudaSuccess &&
+            cudaEventCreate(&b->ev[0]) == cudaSuccess && cudaEventCreate(&b->ev[1]) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    apc_batch_solve_buf_free(b);
+    return nullptr;
+  }
+  return b;
+}
+
+void apc_batch_solve_buf_free(BatchSolveBuf *b) {
+  if (!b) return;
+  cudaFree(b->args);
+  cudaFreeHost(b->args_host);
+  cudaFree(b->queue);
+  cudaFree(b->bars);
+  cudaFree(b->parts);
+  cudaFree(b->err);
+  cudaFreeHost(b->err_host);
+  for (cudaEvent_t e : b->ev)
+    if (e) cudaEventDestroy(e);
+  delete b;
+}
+
+// One cooperative launch for the prepared solves of the given contexts (all of the same
+// inner precision T), on stream s after each context's ready event; boxes are queued
+// largest first.  Group size: the share of the SMs the largest box would get if every
+// block worked on rows in proportion, at least one block.
+template <class T>
+static int batched_launch(apc_context *const *ctx, int n, BatchSolveBuf *B, cudaStream_t s, float *ms) {
+  std::vector<int> order(n);
+  long long total = 0, nmax = 1;
+  for (int i = 0; i < n; ++i) {
+    order[i] = i;
+    const long long rows = deferred<T>(ctx[i]->mg).n;
+    total += rows;
+    nmax = std::max(nmax, rows);
+  }
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return deferred<T>(ctx[a]->mg).n > deferred<T>(ctx[b]->mg).n; });
+  const void *kern = (const void *)ir_solve_batched<T>;
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kPT, 0) != cudaSuccess || occ < 1) {
+    cudaGetLastError();
+    return APC_ERR_UNSUPPORTED;
+  }
+  int sms = 1;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B->dev);
+  const int blocks_all = sms * occ;
+  int gsize = (int)std::min<long long>(blocks_all, (blocks_all * nmax + total - 1) / std::max(1ll, total));
+  gsize = std::max(1, std::min(gsize, std::min(kPMaxBlocks, (int)((nmax + kPT - 1) / kPT))));
+  const int groups = std::max(1, std::min(B->max_groups, blocks_all / gsize));
+  const size_t bytes = sizeof(PSolveArgs<T>) * (size_t)n;
+  if (bytes > B->args_bytes) {
+    cudaFree(B->args);
+    cudaFreeHost(B->args_host);
+    B->args = B->args_host = nullptr;
+    B->args_bytes = 0;
+    if (cudaMalloc(&B->args, bytes) != cudaSuccess || cudaMallocHost(&B->args_host, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return APC_ERR_OUT_OF_MEMORY;
+    }
+    B->args_bytes = bytes;
+  }
+  PSolveArgs<T> *h = static_cast<PSolveArgs<T> *>(B->args_host);
+  for (int k = 0; k < n; ++k) h[k] = deferred<T>(ctx[order[k]]->mg);
+  for (int i = 0; i < n; ++i)
+    if (cudaStreamWaitEvent(s, ctx[i]->batch_ev, 0) != cudaSuccess) return APC_ERR_CUDA;
+  bool ok = cudaMemcpyAsync(B->args, B->args_host, bytes, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+            cudaMemsetAsync(B->queue, 0, sizeof(int) * (groups + 1), s) == cudaSuccess &&
+            cudaMemsetAsync(B->bars, 0, sizeof(GridBar) * groups, s) == cudaSuccess &&
+            cudaMemsetAsync(B->err, 0, sizeof(int), s) == cudaSuccess && cudaEventRecord(B->ev[0], s) == cudaSuccess;
+  if (!ok) return APC_ERR_CUDA;
+  const PSolveArgs<T> *dargs = static_cast<const PSolveArgs<T> *>(B->args);
+  int *queue = B->queue, *slot = B->queue + 1;
+  GridBar *bars = B->bars;
+  double *parts = B->parts;
+  int *err = B->err;
+  int nbox = n;
+  void *kargs[] = {(void *)&dargs, &nbox, &gsize, &queue, &slot, &bars, &parts, &err};
+  if (cudaLaunchCooperativeKernel(kern, dim3(groups * gsize), dim3(kPT), kargs, 0, s) != cudaSuccess) {
+    cudaGetLastError();
+    return APC_ERR_CUDA;
+  }
+  if (cudaEventRecord(B->ev[1], s) != cudaSuccess ||
+      cudaMemcpyAsync(B->err_host, B->err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return APC_ERR_CUDA;
+  float t = 0.f;
+  cudaEventElapsedTime(&t, B->ev[0], B->ev[1]);
+  if (ms) *ms = t;
+  for (int i = 0; i < n; ++i) ctx[i]->launches += 1;
+  return (*B->err_host & DERR_KRYLOV) ? APC_ERR_TIMEOUT : APC_OK;
+}
+
+int apc_mg_batched_solve(apc_context *const *ctx, int n, BatchSolveBuf *B, cudaStream_t s, float *ms) {
+  if (!B || n <= 0) return APC_ERR_INVALID_ARG;
+  std::vector<apc_context *> f32, f64;
+  for (int i = 0; i < n; ++i) {
+    if (!ctx[i]->mg || ctx[i]->mg->deferred_which < 0) continue;
+    (ctx[i]->cfg.precision == APC_PREC_FP64_MULTIGRID ? f64 : f32).push_back(ctx[i]);
+  }
+  float t = 0.f, total = 0.f;
+  if (!f32.empty()) {
+    APC_TRY(batched_launch<float>(f32.data(), (int)f32.size(), B, s, &t));
+    total += t;
+  }
+  if (!f64.empty()) {
+    APC_TRY(batched_launch<double>(f64.data(), (int)f64.size(), B, s, &t));
+    total += t;
+  }
+  if (ms) *ms = total;
+  return APC_OK;
+}
+
+// The outcome of the solve this context prepared for a batched launch, once the launch has
+// completed: its iteration count, residual, reason and refinements; the profile counts its
+// iterations and algorithmic bytes.  A no-op when no solve is pending.
+int apc_ir_finish(apc_context *c, int *its, double *rnorm, int *reason, int *refinements) {
+  MgWork *m = c->mg;
+  if (!m || m->deferred_which < 0) return APC_OK;  // the solve ran at once (FP64 GMRES path)
+  APC_CUDA_TRY(c, cudaMemcpyAsync(m->pres_host, m->pres, sizeof(PResult), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
+  const PResult &R = *m->pres_host;
+  *its = R.total_its;
+  *rnorm = R.rn;
+  *reason = R.reason;
+  *refinements = R.outer;
+  if (m->deferred_mg) {
+    c->prof.mg_iterations += R.total_its;
+    if (c->cfg.precision == APC_PREC_FP64_MULTIGRID) {
+      const PSolveArgs<double> &P = m->deferred64;
+      c->prof.mg_bytes += solve_bytes<double>(m->h64, true, P.n, P.w, P.sweeps, R.total_its, R.outer);
+    } else {
+      const PSolveArgs<float> &P = m->deferred32;
+      c->prof.mg_bytes += solve_bytes<float>(m->h32, true, P.n, P.w, P.sweeps, R.total_its, R.outer);
+    }
+  }
+  m->deferred_which = -1;
+  return APC_OK;
 }

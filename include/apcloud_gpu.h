@@ -369,6 +369,22 @@ apc_context *apc_batch_context(apc_batch *b, int box);
 int apc_batch_step(apc_batch *b, const apc_step_params *params, int *status, double *max_dv,
                    double *max_dx);
 
+/* How a batch step runs the boxes' multigrid solves.
+ *   APC_BATCH_SOLVE_PER_BOX (default): each box's step runs whole in its fiber, its solves
+ *     as its own persistent kernels; per-box results are those of a lone context, bit for bit.
+ *   APC_BATCH_SOLVE_QUEUED: the step runs in three parts over all boxes - selection, assembly
+ *     and the density solve's set-up; the potential rhs and the potential solve's set-up;
+ *     differentiation, kick and drift - and between the parts ONE cooperative kernel runs
+ *     every box's prepared solve: its block groups take boxes from a device work queue,
+ *     largest first, and solve each with group-local barriers.  Per-box results meet the
+ *     same stopping test as a lone context's (the sums run over other block counts, so they
+ *     agree to the solver's tolerance, not bit for bit).  Boxes on the FP64 GMRES path
+ *     (APC_PREC_FP64) solve at once in their fibers either way. */
+enum { APC_BATCH_SOLVE_PER_BOX = 0, APC_BATCH_SOLVE_QUEUED = 1 };
+int apc_batch_set_solve_mode(apc_batch *b, int mode);
+/* Device time (ms) of the last step's two queued solve launches (0 per box). */
+float apc_batch_solve_ms(const apc_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

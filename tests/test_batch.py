@@ -111,3 +111,41 @@ def test_batch_matches_single_contexts(workers):
         ref = np.stack(g.particles())
         g.close()
         assert np.array_equal(arr, ref), c.name
+
+
+@pytest.mark.gpu
+def test_queued_batch_solves_match_single_contexts():
+    """APC_BATCH_SOLVE_QUEUED: every box's density solve, then every potential solve, run in
+    one cooperative launch whose block groups take boxes from a device work queue.  Each
+    box meets the same stopping test as alone, with its sums over other block counts, so
+    the bar is the solver's accuracy: accelerations within 1e-6 RMS (the force-error bound)
+    and positions within 1e-9 after three steps, every box converged."""
+    from apcloud import binding
+    from apcloud.batch import BatchRun
+    from apcloud.controller import Controller
+
+    cfgs = ics.batch_boxes(n_boxes=12, seed=11, sides=(16, 24, 32))[:8]
+    steps = 3
+    br = BatchRun(cfgs, precision=binding.APC_PREC_MIXED, n_workers=4, solve_mode=binding.APC_BATCH_SOLVE_QUEUED)
+    br.start()
+    for _ in range(steps):
+        br.step()
+    assert br.path.solve_ms() > 0.0
+    got = [(np.stack(g.particles()), g.solve_stats()) for g in br.path.boxes]
+    br.close()
+    for c, (arr, st) in zip(cfgs, got):
+        assert st["density_reason"] == 2 and st["potential_reason"] == 2, (c.name, st)
+        g = binding.GpuPath(c.particles(), c.depth, c.gfd_c, c.lm, restart=c.restart, rtol=c.rtol,
+                            precision=binding.APC_PREC_MIXED)
+        ctl = Controller(g, c.n, c.omega0, c.omegal, c.a_start, c.a_end, c.delta_a)
+        ctl.start()
+        for _ in range(steps):
+            ctl.step()
+        ref = np.stack(g.particles())
+        g.close()
+        d = arr[:3] - ref[:3]
+        d -= np.round(d)
+        assert np.max(np.abs(d)) <= 1e-9, c.name
+        a, b = arr[6:9], ref[6:9]
+        rms = float(np.sqrt(np.mean(np.sum((a - b) ** 2, 0)) / np.mean(np.sum(b ** 2, 0))))
+        assert rms <= 1e-6, (c.name, rms)
