@@ -709,6 +709,7 @@ __device__ __forceinline__ void tail_rows(const TailLevel<V> &L, const V *xin, F
     const int i = (int)threadIdx.x / g + rd * per;
     V sacc = V(0);
     if (i < L.n)
+#pragma unroll 4
       for (int k = sub; k < L.w; k += g) {
         const size_t at = (size_t)k * L.ld + i;
         sacc += L.val[at] * xin[L.col[at]];
@@ -813,7 +814,7 @@ struct PLevel {
   const T *val, *dinv;
   const int *agg;             // node -> next coarser node
   const int *mptr, *mem;      // members (on the finer level) of this level's nodes
-  T *x, *x2, *b;
+  T *x, *x2, *b, *r;
 };
 
 struct PResult {
@@ -965,25 +966,30 @@ __device__ void p_sweep(const Grp &g, const PLevel<T> &L, const T *bsrc, T bs, T
   });
 }
 
-// the coarse right-hand side: bc[I] = sum over the members i of I of (b - A x)_i, one
-// warp per coarse row, members' entries taken 32 at a time in member-then-slot order
+// r = b - A x over the rows of L (G lanes per row, coalesced slot-major reads)
 template <class T>
-__device__ void p_residual_restrict(const Grp &g, const PLevel<T> &F, const T *bsrc, T bs, const T *x,
-                                    const PLevel<T> &C) {
-  const int lane = threadIdx.x & 31;
-  const int gw = (g.rank * blockDim.x + threadIdx.x) >> 5, nwarps = (g.size * blockDim.x) >> 5;
-  for (int I = gw; I < C.n; I += nwarps) {
-    const int a = C.mptr[I], e = (I + 1 < C.n) ? C.mptr[I + 1] : F.n;
-    const int cnt = (e - a) * F.w;
+__device__ void p_residual(const Grp &g, const PLevel<T> &L, const T *bsrc, T bs, const T *x, T *r) {
+  grid_rows(g, L, [&](int i, int sub, int G, bool act) {
     T s = T(0);
-    for (int t = lane; t < cnt; t += 32) {
-      const int i = C.mem[a + t / F.w], k = t % F.w;
-      const size_t at = (size_t)k * F.ld + i;
-      s -= F.val[at] * x[F.col[at]];
-    }
-    for (int t = lane; t < e - a; t += 32) s += bs * bsrc[C.mem[a + t]];
-    s = warp_sum(s);
-    if (lane == 0) C.b[I] = s;
+    if (act)
+#pragma unroll 4
+      for (int k = sub; k < L.w; k += G) {
+        const size_t at = (size_t)k * L.ld + i;
+        s += L.val[at] * x[L.col[at]];
+      }
+    s = group_sum(s, G);
+    if (act && sub == 0) r[i] = bs * bsrc[i] - s;
+  });
+}
+
+// the coarse right-hand side: bc[I] = sum of r over the members of I, in member order
+template <class T>
+__device__ void p_restrict(const Grp &g, int nf, const T *r, const PLevel<T> &C) {
+  for (int I = g.rank * blockDim.x + threadIdx.x; I < C.n; I += g.size * blockDim.x) {
+    const int a = C.mptr[I], e = (I + 1 < C.n) ? C.mptr[I + 1] : nf;
+    T s = T(0);
+    for (int q = a; q < e; ++q) s += r[C.mem[q]];
+    C.b[I] = s;
   }
 }
 
@@ -1020,7 +1026,9 @@ __device__ bool p_vcycle(const Grp &g, const PSolveArgs<T> &A, const T *bsrc, T 
       if (!gsync(g)) return false;
     }
     pre[l] = cur;
-    p_residual_restrict(g, L, bl, bsl, cur, A.L[l + 1]);
+    p_residual(g, L, bl, bsl, cur, L.r);
+    if (!gsync(g)) return false;
+    p_restrict(g, L.n, (const T *)L.r, A.L[l + 1]);
     if (!gsync(g)) return false;
   }
   // ---- the tail in block 0 ----
@@ -1948,6 +1956,7 @@ static int fill_psolve(apc_context *c, const IrSolveArgs<T> &a, PSolveArgs<T> &P
       D.x = Q.x;
       D.x2 = Q.x2;
       D.b = Q.b;
+      D.r = Q.r;
     }
     TailArgs<T> &TA = P.ta;
     TA.nl = std::min(H.nlev - P.tail, kTailLevels);
@@ -1960,9 +1969,10 @@ static int fill_psolve(apc_context *c, const IrSolveArgs<T> &a, PSolveArgs<T> &P
       TailLevel<T> &D = TA.L[k];
       D.n = Q.n;
       D.w = Q.w;
+      // lanes per row: each lane takes at most 8 of the row's slots (a row's slots are a
+      // chain of dependent gathers per lane), the block's rows then run in rounds
       D.g = 1;
-      if (Q.w > 24)
-        while (D.g < 8 && 2 * D.g * Q.n <= kPT) D.g *= 2;
+      while (D.g < 16 && D.g * 8 < Q.w) D.g *= 2;
       D.ld = Q.ld;
       D.col = Q.col;
       D.val = Q.val;
