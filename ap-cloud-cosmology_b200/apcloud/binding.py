@@ -195,7 +195,7 @@ def make_config(n: int, depth: int, gfd_c: float, lm: int = 17,
                 max_it: int = 10000, mixed_restart: int = 0, mixed_inner_rtol: float = 0.0,
                 device: int = 0, maxnc: int = 10000, nmax_cap: int = 0, precond: int = APC_PRECOND_MULTIGRID,
                 mg_sweeps: int = 0, mg_omega: float = 0.0, mg_alpha: float = 0.0, mg_reorth: int = 0,
-                warm_start: int = 0, solve_graphs: int = 0) -> "ApcConfig":
+                warm_start: int = 0, solve_graphs: int = 1) -> "ApcConfig":
     """An apc_config: the library defaults with the given fields set."""
     lib = load_library()
     cfg = ApcConfig()

@@ -1,13 +1,13 @@
 """A short, fixed workload for kernel profiling under ncu.
 
     python -m apcloud.profile_case [--precision fp64|mixed|fp64mg] [--workload lcdm128]
-                                   [--warm K] [--max-it N] [--solve-graphs]
+                                   [--warm K] [--max-it N] [--persistent]
 
 Runs K unprofiled Controller steps of the named workload, then one more step bracketed
 by cudaProfilerStart / cudaProfilerStop, so that `ncu --profile-from-start off` sees
 exactly one steady-state step.  --max-it lowers the GMRES iteration cap of the FP64
 path, so that each of its GMRES launches is short enough for a multi-pass capture.
---solve-graphs runs the multigrid solves as CUDA graphs instead of persistent kernels.
+--persistent runs the multigrid solves as persistent kernels instead of CUDA graphs.
 """
 from __future__ import annotations
 
@@ -32,7 +32,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--max-it", type=int, default=10000)
     ap.add_argument("--precision", choices=("fp64", "mixed", "fp64mg"), default="mixed")
-    ap.add_argument("--solve-graphs", action="store_true")
+    ap.add_argument("--persistent", action="store_true")
     ap.add_argument("--workload", default="lcdm128")
     ap.add_argument("--warm", type=int, default=2)
     args = ap.parse_args()
@@ -40,7 +40,7 @@ def main():
     prec = {"fp64": binding.APC_PREC_FP64, "mixed": binding.APC_PREC_MIXED,
             "fp64mg": binding.APC_PREC_FP64_MULTIGRID}[args.precision]
     g = binding.GpuPath(cfg.particles(), cfg.depth, cfg.gfd_c, cfg.lm, precision=prec, max_it=args.max_it,
-                        solve_graphs=int(args.solve_graphs))
+                        solve_graphs=0 if args.persistent else 1)
     ctl = for_config(g, cfg)
     ctl.start()
     for _ in range(args.warm):

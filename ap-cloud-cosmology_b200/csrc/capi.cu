@@ -197,6 +197,7 @@ void apc_config_default(apc_config *cfg) {
   cfg->mg_alpha = 0.0;
   cfg->mg_reorth = 0;
   cfg->warm_start = 0;
+  cfg->mixed_solve_graphs = 1;
 }
 
 const char *apc_status_string(int s) {

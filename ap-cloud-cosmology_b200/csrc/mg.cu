@@ -924,6 +924,7 @@ __device__ void p_first2(const Grp &g, const PLevel<T> &L, const T *bsrc, T bs, 
   grid_rows(g, L, [&](int i, int sub, int G, bool act) {
     T s = T(0);
     if (act)
+#pragma unroll 8
       for (int k = sub; k < L.w; k += G) {
         const size_t at = (size_t)k * L.ld + i;
         const int j = L.col[at];
@@ -952,6 +953,7 @@ __device__ void p_sweep(const Grp &g, const PLevel<T> &L, const T *bsrc, T bs, T
   grid_rows(g, L, [&](int i, int sub, int G, bool act) {
     T s = T(0);
     if (act)
+#pragma unroll 8
       for (int k = sub; k < L.w; k += G) {
         const size_t at = (size_t)k * L.ld + i;
         const int j = L.col[at];
@@ -972,7 +974,7 @@ __device__ void p_residual(const Grp &g, const PLevel<T> &L, const T *bsrc, T bs
   grid_rows(g, L, [&](int i, int sub, int G, bool act) {
     T s = T(0);
     if (act)
-#pragma unroll 4
+#pragma unroll 8
       for (int k = sub; k < L.w; k += G) {
         const size_t at = (size_t)k * L.ld + i;
         s += L.val[at] * x[L.col[at]];
@@ -1179,6 +1181,7 @@ __device__ bool solve_body(const PSolveArgs<T> &A, const Grp &g, PShared &sh, do
       T *w = A.V + (size_t)(it + 1) * A.vn;
       for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
         T acc = T(0);
+#pragma unroll 6
         for (int k = 0; k < A.w; ++k) {
           const size_t at = (size_t)k * A.ld + i;
           const int j = A.col[at];

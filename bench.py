@@ -285,7 +285,7 @@ def run_ours(args) -> dict:
     def make(prec, p):
         return binding.GpuPath(p, cfg.depth, cfg.gfd_c, cfg.lm, restart=cfg.restart, rtol=cfg.rtol,
                                precision=prec, device=dev, mixed_restart=args.mixed_restart,
-                               mixed_inner_rtol=args.inner_rtol, solve_graphs=int(args.solve_graphs))
+                               mixed_inner_rtol=args.inner_rtol, solve_graphs=0 if args.persistent else 1)
 
     # ---- warm-up on the mixed path ----
     mx = make(binding.APC_PREC_MIXED, parts)
@@ -307,7 +307,7 @@ def run_ours(args) -> dict:
     for name, prec, rtol in arms:
         g = binding.GpuPath(state_parts, cfg.depth, cfg.gfd_c, cfg.lm, restart=cfg.restart, rtol=rtol,
                             precision=prec, device=dev, mixed_restart=args.mixed_restart,
-                            mixed_inner_rtol=args.inner_rtol, solve_graphs=int(args.solve_graphs))
+                            mixed_inner_rtol=args.inner_rtol, solve_graphs=0 if args.persistent else 1)
         c2 = for_config(g, cfg)
         c2.t = t_state
         k = c2.constants(c2.t, cfg.delta_a)
@@ -439,16 +439,18 @@ def run_ours(args) -> dict:
                 "cells": cells, "ms_per_launch": gfd_ms,
                 "note": "issue bound (the exact per-cell quicksort and the FP64 least squares); the HBM "
                         "fraction is low by nature of the kernels"}
-    # ---- roofline of the potential solve: one persistent kernel per step (ir_solve_persistent),
-    #      its algorithmic bytes from the library's model (apc_profile.mg_bytes) over its
-    #      CUDA-event time ----
+    # ---- roofline of the potential solve (one graph, or one persistent kernel, per step): its
+    #      algorithmic bytes from the library's model (apc_profile.mg_bytes) over its CUDA-event
+    #      time ----
     mg_ms = prof["mg_solve_ms"] / args.steps
     mg_bytes = prof["mg_bytes"] / args.steps
     mg_achieved = mg_bytes / (mg_ms / 1e3) / 1e9 if mg_ms > 0 else 0.0
     mg_traffic = ncu_traffic_per_unit("mg_solve")
     solve_roof = {"kernel": "potential solve: ir_solve_persistent<float> (FP64 refinement, FP32 FGMRES(16) "
                             "cycles, octree-multigrid V-cycles; one cooperative launch per step)"
-                            if not args.solve_graphs else "potential solve graph (per-phase kernels)",
+                            if args.persistent else
+                            "potential solve: one CUDA graph per step (FP64 refinement, FP32 FGMRES(16) cycles, "
+                            "octree-multigrid V-cycles; ~20 kernels per iteration), timed as a unit",
                   "bound": "hbm", "achieved": mg_achieved, "peak": peak, "unit": "GB/s",
                   "frac": mg_achieved / peak, "peak_kind": peak_kind,
                   "traffic": (mg_traffic * mg_bytes) if mg_traffic else None,
@@ -471,8 +473,8 @@ def run_ours(args) -> dict:
                                   f"(a = {t_state:.4f} onwards); the whole run is in full_run",
                    "mixed_restart": args.mixed_restart or 16,
                    "inner_rtol": args.inner_rtol or 1e-3,
-                   "solve": "CUDA graphs of per-phase kernels" if args.solve_graphs else
-                            "one persistent cooperative kernel per solve"},
+                   "solve": "one persistent cooperative kernel per solve" if args.persistent else
+                            "one CUDA graph of per-phase kernels per solve"},
         "fp64": fp64,
         "force_error": dict(force, bound=1e-6,
                             measure="RMS relative error of the accelerations (and potentials) of one step on the "
@@ -509,7 +511,7 @@ def run_batch(args) -> dict | None:
     apc_batch_step call per rank.  Two forms of the step are timed from the same start:
     queued (the headline: all boxes' density solves, then all potential solves, in one
     cooperative launch each, block groups pulling boxes from a device work queue) and
-    per-box (each box's step whole in its fiber, its solves its own persistent kernels).
+    per-box (each box's step whole in its fiber, its solves its own CUDA graphs).
     Timed on the host around whole batch steps, with the device synchronised on both
     sides (the boxes run on many streams); max over ranks."""
     import torch
@@ -569,7 +571,7 @@ def run_batch(args) -> dict | None:
             "ms_per_step_each": per_q, "queued_solve_launches_ms_each": solve_q,
             "per_box": {"value": total * args.steps / dt_b, "ms_per_step": 1e3 * dt_b / args.steps,
                         "ms_per_step_each": per_b, "gpu_launches": launches_b,
-                        "solves": "each box's solves its own persistent kernels, boxes as fibers"},
+                        "solves": "each box's solves its own CUDA graphs, boxes as fibers"},
             "rank0": {"boxes": len(mine)},
             "gpu_launches": launches_q}
 
@@ -686,9 +688,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-full-run", action="store_true")
-    ap.add_argument("--solve-graphs", action="store_true",
-                    help="run the multigrid solves as CUDA graphs of per-phase kernels instead of one "
-                         "persistent kernel each")
+    ap.add_argument("--persistent", action="store_true",
+                    help="run the multigrid solves as one persistent cooperative kernel each instead of CUDA "
+                         "graphs of per-phase kernels")
     ap.add_argument("--batch-workers", type=int, default=0, help="host worker threads per rank (batch96)")
     args = ap.parse_args()
     if args.warmup < 3:

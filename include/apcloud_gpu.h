@@ -94,10 +94,12 @@ typedef struct apc_config {
   int warm_start;        /* mixed path: start both solves from the previous step's solution at the
                             same octree cells (1) or from zero (0, default); the stopping test stays
                             rtol ||D^-1 b||.  At 128^3 and a < 0.1 it saves ~1 of 20 iterations */
-  int mixed_solve_graphs; /* APC_PREC_MIXED / APC_PREC_FP64_MULTIGRID solves: 0 (default) = each solve
-                            is one persistent cooperative kernel (refinement loop, (F)GMRES cycles and
-                            V-cycles separated by grid barriers); 1 = a CUDA graph of per-phase
-                            kernels with conditional loop nodes (always used with mg_reorth) */
+  int mixed_solve_graphs; /* APC_PREC_MIXED / APC_PREC_FP64_MULTIGRID solves: 1 (default) = a CUDA graph
+                            of per-phase kernels with conditional loop nodes; 0 = each solve is one
+                            persistent cooperative kernel (refinement loop, (F)GMRES cycles and
+                            V-cycles separated by grid barriers).  On a B200 at 128^3 the graph form
+                            is faster (the barriers cost about what the launches they replace cost);
+                            the queued batch mode uses the persistent form across boxes */
 } apc_config;
 
 enum { APC_PRECOND_JACOBI = 0, APC_PRECOND_MULTIGRID = 1 };
