@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(PKG_DIR, "libapcloud_gpu.so")
 APC_PREC_FP64 = 0
 APC_PREC_MIXED = 1
 APC_PREC_FP64_MULTIGRID = 2
+APC_PREC_MIXED_VCYCLE = 3
 APC_PRECOND_JACOBI = 0
 APC_PRECOND_MULTIGRID = 1
 APC_BATCH_SOLVE_PER_BOX = 0

@@ -1,6 +1,6 @@
 """A short, fixed workload for kernel profiling under ncu.
 
-    python -m apcloud.profile_case [--precision fp64|mixed|fp64mg] [--workload lcdm128]
+    python -m apcloud.profile_case [--precision fp64|mixed|fp64mg|vcycle32] [--workload lcdm128]
                                    [--warm K] [--max-it N] [--persistent]
 
 Runs K unprofiled Controller steps of the named workload, then one more step bracketed
@@ -31,14 +31,14 @@ def _cudart():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--max-it", type=int, default=10000)
-    ap.add_argument("--precision", choices=("fp64", "mixed", "fp64mg"), default="mixed")
+    ap.add_argument("--precision", choices=("fp64", "mixed", "fp64mg", "vcycle32"), default="mixed")
     ap.add_argument("--persistent", action="store_true")
     ap.add_argument("--workload", default="lcdm128")
     ap.add_argument("--warm", type=int, default=2)
     args = ap.parse_args()
     cfg = ics.config(args.workload)
     prec = {"fp64": binding.APC_PREC_FP64, "mixed": binding.APC_PREC_MIXED,
-            "fp64mg": binding.APC_PREC_FP64_MULTIGRID}[args.precision]
+            "fp64mg": binding.APC_PREC_FP64_MULTIGRID, "vcycle32": binding.APC_PREC_MIXED_VCYCLE}[args.precision]
     g = binding.GpuPath(cfg.particles(), cfg.depth, cfg.gfd_c, cfg.lm, precision=prec, max_it=args.max_it,
                         solve_graphs=0 if args.persistent else 1)
     ctl = for_config(g, cfg)

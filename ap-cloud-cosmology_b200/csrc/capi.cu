@@ -227,7 +227,7 @@ int apc_create(const apc_config *cfg, apc_context **out) {
       cfg->gmres_restart > 255 || cfg->mixed_restart < 0 || cfg->mixed_restart > 31 || cfg->mg_sweeps < 0 ||
       (cfg->mixed_precond != APC_PRECOND_JACOBI && cfg->mixed_precond != APC_PRECOND_MULTIGRID) ||
       (cfg->precision != APC_PREC_FP64 && cfg->precision != APC_PREC_MIXED &&
-       cfg->precision != APC_PREC_FP64_MULTIGRID))
+       cfg->precision != APC_PREC_FP64_MULTIGRID && cfg->precision != APC_PREC_MIXED_VCYCLE))
     return APC_ERR_INVALID_ARG;
   for (int d = 0; d < 3; ++d)
     if (!(cfg->box[2 * d + 1] > cfg->box[2 * d])) return APC_ERR_INVALID_ARG;
@@ -424,9 +424,11 @@ int apc_solve_part_density(apc_context *c, double c_dens) {
   if (c->cfg.precision == APC_PREC_MIXED) {
     APC_TRY(apc_ensure(c, &c->a1f, (size_t)c->m_cap * c->ell_w, nullptr));
     APC_TRY(apc_ensure(c, &c->a2f, (size_t)c->m_cap * c->ell_w, nullptr));
-  } else if (c->cfg.precision == APC_PREC_FP64_MULTIGRID) {
+  } else if (c->cfg.precision == APC_PREC_FP64_MULTIGRID || c->cfg.precision == APC_PREC_MIXED_VCYCLE) {
     APC_TRY(apc_ensure(c, &c->a1d, (size_t)c->m_cap * c->ell_w, nullptr));
     APC_TRY(apc_ensure(c, &c->a2d, (size_t)c->m_cap * c->ell_w, nullptr));
+    if (c->cfg.precision == APC_PREC_MIXED_VCYCLE)
+      APC_TRY(apc_ensure(c, &c->a2f, (size_t)c->m_cap * c->ell_w, nullptr));
   }
   apc_solve_stats &st = c->stats;
   // multigrid paths: the potential hierarchy is built while the density solve runs

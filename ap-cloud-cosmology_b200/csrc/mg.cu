@@ -473,13 +473,15 @@ __global__ void __launch_bounds__(kT) cgs_pass(int n, IrState *S, T *V, size_t v
 // V_{it+1} = A z and the dots <V_{it+1}, V_j>, j <= it, in the same warp-tile pass.
 // With a preconditioner z is its output, kept as Z_it for the solution; without one
 // (Z == nullptr) z is V_it itself.
-template <class T>
+template <class T, class TZ = T>
 __global__ void __launch_bounds__(kT) spmv_dots(int n, int ew, size_t ld, const int *__restrict__ col,
-                                                 const T *__restrict__ val, const T *zin, T *Z,
+                                                 const T *__restrict__ val, const TZ *zin, T *Z,
                                                  T *V, size_t vn, const IrState *__restrict__ S, double *partial,
                                                  unsigned *counter, double *out) {
   const int it = S->it, nv = it + 1;
-  const T *z = Z ? zin : V + (size_t)it * vn;
+  // the preconditioner's output (of type TZ), or the basis vector itself
+  const TZ *zp = zin;
+  const T *zv = V + (size_t)it * vn;
   T *zk = Z ? Z + (size_t)it * vn : nullptr;
   T *w = V + (size_t)nv * vn;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -491,11 +493,18 @@ __global__ void __launch_bounds__(kT) spmv_dots(int n, int ew, size_t ld, const 
     const int i = tile * 32 + lane;
     if (i >= n) continue;
     T sacc = T(0);
-    for (int k = 0; k < ew; ++k) {
-      const size_t at = (size_t)k * ld + i;
-      sacc += val[at] * z[col[at]];
+    if (Z) {
+      for (int k = 0; k < ew; ++k) {
+        const size_t at = (size_t)k * ld + i;
+        sacc += val[at] * (T)zp[col[at]];
+      }
+      zk[i] = (T)zp[i];
+    } else {
+      for (int k = 0; k < ew; ++k) {
+        const size_t at = (size_t)k * ld + i;
+        sacc += val[at] * zv[col[at]];
+      }
     }
-    if (zk) zk[i] = z[i];
     w[i] = sacc;
     const double wi = (double)sacc;
 #pragma unroll
@@ -507,15 +516,15 @@ __global__ void __launch_bounds__(kT) spmv_dots(int n, int ew, size_t ld, const 
 }
 
 // V_it *= scale (the newest basis vector), and the same into the V-cycle's input if any
-template <class T>
+template <class T, class TV = T>
 __global__ void scale_next(int n, const IrState *__restrict__ S, T *__restrict__ V, size_t vn,
-                           T *__restrict__ vin) {
+                           TV *__restrict__ vin) {
   const T f = (T)S->scale;
   T *v = V + (size_t)S->it * vn;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const T u = v[i] * f;
     v[i] = u;
-    if (vin) vin[i] = u;
+    if (vin) vin[i] = (TV)u;
   }
 }
 
@@ -1773,6 +1782,7 @@ template <class T>
 struct IrSolveArgs {
   int which;               // 0 density, 1 potential
   bool mg;                 // V-cycle preconditioner (else none: GMRES on the scaled system)
+  bool mg32;               // the V-cycle runs on the FP32 hierarchy (T = double only)
   int n, w;
   size_t ld;
   const int *col;          // ELL columns shared by both operators
@@ -1806,7 +1816,11 @@ static int capture_solve(apc_context *c, const IrSolveArgs<T> &a) {
   const bool reorth = c->cfg.mg_reorth != 0;
   double *h1 = m->dots, *h2 = m->dots + 34, *nr = m->dots + 68, *tmp = m->dots + 70;
   T *Z = a.mg ? H.Z : nullptr;
-  T *vin = a.mg ? H.vin : nullptr;
+  // the V-cycle's input and output: this precision's, or the FP32 hierarchy's
+  MgHier<float> &H32 = m->h32;
+  const bool v32 = a.mg && a.mg32;
+  T *vin = a.mg && !v32 ? H.vin : nullptr;
+  float *vin32 = v32 ? H32.vin : nullptr;
   const int64_t l0 = c->launches;
   cudaStream_t s = c->s, s1 = m->cap[0], s2 = m->cap[1];
   cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
@@ -1834,15 +1848,25 @@ static int capture_solve(apc_context *c, const IrSolveArgs<T> &a) {
       cap1 = true;
       if (ok(cudaGraphConditionalHandleCreate(&cond_in, body_out, 0, 0))) {
         ir_to_inner<T><<<G, kT, 0, s1>>>(n, a.r, a.val, m->state, H.V, m->partial, m->counter, tmp, cond_in);
-        scale_next<T><<<Gs, kT, 0, s1>>>(n, m->state, H.V, vn, vin);
+        if (v32)
+          scale_next<T, float><<<Gs, kT, 0, s1>>>(n, m->state, H.V, vn, vin32);
+        else
+          scale_next<T><<<Gs, kT, 0, s1>>>(n, m->state, H.V, vn, vin);
         if (ok(cudaGetLastError()) && ok(add_while(s1, cond_in, &body_in)) &&
             ok(cudaStreamBeginCaptureToGraph(s2, body_in, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal))) {
           cap2 = true;
           const int64_t v0 = c->launches;
-          if (a.mg) vcycle<T>(c, s2, 0, H.vin, H.vout);
+          if (v32)
+            vcycle<float>(c, s2, 0, H32.vin, H32.vout);
+          else if (a.mg)
+            vcycle<T>(c, s2, 0, H.vin, H.vout);
           m->vcycle_nodes[slot] = c->launches - v0;
-          spmv_dots<T><<<G, kT, 0, s2>>>(n, a.w, a.ld, a.col, a.valf, a.mg ? H.vout : nullptr, Z, H.V, vn, m->state,
-                                         m->partial, m->counter, h1);
+          if (v32)
+            spmv_dots<T, float><<<G, kT, 0, s2>>>(n, a.w, a.ld, a.col, a.valf, H32.vout, Z, H.V, vn, m->state,
+                                                  m->partial, m->counter, h1);
+          else
+            spmv_dots<T><<<G, kT, 0, s2>>>(n, a.w, a.ld, a.col, a.valf, a.mg ? H.vout : nullptr, Z, H.V, vn,
+                                           m->state, m->partial, m->counter, h1);
           if (reorth) {
             cgs_pass<1, T><<<G, kT, 0, s2>>>(n, m->state, H.V, vn, h1, m->partial, m->counter, h2, nullptr, nullptr,
                                              cond_in);
@@ -1851,7 +1875,10 @@ static int capture_solve(apc_context *c, const IrSolveArgs<T> &a) {
             cgs_pass<2, T><<<G, kT, 0, s2>>>(n, m->state, H.V, vn, h1, m->partial, m->counter, nr, h1, nullptr,
                                              cond_in);
           }
-          scale_next<T><<<Gs, kT, 0, s2>>>(n, m->state, H.V, vn, vin);
+          if (v32)
+            scale_next<T, float><<<Gs, kT, 0, s2>>>(n, m->state, H.V, vn, vin32);
+          else
+            scale_next<T><<<Gs, kT, 0, s2>>>(n, m->state, H.V, vn, vin);
           ok(cudaGetLastError());
         }
         if (cap2) {
@@ -2031,16 +2058,18 @@ static int persistent_solve(apc_context *c, const IrSolveArgs<T> &a, int blocks)
 //     residual + restriction (ELL, x, b, coarse b written), prolongation + sweep (ELL, x,
 //     b, D^-1, aggregate map, coarse x, out), each further sweep (ELL, x, b, D^-1, out);
 //   the single-block tail: the same per level, from L2.
-template <class T>
-static double solve_bytes(const MgHier<T> &H, bool use_mg, int n, int w, int sweeps, int total_its, int outer) {
-  const double S = sizeof(T), N = n;
+template <class TV>
+static double solve_bytes(const MgHier<TV> &H, bool use_mg, int n, int w, int sweeps, int total_its, int outer,
+                          double S_krylov = sizeof(TV)) {
+  const double S = S_krylov, N = n;
   const double cyc = outer > 0 ? (double)total_its / outer : 0.0;
   const double jbar = cyc > 0 ? 0.5 * (cyc - 1.0) : 0.0;
   const double per_outer = N * (w * 12.0 + 24.0) + N * (16.0 + S) + N * (cyc * S + 16.0);
   double per_it = N * (w * (S + 4) + 2 * S) + N * (jbar + 2) * S + N * (jbar + 3) * S;
   if (use_mg) {
+    const double S = sizeof(TV);  // the V-cycle's element size
     for (int l = 0; l < H.nlev; ++l) {
-      const MgLevel<T> &L = H.lv[l];
+      const MgLevel<TV> &L = H.lv[l];
       const double nl = L.n, ell = L.w * (S + 4);
       const double nc = l + 1 < H.nlev ? H.lv[l + 1].n : 0.0;
       if (l + 1 < H.nlev) {
@@ -2065,11 +2094,18 @@ static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, c
   const int n = c->nc + c->nv;
   const size_t vn = ((size_t)n + 31) & ~(size_t)31;
   const int M = std::max(1, std::min(restart, kMaxM));
+  // FP64 Krylov vectors with the V-cycle on the FP32 hierarchy
+  const bool mg32 = use_mg && sizeof(T) == sizeof(double) && c->cfg.precision == APC_PREC_MIXED_VCYCLE;
   APC_TRY(apc_ensure(c, &H.V, vn * (M + 1)));
   if (use_mg) {
     APC_TRY(apc_ensure(c, &H.Z, vn * M));
-    APC_TRY(apc_ensure(c, &H.vin, vn));
-    APC_TRY(apc_ensure(c, &H.vout, vn));
+    if (mg32) {
+      APC_TRY(apc_ensure(c, &m->h32.vin, vn));
+      APC_TRY(apc_ensure(c, &m->h32.vout, vn));
+    } else {
+      APC_TRY(apc_ensure(c, &H.vin, vn));
+      APC_TRY(apc_ensure(c, &H.vout, vn));
+    }
   }
   APC_TRY(apc_ensure(c, &H.dvec, vn));
   APC_TRY(apc_ensure(c, &m->partial, (size_t)kRedBlocks * 34));
@@ -2089,11 +2125,18 @@ static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, c
   m->prebuilt = false;
   if (use_mg && !prebuilt) {
     APC_CUDA_TRY(c, apc_stream_wait(c));
-    APC_TRY(mg_build<T>(c));
+    APC_TRY(mg32 ? mg_build<float>(c) : mg_build<T>(c));
   }
+  const int nlev = mg32 ? m->h32.nlev : H.nlev;
+  const int sweeps = c->cfg.mg_sweeps > 0 ? c->cfg.mg_sweeps : 2;
+  auto bytes = [&](int its_, int outer_) {
+    return mg32 ? solve_bytes<float>(m->h32, true, n, c->ell_w, sweeps, its_, outer_, sizeof(T))
+                : solve_bytes<T>(H, true, n, c->ell_w, sweeps, its_, outer_);
+  };
   IrSolveArgs<T> a{};
   a.which = which;
   a.mg = use_mg;
+  a.mg32 = mg32;
   a.n = n;
   a.w = c->ell_w;
   a.ld = (size_t)c->m_cap;
@@ -2114,8 +2157,8 @@ static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, c
   a.max_outer = use_mg && sizeof(T) == sizeof(float) ? 40 : std::max(40, cfg.gmres_max_it);
   a.M = M;
   // one persistent kernel per solve unless the graph path is asked for (or needed: the
-  // re-orthogonalising Gram-Schmidt runs only there)
-  bool persistent = !cfg.mixed_solve_graphs && !cfg.mg_reorth;
+  // re-orthogonalising Gram-Schmidt and the FP32 V-cycle under FP64 vectors run only there)
+  bool persistent = !cfg.mixed_solve_graphs && !cfg.mg_reorth && !mg32;
   if (persistent && c->defer_solve) {
     // prepared for a batched launch with other boxes' solves (apc_mg_batched_solve);
     // apc_ir_finish reads the outcome
@@ -2129,7 +2172,7 @@ static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, c
     *rnorm = 0.0;
     *reason = 0;
     *refinements = 0;
-    *levels = use_mg ? H.nlev : 0;
+    *levels = use_mg ? nlev : 0;
     return APC_OK;
   }
   if (persistent) {
@@ -2163,12 +2206,11 @@ static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, c
       *rnorm = R.rn;
       *reason = R.reason;
       *refinements = R.outer;
-      *levels = use_mg ? H.nlev : 0;
+      *levels = use_mg ? nlev : 0;
       if (use_mg) {
         c->prof.mg_solve_ms += ms;
         c->prof.mg_iterations += R.total_its;
-        c->prof.mg_bytes += solve_bytes<T>(H, true, n, c->ell_w, c->cfg.mg_sweeps > 0 ? c->cfg.mg_sweeps : 2,
-                                           R.total_its, R.outer);
+        c->prof.mg_bytes += bytes(R.total_its, R.outer);
       }
       return APC_OK;
     }
@@ -2190,14 +2232,13 @@ static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, c
   *rnorm = S.rn;
   *reason = S.reason;
   *refinements = S.outer;
-  *levels = use_mg ? H.nlev : 0;
+  *levels = use_mg ? nlev : 0;
   const int per_it = (int)m->vcycle_nodes[which] + 3 + (cfg.mg_reorth != 0 ? 1 : 0);
   apc_count_launch(c, 3 + 6 * S.outer + per_it * S.total_its);
   if (use_mg) {
     c->prof.mg_solve_ms += ms;
     c->prof.mg_iterations += S.total_its;
-    c->prof.mg_bytes += solve_bytes<T>(H, true, n, c->ell_w, c->cfg.mg_sweeps > 0 ? c->cfg.mg_sweeps : 2,
-                                       S.total_its, S.outer);
+    c->prof.mg_bytes += bytes(S.total_its, S.outer);
   }
   return APC_OK;
 }
@@ -2205,7 +2246,7 @@ static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, c
 int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, const double *b, double *x, double *r,
                  int restart, double rtol_in, int *its, double *rnorm, int *reason, int *refinements, int *levels,
                  int (*during)(apc_context *)) {
-  if (c->cfg.precision == APC_PREC_FP64_MULTIGRID)
+  if (c->cfg.precision == APC_PREC_FP64_MULTIGRID || c->cfg.precision == APC_PREC_MIXED_VCYCLE)
     return ir_solve<double>(c, which, use_mg, val, which == 0 ? c->a1d : c->a2d, b, x, r, restart, rtol_in, its,
                             rnorm, reason, refinements, levels, during);
   return ir_solve<float>(c, which, use_mg, val, which == 0 ? c->a1f : c->a2f, b, x, r, restart, rtol_in, its, rnorm,
@@ -2236,6 +2277,7 @@ int apc_mg_prebuild(apc_context *c) {
   APC_CUDA_TRY(c, cudaStreamWaitEvent(m->side, m->side_ev[0], 0));
   c->s = m->side;
   apc_potential_scaled(c, c->s);
+  // the FP64 path's hierarchy is FP64; the mixed paths' V-cycles run on an FP32 one
   int rc = c->cfg.precision == APC_PREC_FP64_MULTIGRID ? mg_build<double>(c) : mg_build<float>(c);
   if (rc == APC_OK && cudaEventRecord(m->side_ev[1], c->s) != cudaSuccess) rc = APC_ERR_CUDA;
   c->s = main;

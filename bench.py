@@ -9,10 +9,13 @@ Workload (default): the 128^3 LambdaCDM Zel'dovich box.
   - 128 leapfrog steps to a = 1, depth 21, c = 6.2e-3, lm = 17;
   - GMRES(30), rtol 1e-10, max_it 10000.
 A step is one pass of the Controller sequence (select; solve; kick; drift) over the
-whole particle set.  The timed arm is the mixed-precision path: FP32 Krylov inside FP64
-iterative refinement, FP64 GFD moments and FP64 leapfrog.  The plain FP64 GPU path (the
-same multigrid FGMRES solver with FP64 vectors and operators) is timed beside it from the
-same state.  Both arms' force errors are measured against one FP64 solve converged to
+whole particle set.  The timed arm is a mixed-precision path (--precision):
+  - vcycle32 (default): FP64 FGMRES with FP64 Krylov vectors, right-preconditioned by an
+    FP32 octree-multigrid V-cycle (APC_PREC_MIXED_VCYCLE);
+  - mixed: FP32 FGMRES corrections inside FP64 iterative refinement (APC_PREC_MIXED).
+GFD moments and the leapfrog are FP64 in both.  The plain FP64 GPU path (the same
+multigrid FGMRES solver with FP64 vectors, operators and V-cycle) is timed beside it from
+the same state.  Every arm's force error is measured against one FP64 solve converged to
 rtol 1e-13, together with that of the reference-semantics FP64 GMRES(30)+Jacobi, which at
 this size stops at max_it.  `full_run` times the whole configured run (every step to
 a = 1) on a fresh context.
@@ -47,11 +50,20 @@ sys.path.insert(0, PKG)
 
 import numpy as np  # noqa: E402
 
-from apcloud import ics  # noqa: E402
+from apcloud import binding as _b, ics  # noqa: E402
 
 METRIC = "particle-steps/s at 128^3: mixed-prec vs FP64 GPU path at equal force error"
 UNIT = "particle-steps/s"
 WORKLOAD = "lcdm128"
+# the timed arm's choices: (apc_precision, solver, arithmetic types)
+PRECISIONS = {
+    "vcycle32": (_b.APC_PREC_MIXED_VCYCLE, "FP64 FGMRES(16) with FP64 Krylov vectors, right-preconditioned by an "
+                 "FP32 octree-multigrid V-cycle; density by FP64 GMRES(30)",
+                 "f64 Krylov / f32 multigrid V-cycle; f64 GFD moments and leapfrog"),
+    "mixed": (_b.APC_PREC_MIXED, "FP64 iterative refinement around FP32 FGMRES(16) corrections with the FP32 "
+              "V-cycle; density by FP32 GMRES(30) corrections",
+              "f32 Krylov / f64 refinement, GFD moments and leapfrog"),
+}
 
 
 def workload_desc(cfg) -> str:
@@ -287,8 +299,9 @@ def run_ours(args) -> dict:
                                precision=prec, device=dev, mixed_restart=args.mixed_restart,
                                mixed_inner_rtol=args.inner_rtol, solve_graphs=0 if args.persistent else 1)
 
-    # ---- warm-up on the mixed path ----
-    mx = make(binding.APC_PREC_MIXED, parts)
+    head_prec = PRECISIONS[args.precision][0]
+    # ---- warm-up on the timed path ----
+    mx = make(head_prec, parts)
     ctl = for_config(mx, cfg)
     ctl.start()
     for _ in range(args.warmup):
@@ -297,12 +310,14 @@ def run_ours(args) -> dict:
     state_parts = ics.Particles(*state[:6])
     t_state = ctl.t
 
-    # ---- force error on the same state.  Arms: the mixed path (timed headline), the plain
-    #      FP64 GPU path (the same multigrid FGMRES solver with every vector and operator in
-    #      FP64), and the reference-semantics FP64 GMRES(30)+Jacobi, all to rtol 1e-10.  Each
-    #      is measured against one independent FP64 solve converged to rtol 1e-13 ----
-    arms = (("mixed", binding.APC_PREC_MIXED, cfg.rtol), ("fp64", binding.APC_PREC_FP64_MULTIGRID, cfg.rtol),
-            ("fp64_gmres", binding.APC_PREC_FP64, cfg.rtol), ("converged", binding.APC_PREC_FP64_MULTIGRID, 1e-13))
+    # ---- force error on the same state.  Arms: both mixed paths (one of them the timed
+    #      headline), the plain FP64 GPU path (the same multigrid FGMRES solver with every
+    #      vector and operator in FP64), and the reference-semantics FP64 GMRES(30)+Jacobi, all
+    #      to rtol 1e-10.  Each is measured against one independent FP64 solve converged to
+    #      rtol 1e-13 ----
+    arms = (("mixed_vcycle", binding.APC_PREC_MIXED_VCYCLE, cfg.rtol), ("mixed", binding.APC_PREC_MIXED, cfg.rtol),
+            ("fp64", binding.APC_PREC_FP64_MULTIGRID, cfg.rtol), ("fp64_gmres", binding.APC_PREC_FP64, cfg.rtol),
+            ("converged", binding.APC_PREC_FP64_MULTIGRID, 1e-13))
     acc = {}
     for name, prec, rtol in arms:
         g = binding.GpuPath(state_parts, cfg.depth, cfg.gfd_c, cfg.lm, restart=cfg.restart, rtol=rtol,
@@ -327,7 +342,7 @@ def run_ours(args) -> dict:
                     "potential_its": acc[name][1]["potential_its"],
                     "potential_reason": acc[name][1]["potential_reason"],
                     "potential_refinements": acc[name][1]["potential_refinements"]}
-             for name in ("mixed", "fp64", "fp64_gmres")}
+             for name in ("mixed_vcycle", "mixed", "fp64", "fp64_gmres")}
 
     def timed(g, c):
         dist.barrier()
@@ -351,7 +366,7 @@ def run_ours(args) -> dict:
     #      step to a_end, each step timed on the device (no L2 flush: a real run) ----
     full = None
     if not args.no_full_run:
-        gf = make(binding.APC_PREC_MIXED, parts)
+        gf = make(head_prec, parts)
         cf = for_config(gf, cfg)
         dist.barrier()
         t0 = time.perf_counter()
@@ -385,7 +400,7 @@ def run_ours(args) -> dict:
         st64 = g64.solve_stats()
         g64.close()
         fv = ws * cfg.n * args.steps / (fp64_ms / 1e3)
-        fp64 = {"value": fv, "ms_per_step": fp64_ms / args.steps, "speedup_mixed_over_fp64": value / fv,
+        fp64 = {"value": fv, "ms_per_step": fp64_ms / args.steps, "speedup_timed_arm_over_fp64": value / fv,
                 "solver": "FP64 multigrid FGMRES (APC_PREC_FP64_MULTIGRID): the mixed path's solver with FP64 "
                           "vectors and operators, restarted from the true FP64 residual, rtol 1e-10",
                 "phases_ms_per_step": {k2: p64[k2 + "_ms"] / args.steps for k2 in
@@ -446,18 +461,18 @@ def run_ours(args) -> dict:
     mg_bytes = prof["mg_bytes"] / args.steps
     mg_achieved = mg_bytes / (mg_ms / 1e3) / 1e9 if mg_ms > 0 else 0.0
     mg_traffic = ncu_traffic_per_unit("mg_solve")
-    solve_roof = {"kernel": "potential solve: ir_solve_persistent<float> (FP64 refinement, FP32 FGMRES(16) "
-                            "cycles, octree-multigrid V-cycles; one cooperative launch per step)"
-                            if args.persistent else
-                            "potential solve: one CUDA graph per step (FP64 refinement, FP32 FGMRES(16) cycles, "
-                            "octree-multigrid V-cycles; ~20 kernels per iteration), timed as a unit",
+    solve_roof = {"kernel": "potential solve: ir_solve_persistent (FP64 refinement, FGMRES(16) cycles, "
+                            "octree-multigrid V-cycles; one cooperative launch per step)"
+                            if args.persistent and args.precision == "mixed" else
+                            "potential solve: one CUDA graph per step (" + PRECISIONS[args.precision][1] +
+                            "; ~20 kernels per iteration), timed as a unit",
                   "bound": "hbm", "achieved": mg_achieved, "peak": peak, "unit": "GB/s",
                   "frac": mg_achieved / peak, "peak_kind": peak_kind,
                   "traffic": (mg_traffic * mg_bytes) if mg_traffic else None,
                   "algorithmic_bytes_per_launch": mg_bytes, "ms_per_launch": mg_ms,
                   "iterations_per_launch": prof["mg_iterations"] / args.steps,
-                  "note": "the FP32 working set (~80 MB at 128^3) stays in the 126 MB L2 between phases, so "
-                          "the bytes are served largely from L2; the peak is the HBM copy bandwidth"}
+                  "note": "the working set (~80 MB in FP32, ~130 MB with FP64 Krylov vectors at 128^3) stays "
+                          "largely in the 126 MB L2 between phases; the peak is the HBM copy bandwidth"}
     roofs = sorted([gfd_roof, solve_roof], key=lambda r: -r["ms_per_launch"])
     # ---- whole-step algorithmic bytes (particles, cells, Krylov rows), for context ----
     st = mx.solve_stats()
@@ -465,8 +480,9 @@ def run_ours(args) -> dict:
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": step_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 Krylov / f64 refinement, GFD moments and leapfrog", "data": "synthetic",
-        "config": {"workload": workload_desc(cfg), "precision": "mixed", "parallelism": f"replicas x{ws}",
+        "dtype": PRECISIONS[args.precision][2], "data": "synthetic",
+        "config": {"workload": workload_desc(cfg), "precision": args.precision,
+                   "solver": PRECISIONS[args.precision][1], "parallelism": f"replicas x{ws}",
                    "l2": "flushed (512 MiB write) before every timed step",
                    "start_a": round(t_state, 6),
                    "timed_steps": f"steps {args.warmup + 1}-{args.warmup + args.steps} of {cfg.steps} "
@@ -479,7 +495,8 @@ def run_ours(args) -> dict:
         "force_error": dict(force, bound=1e-6,
                             measure="RMS relative error of the accelerations (and potentials) of one step on the "
                                     "same state, against an FP64 multigrid solve converged to rtol 1e-13",
-                            equal_force_error=bool(force["mixed"]["acc_rms_vs_converged"] <= 1e-6 and
+                            equal_force_error=bool(force["mixed_vcycle"]["acc_rms_vs_converged"] <= 1e-6 and
+                                                   force["mixed"]["acc_rms_vs_converged"] <= 1e-6 and
                                                    force["fp64"]["acc_rms_vs_converged"] <= 1e-6)),
         "phases_ms_per_step": {k: prof[k + "_ms"] / args.steps for k in
                                ("select", "solve", "assemble", "gfd", "density", "potential", "mg_build",
@@ -682,6 +699,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--precision", choices=tuple(PRECISIONS), default="vcycle32",
+                    help="the timed arm's solver precision")
     ap.add_argument("--mixed-restart", type=int, default=0)
     ap.add_argument("--inner-rtol", type=float, default=0.0)
     ap.add_argument("--no-fp64", action="store_true")

@@ -59,10 +59,13 @@ typedef enum apc_status {
 typedef enum apc_precision {
   APC_PREC_FP64 = 0,  /* FP64 GMRES with the reference's semantics: GMRES(restart) + Jacobi */
   APC_PREC_MIXED = 1, /* FP32 SpMV/Krylov inside an FP64 iterative-refinement loop */
-  APC_PREC_FP64_MULTIGRID = 2 /* the mixed path's solver with every vector and operator in FP64:
+  APC_PREC_FP64_MULTIGRID = 2, /* the mixed path's solver with every vector and operator in FP64:
                                  restarted (F)GMRES on the Jacobi-scaled systems, the potential
                                  right-preconditioned by the same octree multigrid, each cycle
                                  restarted from the true FP64 residual; same stopping test */
+  APC_PREC_MIXED_VCYCLE = 3 /* FP64_MULTIGRID's FP64 FGMRES with the V-cycle preconditioner in
+                               FP32 (hierarchy and smoothing sweeps); the density solve as in
+                               FP64_MULTIGRID; same stopping test */
 } apc_precision;
 
 typedef struct apc_config {

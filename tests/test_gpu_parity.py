@@ -236,6 +236,17 @@ def test_mixed_precision_equal_force_error(gpu_lib, path):
     assert smg["potential_reason"] == 2 and smg["density_reason"] == 2 and smg["mg_levels"] >= 2
     assert _acc_rms(pmg[6:9], p64[6:9]) <= 1e-7
     assert _rel(fmg.potential, f64.potential) <= 1e-7
+    # FP64 FGMRES under the FP32 V-cycle: the same stopping test on FP64 residuals, so the
+    # FP64 bound holds although the preconditioner rounds to FP32
+    gp = _gpu(_parts(g), g, precision=binding.APC_PREC_MIXED_VCYCLE)
+    gp.select()
+    gp.solve(float(g["c_dens"]), float(g["c_pot"]), -1.0)
+    gp.move_velocity(float(g["delta_a"]), float(g["c_vel"]))
+    pv, fv, sv = gp.particles(), gp.fields(), gp.solve_stats()
+    gp.close()
+    assert sv["potential_reason"] == 2 and sv["density_reason"] == 2 and sv["mg_levels"] >= 2
+    assert _acc_rms(pv[6:9], p64[6:9]) <= 1e-7
+    assert _rel(fv.potential, f64.potential) <= 1e-7
 
 
 def test_phase_order_and_invalid_input_errors(gpu_lib):
@@ -366,8 +377,8 @@ def test_fused_step_equals_phase_calls(gpu_lib):
 @pytest.mark.parametrize("prec", [binding.APC_PREC_MIXED, binding.APC_PREC_FP64_MULTIGRID], ids=["mixed", "fp64mg"])
 @pytest.mark.parametrize("case", ["ball32k", "eds64"])
 def test_persistent_solve_matches_graph_solve(gpu_lib, prec, case):
-    """The solves run as one persistent kernel by default; the CUDA-graph path of per-phase
-    kernels is the same algorithm.  Both must meet the stopping test, and their fields
+    """The solves run as CUDA graphs of per-phase kernels by default; the persistent kernel
+    (solve_graphs=0) is the same algorithm.  Both must meet the stopping test, and their fields
     agree to the accuracy of the solves.  The states are taken four steps into each run
     (at the start of eds64 the cells hold equal counts, the FP64 density is uniform and the
     potential's rhs vanishes); eds64 then has ~33k cells, two grid levels above the

@@ -243,7 +243,8 @@ def _lcdm128_state_vs_reference(cfg, parts, t):
     m_ref = ref.select()
     ref.solve(k["c_dens"], k["c_pot"], k["c_field"])
     report = {}
-    for name, prec in (("mixed", binding.APC_PREC_MIXED), ("fp64_multigrid", binding.APC_PREC_FP64_MULTIGRID)):
+    for name, prec in (("mixed", binding.APC_PREC_MIXED), ("fp64_multigrid", binding.APC_PREC_FP64_MULTIGRID),
+                       ("mixed_vcycle", binding.APC_PREC_MIXED_VCYCLE)):
         gm = _gpu(cfg, parts, prec)
         cells = _assert_selection_equal(gm, ref, gm.select(), m_ref)
         gm.solve(k["c_dens"], k["c_pot"], k["c_field"])
