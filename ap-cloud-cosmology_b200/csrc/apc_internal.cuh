@@ -156,6 +156,7 @@ struct apc_context {
   double t_select_ms = 0, t_solve_ms = 0, t_move_ms = 0;
   apc_profile prof{};
   bool step_open = false;    // a select has started a step that move_position will close
+  unsigned select_gen = 0;   // completed selections (keys the multigrid aggregation to its cells)
   bool kick_recorded = false;  // ev[4] holds the start of a move_velocity
 };
 
@@ -184,7 +185,8 @@ int apc_octree_levels_count(apc_context *c); // numnodes per level (octree_build
 int apc_selection(apc_context *c);           // top-down + balance + cells (selection.cu)
 constexpr int APC_RETRY_FULL_SORT = -100;    // internal: the selection went deeper than the sort
 int apc_sorted_keys_copy(apc_context *c, uint64_t **keys, uint32_t **ids);  // octree_build.cu
-int apc_gfd_assemble(apc_context *c, double c_dens);    // gfd.cu
+// gfd.cu; `during` runs on the host after the assembly's kernels are queued
+int apc_gfd_assemble(apc_context *c, double c_dens, int (*during)(apc_context *) = nullptr);
 // during (optional): host work run while the mixed solve's graph runs on the GPU, before
 // the host waits for its outcome
 int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int *its,
@@ -228,6 +230,9 @@ int apc_solve_part_fields(apc_context *c, double c_field);
 int apc_step_move(apc_context *c, const apc_step_params *p, double *max_dv, double *max_dx);
 int apc_mg_mark_assembled(apc_context *c);
 int apc_mg_prebuild(apc_context *c);
+// the aggregation of the hierarchy (cell codes only) on the second stream while the GFD
+// assembly runs
+int apc_mg_structure_during_assembly(apc_context *c);
 bool apc_mg_prebuilt(const apc_context *c);
 void apc_mg_clear_prebuilt(apc_context *c);  // a new assembly invalidates a prebuilt hierarchy
 int apc_warm_save(apc_context *c);                       // warmstart.cu

@@ -406,6 +406,7 @@ int apc_select(apc_context *c, int *n_cells) {
   c->prof.select_ms += c->t_select_ms;
   c->numnodes.clear();
   c->have_cells = true;
+  if (++c->select_gen == 0) c->select_gen = 1;
   if (n_cells) *n_cells = c->nc + c->nv + c->nb;
   return APC_OK;
 }
@@ -420,7 +421,10 @@ int apc_solve_part_density(apc_context *c, double c_dens) {
   cudaSetDevice(c->dev);
   c->err.clear();
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[2], c->s));
-  APC_TRY(apc_gfd_assemble(c, c_dens));
+  // multigrid paths: the hierarchy's aggregation is built while the assembly runs, its
+  // operators while the density solve runs
+  const bool overlap = c->cfg.precision != APC_PREC_FP64 && c->cfg.mixed_precond == APC_PRECOND_MULTIGRID;
+  APC_TRY(apc_gfd_assemble(c, c_dens, overlap ? apc_mg_structure_during_assembly : nullptr));
   if (c->cfg.precision == APC_PREC_MIXED) {
     APC_TRY(apc_ensure(c, &c->a1f, (size_t)c->m_cap * c->ell_w, nullptr));
     APC_TRY(apc_ensure(c, &c->a2f, (size_t)c->m_cap * c->ell_w, nullptr));
@@ -431,8 +435,6 @@ int apc_solve_part_density(apc_context *c, double c_dens) {
       APC_TRY(apc_ensure(c, &c->a2f, (size_t)c->m_cap * c->ell_w, nullptr));
   }
   apc_solve_stats &st = c->stats;
-  // multigrid paths: the potential hierarchy is built while the density solve runs
-  const bool overlap = c->cfg.precision != APC_PREC_FP64 && c->cfg.mixed_precond == APC_PRECOND_MULTIGRID;
   if (overlap) APC_TRY(apc_mg_mark_assembled(c));
   APC_CUDA_TRY(c, cudaEventRecord(c->sev[0], c->s));
   APC_TRY(apc_krylov_solve(c, 0, c->rhs, c->density, &st.density_its, &st.density_rnorm, &st.density_reason,

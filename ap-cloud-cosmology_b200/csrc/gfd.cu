@@ -746,7 +746,7 @@ __global__ void __launch_bounds__(256) differentiate_kernel(int m, int lm, int n
 
 }  // namespace
 
-int apc_gfd_assemble(apc_context *c, double c_dens) {
+int apc_gfd_assemble(apc_context *c, double c_dens, int (*during)(apc_context *)) {
   const int M = c->nc + c->nv;
   const int lm = c->lm;
   if (lm > kMaxLm || lm < 9) {
@@ -818,6 +818,7 @@ int apc_gfd_assemble(apc_context *c, double c_dens) {
   APC_CUDA_TRY(c, cudaEventRecord(c->gev[1], c->s));
   apc_count_launch(c, 2);
   APC_CUDA_TRY(c, cudaGetLastError());
+  if (during) APC_TRY(during(c));
   int derr = 0;
   APC_TRY(apc_read_errors(c, &derr));
   float gms = 0.f;

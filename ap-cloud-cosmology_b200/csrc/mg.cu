@@ -1343,11 +1343,30 @@ struct MgLevel {
   size_t ld = 0;
   int *col = nullptr;
   T *val = nullptr, *dinv = nullptr;
-  uint64_t *code = nullptr;
-  int *agg = nullptr;                   // node -> coarser node
-  int *mptr = nullptr, *mem = nullptr;  // members on the finer level (levels >= 1)
+  // the aggregation (MgStruct's arrays, not owned)
+  const int *agg = nullptr;                         // node -> coarser node
+  const int *mptr = nullptr, *mem = nullptr;        // members on the finer level (levels >= 1)
   T *x = nullptr, *x2 = nullptr, *b = nullptr, *r = nullptr;
   bool owns_matrix = true;
+};
+
+// The aggregation of the current cells, level by level: octree-parent codes, the
+// node -> aggregate map and each aggregate's members.  Only the cell codes go in, so it is
+// built while the GFD assembly runs (apc_mg_structure_during_assembly); the operators
+// (Galerkin products) follow the assembly, in the precision of the solve.
+struct MgStructLevel {
+  int n = 0;
+  const uint64_t *code = nullptr;       // level 0: the context's cell codes
+  uint64_t *own_code = nullptr;         // levels >= 1
+  int *agg = nullptr;                   // node -> coarser node (every level but the last)
+  int *mptr = nullptr, *mem = nullptr;  // members on the finer level (levels >= 1)
+};
+
+struct MgStruct {
+  MgStructLevel lv[kMaxLevels];
+  int nlev = 0;
+  unsigned gen = 0;      // the selection it belongs to (apc_context::select_gen; 0: none)
+  bool on_side = false;  // built on the side stream, after which side_ev[2] was recorded
 };
 
 template <class T>
@@ -1362,6 +1381,7 @@ struct MgHier {
 };
 
 struct MgWork {
+  MgStruct st;
   MgHier<float> h32;
   MgHier<double> h64;
   // hierarchy temporaries: parent-code sort, flags, coarse rows before the ELL transpose
@@ -1382,7 +1402,8 @@ struct MgWork {
   int64_t vcycle_nodes[2] = {0, 0};
   // the hierarchy built while the density solve runs (apc_mg_prebuild)
   cudaStream_t side = nullptr;
-  cudaEvent_t side_ev[2] = {nullptr, nullptr};  // operator assembled (main), hierarchy built (side)
+  // operator assembled (main), hierarchy built (side), aggregation built (side)
+  cudaEvent_t side_ev[3] = {nullptr, nullptr, nullptr};
   bool prebuilt = false;
   // the persistent solve kernel: partial sums, grid barrier, outcome (+ its pinned copy)
   double *ppart = nullptr;
@@ -1432,10 +1453,6 @@ static void free_hier(apc_context *c, MgHier<T> &H) {
       apc_free(c, L.val);
     }
     apc_free(c, L.dinv);
-    apc_free(c, L.code);
-    apc_free(c, L.agg);
-    apc_free(c, L.mptr);
-    apc_free(c, L.mem);
     apc_free(c, L.x);
     apc_free(c, L.x2);
     apc_free(c, L.b);
@@ -1450,6 +1467,12 @@ void apc_mg_free(apc_context *c) {
   if (!m) return;
   free_hier(c, m->h32);
   free_hier(c, m->h64);
+  for (auto &L : m->st.lv) {
+    apc_free(c, L.own_code);
+    apc_free(c, L.agg);
+    apc_free(c, L.mptr);
+    apc_free(c, L.mem);
+  }
   void *p[] = {m->pkey, m->pkey_alt, m->pidx, m->pidx_alt, m->eflag, m->epos, m->ucol,
                m->rowstart, m->partial, m->dots, m->counter, m->state, m->total, m->ppart, m->pbar, m->pres};
   for (void *q : p) apc_free(c, q);
@@ -1489,34 +1512,21 @@ const double *scaled_potential<double>(const apc_context *c) {
   return c->a2d;
 }
 
-template <class T>
-static int mg_build(apc_context *c) {
+// The aggregation on c->s: level l + 1's nodes are the distinct parents (code >> 3) of
+// level l's, in code order, down to kCoarsest nodes or until nothing coarsens.
+static int mg_structure(apc_context *c) {
   MgWork *m = mg(c);
-  MgHier<T> &H = hier<T>(m);
-  const int n0 = c->nc + c->nv;
-  MgLevel<T> &L0 = H.lv[0];
-  L0.n = n0;
-  L0.w = c->ell_w;
-  L0.ld = (size_t)c->m_cap;
-  L0.col = c->ell_col;
-  L0.val = const_cast<T *>(scaled_potential<T>(c));
-  L0.owns_matrix = false;
-  APC_TRY(apc_ensure(c, &L0.dinv, (size_t)n0 + 1));
-  APC_TRY(apc_ensure(c, &L0.code, (size_t)n0 + 1));
-  APC_TRY(apc_ensure(c, &L0.x, (size_t)n0 + 1));
-  APC_TRY(apc_ensure(c, &L0.x2, (size_t)n0 + 1));
-  APC_TRY(apc_ensure(c, &L0.b, (size_t)n0 + 1));
-  APC_TRY(apc_ensure(c, &L0.r, (size_t)n0 + 1));
-  APC_CUDA_TRY(c, cudaMemcpyAsync(L0.code, c->ccode, sizeof(uint64_t) * n0, cudaMemcpyDeviceToDevice, c->s));
-  ell_dinv<T><<<grid_for(n0), kT, 0, c->s>>>(n0, L0.ld, L0.val, L0.dinv);
-  apc_count_launch(c);
+  MgStruct &S = m->st;
+  S.gen = 0;
+  S.on_side = false;
+  S.lv[0].n = c->nc + c->nv;
+  S.lv[0].code = c->ccode;
   if (!m->total) APC_TRY(apc_alloc(c, (void **)&m->total, 4 * sizeof(int)));
   int lev = 0;
-  while (H.lv[lev].n > kCoarsest && lev + 1 < kMaxLevels) {
-    MgLevel<T> &F = H.lv[lev];
-    MgLevel<T> &C = H.lv[lev + 1];
+  while (S.lv[lev].n > kCoarsest && lev + 1 < kMaxLevels) {
+    MgStructLevel &F = S.lv[lev];
+    MgStructLevel &C = S.lv[lev + 1];
     const int nf = F.n;
-    // ---- aggregates: parents of this level's nodes ----
     APC_TRY(apc_ensure(c, &m->pkey, (size_t)nf));
     APC_TRY(apc_ensure(c, &m->pkey_alt, (size_t)nf));
     APC_TRY(apc_ensure(c, &m->pidx, (size_t)nf));
@@ -1545,11 +1555,57 @@ static int mg_build(apc_context *c) {
     APC_TRY(read_int(c, m->total, &nc));
     if (nc >= nf) break;  // no coarsening left
     C.n = nc;
-    APC_TRY(apc_ensure(c, &C.code, (size_t)nc + 1));
+    APC_TRY(apc_ensure(c, &C.own_code, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &C.mptr, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &C.mem, (size_t)nf + 1));
-    aggregate_map<<<grid_for(nf), kT, 0, c->s>>>(nf, pk, pi, m->eflag, m->epos, F.agg, C.code, C.mptr, C.mem);
+    C.code = C.own_code;
+    aggregate_map<<<grid_for(nf), kT, 0, c->s>>>(nf, pk, pi, m->eflag, m->epos, F.agg, C.own_code, C.mptr, C.mem);
     apc_count_launch(c);
+    APC_CUDA_TRY(c, cudaGetLastError());
+    ++lev;
+  }
+  S.nlev = lev + 1;
+  S.gen = c->select_gen;
+  return APC_OK;
+}
+
+// The operators over the aggregation, on c->s: the Jacobi-scaled potential operator in
+// precision T on level 0, Galerkin products below it, the coarsest level's inverse.
+template <class T>
+static int mg_build(apc_context *c) {
+  MgWork *m = mg(c);
+  MgStruct &S = m->st;
+  if (S.gen == 0 || S.gen != c->select_gen) {
+    APC_TRY(mg_structure(c));
+  } else if (S.on_side && c->s != m->side) {
+    APC_CUDA_TRY(c, cudaStreamWaitEvent(c->s, m->side_ev[2], 0));
+  }
+  MgHier<T> &H = hier<T>(m);
+  const int n0 = c->nc + c->nv;
+  MgLevel<T> &L0 = H.lv[0];
+  L0.n = n0;
+  L0.w = c->ell_w;
+  L0.ld = (size_t)c->m_cap;
+  L0.col = c->ell_col;
+  L0.val = const_cast<T *>(scaled_potential<T>(c));
+  L0.owns_matrix = false;
+  APC_TRY(apc_ensure(c, &L0.dinv, (size_t)n0 + 1));
+  APC_TRY(apc_ensure(c, &L0.x, (size_t)n0 + 1));
+  APC_TRY(apc_ensure(c, &L0.x2, (size_t)n0 + 1));
+  APC_TRY(apc_ensure(c, &L0.b, (size_t)n0 + 1));
+  APC_TRY(apc_ensure(c, &L0.r, (size_t)n0 + 1));
+  ell_dinv<T><<<grid_for(n0), kT, 0, c->s>>>(n0, L0.ld, L0.val, L0.dinv);
+  apc_count_launch(c);
+  int lev = 0;
+  for (; lev + 1 < S.nlev; ++lev) {
+    MgLevel<T> &F = H.lv[lev];
+    MgLevel<T> &C = H.lv[lev + 1];
+    const int nf = F.n;
+    const int nc = S.lv[lev + 1].n;
+    F.agg = S.lv[lev].agg;
+    C.n = nc;
+    C.mptr = S.lv[lev + 1].mptr;
+    C.mem = S.lv[lev + 1].mem;
     // ---- Galerkin product, one warp per coarse row ----
     const int wcap = 256;
     APC_TRY(apc_ensure(c, &m->rowstart, (size_t)nc + 1));
@@ -1584,8 +1640,8 @@ static int mg_build(apc_context *c) {
                                                  C.dinv);
     apc_count_launch(c);
     APC_CUDA_TRY(c, cudaGetLastError());
-    ++lev;
   }
+  H.lv[lev].agg = S.lv[lev].agg;
   H.nlev = lev + 1;
   {
     int first_tail = 0;
@@ -2158,8 +2214,9 @@ static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, c
   a.M = M;
   // one persistent kernel per solve unless the graph path is asked for (or needed: the
   // re-orthogonalising Gram-Schmidt and the FP32 V-cycle under FP64 vectors run only there)
-  bool persistent = !cfg.mixed_solve_graphs && !cfg.mg_reorth && !mg32;
-  if (persistent && c->defer_solve) {
+  const bool can_persist = !cfg.mg_reorth && !mg32;
+  bool persistent = can_persist && !cfg.mixed_solve_graphs;
+  if (can_persist && c->defer_solve) {
     // prepared for a batched launch with other boxes' solves (apc_mg_batched_solve);
     // apc_ir_finish reads the outcome
     if (use_mg)
@@ -2253,12 +2310,35 @@ int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, cons
                          reason, refinements, levels, during);
 }
 
-int apc_mg_mark_assembled(apc_context *c) {
-  MgWork *m = mg(c);
+static int ensure_side(apc_context *c, MgWork *m) {
   if (!m->side) {
     APC_CUDA_TRY(c, cudaStreamCreateWithFlags(&m->side, cudaStreamNonBlocking));
     for (cudaEvent_t &e : m->side_ev) APC_CUDA_TRY(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
+  return APC_OK;
+}
+
+// Runs while the GFD assembly's kernels execute on the context's stream: the aggregation
+// of the new cells is built on the side stream.  It reads only the cell codes, which were
+// complete when the selection returned to the host.
+int apc_mg_structure_during_assembly(apc_context *c) {
+  MgWork *m = mg(c);
+  APC_TRY(ensure_side(c, m));
+  const auto t0 = std::chrono::steady_clock::now();
+  cudaStream_t main = c->s;
+  c->s = m->side;
+  int rc = mg_structure(c);
+  if (rc == APC_OK && cudaEventRecord(m->side_ev[2], c->s) != cudaSuccess) rc = APC_ERR_CUDA;
+  c->s = main;
+  APC_TRY(rc);
+  m->st.on_side = true;
+  c->prof.mg_build_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return APC_OK;
+}
+
+int apc_mg_mark_assembled(apc_context *c) {
+  MgWork *m = mg(c);
+  APC_TRY(ensure_side(c, m));
   m->prebuilt = false;
   APC_CUDA_TRY(c, cudaEventRecord(m->side_ev[0], c->s));
   return APC_OK;
