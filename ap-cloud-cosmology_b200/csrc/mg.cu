@@ -207,6 +207,94 @@ __global__ void max_int(int n, const int *__restrict__ a, int *out) {
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
+// The coarsest level's explicit inverse: Gauss-Jordan elimination on [A | I] in FP64
+// with partial pivoting (the first row of largest |a_ik| at or below the diagonal), in one
+// block with the augmented matrix in shared memory.  Every element sees the operations of
+// a serial elimination in the same order, each rounded on its own (no contraction), and
+// rows whose multiplier is zero are skipped, so the inverse is the serial one bit for bit.
+// A zero pivot sets *status = 1 and leaves inv unwritten.
+constexpr int kCoarseInvMax = 96;  // [A | I] of 96 rows is 147 KB of shared memory
+
+template <class T>
+__global__ void __launch_bounds__(256) coarse_inverse(int n, int w, size_t ld, const int *__restrict__ col,
+                                                      const T *__restrict__ val, T *__restrict__ inv,
+                                                      int *status) {
+  extern __shared__ double aug[];
+  __shared__ double fk[kCoarseInvMax];
+  __shared__ int piv, singular;
+  const int n2 = 2 * n;
+  for (int e = threadIdx.x; e < n * n2; e += blockDim.x) {
+    const int i = e / n2, j = e - i * n2;
+    aug[e] = (j == n + i) ? 1.0 : 0.0;
+  }
+  if (threadIdx.x == 0) singular = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    for (int q = 0; q < w; ++q) {
+      const size_t at = (size_t)q * ld + i;
+      double &d = aug[(size_t)i * n2 + col[at]];
+      d = __dadd_rn(d, (double)val[at]);
+    }
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    if (threadIdx.x < 32) {
+      double best = -1.0;
+      int bi = n;
+      for (int i = k + threadIdx.x; i < n; i += 32) {
+        const double v = fabs(aug[(size_t)i * n2 + k]);
+        if (v > best) {
+          best = v;
+          bi = i;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      if (threadIdx.x == 0) {
+        piv = bi < n ? bi : k;
+        if (!(aug[(size_t)piv * n2 + k] != 0.0)) singular = 1;
+      }
+    }
+    __syncthreads();
+    if (singular) {
+      if (threadIdx.x == 0) *status = 1;
+      return;
+    }
+    const int p = piv;
+    if (p != k)
+      for (int j = threadIdx.x; j < n2; j += blockDim.x) {
+        const double t = aug[(size_t)p * n2 + j];
+        aug[(size_t)p * n2 + j] = aug[(size_t)k * n2 + j];
+        aug[(size_t)k * n2 + j] = t;
+      }
+    __syncthreads();
+    const double d = 1.0 / aug[(size_t)k * n2 + k];
+    __syncthreads();
+    for (int j = threadIdx.x; j < n2; j += blockDim.x) aug[(size_t)k * n2 + j] = __dmul_rn(aug[(size_t)k * n2 + j], d);
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+      if (i != k) fk[i] = aug[(size_t)i * n2 + k];
+    __syncthreads();
+    for (int e = threadIdx.x; e < n * n2; e += blockDim.x) {
+      const int i = e / n2, j = e - i * n2;
+      const double f = fk[i];
+      if (i == k || f == 0.0) continue;
+      aug[e] = __dsub_rn(aug[e], __dmul_rn(f, aug[(size_t)k * n2 + j]));
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int i = e / n, j = e - i * n;
+    inv[e] = (T)aug[(size_t)i * n2 + n + j];
+  }
+  if (threadIdx.x == 0) *status = 0;
+}
+
 // ------------------------------------------------------------------ V-cycle
 
 template <class V>
@@ -1410,6 +1498,10 @@ struct MgWork {
   GridBar *pbar = nullptr;
   PResult *pres = nullptr;
   PResult *pres_host = nullptr;
+  // the device-side coarse inverse's outcome (0 or 1 = singular) and its pinned copy,
+  // checked after the next solve's readback
+  int *cstat = nullptr;
+  int *cstat_host = nullptr;
   // a solve prepared for a batched launch (apc_mg_batched_solve): its arguments, which
   // solve it is, and whether it is multigrid-preconditioned
   PSolveArgs<float> deferred32{};
@@ -1474,10 +1566,12 @@ void apc_mg_free(apc_context *c) {
     apc_free(c, L.mem);
   }
   void *p[] = {m->pkey, m->pkey_alt, m->pidx, m->pidx_alt, m->eflag, m->epos, m->ucol,
-               m->rowstart, m->partial, m->dots, m->counter, m->state, m->total, m->ppart, m->pbar, m->pres};
+               m->rowstart, m->partial, m->dots, m->counter, m->state, m->total, m->ppart, m->pbar, m->pres,
+               m->cstat};
   for (void *q : p) apc_free(c, q);
   if (m->host) cudaFreeHost(m->host);
   if (m->pres_host) cudaFreeHost(m->pres_host);
+  if (m->cstat_host) cudaFreeHost(m->cstat_host);
   for (int k = 0; k < 2; ++k) {
     if (m->solve_exec[k]) cudaGraphExecDestroy(m->solve_exec[k]);
     if (m->solve_graph[k]) cudaGraphDestroy(m->solve_graph[k]);
@@ -1651,13 +1745,34 @@ static int mg_build(apc_context *c) {
       return APC_ERR_UNSUPPORTED;
     }
   }
-  // ---- coarsest level: explicit inverse in FP64 on the host ----
+  // ---- coarsest level: explicit inverse in FP64 ----
   MgLevel<T> &K = H.lv[lev];
   const int n = K.n;
   if (n > 4 * kCoarsest) {
     c->err = "multigrid coarsening stalled";
     return APC_ERR_UNSUPPORTED;
   }
+  APC_TRY(apc_ensure(c, &H.coarse_inv, (size_t)n * n + 1));
+  H.coarse_n = n;
+  if (n <= kCoarseInvMax) {
+    // on the device, in stream order: no host round trip; a singular operator is reported
+    // by the solve that follows (check_coarse)
+    if (!m->cstat) {
+      APC_TRY(apc_alloc(c, (void **)&m->cstat, sizeof(int)));
+      APC_CUDA_TRY(c, cudaMallocHost((void **)&m->cstat_host, sizeof(int)));
+      APC_CUDA_TRY(c, cudaFuncSetAttribute(coarse_inverse<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kCoarseInvMax * 2 * kCoarseInvMax * (int)sizeof(double)));
+      APC_CUDA_TRY(c, cudaFuncSetAttribute(coarse_inverse<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kCoarseInvMax * 2 * kCoarseInvMax * (int)sizeof(double)));
+    }
+    const size_t smem = (size_t)n * 2 * n * sizeof(double);
+    coarse_inverse<T><<<1, 256, smem, c->s>>>(n, K.w, K.ld, K.col, K.val, H.coarse_inv, m->cstat);
+    apc_count_launch(c);
+    APC_CUDA_TRY(c, cudaGetLastError());
+    APC_CUDA_TRY(c, cudaMemcpyAsync(m->cstat_host, m->cstat, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+    return APC_OK;
+  }
+  // a stalled coarsening leaves more rows: on the host
   std::vector<int> col(K.ld * K.w);
   std::vector<T> val(K.ld * K.w);
   APC_CUDA_TRY(c, cudaMemcpyAsync(col.data(), K.col, sizeof(int) * col.size(), cudaMemcpyDeviceToHost, c->s));
@@ -1697,11 +1812,21 @@ static int mg_build(apc_context *c) {
     }
   }
   std::vector<T> invf(inv.begin(), inv.end());
-  APC_TRY(apc_ensure(c, &H.coarse_inv, (size_t)n * n + 1));
   APC_CUDA_TRY(c, cudaMemcpyAsync(H.coarse_inv, invf.data(), sizeof(T) * invf.size(), cudaMemcpyHostToDevice,
                                   c->s));
   APC_CUDA_TRY(c, apc_stream_wait(c));
-  H.coarse_n = n;
+  if (m->cstat_host) *m->cstat_host = 0;
+  return APC_OK;
+}
+
+// After a host wait that follows the hierarchy build in stream order: the device-side
+// coarse inverse's outcome.
+static int check_coarse(apc_context *c) {
+  MgWork *m = c->mg;
+  if (m && m->cstat_host && *m->cstat_host) {
+    c->err = "singular coarsest multigrid operator";
+    return APC_ERR_RANK;
+  }
   return APC_OK;
 }
 
@@ -2256,6 +2381,7 @@ static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, c
         c->err = "solve kernel grid barrier timed out";
         return APC_ERR_TIMEOUT;
       }
+      if (use_mg) APC_TRY(check_coarse(c));
       const PResult &R = *m->pres_host;
       float ms = 0.f;
       APC_CUDA_TRY(c, cudaEventElapsedTime(&ms, c->kev[0], c->kev[1]));
@@ -2282,6 +2408,7 @@ static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, c
   if (during) APC_TRY(during(c));
   APC_CUDA_TRY(c, apc_stream_wait(c));
   APC_CUDA_TRY(c, cudaGetLastError());
+  if (use_mg) APC_TRY(check_coarse(c));
   const IrState &S = *reinterpret_cast<const IrState *>(m->host);
   float ms = 0.f;
   APC_CUDA_TRY(c, cudaEventElapsedTime(&ms, c->kev[0], c->kev[1]));
@@ -2524,6 +2651,7 @@ int apc_ir_finish(apc_context *c, int *its, double *rnorm, int *reason, int *ref
   if (!m || m->deferred_which < 0) return APC_OK;  // the solve ran at once (FP64 GMRES path)
   APC_CUDA_TRY(c, cudaMemcpyAsync(m->pres_host, m->pres, sizeof(PResult), cudaMemcpyDeviceToHost, c->s));
   APC_CUDA_TRY(c, apc_stream_wait(c));
+  if (m->deferred_mg) APC_TRY(check_coarse(c));
   const PResult &R = *m->pres_host;
   *its = R.total_its;
   *rnorm = R.rn;

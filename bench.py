@@ -389,12 +389,15 @@ def run_ours(args) -> dict:
                 "timing": "device events per step (select to drift), summed; seconds_wall = host clock around "
                           "the whole run incl. the initial select + half drift"}
 
-    # ---- the plain FP64 GPU path from the same state, timed the same way ----
+    # ---- the plain FP64 GPU path over the same steps (the same initial state and warm-up
+    #      steps, so that both arms' timed steps start from warm contexts), timed the same way ----
     fp64 = None
     if not args.no_fp64:
-        g64 = make(binding.APC_PREC_FP64_MULTIGRID, state_parts)
+        g64 = make(binding.APC_PREC_FP64_MULTIGRID, parts)
         c64 = for_config(g64, cfg)
-        c64.t = t_state
+        c64.start()
+        for _ in range(args.warmup):
+            c64.step()
         p64, l64, clk64 = timed(g64, c64)
         fp64_ms = dist.max(p64["step_ms"])
         st64 = g64.solve_stats()
