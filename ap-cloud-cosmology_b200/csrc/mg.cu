@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "apc_internal.cuh"
@@ -315,10 +316,48 @@ __global__ void restrict_sum(int nc, const int *__restrict__ mptr, int nf, const
   }
 }
 
-// The row operations of the grid levels, with G lanes per row: coarse Galerkin rows are
-// 30-70 entries wide, and one thread per row would walk them serially.  The lanes of a
-// group take slots sub, sub + G, ... (the slot-major ELL keeps each slot's rows adjacent,
-// so a warp still reads whole sectors) and add their sums by a fixed shuffle tree.
+// sum over this lane's slots k = sub, sub + g, ... < w of val[k][i] * xj(col[k][i]), added in
+// slot order.  The loads of up to kRowBatch slots are issued before the first product, so
+// a short row costs two dependent round trips to L2 (columns, then the gathered values)
+// rather than two per slot: the coarse levels have few rows per SM, and their time is
+// load latency, not bandwidth.
+template <class V>
+struct RowBatch {
+  static constexpr int n = sizeof(V) == 4 ? 12 : 6;  // registers: 1024-thread blocks have 64
+};
+
+// STREAM: the matrix values are read with the evict-first hint (a pass over data too large
+// to stay in L2, which should not push out the data that can).
+template <class V, int B = RowBatch<V>::n, bool STREAM = false, class XJ>
+__device__ __forceinline__ V row_sum(int w, size_t ld, long long i, int sub, int g, const int *__restrict__ col,
+                                     const V *__restrict__ val, XJ xj) {
+  V sacc = V(0);
+  for (int k0 = sub; k0 < w; k0 += g * B) {
+    int c[B];
+    V a[B], x[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+      const int k = k0 + u * g;
+      if (k < w) {
+        const size_t at = (size_t)k * ld + i;
+        c[u] = col[at];  // the columns are shared with the V-cycle's fine level
+        a[u] = STREAM ? __ldcs(val + at) : val[at];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < B; ++u)
+      if (k0 + u * g < w) x[u] = xj(c[u]);
+#pragma unroll
+    for (int u = 0; u < B; ++u)
+      if (k0 + u * g < w) sacc += a[u] * x[u];
+  }
+  return sacc;
+}
+
+// The row operations of the grid levels, with G lanes per row: the lanes of a group take
+// slots sub, sub + G, ... (the slot-major ELL keeps each slot's rows adjacent, so a warp
+// still reads whole sectors) and add their sums by a fixed shuffle tree.  Levels with few
+// rows get more lanes per row (vcycle), so that each lane's loads fit one batch.
 enum RowOp { kOpFirst2, kOpSweep, kOpResidual, kOpProlongSweep };
 
 template <int G, int OP, class V>
@@ -335,18 +374,14 @@ __global__ void __launch_bounds__(kT) row_op(int n, int w, size_t ld, const int 
     const long long i = tid / G + rd * groups;
     const bool act = i < n;
     V sacc = V(0);
-    if (act) {
-#pragma unroll 4
-      for (int k = sub; k < w; k += G) {
-        const size_t at = (size_t)k * ld + i;
-        const int j = col[at];
-        V xj;
-        if (OP == kOpFirst2) xj = omega * dinv[j] * b[j];
-        else if (OP == kOpProlongSweep) xj = xin[j] + alpha * xc[agg[j]];
-        else xj = xin[j];
-        sacc += val[at] * xj;
-      }
-    }
+    if (act)
+      // one lane per row only on levels with many rows: there occupancy hides the latency,
+      // and a short batch keeps the registers (and so the occupancy) of the old loop
+      sacc = row_sum<V, G == 1 ? 4 : RowBatch<V>::n>(w, ld, i, sub, G, col, val, [&](int j) {
+        if (OP == kOpFirst2) return omega * dinv[j] * b[j];
+        if (OP == kOpProlongSweep) return xin[j] + alpha * xc[agg[j]];
+        return xin[j];
+      });
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
     if (act && sub == 0) {
@@ -397,7 +432,7 @@ constexpr int kConvergedRtol = 2, kConvergedAtol = 3, kDivergedIts = -3, kDiverg
 
 // Every reduction finishes in the last block to arrive, which adds the per-block
 // partials in a fixed order (deterministic).
-constexpr int kRedBlocks = 296;  // grid of the reduction kernels (2 per SM)
+constexpr int kRedBlocks = 444;  // grid of the reduction kernels (3 per SM)
 
 __device__ __forceinline__ bool last_block_arrived(unsigned *counter) {
   __shared__ bool last;
@@ -433,12 +468,13 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // block partials of nv per-lane accumulators: reduced across each warp once, then
 // across the block's warps in warp order
-__device__ __forceinline__ void block_partials(const double (&acc)[32], int nv, double *partial) {
+template <int NV>
+__device__ __forceinline__ void block_partials(const double (&acc)[NV], int nv, double *partial) {
   __shared__ double sm[kT / 32][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   double mine = 0.0;
 #pragma unroll
-  for (int j = 0; j < 32; ++j) {
+  for (int j = 0; j < NV; ++j) {
     if (j < nv) {
       const double p = warp_sum(acc[j]);
       if (lane == j) mine = p;
@@ -466,36 +502,58 @@ __device__ __forceinline__ void block_partial1(double acc, double *partial) {
   }
 }
 
-// One Arnoldi step's scalar work, by one thread: Hessenberg column (h1 + h2, h2 the
-// re-orthogonalisation pass or null), Givens rotations, residual estimate, and whether
-// the cycle goes on (sets the inner loop's condition).
+// One Arnoldi step's scalar work, by the first warp of a block: Hessenberg column (h1 + h2,
+// h2 the re-orthogonalisation pass or null), Givens rotations, residual estimate, and
+// whether the cycle goes on (sets the inner loop's condition).  The lanes load the column
+// and the previous rotations into shared memory at once; lane 0 then runs the serial
+// recurrences there (the same operations in the same order), so the step costs one round
+// trip to memory instead of one per rotation.
 __device__ void arnoldi_step(IrState *S, const double *h1, const double *h2, double nr,
                              cudaGraphConditionalHandle cond) {
+  __shared__ double hs[kMaxM + 2], css[kMaxM], sns[kMaxM];
+  const int lane = threadIdx.x;
   const int it = S->it, M1 = S->M + 1;
-  const double tt = sqrt(nr);
+  if (lane <= it) hs[lane] = __ldcg(h1 + lane) + (h2 ? __ldcg(h2 + lane) : 0.0);
+  if (lane < it) {
+    css[lane] = S->cs[lane];
+    sns[lane] = S->sn[lane];
+  }
+  __syncwarp();
+  if (lane == 0) {
+    const double tt = sqrt(nr);
+    hs[it + 1] = tt;
+    for (int j = 1; j <= it; ++j) {
+      const double t0 = hs[j - 1];
+      hs[j - 1] = css[j - 1] * t0 + sns[j - 1] * hs[j];
+      hs[j] = css[j - 1] * hs[j] - sns[j - 1] * t0;
+    }
+    const double t = sqrt(hs[it] * hs[it] + hs[it + 1] * hs[it + 1]);
+    bool more = false;
+    if (t != 0.0 && t == t) {
+      const double cs = hs[it] / t, sn = hs[it + 1] / t;
+      S->cs[it] = cs;
+      S->sn[it] = sn;
+      const double g = S->g[it];
+      S->g[it + 1] = -sn * g;
+      S->g[it] = cs * g;
+      hs[it] = cs * hs[it] + sn * hs[it + 1];
+      more = !(fabs(S->g[it + 1]) <= S->rtol_in * S->beta) && tt != 0.0;
+    }
+    S->it = it + 1;
+    more = more && S->it < S->inner_max;
+    S->scale = tt > 0.0 ? 1.0 / tt : 0.0;
+    cudaGraphSetConditional(cond, more ? 1u : 0u);
+  }
+  __syncwarp();
   double *hc = S->H + (size_t)it * M1;
-  for (int j = 0; j <= it; ++j) hc[j] = __ldcg(h1 + j) + (h2 ? __ldcg(h2 + j) : 0.0);
-  hc[it + 1] = tt;
-  for (int j = 1; j <= it; ++j) {
-    const double t0 = hc[j - 1];
-    hc[j - 1] = S->cs[j - 1] * t0 + S->sn[j - 1] * hc[j];
-    hc[j] = S->cs[j - 1] * hc[j] - S->sn[j - 1] * t0;
-  }
-  const double t = sqrt(hc[it] * hc[it] + hc[it + 1] * hc[it + 1]);
-  bool more = false;
-  if (t != 0.0 && t == t) {
-    const double cs = hc[it] / t, sn = hc[it + 1] / t;
-    S->cs[it] = cs;
-    S->sn[it] = sn;
-    S->g[it + 1] = -sn * S->g[it];
-    S->g[it] = cs * S->g[it];
-    hc[it] = cs * hc[it] + sn * hc[it + 1];
-    more = !(fabs(S->g[it + 1]) <= S->rtol_in * S->beta) && tt != 0.0;
-  }
-  S->it = it + 1;
-  more = more && S->it < S->inner_max;
-  S->scale = tt > 0.0 ? 1.0 / tt : 0.0;
-  cudaGraphSetConditional(cond, more ? 1u : 0u);
+  if (lane <= it + 1) hc[lane] = hs[lane];
+}
+
+// a basis-vector load of the Krylov passes (evict-first in FP64, see kKrylovStream)
+template <class T>
+__device__ __forceinline__ T ld_krylov(const T *p) {
+  if constexpr (sizeof(T) == 8) return __ldcs(p);
+  else return *p;
 }
 
 // Basis vectors V_0..V_it are rows of V (stride vn); the vector being orthogonalised is
@@ -503,7 +561,7 @@ __device__ void arnoldi_step(IrState *S, const double *h1, const double *h2, dou
 // (one per lane); a row's basis values stay in registers for the update and the dots.
 //   MODE 1: w -= V h_in; h = V^T w.   MODE 2: w -= V h_in; out[0] = ||w||^2.
 // MODE 2 also finishes the Arnoldi step in its last block (h1, h2 as arnoldi_step).
-template <int MODE, class T>
+template <int MODE, class T, int NV>
 __global__ void __launch_bounds__(kT) cgs_pass(int n, IrState *S, T *V, size_t vn,
                                                 const double *__restrict__ h_in, double *partial, unsigned *counter,
                                                 double *out, const double *h1, const double *h2,
@@ -514,32 +572,32 @@ __global__ void __launch_bounds__(kT) cgs_pass(int n, IrState *S, T *V, size_t v
   if ((int)threadIdx.x < nv) hsh[threadIdx.x] = h_in[threadIdx.x];
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  double acc[32];
+  double acc[NV];
 #pragma unroll
-  for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+  for (int j = 0; j < NV; ++j) acc[j] = 0.0;
   double acc1 = 0.0;
   const int ntiles = (n + 31) / 32;
   for (int tile = blockIdx.x * nw + warp; tile < ntiles; tile += gridDim.x * nw) {
     const int i = tile * 32 + lane;
     const bool ok = i < n;
     if (MODE == 1) {
-      T vj[32];
+      T vj[NV];
 #pragma unroll
-      for (int j = 0; j < 32; ++j) vj[j] = (j < nv && ok) ? V[(size_t)j * vn + i] : T(0);
+      for (int j = 0; j < NV; ++j) vj[j] = (j < nv && ok) ? ld_krylov(V + (size_t)j * vn + i) : T(0);
       double wi = ok ? (double)w[i] : 0.0;
 #pragma unroll
-      for (int j = 0; j < 32; ++j)
+      for (int j = 0; j < NV; ++j)
         if (j < nv) wi -= hsh[j] * (double)vj[j];
       if (ok) w[i] = (T)wi;
       wi = (double)(T)wi;
 #pragma unroll
-      for (int j = 0; j < 32; ++j)
+      for (int j = 0; j < NV; ++j)
         if (j < nv) acc[j] += wi * (double)vj[j];
     } else if (ok) {
       double wi = (double)w[i];
 #pragma unroll
-      for (int j = 0; j < 32; ++j)
-        if (j < nv) wi -= hsh[j] * (double)V[(size_t)j * vn + i];
+      for (int j = 0; j < NV; ++j)
+        if (j < nv) wi -= hsh[j] * (double)ld_krylov(V + (size_t)j * vn + i);
       w[i] = (T)wi;
       wi = (double)(T)wi;
       acc1 += wi * wi;
@@ -553,16 +611,26 @@ __global__ void __launch_bounds__(kT) cgs_pass(int n, IrState *S, T *V, size_t v
     if (last_block_arrived(counter)) {
       finish_sums(1, partial, counter, out);
       __syncthreads();
-      if (threadIdx.x == 0) arnoldi_step(S, h1, h2, __ldcg(out), cond);
+      if (threadIdx.x < 32) arnoldi_step(S, h1, h2, __ldcg(out), cond);
     }
   }
 }
 
+// slots per batch of the Krylov SpMV: with 16 basis vectors three 256-thread blocks fit
+// an SM (85 registers, the dot accumulators taking 32), with 32 two
+template <class T>
+constexpr int kSpmvBatch = sizeof(T) == 4 ? 8 : 4;
+// FP64 Krylov passes (the operator and the basis, ~130 MB at 128^3) stream with the
+// evict-first hint so that the FP32 V-cycle's levels (~50 MB) stay in the 126 MB L2
+// between iterations; the FP32 passes fit beside them
+template <class T>
+constexpr bool kKrylovStream = sizeof(T) == 8;
+
 // V_{it+1} = A z and the dots <V_{it+1}, V_j>, j <= it, in the same warp-tile pass.
 // With a preconditioner z is its output, kept as Z_it for the solution; without one
 // (Z == nullptr) z is V_it itself.
-template <class T, class TZ = T>
-__global__ void __launch_bounds__(kT) spmv_dots(int n, int ew, size_t ld, const int *__restrict__ col,
+template <class T, class TZ, int NV>
+__global__ void __launch_bounds__(kT, NV <= 16 ? 3 : 2) spmv_dots(int n, int ew, size_t ld, const int *__restrict__ col,
                                                  const T *__restrict__ val, const TZ *zin, T *Z,
                                                  T *V, size_t vn, const IrState *__restrict__ S, double *partial,
                                                  unsigned *counter, double *out) {
@@ -573,31 +641,27 @@ __global__ void __launch_bounds__(kT) spmv_dots(int n, int ew, size_t ld, const 
   T *zk = Z ? Z + (size_t)it * vn : nullptr;
   T *w = V + (size_t)nv * vn;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  double acc[32];
+  double acc[NV];
 #pragma unroll
-  for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+  for (int j = 0; j < NV; ++j) acc[j] = 0.0;
   const int ntiles = (n + 31) / 32;
   for (int tile = blockIdx.x * nw + warp; tile < ntiles; tile += gridDim.x * nw) {
     const int i = tile * 32 + lane;
     if (i >= n) continue;
-    T sacc = T(0);
+    T sacc;
     if (Z) {
-      for (int k = 0; k < ew; ++k) {
-        const size_t at = (size_t)k * ld + i;
-        sacc += val[at] * (T)zp[col[at]];
-      }
+      sacc = row_sum<T, kSpmvBatch<T>, kKrylovStream<T>>(ew, ld, i, 0, 1, col, val,
+                                                          [&](int j) { return (T)zp[j]; });
       zk[i] = (T)zp[i];
     } else {
-      for (int k = 0; k < ew; ++k) {
-        const size_t at = (size_t)k * ld + i;
-        sacc += val[at] * zv[col[at]];
-      }
+      sacc = row_sum<T, kSpmvBatch<T>, kKrylovStream<T>>(ew, ld, i, 0, 1, col, val,
+                                                          [&](int j) { return zv[j]; });
     }
     w[i] = sacc;
     const double wi = (double)sacc;
 #pragma unroll
-    for (int j = 0; j < 32; ++j)
-      if (j < nv) acc[j] += wi * (double)V[(size_t)j * vn + i];
+    for (int j = 0; j < NV; ++j)
+      if (j < nv) acc[j] += wi * (double)ld_krylov(V + (size_t)j * vn + i);
   }
   block_partials(acc, nv, partial);
   if (last_block_arrived(counter)) finish_sums(nv, partial, counter, out);
@@ -617,16 +681,24 @@ __global__ void scale_next(int n, const IrState *__restrict__ S, T *__restrict__
 }
 
 // y = H^-1 g (upper triangular) for the cycle's iterations
+// (one warp: the triangle and g are staged in shared memory, lane 0 solves)
 __global__ void fg_finish(IrState *S) {
-  if (threadIdx.x != 0) return;
+  __shared__ double Hs[(kMaxM + 1) * kMaxM], gs[kMaxM + 1], ys[kMaxM];
   const int it = S->it, M1 = S->M + 1;
-  for (int k = it - 1; k >= 0; --k) {
-    double s = S->g[k];
-    for (int j = k + 1; j < it; ++j) s -= S->H[(size_t)j * M1 + k] * S->y[j];
-    const double hkk = S->H[(size_t)k * M1 + k];
-    S->y[k] = hkk != 0.0 ? s / hkk : 0.0;
+  for (int e = threadIdx.x; e < it * M1; e += blockDim.x) Hs[e] = S->H[e];
+  for (int k = threadIdx.x; k < it; k += blockDim.x) gs[k] = S->g[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = it - 1; k >= 0; --k) {
+      double s = gs[k];
+      for (int j = k + 1; j < it; ++j) s -= Hs[(size_t)j * M1 + k] * ys[j];
+      const double hkk = Hs[(size_t)k * M1 + k];
+      ys[k] = hkk != 0.0 ? s / hkk : 0.0;
+    }
+    S->total_its += it;
   }
-  S->total_its += it;
+  __syncthreads();
+  for (int k = threadIdx.x; k < it; k += blockDim.x) S->y[k] = ys[k];
 }
 
 // d = Z y
@@ -795,92 +867,265 @@ struct TailArgs {
   V omega, alpha;
 };
 
-// (A x)_i for every row of a tail level, L.g lanes per row; emit(i, sum) runs on the
-// group's first lane.  The trip count is the same for the whole block (shuffles).
-template <class V, class F>
-__device__ __forceinline__ void tail_rows(const TailLevel<V> &L, const V *xin, F emit) {
+// lanes per row of a tail level run by `threads` threads: as many as keep the level in one
+// round, at most 16 and no more than the row's slots
+static inline int tail_lanes(int n, int w, int threads) {
+  int g = 1;
+  while (g < 16 && g < w && 2 * g * n <= threads) g *= 2;
+  return g;
+}
+
+// the graph path's tail kernel: 512 threads leave 128 registers a thread for the batched
+// row loads (a 1024-thread block has 64)
+constexpr int kTailThreads = 512;
+
+// sum_j a_ij xj(j) for every row of a tail level, L.g lanes per row; emit(i, sum) runs on
+// the group's first lane.  The trip count is the same for the whole block (shuffles).
+template <class V, int B, class XJ, class F>
+__device__ __forceinline__ void tail_rows(const TailLevel<V> L, XJ xj, F emit) {
   const int g = L.g, sub = threadIdx.x & (g - 1);
   const int per = blockDim.x / g;
   const int rounds = (L.n + per - 1) / per;
   for (int rd = 0; rd < rounds; ++rd) {
     const int i = (int)threadIdx.x / g + rd * per;
     V sacc = V(0);
-    if (i < L.n)
-#pragma unroll 4
-      for (int k = sub; k < L.w; k += g) {
-        const size_t at = (size_t)k * L.ld + i;
-        sacc += L.val[at] * xin[L.col[at]];
-      }
+    if (i < L.n) sacc = row_sum<V, B>(L.w, L.ld, i, sub, g, L.col, L.val, xj);
     for (int o = g >> 1; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
     if (i < L.n && sub == 0) emit(i, sacc);
   }
 }
 
-template <class V>
-__device__ __forceinline__ void tail_sweep(const TailLevel<V> &L, const V *xin, V *xout, V omega) {
-  tail_rows(L, xin, [&](int i, V sacc) { xout[i] = xin[i] + omega * L.dinv[i] * (L.b[i] - sacc); });
-  __syncthreads();
-}
-
 // The tail's levels in one block (every thread of the block takes part; the block
-// barriers separate the phases).
-template <class V>
+// barriers separate the phases).  Per level: pre-smoothing (the first two sweeps from
+// zero in one pass), residual and restriction in one pass, and on the way up the coarse
+// correction inside the first post-sweep, so a level costs four barriers.  The
+// pre-smoothed iterate is placed so that the post-sweeps end in L.x.  B: slots per lane whose
+// loads are issued together (registers).
+template <class V, int B>
 __device__ __forceinline__ void tail_body(const TailArgs<V> &A) {
-  V *cur[kTailLevels];
+  const V om = A.omega, al = A.alpha;
+  const int sw = A.sweeps;
+  V *cur[kTailLevels];  // each level's pre-smoothed iterate
   for (int l = 0; l < A.nl - 1; ++l) {
-    const TailLevel<V> &L = A.L[l];
-    for (int i = threadIdx.x; i < L.n; i += blockDim.x) L.x[i] = A.omega * L.dinv[i] * L.b[i];
-    __syncthreads();
-    V *c = L.x, *o = L.x2;
-    for (int k = 1; k < A.sweeps; ++k) {
-      tail_sweep(L, c, o, A.omega);
-      V *t = c; c = o; o = t;
+    const TailLevel<V> L = A.L[l];  // by value: the stores below cannot alias it
+    V *c;
+    if (sw >= 2) {
+      tail_rows<V, B>(L, [&](int j) { return om * L.dinv[j] * L.b[j]; }, [&](int i, V sacc) {
+        const V x1 = om * L.dinv[i] * L.b[i];
+        L.x[i] = x1 + om * L.dinv[i] * (L.b[i] - sacc);
+      });
+      __syncthreads();
+      c = L.x;
+      V *o = L.x2;
+      for (int k = 2; k < sw; ++k) {
+        tail_rows<V, B>(L, [&](int j) { return c[j]; },
+                  [&](int i, V sacc) { o[i] = c[i] + om * L.dinv[i] * (L.b[i] - sacc); });
+        __syncthreads();
+        V *t = c; c = o; o = t;
+      }
+    } else {
+      for (int i = threadIdx.x; i < L.n; i += blockDim.x) L.x2[i] = om * L.dinv[i] * L.b[i];
+      __syncthreads();
+      c = L.x2;
     }
     cur[l] = c;
-    tail_rows(L, c, [&](int i, V sacc) { L.r[i] = L.b[i] - sacc; });
-    __syncthreads();
-    const TailLevel<V> &C = A.L[l + 1];
-    for (int I = threadIdx.x; I < C.n; I += blockDim.x) {
-      const int a = C.mptr[I], e = (I + 1 < C.n) ? C.mptr[I + 1] : L.n;
-      V sacc = V(0);
-      for (int q = a; q < e; ++q) sacc += L.r[C.mem[q]];
-      C.b[I] = sacc;
+    // residual of every member row and the coarse row's sum, in member order: 8 lanes per
+    // coarse row, one member row each (more members go round in turns)
+    const TailLevel<V> C = A.L[l + 1];
+    const int lane8 = threadIdx.x & 7, per = blockDim.x / 8;
+    const int rounds = (C.n + per - 1) / per;
+    for (int rd = 0; rd < rounds; ++rd) {
+      const int I = (int)threadIdx.x / 8 + rd * per;
+      const bool act = I < C.n;
+      const int q0 = act ? C.mptr[I] : 0, q1 = act ? ((I + 1 < C.n) ? C.mptr[I + 1] : L.n) : 0;
+      // turns of 8 members: the same count across the warp, for the shuffles
+      const int turns = __reduce_max_sync(0xffffffffu, (unsigned)((q1 - q0 + 7) / 8));
+      V total = V(0);
+      for (int tn = 0; tn < turns; ++tn) {
+        const int qb = q0 + 8 * tn;
+        const int q = qb + lane8;
+        V r = V(0);
+        if (q < q1) {
+          const int i = C.mem[q];
+          r = L.b[i] - row_sum<V, B>(L.w, L.ld, i, 0, 1, L.col, L.val, [&](int j) { return c[j]; });
+        }
+        const int cnt = min(8, q1 - qb);
+        for (int m = 0; m < 8; ++m) {
+          const V t = __shfl_sync(0xffffffffu, r, (threadIdx.x & 31 & ~7) + m, 32);
+          if (m < cnt) total += t;
+        }
+      }
+      if (act && lane8 == 0) C.b[I] = total;
     }
     __syncthreads();
   }
   {
-    const TailLevel<V> &K = A.L[A.nl - 1];
-    for (int i = threadIdx.x; i < K.n; i += blockDim.x) {
+    // the coarsest level: x = K^-1 b, g lanes per row (a row is up to 96 entries)
+    const TailLevel<V> K = A.L[A.nl - 1];
+    const V *inv = A.inv;
+    const int nk = K.n;
+    int g = 32;
+    while (g > 1 && g * nk > (int)blockDim.x) g >>= 1;
+    const int sub = threadIdx.x & (g - 1), per = blockDim.x / g;
+    const int rounds = (nk + per - 1) / per;
+    for (int rd = 0; rd < rounds; ++rd) {
+      const int i = (int)threadIdx.x / g + rd * per;
       V sacc = V(0);
-      for (int j = 0; j < K.n; ++j) sacc += A.inv[(size_t)i * K.n + j] * K.b[j];
-      K.x[i] = sacc;
+      if (i < nk)
+#pragma unroll 4
+        for (int j = sub; j < nk; j += g) sacc += inv[(size_t)i * nk + j] * K.b[j];
+      for (int o = g >> 1; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
+      if (i < nk && sub == 0) K.x[i] = sacc;
     }
     __syncthreads();
-    cur[A.nl - 1] = K.x;
   }
   for (int l = A.nl - 2; l >= 0; --l) {
-    const TailLevel<V> &L = A.L[l];
+    const TailLevel<V> L = A.L[l];  // by value: the stores below cannot alias it
+    const V *xc = A.L[l + 1].x;
     V *c = cur[l];
     V *o = (c == L.x) ? L.x2 : L.x;
-    const V *xc = cur[l + 1];
-    for (int i = threadIdx.x; i < L.n; i += blockDim.x) c[i] += A.alpha * xc[L.agg[i]];
+    tail_rows<V, B>(L, [&](int j) { return c[j] + al * xc[L.agg[j]]; }, [&](int i, V sacc) {
+      const V y = c[i] + al * xc[L.agg[i]];
+      o[i] = y + om * L.dinv[i] * (L.b[i] - sacc);
+    });
     __syncthreads();
-    for (int k = 0; k < A.sweeps; ++k) {
-      tail_sweep(L, c, o, A.omega);
+    { V *t = c; c = o; o = t; }
+    for (int k = 1; k < sw; ++k) {
+      tail_rows<V, B>(L, [&](int j) { return c[j]; },
+                [&](int i, V sacc) { o[i] = c[i] + om * L.dinv[i] * (L.b[i] - sacc); });
+      __syncthreads();
       V *t = c; c = o; o = t;
     }
-    if (c != L.x) {
-      for (int i = threadIdx.x; i < L.n; i += blockDim.x) L.x[i] = c[i];
-      __syncthreads();
-    }
-    cur[l] = L.x;
   }
 }
 
+template <class V>
+__global__ void __launch_bounds__(kTailThreads) vcycle_tail(TailArgs<V> A) {
+  tail_body<V, RowBatch<V>::n>(A);
+}
+
+constexpr size_t kTailSmemMax = 227 * 1024;  // dynamic shared memory a block may opt into
+
+// The tail with every level staged in shared memory (the levels are constant for a solve
+// and, at a few hundred rows, take tens of KB): each launch copies the tail's matrices,
+// maps and the first level's right-hand side in, runs the same body on the copies, and
+// writes the first level's solution back.  Staging turns each phase's gathers from L2
+// round trips into shared-memory loads.  The layout is tail_smem_bytes's.
+__host__ __device__ inline size_t tail_align(size_t b) { return (b + 15) & ~(size_t)15; }
 
 template <class V>
-__global__ void __launch_bounds__(1024) vcycle_tail(TailArgs<V> A) {
-  tail_body(A);
+__host__ __device__ inline size_t tail_smem_bytes(const TailArgs<V> &A) {
+  size_t b = tail_align(sizeof(TailArgs<V>));
+  for (int k = 0; k < A.nl; ++k) {
+    const size_t n = (size_t)A.L[k].n, nw = n * (size_t)A.L[k].w;
+    b += tail_align(nw * sizeof(int)) + tail_align(nw * sizeof(V)) + tail_align(n * sizeof(V));  // col, val, dinv
+    if (k + 1 < A.nl) b += tail_align(n * sizeof(int));                                          // agg
+    if (k > 0) b += tail_align(n * sizeof(int)) + tail_align((size_t)A.L[k - 1].n * sizeof(int)); // mptr, mem
+    b += 4 * tail_align(n * sizeof(V));                                                          // x, x2, b, r
+  }
+  const size_t nk = (size_t)A.L[A.nl - 1].n;
+  return b + tail_align(nk * nk * sizeof(V));  // the coarsest inverse
+}
+
+// Block-wide asynchronous copy of `bytes` (a multiple of 4) from global to shared memory:
+// 16-byte cp.async where both addresses allow it, 4-byte otherwise.  Completion is waited
+// for by stage_wait.
+__device__ __forceinline__ void stage_copy(void *dst, const void *src, size_t bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const char *sp = static_cast<const char *>(src);
+  size_t done = 0;
+  if (((reinterpret_cast<uintptr_t>(src) | d) & 15) == 0) {
+    const size_t n16 = bytes / 16;
+    for (size_t k = threadIdx.x; k < n16; k += blockDim.x)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d + (unsigned)(16 * k)), "l"(sp + 16 * k)
+                   : "memory");
+    done = n16 * 16;
+  }
+  for (size_t k = done / 4 + threadIdx.x; k < bytes / 4; k += blockDim.x)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d + (unsigned)(4 * k)), "l"(sp + 4 * k)
+                 : "memory");
+}
+
+__device__ __forceinline__ void stage_wait() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
+}
+
+template <class V>
+__global__ void __launch_bounds__(kTailThreads) vcycle_tail_smem(TailArgs<V> A) {
+  extern __shared__ __align__(16) unsigned char tsm[];
+  TailArgs<V> &S = *reinterpret_cast<TailArgs<V> *>(tsm);
+  unsigned char *p = tsm + tail_align(sizeof(TailArgs<V>));
+  auto take = [&](size_t bytes) {
+    unsigned char *q = p;
+    p += tail_align(bytes);
+    return q;
+  };
+  const int t = threadIdx.x, T = blockDim.x;
+  if (t == 0) S = A;
+  __syncthreads();
+  for (int k = 0; k < A.nl; ++k) {
+    const TailLevel<V> &G = A.L[k];
+    const int n = G.n, w = G.w;
+    int *col = (int *)take((size_t)n * w * sizeof(int));
+    V *val = (V *)take((size_t)n * w * sizeof(V));
+    V *dinv = (V *)take((size_t)n * sizeof(V));
+    if (G.ld == (size_t)n) {
+      // coarse levels: the slot-major arrays are contiguous
+      stage_copy(col, G.col, (size_t)n * w * sizeof(int));
+      stage_copy(val, G.val, (size_t)n * w * sizeof(V));
+    } else {
+      for (int e = t; e < n * w; e += T) {
+        const int slot = e / n, i = e - slot * n;
+        const size_t at = (size_t)slot * G.ld + i;
+        col[e] = G.col[at];
+        val[e] = G.val[at];
+      }
+    }
+    stage_copy(dinv, G.dinv, (size_t)n * sizeof(V));
+    int *agg = nullptr, *mptr = nullptr, *mem = nullptr;
+    if (k + 1 < A.nl) {
+      agg = (int *)take((size_t)n * sizeof(int));
+      stage_copy(agg, G.agg, (size_t)n * sizeof(int));
+    }
+    if (k > 0) {
+      const int nf = A.L[k - 1].n;
+      mptr = (int *)take((size_t)n * sizeof(int));
+      mem = (int *)take((size_t)nf * sizeof(int));
+      stage_copy(mptr, G.mptr, (size_t)n * sizeof(int));
+      stage_copy(mem, G.mem, (size_t)nf * sizeof(int));
+    }
+    V *x = (V *)take((size_t)n * sizeof(V));
+    V *x2 = (V *)take((size_t)n * sizeof(V));
+    V *b = (V *)take((size_t)n * sizeof(V));
+    V *r = (V *)take((size_t)n * sizeof(V));
+    if (k == 0) stage_copy(b, G.b, (size_t)n * sizeof(V));
+    if (t == 0) {
+      TailLevel<V> &D = S.L[k];
+      D.ld = (size_t)n;
+      D.col = col;
+      D.val = val;
+      D.dinv = dinv;
+      D.agg = agg;
+      D.mptr = mptr;
+      D.mem = mem;
+      D.x = x;
+      D.x2 = x2;
+      D.b = b;
+      D.r = r;
+    }
+  }
+  {
+    const int nk = A.L[A.nl - 1].n;
+    V *inv = (V *)take((size_t)nk * nk * sizeof(V));
+    stage_copy(inv, A.inv, (size_t)nk * nk * sizeof(V));
+    if (t == 0) S.inv = inv;
+  }
+  stage_wait();
+  tail_body<V, RowBatch<V>::n>(S);
+  __syncthreads();
+  for (int i = t; i < A.L[0].n; i += T) A.L[0].x[i] = S.L[0].x[i];
 }
 // ---------------------------------------------- the whole solve as one persistent kernel
 //
@@ -1137,7 +1382,7 @@ __device__ bool p_vcycle(const Grp &g, const PSolveArgs<T> &A, const T *bsrc, T 
       for (int i = threadIdx.x; i < L.n; i += blockDim.x) L.b[i] = bs * bsrc[i];
       __syncthreads();
     }
-    tail_body(A.ta);
+    tail_body<T, 4>(A.ta);
     if (A.tail == 0) {
       const PLevel<T> &L = A.L[0];
       for (int i = threadIdx.x; i < L.n; i += blockDim.x) zout[i] = L.x[i];
@@ -1502,6 +1747,7 @@ struct MgWork {
   // checked after the next solve's readback
   int *cstat = nullptr;
   int *cstat_host = nullptr;
+  bool tail_smem_set = false;  // the staged tail kernels may take kTailSmemMax
   // a solve prepared for a batched launch (apc_mg_batched_solve): its arguments, which
   // solve it is, and whether it is multigrid-preconditioned
   PSolveArgs<float> deferred32{};
@@ -1754,6 +2000,13 @@ static int mg_build(apc_context *c) {
   }
   APC_TRY(apc_ensure(c, &H.coarse_inv, (size_t)n * n + 1));
   H.coarse_n = n;
+  if (!m->tail_smem_set) {
+    APC_CUDA_TRY(c, cudaFuncSetAttribute(vcycle_tail_smem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTailSmemMax));
+    APC_CUDA_TRY(c, cudaFuncSetAttribute(vcycle_tail_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTailSmemMax));
+    m->tail_smem_set = true;
+  }
   if (n <= kCoarseInvMax) {
     // on the device, in stream order: no host round trip; a singular operator is reported
     // by the solve that follows (check_coarse)
@@ -1856,9 +2109,7 @@ static void vcycle(apc_context *c, cudaStream_t s, int l, const T *b, T *x) {
       D.n = Q.n;
       D.w = Q.w;
       // wide rows get several lanes while the block has lanes to spare
-      D.g = 1;
-      if (Q.w > 24)
-        while (D.g < 8 && 2 * D.g * Q.n <= 1024) D.g *= 2;
+      D.g = tail_lanes(Q.n, Q.w, kTailThreads);
       D.ld = Q.ld;
       D.col = Q.col;
       D.val = Q.val;
@@ -1871,13 +2122,21 @@ static void vcycle(apc_context *c, cudaStream_t s, int l, const T *b, T *x) {
       D.x2 = Q.x2;
       D.r = Q.r;
     }
-    vcycle_tail<T><<<1, 1024, 0, s>>>(A);
+    // staged in shared memory when the tail's levels fit (they do at 128^3: ~90 KB in FP32)
+    const size_t tb = tail_smem_bytes(A);
+    if (tb <= kTailSmemMax)
+      vcycle_tail_smem<T><<<1, kTailThreads, tb, s>>>(A);
+    else
+      vcycle_tail<T><<<1, kTailThreads, 0, s>>>(A);
     apc_count_launch(c);
     return;
   }
   MgLevel<T> &C = H.lv[l + 1];
-  // lanes per row from the width of this level's rows
-  const int g = L.w <= 24 ? 1 : (L.w <= 48 ? 4 : 8);
+  // lanes per row: wide rows get several, and so do levels with few rows (up to one
+  // resident lane-group per SM thread slot), whose time is load latency
+  int g = L.w <= 24 ? 1 : (L.w <= 48 ? 4 : 8);
+  const long long budget = (long long)apc_sm_count(c) * 1024;
+  while (g < 16 && g < L.w && 2LL * g * n <= budget) g *= 2;
   const int G = grid_for((long long)n * g);
   auto op = [&](int kind, const T *xin, T *out) {
 #define APC_ROW_OP(GG)                                                                                            \
@@ -1900,10 +2159,14 @@ static void vcycle(apc_context *c, cudaStream_t s, int l, const T *b, T *x) {
   }
     if (g == 1) {
       APC_ROW_OP(1)
+    } else if (g == 2) {
+      APC_ROW_OP(2)
     } else if (g == 4) {
       APC_ROW_OP(4)
-    } else {
+    } else if (g == 8) {
       APC_ROW_OP(8)
+    } else {
+      APC_ROW_OP(16)
     }
 #undef APC_ROW_OP
     apc_count_launch(c);
@@ -2042,20 +2305,30 @@ static int capture_solve(apc_context *c, const IrSolveArgs<T> &a) {
           else if (a.mg)
             vcycle<T>(c, s2, 0, H.vin, H.vout);
           m->vcycle_nodes[slot] = c->launches - v0;
-          if (v32)
-            spmv_dots<T, float><<<G, kT, 0, s2>>>(n, a.w, a.ld, a.col, a.valf, H32.vout, Z, H.V, vn, m->state,
-                                                  m->partial, m->counter, h1);
+          // basis vectors per cycle: 16 (the potential's FGMRES(16)) or up to 32; the dot
+          // accumulators are registers
+          auto krylov = [&](auto nvt) {
+            constexpr int NV = decltype(nvt)::value;
+            if (v32)
+              spmv_dots<T, float, NV><<<G, kT, 0, s2>>>(n, a.w, a.ld, a.col, a.valf, H32.vout, Z, H.V, vn,
+                                                        m->state, m->partial, m->counter, h1);
+            else
+              spmv_dots<T, T, NV><<<G, kT, 0, s2>>>(n, a.w, a.ld, a.col, a.valf, a.mg ? H.vout : nullptr, Z, H.V,
+                                                    vn, m->state, m->partial, m->counter, h1);
+            if (reorth) {
+              cgs_pass<1, T, NV><<<G, kT, 0, s2>>>(n, m->state, H.V, vn, h1, m->partial, m->counter, h2, nullptr,
+                                                   nullptr, cond_in);
+              cgs_pass<2, T, NV><<<G, kT, 0, s2>>>(n, m->state, H.V, vn, h2, m->partial, m->counter, nr, h1, h2,
+                                                   cond_in);
+            } else {
+              cgs_pass<2, T, NV><<<G, kT, 0, s2>>>(n, m->state, H.V, vn, h1, m->partial, m->counter, nr, h1,
+                                                   nullptr, cond_in);
+            }
+          };
+          if (a.M <= 16)
+            krylov(std::integral_constant<int, 16>{});
           else
-            spmv_dots<T><<<G, kT, 0, s2>>>(n, a.w, a.ld, a.col, a.valf, a.mg ? H.vout : nullptr, Z, H.V, vn,
-                                           m->state, m->partial, m->counter, h1);
-          if (reorth) {
-            cgs_pass<1, T><<<G, kT, 0, s2>>>(n, m->state, H.V, vn, h1, m->partial, m->counter, h2, nullptr, nullptr,
-                                             cond_in);
-            cgs_pass<2, T><<<G, kT, 0, s2>>>(n, m->state, H.V, vn, h2, m->partial, m->counter, nr, h1, h2, cond_in);
-          } else {
-            cgs_pass<2, T><<<G, kT, 0, s2>>>(n, m->state, H.V, vn, h1, m->partial, m->counter, nr, h1, nullptr,
-                                             cond_in);
-          }
+            krylov(std::integral_constant<int, 32>{});
           if (v32)
             scale_next<T, float><<<Gs, kT, 0, s2>>>(n, m->state, H.V, vn, vin32);
           else
@@ -2182,8 +2455,7 @@ static int fill_psolve(apc_context *c, const IrSolveArgs<T> &a, PSolveArgs<T> &P
       D.w = Q.w;
       // lanes per row: each lane takes at most 8 of the row's slots (a row's slots are a
       // chain of dependent gathers per lane), the block's rows then run in rounds
-      D.g = 1;
-      while (D.g < 16 && D.g * 8 < Q.w) D.g *= 2;
+      D.g = tail_lanes(Q.n, Q.w, kPT);
       D.ld = Q.ld;
       D.col = Q.col;
       D.val = Q.val;

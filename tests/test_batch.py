@@ -119,7 +119,10 @@ def test_queued_batch_solves_match_single_contexts():
     one cooperative launch whose block groups take boxes from a device work queue.  Each
     box meets the same stopping test as alone, with its sums over other block counts, so
     the bar is the solver's accuracy: accelerations within 1e-6 RMS (the force-error bound)
-    and positions within 1e-9 after three steps, every box converged."""
+    and positions within 1e-8 of the box after three steps, every box converged.  Two
+    solutions that both meet rtol 1e-10 differ by up to cond(A) 1e-10, about 1e-8 in the
+    accelerations of these boxes; the persistent body and the graph kernels also split
+    their row sums over different lane counts."""
     from apcloud import binding
     from apcloud.batch import BatchRun
     from apcloud.controller import Controller
@@ -145,7 +148,7 @@ def test_queued_batch_solves_match_single_contexts():
         g.close()
         d = arr[:3] - ref[:3]
         d -= np.round(d)
-        assert np.max(np.abs(d)) <= 1e-9, c.name
+        assert np.max(np.abs(d)) <= 1e-8, c.name
         a, b = arr[6:9], ref[6:9]
         rms = float(np.sqrt(np.mean(np.sum((a - b) ** 2, 0)) / np.mean(np.sum(b ** 2, 0))))
         assert rms <= 1e-6, (c.name, rms)
