@@ -660,9 +660,11 @@ int apc_krylov_solve(apc_context *c, int which, const double *b, double *x, int 
     apc_count_launch(c);
   }
   // inner restart: 16 for the multigrid FGMRES (a V-cycle per iteration makes short
-  // cycles cheapest at 128^3), 30 without a preconditioner
+  // cycles cheapest at 128^3) and for the density solve (it converges in about 10
+  // iterations, and a 16-vector basis keeps the Krylov kernels' accumulators in half the
+  // registers); 30 for the potential without a preconditioner
   const bool use_mg = which == 1 && cfg.mixed_precond == APC_PRECOND_MULTIGRID;
-  const int m32 = cfg.mixed_restart > 0 ? cfg.mixed_restart : (use_mg ? 16 : 30);
+  const int m32 = cfg.mixed_restart > 0 ? cfg.mixed_restart : ((use_mg || which == 0) ? 16 : 30);
   // inner tolerance: a correction gains only ~2-3 digits of the FP64 residual whatever its
   // inner accuracy (the FP32 operator's rounding, ~cond(A) 6e-8, bounds it), so the
   // multigrid cycles stop at 1e-3; the density solve keeps 1e-5

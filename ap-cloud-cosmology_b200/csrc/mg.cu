@@ -304,6 +304,18 @@ __global__ void jacobi_first(int n, const V *__restrict__ dinv, const V *__restr
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = omega * dinv[i] * b[i];
 }
 
+// x += alpha P xc (piecewise-constant prolongation), in place
+template <class V>
+__global__ void prolong_add(int n, const int *__restrict__ agg, const V *__restrict__ xc, V alpha,
+                            V *__restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] += alpha * xc[agg[i]];
+}
+
+// levels with more rows than this apply the coarse correction in its own pass and then
+// sweep, instead of inside the sweep: the fused form gathers three arrays per slot
+// (x, the aggregate map and the coarse x), which costs more than a pass on the fine level
+constexpr int kSplitProlongRows = 1 << 17;
+
 // b_c[I] = sum of r over the members of I, in member order
 template <class V>
 __global__ void restrict_sum(int nc, const int *__restrict__ mptr, int nf, const int *__restrict__ mem,
@@ -2192,7 +2204,13 @@ static void vcycle(apc_context *c, cudaStream_t s, int l, const T *b, T *x) {
   restrict_sum<T><<<grid_for(C.n), kT, 0, s>>>(C.n, C.mptr, n, C.mem, L.r, C.b);
   apc_count_launch(c);
   vcycle<T>(c, s, l + 1, C.b, C.x);
-  op(kOpProlongSweep, cur, nxt);
+  if (n > kSplitProlongRows) {
+    prolong_add<T><<<grid_for(n), kT, 0, s>>>(n, L.agg, C.x, alpha, cur);
+    apc_count_launch(c);
+    op(kOpSweep, cur, nxt);
+  } else {
+    op(kOpProlongSweep, cur, nxt);
+  }
   std::swap(cur, nxt);
   for (int k = 1; k < sweeps; ++k) {
     op(kOpSweep, cur, nxt);
@@ -2711,7 +2729,11 @@ int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, cons
 
 static int ensure_side(apc_context *c, MgWork *m) {
   if (!m->side) {
-    APC_CUDA_TRY(c, cudaStreamCreateWithFlags(&m->side, cudaStreamNonBlocking));
+    // the highest priority: the hierarchy's kernels and round trips are the critical path
+    // while the GFD kernels (or the density solve) fill the SMs beside them
+    int least = 0, greatest = 0;
+    APC_CUDA_TRY(c, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    APC_CUDA_TRY(c, cudaStreamCreateWithPriority(&m->side, cudaStreamNonBlocking, greatest));
     for (cudaEvent_t &e : m->side_ev) APC_CUDA_TRY(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
   return APC_OK;
