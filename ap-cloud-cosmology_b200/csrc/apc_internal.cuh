@@ -21,6 +21,7 @@ enum : int {
   DERR_NEIGH = 16,         // a face neighbour required by 2:1 balance was not found
   DERR_NOT_FINITE = 32,
   DERR_KRYLOV = 64,
+  DERR_SORT = 128,         // a radix-sort tile's look-back wait ran past its bound
 };
 
 #define APC_CUDA_TRY(ctx, call)                                                      \

@@ -84,6 +84,10 @@ int apc_read_errors(apc_context *c, int *flags) {
   APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 1, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->s));
   APC_CUDA_TRY(c, apc_stream_wait(c));
   *flags = c->h_pinned[1];
+  if (*flags & DERR_SORT) {
+    c->err = "radix sort: a tile's look-back wait ran past its bound";
+    return APC_ERR_TIMEOUT;
+  }
   return APC_OK;
 }
 

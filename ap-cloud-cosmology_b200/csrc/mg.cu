@@ -412,6 +412,43 @@ __global__ void __launch_bounds__(kT) row_op(int n, int w, size_t ld, const int 
   }
 }
 
+// b_c[I] = sum over the members q of I (in member order) of r_q = b_q - (A x)_q: the
+// residual and the restriction in one pass, 8 lanes per coarse row, one member row each
+// (more members go round in turns).  For the coarse levels, whose rows are in code order,
+// so that a coarse row's members are adjacent rows and a warp's loads stay coalesced.
+template <class V>
+__global__ void __launch_bounds__(kT) residual_restrict(int nc, const int *__restrict__ mptr,
+                                                        const int *__restrict__ mem, int nf, int w, size_t ld,
+                                                        const int *__restrict__ col, const V *__restrict__ val,
+                                                        const V *__restrict__ b, const V *__restrict__ x,
+                                                        V *__restrict__ bc) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane8 = (int)(tid & 7), lane = threadIdx.x & 31;
+  const long long groups = ((long long)gridDim.x * blockDim.x) / 8;
+  const long long rounds = (nc + groups - 1) / groups;  // the same for every lane
+  for (long long rd = 0; rd < rounds; ++rd) {
+    const long long I = tid / 8 + rd * groups;
+    const bool act = I < nc;
+    const int q0 = act ? mptr[I] : 0, q1 = act ? ((I + 1 < nc) ? mptr[I + 1] : nf) : 0;
+    const int turns = __reduce_max_sync(0xffffffffu, (unsigned)((q1 - q0 + 7) / 8));
+    V total = V(0);
+    for (int tn = 0; tn < turns; ++tn) {
+      const int qb = q0 + 8 * tn, q = qb + lane8;
+      V r = V(0);
+      if (q < q1) {
+        const int i = mem[q];
+        r = b[i] - row_sum<V>(w, ld, i, 0, 1, col, val, [&](int j) { return x[j]; });
+      }
+      const int cnt = min(8, q1 - qb);
+      for (int m = 0; m < 8; ++m) {
+        const V t = __shfl_sync(0xffffffffu, r, (lane & ~7) + m);
+        if (m < cnt) total += t;
+      }
+    }
+    if (act && lane8 == 0) bc[I] = total;
+  }
+}
+
 // ------------------------------------------------------------------ FGMRES
 
 // State of the device-resident mixed solve: the FP64 refinement loop and the FP32
@@ -2200,9 +2237,16 @@ static void vcycle(apc_context *c, cudaStream_t s, int l, const T *b, T *x) {
     nxt = x;
     apc_count_launch(c);
   }
-  op(kOpResidual, cur, L.r);
-  restrict_sum<T><<<grid_for(C.n), kT, 0, s>>>(C.n, C.mptr, n, C.mem, L.r, C.b);
-  apc_count_launch(c);
+  if (l > 0) {
+    // coarse levels are in code order: residual and restriction in one pass
+    residual_restrict<T><<<grid_for((long long)C.n * 8), kT, 0, s>>>(C.n, C.mptr, C.mem, n, L.w, L.ld, L.col,
+                                                                     L.val, b, cur, C.b);
+    apc_count_launch(c);
+  } else {
+    op(kOpResidual, cur, L.r);
+    restrict_sum<T><<<grid_for(C.n), kT, 0, s>>>(C.n, C.mptr, n, C.mem, L.r, C.b);
+    apc_count_launch(c);
+  }
   vcycle<T>(c, s, l + 1, C.b, C.x);
   if (n > kSplitProlongRows) {
     prolong_add<T><<<grid_for(n), kT, 0, s>>>(n, L.agg, C.x, alpha, cur);

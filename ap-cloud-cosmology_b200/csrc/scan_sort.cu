@@ -134,28 +134,48 @@ constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortRows = 16;                       // rows of 32 items per warp
 constexpr int kSortTile = kSortThreads * kSortRows; // 4096 items per block
 
-__global__ void __launch_bounds__(kSortThreads) radix_hist(const uint64_t *keys, int n, int shift,
-                                                           int nblocks, uint32_t *hist) {
-  __shared__ uint32_t h[256];
-  h[threadIdx.x] = 0;
+constexpr int kSortMaxPasses = 8;                  // 64-bit keys, 8-bit digits
+constexpr uint32_t kLookAggregate = 1u << 30;      // look-back word: the tile's own count
+constexpr uint32_t kLookPrefix = 2u << 30;         // look-back word: count of every tile up to this one
+constexpr uint32_t kLookValue = (1u << 30) - 1u;
+constexpr long long kSortSpinLimit = 1ll << 22;
+
+// Every pass's digit histogram over the whole array in one read of the keys: per block in
+// shared memory (one atomic per distinct digit of a warp row), then added to ghist.
+__global__ void __launch_bounds__(kSortThreads) radix_hist_all(const uint64_t *__restrict__ keys, int n,
+                                                               int lo_bit, int npasses, uint32_t *ghist) {
+  __shared__ uint32_t h[kSortMaxPasses][256];
+  for (int k = threadIdx.x; k < kSortMaxPasses * 256; k += kSortThreads) (&h[0][0])[k] = 0;
   __syncthreads();
-  const long long t0 = (long long)blockIdx.x * kSortTile;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int r = 0; r < kSortRows; ++r) {
-    long long i = t0 + (long long)warp * 32 * kSortRows + r * 32 + lane;
-    bool ok = i < n;
-    unsigned d = ok ? (unsigned)((keys[i] >> shift) & 0xffu) : 256u;
-    unsigned peers = __match_any_sync(0xffffffffu, d);
-    if (ok && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
+  const int lane = threadIdx.x & 31;
+  const long long stride = (long long)gridDim.x * kSortThreads;
+  const long long rounds = (n + stride - 1) / stride;  // the same for every lane (match_any)
+  for (long long rd = 0; rd < rounds; ++rd) {
+    const long long i = rd * stride + (long long)blockIdx.x * kSortThreads + threadIdx.x;
+    const bool ok = i < n;
+    const uint64_t k = ok ? keys[i] : 0ull;
+    for (int p = 0; p < npasses; ++p) {
+      const unsigned d = ok ? (unsigned)((k >> (lo_bit + 8 * p)) & 0xffu) : 256u;
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      if (ok && lane == __ffs(peers) - 1) atomicAdd(&h[p][d], (uint32_t)__popc(peers));
+    }
   }
   __syncthreads();
-  hist[(size_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+  for (int k = threadIdx.x; k < npasses * 256; k += kSortThreads) {
+    const uint32_t v = (&h[0][0])[k];
+    if (v) atomicAdd(ghist + k, v);
+  }
 }
 
-// Stable scatter.  Within a tile, an item's rank among the tile's items of its digit is
-// (earlier warps' counts) + (earlier rows of its warp) + (earlier lanes of its row).  The
-// tile is first staged in shared memory in digit order, then written out by consecutive
-// threads, so each digit's run goes to consecutive global addresses (coalesced).
+// One pass, stable (one-sweep form).  Each block takes the next tile from a counter, so
+// every tile before it is held by a block that is running or done.  Within the tile an
+// item's rank among the tile's items of its digit is (earlier warps' counts) + (earlier
+// rows of its warp) + (earlier lanes of its row).  The tile publishes its digit counts,
+// then finds the counts of all earlier tiles by walking back over their published words
+// (an earlier tile's inclusive prefix ends the walk), and publishes its own prefix.  Its
+// items go to (items of smaller digits) + (earlier tiles' items of the digit) + rank,
+// staged in shared memory in digit order so that each digit's run is written by
+// consecutive threads.  A walk that waits more than kSortSpinLimit polls raises DERR_SORT.
 struct ScatterSmem {
   uint64_t key[kSortTile];
   uint32_t val[kSortTile];
@@ -163,18 +183,22 @@ struct ScatterSmem {
   uint32_t bstart[256];  // tile-local start of each digit
   uint32_t goff[256];    // global start of each digit's run of this tile
   uint32_t wsum[kSortWarps];
+  int tile;
 };
 
-__global__ void __launch_bounds__(kSortThreads) radix_scatter(const uint64_t *keys_in,
-                                                              const uint32_t *vals_in,
-                                                              uint64_t *keys_out, uint32_t *vals_out,
-                                                              int n, int shift, int nblocks,
-                                                              const uint32_t *offsets) {
+__global__ void __launch_bounds__(kSortThreads) radix_onesweep(const uint64_t *__restrict__ keys_in,
+                                                               const uint32_t *__restrict__ vals_in,
+                                                               uint64_t *__restrict__ keys_out,
+                                                               uint32_t *__restrict__ vals_out, int n, int shift,
+                                                               const uint32_t *__restrict__ hist, uint32_t *look,
+                                                               unsigned *counter, int *err) {
   extern __shared__ __align__(16) unsigned char scatter_smem[];
   ScatterSmem &S = *reinterpret_cast<ScatterSmem *>(scatter_smem);
   for (int k = threadIdx.x; k < kSortWarps * 256; k += kSortThreads) (&S.wcount[0][0])[k] = 0;
+  if (threadIdx.x == 0) S.tile = (int)atomicAdd(counter, 1u);
   __syncthreads();
-  const long long t0 = (long long)blockIdx.x * kSortTile;
+  const int tile = S.tile;
+  const long long t0 = (long long)tile * kSortTile;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
   uint64_t kk[kSortRows];
@@ -196,8 +220,9 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter(const uint64_t *ke
   }
   __syncthreads();
   {
-    // thread d: the tile's count of digit d and the earlier warps' counts; then the
-    // tile-local digit starts by a block exclusive scan over d
+    // thread d: the tile's count of digit d and the earlier warps' counts, the tile-local
+    // digit starts (block scan over d), the digit's start in the output (scan of the
+    // histogram over d) and the earlier tiles' count of d (look-back)
     const int d = threadIdx.x;
     uint32_t run = 0;
     for (int w = 0; w < kSortWarps; ++w) {
@@ -205,18 +230,47 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter(const uint64_t *ke
       S.wcount[w][d] = run;
       run += c;
     }
-    uint32_t incl = run;
+    uint32_t *mine = look + (size_t)tile * 256 + d;
+    atomicExch(mine, (tile == 0 ? kLookPrefix : kLookAggregate) | run);
+    const uint32_t hd = hist[d];
+    uint32_t incl = run, hincl = hd;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
+      const uint32_t th = __shfl_up_sync(0xffffffffu, hincl, o);
+      if (lane >= o) {
+        incl += t;
+        hincl += th;
+      }
     }
     if (lane == 31) S.wsum[warp] = incl;
+    __shared__ uint32_t hsum[kSortWarps];
+    if (lane == 31) hsum[warp] = hincl;
+    uint32_t excl = 0;
+    if (tile > 0) {
+      int tp = tile - 1;
+      long long spins = 0;
+      while (true) {
+        const uint32_t v = *reinterpret_cast<volatile uint32_t *>(look + (size_t)tp * 256 + d);
+        if (v & (kLookAggregate | kLookPrefix)) {
+          excl += v & kLookValue;
+          if ((v & kLookPrefix) || tp == 0) break;
+          --tp;
+        } else if (++spins > kSortSpinLimit) {
+          atomicOr(err, DERR_SORT);
+          break;
+        }
+      }
+      atomicExch(mine, kLookPrefix | (excl + run));
+    }
     __syncthreads();
-    uint32_t before = 0;
-    for (int w = 0; w < warp; ++w) before += S.wsum[w];
+    uint32_t before = 0, hbefore = 0;
+    for (int w = 0; w < warp; ++w) {
+      before += S.wsum[w];
+      hbefore += hsum[w];
+    }
     S.bstart[d] = before + incl - run;
-    S.goff[d] = offsets[(size_t)d * nblocks + blockIdx.x];
+    S.goff[d] = hbefore + hincl - hd + excl;
   }
   __syncthreads();
 #pragma unroll
@@ -266,20 +320,29 @@ int apc_exclusive_scan(apc_context *c, const int *in, int *out, int n, int *tota
 int apc_radix_sort_u64(apc_context *c, uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
                        uint32_t *vals_alt, int n, int lo_bit, int hi_bit, bool *in_alt) {
   *in_alt = false;
-  if (n <= 1) return APC_OK;
-  const int nblocks = (n + kSortTile - 1) / kSortTile;
-  const size_t hn = (size_t)nblocks * 256;
-  APC_TRY(apc_ensure(c, &c->sort_hist, hn, nullptr));
+  if (n <= 1 || hi_bit <= lo_bit) return APC_OK;
+  const int npasses = std::min(kSortMaxPasses, (hi_bit - lo_bit + 7) / 8);
+  const int ntiles = (n + kSortTile - 1) / kSortTile;
+  // workspace: every pass's histogram (256 each), the passes' tile counters, and the
+  // passes' look-back words (ntiles x 256 each), all zeroed for this sort
+  const size_t nh = (size_t)kSortMaxPasses * 256, nc = 256, nl = (size_t)npasses * ntiles * 256;
+  APC_TRY(apc_ensure(c, &c->sort_hist, nh + nc + nl, nullptr));
+  uint32_t *ghist = c->sort_hist;
+  unsigned *counters = c->sort_hist + nh;
+  uint32_t *look = c->sort_hist + nh + nc;
+  APC_CUDA_TRY(c, cudaMemsetAsync(c->sort_hist, 0, sizeof(uint32_t) * (nh + nc + nl), c->s));
+  APC_CUDA_TRY(c, cudaFuncSetAttribute(radix_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sizeof(ScatterSmem)));
+  const int hblocks = std::max(1, std::min(ntiles * 4, apc_sm_count(c) * 8));
+  radix_hist_all<<<hblocks, kSortThreads, 0, c->s>>>(keys, n, lo_bit, npasses, ghist);
+  apc_count_launch(c);
   uint64_t *ki = keys, *ko = keys_alt;
   uint32_t *vi = vals, *vo = vals_alt;
-  APC_CUDA_TRY(c, cudaFuncSetAttribute(radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sizeof(ScatterSmem)));
-  for (int shift = lo_bit; shift < hi_bit; shift += 8) {
-    radix_hist<<<nblocks, kSortThreads, 0, c->s>>>(ki, n, shift, nblocks, c->sort_hist);
-    APC_TRY(apc_exclusive_scan(c, (const int *)c->sort_hist, (int *)c->sort_hist, (int)hn, nullptr));
-    radix_scatter<<<nblocks, kSortThreads, sizeof(ScatterSmem), c->s>>>(ki, vi, ko, vo, n, shift, nblocks,
-                                                                        c->sort_hist);
-    apc_count_launch(c, 2);
+  for (int p = 0; p < npasses; ++p) {
+    radix_onesweep<<<ntiles, kSortThreads, sizeof(ScatterSmem), c->s>>>(
+        ki, vi, ko, vo, n, lo_bit + 8 * p, ghist + (size_t)p * 256, look + (size_t)p * ntiles * 256,
+        counters + p, c->d_err);
+    apc_count_launch(c);
     APC_CUDA_TRY(c, cudaGetLastError());
     uint64_t *tk = ki; ki = ko; ko = tk;
     uint32_t *tv = vi; vi = vo; vo = tv;
