@@ -313,8 +313,9 @@ __global__ void prolong_add(int n, const int *__restrict__ agg, const V *__restr
 
 // levels with more rows than this apply the coarse correction in its own pass and then
 // sweep, instead of inside the sweep: the fused form gathers three arrays per slot
-// (x, the aggregate map and the coarse x), which costs more than a pass on the fine level
-constexpr int kSplitProlongRows = 1 << 17;
+// (x, the aggregate map and the coarse x), which on the levels with many rows costs more
+// than the extra pass (measured at 128^3 on levels of 262k and 33k rows)
+constexpr int kSplitProlongRows = 1 << 14;
 
 // b_c[I] = sum of r over the members of I, in member order
 template <class V>
@@ -927,6 +928,11 @@ static inline int tail_lanes(int n, int w, int threads) {
 // the graph path's tail kernel: 512 threads leave 128 registers a thread for the batched
 // row loads (a 1024-thread block has 64)
 constexpr int kTailThreads = 512;
+// the staged tail: its loads hit shared memory, so short batches suffice and the block can
+// take 1024 threads (64 registers), one round for levels of up to 1024 rows
+constexpr int kTailSmemThreads = 1024;
+template <class V>
+constexpr int kTailSmemBatch = 4;
 
 // sum_j a_ij xj(j) for every row of a tail level, L.g lanes per row; emit(i, sum) runs on
 // the group's first lane.  The trip count is the same for the whole block (shuffles).
@@ -1102,7 +1108,7 @@ __device__ __forceinline__ void stage_wait() {
 }
 
 template <class V>
-__global__ void __launch_bounds__(kTailThreads) vcycle_tail_smem(TailArgs<V> A) {
+__global__ void __launch_bounds__(kTailSmemThreads) vcycle_tail_smem(TailArgs<V> A) {
   extern __shared__ __align__(16) unsigned char tsm[];
   TailArgs<V> &S = *reinterpret_cast<TailArgs<V> *>(tsm);
   unsigned char *p = tsm + tail_align(sizeof(TailArgs<V>));
@@ -1172,7 +1178,7 @@ __global__ void __launch_bounds__(kTailThreads) vcycle_tail_smem(TailArgs<V> A) 
     if (t == 0) S.inv = inv;
   }
   stage_wait();
-  tail_body<V, RowBatch<V>::n>(S);
+  tail_body<V, kTailSmemBatch<V>>(S);
   __syncthreads();
   for (int i = t; i < A.L[0].n; i += T) A.L[0].x[i] = S.L[0].x[i];
 }
@@ -2157,8 +2163,6 @@ static void vcycle(apc_context *c, cudaStream_t s, int l, const T *b, T *x) {
       TailLevel<T> &D = A.L[k];
       D.n = Q.n;
       D.w = Q.w;
-      // wide rows get several lanes while the block has lanes to spare
-      D.g = tail_lanes(Q.n, Q.w, kTailThreads);
       D.ld = Q.ld;
       D.col = Q.col;
       D.val = Q.val;
@@ -2173,10 +2177,14 @@ static void vcycle(apc_context *c, cudaStream_t s, int l, const T *b, T *x) {
     }
     // staged in shared memory when the tail's levels fit (they do at 128^3: ~90 KB in FP32)
     const size_t tb = tail_smem_bytes(A);
-    if (tb <= kTailSmemMax)
-      vcycle_tail_smem<T><<<1, kTailThreads, tb, s>>>(A);
+    const bool staged = tb <= kTailSmemMax;
+    const int threads = staged ? kTailSmemThreads : kTailThreads;
+    // wide rows get several lanes while the block has lanes to spare
+    for (int k = 0; k < A.nl; ++k) A.L[k].g = tail_lanes(A.L[k].n, A.L[k].w, threads);
+    if (staged)
+      vcycle_tail_smem<T><<<1, threads, tb, s>>>(A);
     else
-      vcycle_tail<T><<<1, kTailThreads, 0, s>>>(A);
+      vcycle_tail<T><<<1, threads, 0, s>>>(A);
     apc_count_launch(c);
     return;
   }

@@ -84,8 +84,9 @@ typedef struct apc_config {
   double gmres_dtol;     /* -ksp_divtol */
   int gmres_max_it;      /* -ksp_max_it */
   int precision;         /* apc_precision */
-  int mixed_restart;     /* inner restart of both APC_PREC_MIXED / APC_PREC_FP64_MULTIGRID solves (0 = 16
-                            for the multigrid potential solve, 30 for the others), at most 31 */
+  int mixed_restart;     /* inner restart of both multigrid-path solves (0 = 16 for the density solve and
+                            the multigrid potential solve, 30 for the potential without multigrid),
+                            at most 31 */
   double mixed_inner_rtol; /* FP32 inner solve relative tolerance (0 = 1e-3 with multigrid, 1e-5 without) */
   int device;            /* CUDA device ordinal */
   int mixed_precond;     /* APC_PREC_MIXED / APC_PREC_FP64_MULTIGRID potential solve: APC_PRECOND_JACOBI
@@ -102,7 +103,8 @@ typedef struct apc_config {
                             persistent cooperative kernel (refinement loop, (F)GMRES cycles and
                             V-cycles separated by grid barriers).  On a B200 at 128^3 the graph form
                             is faster (the barriers cost about what the launches they replace cost);
-                            the queued batch mode uses the persistent form across boxes */
+                            the queued batch mode uses the persistent form across boxes.
+                            APC_PREC_MIXED_VCYCLE solves always run as graphs */
 } apc_config;
 
 enum { APC_PRECOND_JACOBI = 0, APC_PRECOND_MULTIGRID = 1 };
