@@ -97,7 +97,8 @@ constexpr int kGalRows = 256;  // distinct coarse columns per row
 
 template <class V>
 __global__ void __launch_bounds__(32 * kGalWarps) galerkin_rows(int nc, const int *__restrict__ mptr, int nf,
-                                                              const int *__restrict__ mem, int wf, size_t ldf,
+                                                              const int *__restrict__ mem, int wf_host,
+                                                              const int *__restrict__ wf_dev, int wf_cap, size_t ldf,
                                                               const int *__restrict__ colf,
                                                               const V *__restrict__ valf,
                                                               const int *__restrict__ agg, int wcap,
@@ -108,6 +109,9 @@ __global__ void __launch_bounds__(32 * kGalWarps) galerkin_rows(int nc, const in
   __shared__ double stage[kGalWarps][32];
   __shared__ int dkey[kGalWarps][kGalRows];
   __shared__ double dval[kGalWarps][kGalRows];
+  // the fine level's width: from the device when that level was built just before (capped by
+  // its ELL's slots: a wider level is flagged and the build repeated)
+  const int wf = wf_dev ? min(*wf_dev, wf_cap) : wf_host;
   const int lane = threadIdx.x & 31, wv = threadIdx.x >> 5;
   int *K = tkey[wv];
   double *T = tsum[wv];
@@ -182,9 +186,15 @@ __global__ void __launch_bounds__(32 * kGalWarps) galerkin_rows(int nc, const in
 }
 
 template <class V>
-__global__ void rows_to_ell(int n, int w, size_t ld, int wcap, const int *__restrict__ rowlen,
-                            const int *__restrict__ tcol, const V *__restrict__ tval, int *__restrict__ col,
-                            V *__restrict__ val, V *__restrict__ dinv) {
+__global__ void rows_to_ell(int n, const int *__restrict__ w_dev, int wslots, size_t ld, int wcap,
+                            const int *__restrict__ rowlen, const int *__restrict__ tcol,
+                            const V *__restrict__ tval, int *__restrict__ col, V *__restrict__ val,
+                            V *__restrict__ dinv, int *__restrict__ overflow) {
+  // the level's width (max_int, just before); the ELL holds wslots slots, and a wider level
+  // is flagged (the build then runs again with room for it)
+  const int wd = *w_dev;
+  const int w = min(wd, wslots);
+  if (wd > wslots && blockIdx.x == 0 && threadIdx.x == 0) atomicExch(overflow, 1);
   for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < n; I += gridDim.x * blockDim.x) {
     const int len = rowlen[I];
     V d = V(0);
@@ -1803,6 +1813,11 @@ struct MgWork {
   int *cstat = nullptr;
   int *cstat_host = nullptr;
   bool tail_smem_set = false;  // the staged tail kernels may take kTailSmemMax
+  // the numeric build's per-level widths (device, and its pinned readback; [kMaxLevels + 1]
+  // is the ELL overflow flag) and the ELL slots allocated per level (host, the widest seen)
+  int *wdev = nullptr;
+  int *whost = nullptr;
+  int wslots[kMaxLevels] = {};
   // a solve prepared for a batched launch (apc_mg_batched_solve): its arguments, which
   // solve it is, and whether it is multigrid-preconditioned
   PSolveArgs<float> deferred32{};
@@ -1868,11 +1883,12 @@ void apc_mg_free(apc_context *c) {
   }
   void *p[] = {m->pkey, m->pkey_alt, m->pidx, m->pidx_alt, m->eflag, m->epos, m->ucol,
                m->rowstart, m->partial, m->dots, m->counter, m->state, m->total, m->ppart, m->pbar, m->pres,
-               m->cstat};
+               m->cstat, m->wdev};
   for (void *q : p) apc_free(c, q);
   if (m->host) cudaFreeHost(m->host);
   if (m->pres_host) cudaFreeHost(m->pres_host);
   if (m->cstat_host) cudaFreeHost(m->cstat_host);
+  if (m->whost) cudaFreeHost(m->whost);
   for (int k = 0; k < 2; ++k) {
     if (m->solve_exec[k]) cudaGraphExecDestroy(m->solve_exec[k]);
     if (m->solve_graph[k]) cudaGraphDestroy(m->solve_graph[k]);
@@ -1991,7 +2007,22 @@ static int mg_build(apc_context *c) {
   APC_TRY(apc_ensure(c, &L0.r, (size_t)n0 + 1));
   ell_dinv<T><<<grid_for(n0), kT, 0, c->s>>>(n0, L0.ld, L0.val, L0.dinv);
   apc_count_launch(c);
+  // Every level's Galerkin product and ELL are queued without a host round trip: the
+  // kernels read each level's width from wdev, and the ELL is allocated for the widths of
+  // the last build (at least 32 slots).  One readback at the end gives the widths; when a
+  // level is wider than its allocation, the build runs again with room for it (the levels
+  // below it were built from its truncated rows, so each repeat settles at least one more
+  // level).
+  if (!m->wdev) {
+    APC_TRY(apc_alloc(c, (void **)&m->wdev, (kMaxLevels + 2) * sizeof(int)));
+    APC_CUDA_TRY(c, cudaMallocHost((void **)&m->whost, (kMaxLevels + 2) * sizeof(int)));
+  }
   int lev = 0;
+  for (int attempt = 0; attempt <= S.nlev; ++attempt) {
+  APC_CUDA_TRY(c, cudaMemsetAsync(m->wdev, 0, (kMaxLevels + 2) * sizeof(int), c->s));
+  APC_CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->s));
+  int *overflow = m->wdev + kMaxLevels + 1;
+  lev = 0;
   for (; lev + 1 < S.nlev; ++lev) {
     MgLevel<T> &F = H.lv[lev];
     MgLevel<T> &C = H.lv[lev + 1];
@@ -2006,35 +2037,46 @@ static int mg_build(apc_context *c) {
     APC_TRY(apc_ensure(c, &m->rowstart, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &m->ucol, (size_t)nc * wcap));
     APC_TRY(apc_ensure(c, &H.uval, (size_t)nc * wcap));
-    APC_CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->s));
-    APC_CUDA_TRY(c, cudaMemsetAsync(m->total, 0, sizeof(int), c->s));
     galerkin_rows<<<std::max(1, std::min((nc + kGalWarps - 1) / kGalWarps, apc_sm_count(c) * 8)), 32 * kGalWarps, 0,
-                    c->s>>>(nc, C.mptr, nf, C.mem, F.w, F.ld, F.col, F.val, F.agg, wcap, m->rowstart, m->ucol,
-                            H.uval, c->d_err);
-    max_int<<<grid_for(nc, 256), kT, 0, c->s>>>(nc, m->rowstart, m->total);
+                    c->s>>>(nc, C.mptr, nf, C.mem, F.w, lev == 0 ? nullptr : m->wdev + lev, F.w, F.ld, F.col,
+                            F.val, F.agg, wcap, m->rowstart, m->ucol, H.uval, c->d_err);
+    max_int<<<grid_for(nc, 256), kT, 0, c->s>>>(nc, m->rowstart, m->wdev + lev + 1);
     apc_count_launch(c, 2);
-    // the row width and the error flags in one round trip
-    APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 8, m->total, sizeof(int), cudaMemcpyDeviceToHost, c->s));
-    APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 9, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->s));
-    APC_CUDA_TRY(c, apc_stream_wait(c));
-    const int wc = c->h_pinned[8], derr = c->h_pinned[9];
-    if (derr & DERR_STENCIL_MANY) {
-      c->err = "multigrid coarse row exceeds its buffers";
-      return APC_ERR_UNSUPPORTED;
-    }
-    C.w = wc;
+    const int wslots = std::max(32, m->wslots[lev + 1]);
+    C.w = wslots;  // until the readback below
     C.ld = (size_t)nc;
-    APC_TRY(apc_ensure(c, &C.col, C.ld * wc));
-    APC_TRY(apc_ensure(c, &C.val, C.ld * wc));
+    APC_TRY(apc_ensure(c, &C.col, C.ld * wslots));
+    APC_TRY(apc_ensure(c, &C.val, C.ld * wslots));
     APC_TRY(apc_ensure(c, &C.dinv, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &C.x, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &C.x2, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &C.b, (size_t)nc + 1));
     APC_TRY(apc_ensure(c, &C.r, (size_t)nc + 1));
-    rows_to_ell<T><<<grid_for(nc), kT, 0, c->s>>>(nc, wc, C.ld, wcap, m->rowstart, m->ucol, H.uval, C.col, C.val,
-                                                 C.dinv);
+    rows_to_ell<T><<<grid_for(nc), kT, 0, c->s>>>(nc, m->wdev + lev + 1, wslots, C.ld, wcap, m->rowstart, m->ucol,
+                                                 H.uval, C.col, C.val, C.dinv, overflow);
     apc_count_launch(c);
     APC_CUDA_TRY(c, cudaGetLastError());
+  }
+  // the widths and the error flags in one round trip
+  APC_CUDA_TRY(c, cudaMemcpyAsync(m->whost, m->wdev, (kMaxLevels + 2) * sizeof(int), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 9, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
+  if (c->h_pinned[9] & DERR_STENCIL_MANY) {
+    c->err = "multigrid coarse row exceeds its buffers";
+    return APC_ERR_UNSUPPORTED;
+  }
+  bool wider = false;
+  for (int k = 1; k < S.nlev; ++k) {
+    const int wk = m->whost[k];
+    if (wk > std::max(32, m->wslots[k])) wider = true;
+    m->wslots[k] = std::max(m->wslots[k], wk);
+    H.lv[k].w = wk;
+  }
+  if (!wider) break;
+  if (attempt == S.nlev) {
+    c->err = "multigrid coarse level wider than its rebuilt allocation";
+    return APC_ERR_UNSUPPORTED;
+  }
   }
   H.lv[lev].agg = S.lv[lev].agg;
   H.nlev = lev + 1;
