@@ -477,10 +477,9 @@ static int select_once(apc_context *c, int *hash_full) {
     if (2ll * n_open > c->hcap) { *hash_full = 1; return APC_OK; }
   }
   c->n_open = n_open;
-
+  // a full hash table is read with the output's errors below: every probe is bounded, so
+  // the output pass runs safely on an incomplete table, and the selection is then redone
   int derr = 0;
-  APC_TRY(apc_read_errors(c, &derr));
-  if (derr & DERR_HASH_FULL) { *hash_full = 1; return APC_OK; }
 
   // ---- output cells ----
   if (n_open == 0) {
@@ -498,12 +497,14 @@ static int select_once(apc_context *c, int *hash_full) {
   apc_count_launch(c);
   APC_TRY(apc_exclusive_scan(c, c->flags, c->req_pos, (int)m8, c->counters));
   int M = 0, nc = 0;
-  APC_TRY(read_int(c, c->counters, &M));
-  if (8ll * n_open_td < m8) {
-    APC_TRY(read_int(c, c->req_pos + 8ll * n_open_td, &nc));
-  } else {
-    nc = M;
-  }
+  // the cell count and the computational-cell count in one round trip
+  APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned, c->counters, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+  if (8ll * n_open_td < m8)
+    APC_CUDA_TRY(c, cudaMemcpyAsync(c->h_pinned + 3, c->req_pos + 8ll * n_open_td, sizeof(int),
+                                    cudaMemcpyDeviceToHost, c->s));
+  APC_CUDA_TRY(c, apc_stream_wait(c));
+  M = c->h_pinned[0];
+  nc = (8ll * n_open_td < m8) ? c->h_pinned[3] : M;
   c->nc = nc;
   c->nv = M - nc;
   c->nb = 0;
