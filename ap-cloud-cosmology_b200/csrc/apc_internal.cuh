@@ -51,6 +51,11 @@ struct apc_context {
   // owning pointer; per context, so contexts can be driven from different host threads
   std::unordered_map<const void *, size_t> caps;
   cudaStream_t s = nullptr;
+  // host uploads of the velocities run on a copy stream beside the step's kernels: they are
+  // needed only at the kick, so the upload overlaps the selection, assembly and solves
+  cudaStream_t cs = nullptr;
+  cudaEvent_t cs_ev = nullptr, vel_ev = nullptr;  // c->s before the upload; upload done
+  bool vel_caller_order = false;  // pvx.. hold the caller's order (a fresh upload), not the sorted one
   cudaMemPool_t pool = nullptr;  // the device's stream-ordered pool (all device buffers)
   std::string err;
   int64_t launches = 0;
@@ -169,6 +174,9 @@ cudaMemPool_t apc_device_pool(int dev);
 template <class T>
 int apc_ensure(apc_context *c, T **p, size_t count, size_t *cap_elems_io = nullptr);
 int apc_read_errors(apc_context *c, int *flags);
+// the velocities in the particles' sorted order on c->s (waits for a pending upload and
+// gathers a fresh one through the particle ids); every kernel that reads them calls it first
+int apc_velocities_sorted(apc_context *c);
 
 // Host waits for the context's stream (or one of its events).  On an ordinary thread they
 // block like cudaStreamSynchronize / cudaEventSynchronize.  Inside a batch fiber

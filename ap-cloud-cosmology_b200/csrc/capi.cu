@@ -111,11 +111,34 @@ __global__ void iota_int(int n, int *p) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = i;
 }
 
-__global__ void unpermute(int n, const int *__restrict__ pid, const double *__restrict__ src, double *__restrict__ dst) {
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) dst[pid[s]] = src[s];
+// up to 6 arrays from the sorted order to the caller's: dst_k[pid[s]] = src_k[s]
+struct Arrays6 {
+  const double *src[6];
+  double *dst[6];
+  int count;
+};
+
+__global__ void unpermute6(int n, const int *__restrict__ pid, Arrays6 a) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const int p = pid[s];
+    for (int k = 0; k < a.count; ++k) a.dst[k][p] = a.src[k][s];
+  }
+}
+
+// dst_k[s] = src_k[pid[s]]: the caller-order velocities of a fresh upload, in sorted order
+__global__ void gather3(int n, const int *__restrict__ pid, const double *__restrict__ x, const double *__restrict__ y,
+                        const double *__restrict__ z, double *__restrict__ ox, double *__restrict__ oy,
+                        double *__restrict__ oz) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const int p = pid[s];
+    ox[s] = x[p];
+    oy[s] = y[p];
+    oz[s] = z[p];
+  }
 }
 
 void free_all(apc_context *c) {
+  if (c->cs) cudaStreamSynchronize(c->cs);  // a velocity upload still writing the buffers
   apc_krylov_free(c);
   apc_mg_free(c);
   void *ptrs[] = {c->px, c->py, c->pz, c->pvx, c->pvy, c->pvz, c->pax, c->pay, c->paz, c->pid,
@@ -146,6 +169,9 @@ void free_all(apc_context *c) {
     if (e) cudaEventDestroy(e);
   for (auto &e : c->sev)
     if (e) cudaEventDestroy(e);
+  if (c->cs) cudaStreamDestroy(c->cs);
+  if (c->cs_ev) cudaEventDestroy(c->cs_ev);
+  if (c->vel_ev) cudaEventDestroy(c->vel_ev);
   if (c->s) cudaStreamDestroy(c->s);
 }
 
@@ -252,6 +278,9 @@ int apc_create(const apc_config *cfg, apc_context **out) {
     return fail(APC_ERR_CUDA);
   }
   if (cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking) != cudaSuccess) return fail(APC_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&c->cs, cudaStreamNonBlocking) != cudaSuccess) return fail(APC_ERR_CUDA);
+  if (cudaEventCreateWithFlags(&c->cs_ev, cudaEventDisableTiming) != cudaSuccess) return fail(APC_ERR_CUDA);
+  if (cudaEventCreateWithFlags(&c->vel_ev, cudaEventDisableTiming) != cudaSuccess) return fail(APC_ERR_CUDA);
   c->pool = apc_device_pool(c->dev);
   if (!c->pool) return fail(APC_ERR_CUDA);
   for (auto &e : c->ev)
@@ -326,7 +355,14 @@ static int set_particles_impl(apc_context *c, const double *const *src, cudaMemc
   cudaSetDevice(c->dev);
   const size_t bytes = sizeof(double) * (size_t)c->n;
   double *dst[6] = {c->px, c->py, c->pz, c->pvx, c->pvy, c->pvz};
-  for (int k = 0; k < 6; ++k) APC_CUDA_TRY(c, cudaMemcpyAsync(dst[k], src[k], bytes, kind, c->s));
+  for (int k = 0; k < 3; ++k) APC_CUDA_TRY(c, cudaMemcpyAsync(dst[k], src[k], bytes, kind, c->s));
+  // the velocities in the caller's order, on the copy stream after the work already queued
+  // (which may still read them); the kick gathers them into the sorted order
+  APC_CUDA_TRY(c, cudaEventRecord(c->cs_ev, c->s));
+  APC_CUDA_TRY(c, cudaStreamWaitEvent(c->cs, c->cs_ev, 0));
+  for (int k = 3; k < 6; ++k) APC_CUDA_TRY(c, cudaMemcpyAsync(dst[k], src[k], bytes, kind, c->cs));
+  APC_CUDA_TRY(c, cudaEventRecord(c->vel_ev, c->cs));
+  c->vel_caller_order = true;
   iota_int<<<std::max(1, std::min((c->n + 255) / 256, apc_sm_count(c) * 8)), 256, 0, c->s>>>(c->n, c->pid);
   apc_count_launch(c);
   APC_CUDA_TRY(c, cudaGetLastError());
@@ -353,19 +389,48 @@ int apc_set_particles_device(apc_context *c, const double *x, const double *y, c
 static int get_particles_impl(apc_context *c, double *const *dst, int count, cudaMemcpyKind kind) {
   APC_TRY(check_ready(c, true, false, false));
   cudaSetDevice(c->dev);
+  APC_TRY(apc_velocities_sorted(c));
   const double *src[9] = {c->px, c->py, c->pz, c->pvx, c->pvy, c->pvz, c->pax, c->pay, c->paz};
+  double *spare[6] = {c->qx, c->qy, c->qz, c->qvx, c->qvy, c->qvz};
   const size_t bytes = sizeof(double) * (size_t)c->n;
   const int G = std::max(1, std::min((c->n + 255) / 256, apc_sm_count(c) * 8));
-  // caller order: scatter through the particle ids into the spare buffer, then copy
-  for (int k = 0; k < count; ++k) {
-    if (!dst[k]) continue;
-    unpermute<<<G, 256, 0, c->s>>>(c->n, c->pid, src[k], c->qx);
+  // caller order: up to six arrays at a time are scattered through the particle ids into
+  // the spare buffers by one kernel, then copied out back to back
+  for (int k0 = 0; k0 < count; k0 += 6) {
+    Arrays6 a{};
+    int which[6];
+    for (int k = k0; k < count && k < k0 + 6; ++k) {
+      if (!dst[k]) continue;
+      a.src[a.count] = src[k];
+      a.dst[a.count] = spare[a.count];
+      which[a.count++] = k;
+    }
+    if (a.count == 0) continue;
+    unpermute6<<<G, 256, 0, c->s>>>(c->n, c->pid, a);
     apc_count_launch(c);
-    APC_CUDA_TRY(c, cudaMemcpyAsync(dst[k], c->qx, bytes, kind, c->s));
+    for (int j = 0; j < a.count; ++j) APC_CUDA_TRY(c, cudaMemcpyAsync(dst[which[j]], a.dst[j], bytes, kind, c->s));
   }
   APC_CUDA_TRY(c, apc_stream_wait(c));
   return APC_OK;
 }
+
+}  // extern "C"
+
+int apc_velocities_sorted(apc_context *c) {
+  if (!c->vel_caller_order) return APC_OK;
+  APC_CUDA_TRY(c, cudaStreamWaitEvent(c->s, c->vel_ev, 0));
+  const int G = std::max(1, std::min((c->n + 255) / 256, apc_sm_count(c) * 8));
+  gather3<<<G, 256, 0, c->s>>>(c->n, c->pid, c->pvx, c->pvy, c->pvz, c->qvx, c->qvy, c->qvz);
+  apc_count_launch(c);
+  APC_CUDA_TRY(c, cudaGetLastError());
+  std::swap(c->pvx, c->qvx);
+  std::swap(c->pvy, c->qvy);
+  std::swap(c->pvz, c->qvz);
+  c->vel_caller_order = false;
+  return APC_OK;
+}
+
+extern "C" {
 
 int apc_get_particles(apc_context *c, double *x, double *y, double *z, double *vx, double *vy, double *vz,
                       double *ax, double *ay, double *az) {
@@ -406,6 +471,9 @@ int apc_select(apc_context *c, int *n_cells) {
   APC_TRY(rc);
   APC_CUDA_TRY(c, cudaEventRecord(c->ev[1], c->s));
   APC_CUDA_TRY(c, apc_event_wait(c->ev[1]));
+  // the velocity upload ran beside the selection: once a phase call returns, the caller's
+  // arrays are no longer read, as with the positions
+  if (c->vel_caller_order) APC_CUDA_TRY(c, apc_event_wait(c->vel_ev));
   c->t_select_ms = elapsed(c->ev[0], c->ev[1]);
   c->prof.select_ms += c->t_select_ms;
   c->numnodes.clear();

@@ -195,6 +195,7 @@ int apc_mover_max_density(apc_context *c, double *out) {
 
 int apc_mover_velocity(apc_context *c, double dt, double c_vel, double *max_dv) {
   const int n = c->n, M = c->nc + c->nv;
+  APC_TRY(apc_velocities_sorted(c));
   APC_TRY(apc_ensure(c, &c->cell_of, (size_t)n + 1, nullptr));
   APC_CUDA_TRY(c, cudaMemsetAsync(c->cell_of, 0xff, sizeof(int) * (size_t)n, c->s));
   APC_CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->s));
@@ -227,6 +228,7 @@ int apc_mover_velocity(apc_context *c, double dt, double c_vel, double *max_dv) 
 
 int apc_mover_position(apc_context *c, double dt, double c_pos, double *max_dx) {
   const int n = c->n;
+  APC_TRY(apc_velocities_sorted(c));
   unsigned long long *mb = (unsigned long long *)(c->counters + 100);
   APC_CUDA_TRY(c, cudaMemsetAsync(mb, 0, sizeof(unsigned long long), c->s));
   const int G = std::max(1, std::min((n + 255) / 256, apc_sm_count(c) * 8));
@@ -250,6 +252,7 @@ int apc_mover_position(apc_context *c, double dt, double c_pos, double *max_dx) 
 // the error flag.
 int apc_mover_kick_drift(apc_context *c, double dt, double c_vel, double c_pos, double *max_dv, double *max_dx) {
   const int n = c->n, M = c->nc + c->nv;
+  APC_TRY(apc_velocities_sorted(c));
   APC_TRY(apc_ensure(c, &c->cell_of, (size_t)n + 1, nullptr));
   APC_CUDA_TRY(c, cudaMemsetAsync(c->cell_of, 0xff, sizeof(int) * (size_t)n, c->s));
   APC_CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->s));

@@ -58,9 +58,11 @@ __global__ void permute_particles(const uint32_t *__restrict__ perm, int n,
   ox[s] = x[p];
   oy[s] = y[p];
   oz[s] = z[p];
-  ovx[s] = vx[p];
-  ovy[s] = vy[p];
-  ovz[s] = vz[p];
+  if (vx) {  // velocities still in the caller's order are gathered at the kick instead
+    ovx[s] = vx[p];
+    ovy[s] = vy[p];
+    ovz[s] = vz[p];
+  }
   oid[s] = id[p];
 }
 
@@ -103,16 +105,19 @@ int apc_octree_build(apc_context *c) {
     uint64_t *tk = c->keys; c->keys = c->keys_alt; c->keys_alt = tk;
     uint32_t *tp = c->perm; c->perm = c->perm_alt; c->perm_alt = tp;
   }
-  permute_particles<<<G, T, 0, c->s>>>(c->perm, n, c->px, c->py, c->pz, c->pvx, c->pvy, c->pvz, c->pid,
-                                       c->qx, c->qy, c->qz, c->qvx, c->qvy, c->qvz, c->qid);
+  const bool vel = !c->vel_caller_order;
+  permute_particles<<<G, T, 0, c->s>>>(c->perm, n, c->px, c->py, c->pz, vel ? c->pvx : nullptr, c->pvy, c->pvz,
+                                       c->pid, c->qx, c->qy, c->qz, c->qvx, c->qvy, c->qvz, c->qid);
   apc_count_launch(c);
   APC_CUDA_TRY(c, cudaGetLastError());
   std::swap(c->px, c->qx);
   std::swap(c->py, c->qy);
   std::swap(c->pz, c->qz);
-  std::swap(c->pvx, c->qvx);
-  std::swap(c->pvy, c->qvy);
-  std::swap(c->pvz, c->qvz);
+  if (vel) {
+    std::swap(c->pvx, c->qvx);
+    std::swap(c->pvy, c->qvy);
+    std::swap(c->pvz, c->qvz);
+  }
   std::swap(c->pid, c->qid);
   return APC_OK;
 }

@@ -26,8 +26,9 @@
  *
  * Conventions: every call returns an apc_status (0 = success; never exit()).
  * Host pointers are caller-owned; device buffers are owned by the context.  Each
- * context issues its work on one CUDA stream of its own; a context is not
- * thread-safe, distinct contexts are independent.
+ * context issues its work on CUDA streams of its own (its main stream, plus a copy stream
+ * and a stream for the multigrid hierarchy that the main stream waits for); a context is
+ * not thread-safe, distinct contexts are independent.
  */
 #ifndef APCLOUD_GPU_H
 #define APCLOUD_GPU_H
@@ -135,7 +136,11 @@ int apc_destroy(apc_context *ctx);
 
 /* Particles: SoA FP64 host arrays of n_particles each.  apc_get_particles may be
  * given NULL for arrays the caller does not want; accelerations are those of the
- * last apc_move_velocity.  Particle order is the caller's order throughout. */
+ * last apc_move_velocity.  Particle order is the caller's order throughout.
+ * apc_set_particles queues the copies and returns: from pinned host memory they run
+ * asynchronously (the velocities on a copy stream beside the selection, as they are first
+ * read by the kick), and the arrays must stay unchanged until the next phase call
+ * (apc_select or apc_step) returns; pageable memory is staged during the call. */
 int apc_set_particles(apc_context *ctx, const double *x, const double *y, const double *z,
                       const double *vx, const double *vy, const double *vz);
 int apc_get_particles(apc_context *ctx, double *x, double *y, double *z, double *vx, double *vy,
