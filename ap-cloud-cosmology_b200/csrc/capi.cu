@@ -21,6 +21,11 @@
 // boxes of a batch).  Freed blocks stay in the pool for reuse until a context is
 // destroyed, which trims the pool's unused memory.  Reuse across streams waits for the
 // free to complete instead of adding a cross-stream dependency.
+// live contexts per device: the pool keeps its freed blocks while any context of the device
+// is alive (a new context reuses them instead of mapping fresh memory), and is trimmed when
+// the last one goes
+static std::atomic<int> g_live[64];
+
 cudaMemPool_t apc_device_pool(int dev) {
   static std::mutex mu;
   static cudaMemPool_t pools[64] = {};
@@ -157,7 +162,7 @@ void free_all(apc_context *c) {
     for (void *p : ptrs) apc_free(c, p);
     cudaStreamSynchronize(c->s);
   }
-  if (c->pool) cudaMemPoolTrimTo(c->pool, 0);
+  if (c->pool && g_live[c->dev].fetch_sub(1) == 1) cudaMemPoolTrimTo(c->pool, 0);
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
@@ -283,6 +288,7 @@ int apc_create(const apc_config *cfg, apc_context **out) {
   if (cudaEventCreateWithFlags(&c->vel_ev, cudaEventDisableTiming) != cudaSuccess) return fail(APC_ERR_CUDA);
   c->pool = apc_device_pool(c->dev);
   if (!c->pool) return fail(APC_ERR_CUDA);
+  g_live[c->dev].fetch_add(1);
   for (auto &e : c->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(APC_ERR_CUDA);
   for (auto &e : c->kev)
