@@ -506,11 +506,14 @@ int apc_solve_part_density(apc_context *c, double c_dens) {
   if (c->cfg.precision == APC_PREC_MIXED) {
     APC_TRY(apc_ensure(c, &c->a1f, (size_t)c->m_cap * c->ell_w, nullptr));
     APC_TRY(apc_ensure(c, &c->a2f, (size_t)c->m_cap * c->ell_w, nullptr));
-  } else if (c->cfg.precision == APC_PREC_FP64_MULTIGRID || c->cfg.precision == APC_PREC_MIXED_VCYCLE) {
+  } else if (c->cfg.precision == APC_PREC_FP64_MULTIGRID) {
     APC_TRY(apc_ensure(c, &c->a1d, (size_t)c->m_cap * c->ell_w, nullptr));
     APC_TRY(apc_ensure(c, &c->a2d, (size_t)c->m_cap * c->ell_w, nullptr));
-    if (c->cfg.precision == APC_PREC_MIXED_VCYCLE)
-      APC_TRY(apc_ensure(c, &c->a2f, (size_t)c->m_cap * c->ell_w, nullptr));
+  } else if (c->cfg.precision == APC_PREC_MIXED_VCYCLE) {
+    // FP32 density corrections; FP64 potential FGMRES over the FP32 V-cycle
+    APC_TRY(apc_ensure(c, &c->a1f, (size_t)c->m_cap * c->ell_w, nullptr));
+    APC_TRY(apc_ensure(c, &c->a2f, (size_t)c->m_cap * c->ell_w, nullptr));
+    APC_TRY(apc_ensure(c, &c->a2d, (size_t)c->m_cap * c->ell_w, nullptr));
   }
   apc_solve_stats &st = c->stats;
   if (overlap) APC_TRY(apc_mg_mark_assembled(c));

@@ -622,12 +622,14 @@ static void to_scaled(apc_context *c, cudaStream_t s, int which) {
   const int G = (int)std::min<size_t>((ell_count + 255) / 256, 8192);
   const double *a = which == 0 ? c->a1 : c->a2;
   const int prec = c->cfg.precision;
-  if (prec == APC_PREC_FP64_MULTIGRID || prec == APC_PREC_MIXED_VCYCLE) {
+  // FP64: the FP64 path's operators, and MIXED_VCYCLE's potential (its FGMRES is FP64)
+  if (prec == APC_PREC_FP64_MULTIGRID || (prec == APC_PREC_MIXED_VCYCLE && which == 1)) {
     ell_to_scaled<double><<<G, 256, 0, s>>>((size_t)c->m_cap, c->ell_w, n, a, which == 0 ? c->a1d : c->a2d);
     apc_count_launch(c);
   }
-  // FP32: the mixed path's operators, or the potential's V-cycle hierarchy of MIXED_VCYCLE
-  if (prec == APC_PREC_MIXED || (prec == APC_PREC_MIXED_VCYCLE && which == 1)) {
+  // FP32: the mixed paths' operators (MIXED_VCYCLE: the density's FP32 corrections and the
+  // potential's V-cycle hierarchy)
+  if (prec == APC_PREC_MIXED || prec == APC_PREC_MIXED_VCYCLE) {
     ell_to_scaled<float><<<G, 256, 0, s>>>((size_t)c->m_cap, c->ell_w, n, a, which == 0 ? c->a1f : c->a2f);
     apc_count_launch(c);
   }

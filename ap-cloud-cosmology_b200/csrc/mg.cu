@@ -2814,7 +2814,8 @@ static int ir_solve(apc_context *c, int which, bool use_mg, const double *val, c
 int apc_ir_solve(apc_context *c, int which, bool use_mg, const double *val, const double *b, double *x, double *r,
                  int restart, double rtol_in, int *its, double *rnorm, int *reason, int *refinements, int *levels,
                  int (*during)(apc_context *)) {
-  if (c->cfg.precision == APC_PREC_FP64_MULTIGRID || c->cfg.precision == APC_PREC_MIXED_VCYCLE)
+  // FP64 Krylov: the FP64 path, and MIXED_VCYCLE's potential; FP32 corrections otherwise
+  if (c->cfg.precision == APC_PREC_FP64_MULTIGRID || (c->cfg.precision == APC_PREC_MIXED_VCYCLE && which == 1))
     return ir_solve<double>(c, which, use_mg, val, which == 0 ? c->a1d : c->a2d, b, x, r, restart, rtol_in, its,
                             rnorm, reason, refinements, levels, during);
   return ir_solve<float>(c, which, use_mg, val, which == 0 ? c->a1f : c->a2f, b, x, r, restart, rtol_in, its, rnorm,

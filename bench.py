@@ -58,10 +58,10 @@ WORKLOAD = "lcdm128"
 # the timed arm's choices: (apc_precision, solver, arithmetic types)
 PRECISIONS = {
     "vcycle32": (_b.APC_PREC_MIXED_VCYCLE, "FP64 FGMRES(16) with FP64 Krylov vectors, right-preconditioned by an "
-                 "FP32 octree-multigrid V-cycle; density by FP64 GMRES(30)",
+                 "FP32 octree-multigrid V-cycle; density by FP32 GMRES(16) corrections in FP64 refinement",
                  "f64 Krylov / f32 multigrid V-cycle; f64 GFD moments and leapfrog"),
     "mixed": (_b.APC_PREC_MIXED, "FP64 iterative refinement around FP32 FGMRES(16) corrections with the FP32 "
-              "V-cycle; density by FP32 GMRES(30) corrections",
+              "V-cycle; density by FP32 GMRES(16) corrections",
               "f32 Krylov / f64 refinement, GFD moments and leapfrog"),
 }
 

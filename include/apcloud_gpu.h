@@ -64,9 +64,10 @@ typedef enum apc_precision {
                                  restarted (F)GMRES on the Jacobi-scaled systems, the potential
                                  right-preconditioned by the same octree multigrid, each cycle
                                  restarted from the true FP64 residual; same stopping test */
-  APC_PREC_MIXED_VCYCLE = 3 /* FP64_MULTIGRID's FP64 FGMRES with the V-cycle preconditioner in
-                               FP32 (hierarchy and smoothing sweeps); the density solve as in
-                               FP64_MULTIGRID; same stopping test */
+  APC_PREC_MIXED_VCYCLE = 3 /* the potential by FP64_MULTIGRID's FP64 FGMRES with the V-cycle
+                               preconditioner in FP32 (hierarchy and smoothing sweeps); the density
+                               as in MIXED (FP32 GMRES corrections in FP64 refinement); same
+                               stopping test */
 } apc_precision;
 
 typedef struct apc_config {
