@@ -135,7 +135,7 @@ struct apc_context {
   // ---- GFD / solver ----
   int lm = 17;
   int *st_idx = nullptr;     // lm per cell
-  double *st_dist = nullptr; // lm per cell
+  double *st_dist = nullptr; // lm per cell, filled on request (apc_get_stencils)
   double *gfd_x = nullptr;   // 9 x lm least-squares operator per cell
   int ell_w = 18;            // ELL width lm + 1
   int *ell_col = nullptr;    // [slot][row]
@@ -248,6 +248,7 @@ int apc_warm_save(apc_context *c);                       // warmstart.cu
 int apc_warm_guess(apc_context *c, int which, double *x);
 int apc_potential_rhs(apc_context *c, double c_pot);    // gfd.cu
 int apc_differentiate(apc_context *c, double c_field);  // gfd.cu
+int apc_gfd_stencil_dist(apc_context *c);  // gfd.cu: stencil distances into st_dist
 int apc_mover_velocity(apc_context *c, double dt, double c_vel, double *max_dv);  // mover.cu
 int apc_mover_position(apc_context *c, double dt, double c_pos, double *max_dx);  // mover.cu
 int apc_mover_kick_drift(apc_context *c, double dt, double c_vel, double c_pos, double *max_dv,

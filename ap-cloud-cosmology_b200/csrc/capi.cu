@@ -705,7 +705,10 @@ int apc_get_stencils(apc_context *c, int *idx, double *dist) {
   APC_TRY(check_ready(c, true, true, true));
   const size_t k = (size_t)(c->nc + c->nv) * c->lm;
   if (idx) APC_CUDA_TRY(c, cudaMemcpy(idx, c->st_idx, sizeof(int) * k, cudaMemcpyDeviceToHost));
-  if (dist) APC_CUDA_TRY(c, cudaMemcpy(dist, c->st_dist, sizeof(double) * k, cudaMemcpyDeviceToHost));
+  if (dist) {
+    APC_TRY(apc_gfd_stencil_dist(c));
+    APC_CUDA_TRY(c, cudaMemcpy(dist, c->st_dist, sizeof(double) * k, cudaMemcpyDeviceToHost));
+  }
   return APC_OK;
 }
 

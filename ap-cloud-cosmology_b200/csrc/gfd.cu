@@ -4,24 +4,27 @@
 // (solver.cpp:456-570), Solver::Solve_Potential's right-hand side (solver.cpp:236-259)
 // and Solver::Differentiate (solver.cpp:295-362).
 //
-// One warp per cell (computational or vacuum particle):
+// One warp per cell (computational or vacuum particle), except where noted:
 //  * Neighbour search.  The cell's Neigh24 entries are bucketed into 8 octants of a
 //    slightly rotated frame, then grown ring by ring through the neighbours' Neigh24
 //    lists until at least lm candidates exist.  Discovery order is kept exactly: one
 //    warp-wide batch per candidate, ordered appends by ballot, duplicates removed
 //    against the buckets and within the batch.  The rotation and distance products
 //    are evaluated without FMA contraction, in the reference's operand order, so the
-//    octant signs and distance ties are bit-identical.  Lane 0 then runs the
-//    reference's sort exactly:
+//    octant signs and distance ties are bit-identical.  A warp takes 16 consecutive
+//    cells this way and stages their lists in shared memory; then one lane per cell
+//    runs the reference's sort sequentially, exactly:
 //      - quicksort of octant 0 only (solver.cpp:557 passes the running offset);
 //      - 1e4^rank penalties within each octant;
 //      - a global quicksort with the same partition scheme, so ties break identically.
-//  * Least squares.  The lm x 9 weighted monomial matrix is factored by FP64 Householder
-//    QR held one row per lane, with warp-shuffle reductions.  The full operator
-//    X = R^-1 Q1^T diag(w) (9 x lm) is formed, i.e. the dgels solution for the
-//    lm right-hand sides of solver.cpp:101-106, and kept for the differentiation step.
-//    The second neighbour search and QR of Solver::Differentiate (solver.cpp:307-342)
-//    repeat the same computation, so they are not redone.
+//  * Least squares.  The lm x 9 weighted monomial matrix B (rows b_j) is solved through
+//    the Cholesky factor of its Gram matrix G = B^T B; a cell whose pivots show cond(B)
+//    over ~100 is solved by FP64 Householder QR instead
+//    (one row per lane, warp-shuffle reductions).  Either way the full operator
+//    X = G^-1 B^T W (9 x lm) is formed, i.e. the dgels solution for the lm right-hand
+//    sides of solver.cpp:101-106, and kept for the differentiation step.  The second
+//    neighbour search and QR of Solver::Differentiate (solver.cpp:307-342) repeat the
+//    same computation, so they are not redone.
 //  * Assembly.  A1 = I + (h^2/24) Lap and A2 = Lap go to slot-major ELL of width lm+1:
 //    slot 0 is the diagonal, slot 1+j neighbour j.  Row 0 of A2 is the Dirichlet pin of
 //    periodic boxes (solver.cpp:147-152).
@@ -49,7 +52,7 @@ struct GfdParams {
   const double *cx, *cy, *cz, *ch;
   const int *count, *type, *nb24, *nnb;
   int *st_idx;
-  double *st_dist, *gx;
+  double *gx;  // per cell the 9 x lm least-squares operator X
   double *scr_d;  // per search warp: kListCap sort keys and indices (lists over 32)
   int *scr_i;
   int *qr_list, *qr_count;  // cells for the Householder pass
@@ -115,90 +118,25 @@ __device__ void aquicksort(double *a, int *b, int l, int r, int limit) {
   }
 }
 
-// position of the (k+1)-th lowest set bit of mask (k < popc(mask)), by binary search
-__device__ __forceinline__ int select_bit(unsigned mask, int k) {
-  int p = 0;
-#pragma unroll
-  for (int s = 16; s > 0; s >>= 1) {
-    const int c = __popc(mask & ((1u << s) - 1u));
-    if (k >= c) {
-      k -= c;
-      mask >>= s;
-      p += s;
-    }
-  }
-  return p;
-}
-
-// aquicksort (solver.cpp:600-632) of n <= 32 (key, idx) pairs held one per lane, lane =
-// position.  Each partition is the reference's: with pivot a[l], the i scan stops at the
-// elements > pivot in (l, r] (g_0 < g_1 < ...), the j scan at the elements <= pivot in
-// [l, r] (s_0 > s_1 > ...); the k-th swap exchanges g_k and s_k while g_k < s_k, and
-// the pivot goes to j = s_0 (no swap) or max(s_K, g_{K-1}) after K swaps.
-// The result of a quicksort depends only on the partition applied to each sub-range, not
-// on the order in which disjoint sub-ranges are taken.  So every pass partitions all
-// unsorted sub-ranges at once: each lane finds its sub-range (the run of not-yet-final
-// positions around it) and takes its part in that sub-range's ballots and shuffles.  The
-// passes number the recursion depth, not the number of pivots.  Sub-ranges starting at
-// or beyond `limit` are left unsorted, as the reference leaves them; positions below the
-// limit end exactly as in the full sort, ties included.
-__device__ void warp_aquicksort(double &key, int &idx, int n, int limit, int lane) {
-  constexpr unsigned kAll = 0xffffffffu;
-  unsigned U = n >= 32 ? kAll : ((1u << n) - 1u);  // positions not yet final
-  const unsigned lim = limit >= 32 ? kAll : ((1u << limit) - 1u);
-  const unsigned below = (1u << lane) - 1u;       // positions < lane
-  const unsigned upto = (2u << lane) - 1u;        // positions <= lane (all bits for lane 31)
-  for (;;) {
-    unsigned R = U & ~(U << 1), E = U & ~(U >> 1);  // first and last positions of the runs
-    U &= ~(R & E & lim);                            // runs of one position are final
-    R = U & ~(U << 1);
-    E = U & ~(U >> 1);
-    const bool inU = (U >> lane) & 1u;
-    int start = 0, end = 0;
-    if (inU) {
-      start = 31 - __clz(R & upto);
-      end = __ffs(E & ~below) - 1;
-    }
-    const bool active = inU && start < limit && start < end;
-    if (!__any_sync(kAll, active)) break;
-    const double pivot = __shfl_sync(kAll, key, active ? start : lane);
-    const unsigned gt = __ballot_sync(kAll, active && lane > start && key > pivot);
-    const unsigned le = __ballot_sync(kAll, active && key <= pivot);
-    const unsigned seg = active ? (((2u << end) - 1u) & ~((1u << start) - 1u)) : 0u;
-    const unsigned gts = gt & seg, les = le & seg;
-    const int nle = __popc(les);
-    int partner = -1;
-    if ((gts >> lane) & 1u) {
-      const int k = __popc(gts & below);
-      if (k < nle) {
-        const int sk = select_bit(les, nle - 1 - k);
-        if (sk > lane) partner = sk;
-      }
-    }
-    const int K = __popc(__ballot_sync(kAll, partner >= 0) & seg);
-    if ((les >> lane) & 1u) {
-      const int k = nle - 1 - __popc(les & below);
-      if (k < K) partner = select_bit(gts, k);
-    }
-    const int src = partner >= 0 ? partner : lane;
-    key = __shfl_sync(kAll, key, src);
-    idx = __shfl_sync(kAll, idx, src);
-    int j = lane;
-    if (active) j = K == 0 ? 31 - __clz(les) : max(select_bit(les, nle - 1 - K), select_bit(gts, K - 1));
-    const int src2 = !active ? lane : (lane == start ? j : (lane == j ? start : lane));
-    key = __shfl_sync(kAll, key, src2);
-    idx = __shfl_sync(kAll, idx, src2);
-    U &= ~__ballot_sync(kAll, active && lane == j);
-  }
-}
-
-// neighbour search and sort, per warp
+// neighbour search, per warp: the candidates of the cell in hand, by octant bucket
 // 16-byte aligned so that bucket rows (kBucketCap ints, a multiple of 4) can be read as int4
 static_assert(kBucketCap % 4 == 0, "bucket rows are scanned four entries at a time");
 struct __align__(16) WarpSmem {
   int soff[32], sp[32];  // expansion ring: item offset and cell of each candidate
   int bidx[8][kBucketCap];
-  double bd2[8][kBucketCap];
+};
+
+// The search handles kChunk consecutive cells per warp: their lists (at most 32
+// candidates each, the usual case) are staged here, then lane q sorts cell q's list
+// sequentially.  Rows are padded to 33 entries so that lanes at the same position fall
+// in different banks.
+constexpr int kChunk = 16;
+constexpr int kStageLd = 33;
+struct SortStage {
+  double key[kChunk][kStageLd];
+  int idx[kChunk][kStageLd];
+  int nn[kChunk][8];
+  int staged[kChunk];
 };
 
 // Least squares, per warp: a slice of the dynamic shared memory laid out as
@@ -251,8 +189,7 @@ __device__ __forceinline__ double sq3(double wx, double wy, double wz) {
 
 // ordered append of the valid lanes' candidates to their octant buckets: a lane's slot is
 // its bucket's fill plus the number of lower valid lanes of the same octant
-__device__ __forceinline__ bool append(WarpSmem &S, int (&nn)[8], bool valid, int m, int oct,
-                                       double d2, int lane) {
+__device__ __forceinline__ bool append(WarpSmem &S, int (&nn)[8], bool valid, int m, int oct, int lane) {
   bool ok = true;
   const unsigned lt = (1u << lane) - 1u;
   // invalid lanes get keys no octant has, so they match only themselves
@@ -262,10 +199,7 @@ __device__ __forceinline__ bool append(WarpSmem &S, int (&nn)[8], bool valid, in
 #pragma unroll
     for (int o = 0; o < 8; ++o) base = (oct == o) ? nn[o] : base;
     const int p = base + __popc(peers & lt);
-    if (p < kBucketCap) {
-      S.bidx[oct][p] = m;
-      S.bd2[oct][p] = d2;
-    }
+    if (p < kBucketCap) S.bidx[oct][p] = m;
   }
 #pragma unroll
   for (int o = 0; o < 8; ++o) {
@@ -299,163 +233,206 @@ __device__ __forceinline__ void col_sums(const LsqView &S, const double (&val)[9
   __syncwarp();
 }
 
-// Phase 1, one warp per cell: the neighbour search and the reference's sort; the first lm
-// candidates go to st_idx.  A cell whose search fails raises its flag and gets its own
-// index in every slot, so that phase 2 stays in bounds (the step then fails).
+// Solver::searchneighboroctant's sort (solver.cpp:553-569) of one cell's candidate list,
+// given in bucket order (octant 0's entries, then octant 1's, ...) with raw squared
+// distances as keys, sequentially as the reference runs it: the quicksort of octant 0
+// (solver.cpp:557 passes the running offset, so only octant 0's run is sorted), the
+// 1e4^rank penalties within each octant, then the quicksort of the whole list.  Positions
+// below lm end as in the reference; the rest are not needed.
+__device__ void reference_sort(double *key, int *idx, const int *nn, int l, int lm) {
+  aquicksort(key, idx, 0, nn[0] - 1, nn[0]);
+  int k = 0;
+  for (int b = 0; b < 8; ++b) {
+    double penalty = 1.0;
+    for (int e = 0; e < nn[b]; ++e) {
+      key[k] = __dmul_rn(penalty, key[k]);
+      penalty = __dmul_rn(penalty, 10000.0);
+      ++k;
+    }
+  }
+  aquicksort(key, idx, 0, l - 1, lm);
+}
+
+// Phase 1: the neighbour search and the reference's sort; the first lm candidates go to
+// st_idx.  A warp takes kChunk consecutive cells.  For each in turn the whole warp finds
+// the candidates (rings of Neigh24 lists, discovery order kept per octant); a list of at
+// most 32 candidates is staged in shared memory.  Then lane q runs cell q's sort
+// (reference_sort), and the warp writes the chunk's stencils with coalesced stores.
+// Longer lists are sorted at once by lane 0 in a global scratch slice.  A cell whose
+// search fails raises its flag and gets its own index in every slot, so that phase 2
+// stays in bounds (the step then fails).
 __global__ void __launch_bounds__(32 * kSearchWarps) gfd_search(GfdParams P) {
   __shared__ WarpSmem smem[kSearchWarps];
+  __shared__ SortStage stage[kSearchWarps];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   WarpSmem &S = smem[w];
+  SortStage &T = stage[w];
   const int lm = P.lm;
-  for (int i0 = blockIdx.x * kSearchWarps + w; i0 < P.m; i0 += gridDim.x * kSearchWarps) {
-    int nn[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    bool ok = true;   // false once a bucket overflowed
-    bool few = false; // true when 5 expansions did not reach lm candidates
-    // ---- first ring: Neigh24 of i0 (solver.cpp:479-492), no de-duplication ----
-    {
-      const int cnt = P.nnb[i0];
-      const bool v = lane < cnt;
-      int m = v ? P.nb24[24 * (size_t)i0 + lane] : -1;
-      double wx = 0, wy = 0, wz = 0;
-      int oct = 0;
-      double d2 = 0;
-      if (v) {
-        offset_of(P, m, i0, wx, wy, wz);
-        oct = octant_of(P, wx, wy, wz);
-        d2 = sq3(wx, wy, wz);
-      }
-      ok &= append(S, nn, v, m, oct, d2, lane);
-    }
-    int l = 0;
-#pragma unroll
-    for (int o = 0; o < 8; ++o) l += nn[o];
-    // ---- expansion rings (solver.cpp:494-552) ----
-    int ite = 0;
-    while (ok && l < lm) {
-      // the reference exits on its sixth expansion whatever it finds (solver.cpp:544-550)
-      if (ite == 5) {
-        few = true;
-        break;
-      }
-      // the ring's (candidate, Neigh24 entry) items in the reference's order, processed 32
-      // at a time: candidates of the snapshot are < lm <= 32, so one lane holds each
-      int pre[9];
-      pre[0] = 0;
-#pragma unroll
-      for (int o = 0; o < 8; ++o) pre[o + 1] = pre[o] + nn[o];
-      const int lsnap = pre[8];
-      int pc = 0, cc = 0;
-      if (lane < lsnap) {
-        int b = 0;
-#pragma unroll
-        for (int o = 1; o < 8; ++o) b += (lane >= pre[o]) ? 1 : 0;
-        pc = S.bidx[b][lane - pre[b]];
-        cc = P.nnb[pc];
-      }
-      int incl = cc;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-      }
-      S.soff[lane] = incl - cc;
-      S.sp[lane] = pc;
-      const int total = __shfl_sync(0xffffffffu, incl, 31);
-      __syncwarp();
-      for (int f0 = 0; f0 < total && ok; f0 += 32) {
-        const int f = f0 + lane;
-        bool v = f < total;
-        int m = -1, oct = 0;
-        double d2 = 0;
+  const int gw = blockIdx.x * kSearchWarps + w;
+  for (int c0 = gw * kChunk; c0 < P.m; c0 += gridDim.x * kSearchWarps * kChunk) {
+    const int nq = min(kChunk, P.m - c0);
+    // the next cell's Neigh24 row is loaded while the current cell is searched
+    int cnt_next = P.nnb[c0];
+    int m_next = lane < cnt_next ? P.nb24[24 * (size_t)c0 + lane] : -1;
+    for (int q = 0; q < nq; ++q) {
+      const int i0 = c0 + q;
+      int nn[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      bool ok = true;   // false once a bucket overflowed
+      bool few = false; // true when 5 expansions did not reach lm candidates
+      // ---- first ring: Neigh24 of i0 (solver.cpp:479-492), no de-duplication ----
+      {
+        const int cnt = cnt_next;
+        const bool v = lane < cnt;
+        const int m = m_next;
+        if (q + 1 < nq) {
+          cnt_next = P.nnb[i0 + 1];
+          m_next = lane < cnt_next ? P.nb24[24 * (size_t)(i0 + 1) + lane] : -1;
+        }
+        int oct = 0;
         if (v) {
-          // the snapshot candidate whose Neigh24 list holds item f: the last q with
-          // soff[q] <= f (soff is a non-decreasing exclusive scan, soff[0] = 0 <= f), by
-          // binary search
-          int c = 0;
-          for (int step = 16; step > 0; step >>= 1)
-            if (c + step < lsnap && S.soff[c + step] <= f) c += step;
-          m = P.nb24[24 * (size_t)S.sp[c] + (f - S.soff[c])];
           double wx, wy, wz;
           offset_of(P, m, i0, wx, wy, wz);
           oct = octant_of(P, wx, wy, wz);
-          d2 = sq3(wx, wy, wz);
-          bool dup = (m == i0);
-          const int cap = min(nn[oct], kBucketCap);
-          // membership among the bucket's first cap entries, four per shared-memory load
-          for (int q = 0; q < cap && !dup; q += 4) {
-            const int4 e = *reinterpret_cast<const int4 *>(&S.bidx[oct][q]);
-            dup = (e.x == m) | ((q + 1 < cap) & (e.y == m)) | ((q + 2 < cap) & (e.z == m)) |
-                  ((q + 3 < cap) & (e.w == m));
-          }
-          v = !dup;
         }
-        // only the first lane holding a given index survives within the chunk
-        unsigned peers = __match_any_sync(0xffffffffu, v ? m : -1 - lane);
-        if (v && lane != __ffs(peers) - 1) v = false;
-        ok &= append(S, nn, v, m, oct, d2, lane);
+        ok &= append(S, nn, v, m, oct, lane);
       }
-      if (!ok) break;
-      ++ite;
-      l = 0;
+      int l = 0;
 #pragma unroll
       for (int o = 0; o < 8; ++o) l += nn[o];
-    }
-    if (few || !ok || l > P.sort_cap) {
-      if (lane == 0) atomicOr(P.err, few ? DERR_STENCIL_FEW : DERR_STENCIL_MANY);
-      if (lane < lm) P.st_idx[(size_t)i0 * lm + lane] = i0;
-      __syncwarp();
-      continue;
-    }
-    // ---- sorting (solver.cpp:553-569) ----
-    if (l <= 32 && nn[0] <= 32) {
-      // bucket 0, then the penalised list, by the warp-parallel quicksort
-      double key = 0.0;
-      int idx = 0;
-      if (lane < nn[0]) {
-        key = S.bd2[0][lane];
-        idx = S.bidx[0][lane];
-      }
-      warp_aquicksort(key, idx, nn[0], nn[0], lane);
-      if (lane < nn[0]) {
-        S.bd2[0][lane] = key;
-        S.bidx[0][lane] = idx;
-      }
-      __syncwarp();
-      if (lane < l) {
-        int b = 0, e = lane;
+      // ---- expansion rings (solver.cpp:494-552) ----
+      int ite = 0;
+      while (ok && l < lm) {
+        // the reference exits on its sixth expansion whatever it finds (solver.cpp:544-550)
+        if (ite == 5) {
+          few = true;
+          break;
+        }
+        // the ring's (candidate, Neigh24 entry) items in the reference's order, processed
+        // 32 at a time: candidates of the snapshot are < lm <= 32, so one lane holds each
+        int pre[9];
+        pre[0] = 0;
 #pragma unroll
-        for (int o = 0; o < 8; ++o) {
-          if (b == o && e >= nn[o]) {
-            e -= nn[o];
-            b = o + 1;
+        for (int o = 0; o < 8; ++o) pre[o + 1] = pre[o] + nn[o];
+        const int lsnap = pre[8];
+        int pc = 0, cc = 0;
+        if (lane < lsnap) {
+          int b = 0;
+#pragma unroll
+          for (int o = 1; o < 8; ++o) b += (lane >= pre[o]) ? 1 : 0;
+          pc = S.bidx[b][lane - pre[b]];
+          cc = P.nnb[pc];
+        }
+        int incl = cc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += t;
+        }
+        S.soff[lane] = incl - cc;
+        S.sp[lane] = pc;
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        __syncwarp();
+        for (int f0 = 0; f0 < total && ok; f0 += 32) {
+          const int f = f0 + lane;
+          bool v = f < total;
+          int m = -1, oct = 0;
+          if (v) {
+            // the snapshot candidate whose Neigh24 list holds item f: the last q with
+            // soff[q] <= f (soff is a non-decreasing exclusive scan, soff[0] = 0 <= f), by
+            // binary search
+            int c = 0;
+            for (int step = 16; step > 0; step >>= 1)
+              if (c + step < lsnap && S.soff[c + step] <= f) c += step;
+            m = P.nb24[24 * (size_t)S.sp[c] + (f - S.soff[c])];
+            double wx, wy, wz;
+            offset_of(P, m, i0, wx, wy, wz);
+            oct = octant_of(P, wx, wy, wz);
+            bool dup = (m == i0);
+            const int cap = min(nn[oct], kBucketCap);
+            // membership among the bucket's first cap entries, four per shared-memory load
+            for (int t = 0; t < cap && !dup; t += 4) {
+              const int4 e = *reinterpret_cast<const int4 *>(&S.bidx[oct][t]);
+              dup = (e.x == m) | ((t + 1 < cap) & (e.y == m)) | ((t + 2 < cap) & (e.z == m)) |
+                    ((t + 3 < cap) & (e.w == m));
+            }
+            v = !dup;
           }
+          // only the first lane holding a given index survives within the chunk
+          const unsigned peers = __match_any_sync(0xffffffffu, v ? m : -1 - lane);
+          if (v && lane != __ffs(peers) - 1) v = false;
+          ok &= append(S, nn, v, m, oct, lane);
         }
-        double penalty = 1.0;
-        for (int t = 0; t < e; ++t) penalty = __dmul_rn(penalty, 10000.0);
-        key = __dmul_rn(penalty, S.bd2[b][e]);
-        idx = S.bidx[b][e];
+        if (!ok) break;
+        ++ite;
+        l = 0;
+#pragma unroll
+        for (int o = 0; o < 8; ++o) l += nn[o];
       }
-      warp_aquicksort(key, idx, l, lm, lane);
-      if (lane < lm) P.st_idx[(size_t)i0 * lm + lane] = idx;
-    } else if (lane == 0) {
-      // longer lists: the reference's sequential sort by lane 0, on this warp's slice of
-      // a global scratch list
-      const size_t gw = (size_t)blockIdx.x * kSearchWarps + w;
-      double *ldist = P.scr_d + gw * kListCap;
-      int *lidx = P.scr_i + gw * kListCap;
-      aquicksort(S.bd2[0], S.bidx[0], 0, nn[0] - 1, nn[0]);
-      int k = 0;
-      for (int b = 0; b < 8; ++b) {
-        double penalty = 1.0;
-        for (int e = 0; e < nn[b]; ++e) {
-          lidx[k] = S.bidx[b][e];
-          ldist[k] = __dmul_rn(penalty, S.bd2[b][e]);
-          penalty = __dmul_rn(penalty, 10000.0);
-          ++k;
+      if (few || !ok || l > P.sort_cap) {
+        if (lane == 0) {
+          atomicOr(P.err, few ? DERR_STENCIL_FEW : DERR_STENCIL_MANY);
+          T.staged[q] = 0;
+        }
+        if (lane < lm) P.st_idx[(size_t)i0 * lm + lane] = i0;
+        __syncwarp();
+        continue;
+      }
+      // ---- the list in bucket order, keyed by the squared distances (recomputed from
+      //      the indices by the same operations as at discovery) ----
+      {
+        int v = 0;
+#pragma unroll
+        for (int o = 0; o < 8; ++o)
+          if (lane == o) v = nn[o];
+        if (lane < 8) T.nn[q][lane] = v;
+        __syncwarp();
+      }
+      if (l <= 32) {
+        if (lane < l) {
+          int b = 0, e = lane;
+#pragma unroll
+          for (int o = 0; o < 8; ++o) {
+            if (b == o && e >= nn[o]) {
+              e -= nn[o];
+              b = o + 1;
+            }
+          }
+          const int m = S.bidx[b][e];
+          double wx, wy, wz;
+          offset_of(P, m, i0, wx, wy, wz);
+          T.key[q][lane] = sq3(wx, wy, wz);
+          T.idx[q][lane] = m;
+        }
+        if (lane == 0) T.staged[q] = l;
+      } else {
+        // a longer list: lane 0 sorts it now, in this warp's slice of a global scratch list
+        if (lane == 0) {
+          double *ldist = P.scr_d + (size_t)gw * kListCap;
+          int *lidx = P.scr_i + (size_t)gw * kListCap;
+          int k = 0;
+          for (int b = 0; b < 8; ++b) {
+            for (int e = 0; e < nn[b]; ++e) {
+              const int m = S.bidx[b][e];
+              double wx, wy, wz;
+              offset_of(P, m, i0, wx, wy, wz);
+              ldist[k] = sq3(wx, wy, wz);
+              lidx[k] = m;
+              ++k;
+            }
+          }
+          reference_sort(ldist, lidx, T.nn[q], l, lm);
+          for (int k2 = 0; k2 < lm; ++k2) P.st_idx[(size_t)i0 * lm + k2] = lidx[k2];
+          T.staged[q] = 0;
         }
       }
-      aquicksort(ldist, lidx, 0, l - 1, lm);
-      for (int k = 0; k < lm; ++k) P.st_idx[(size_t)i0 * lm + k] = lidx[k];
+      __syncwarp();
+    }
+    // ---- the staged lists: lane q sorts cell q's, then coalesced stores of the chunk ----
+    if (lane < nq && T.staged[lane] > 0) reference_sort(T.key[lane], T.idx[lane], T.nn[lane], T.staged[lane], lm);
+    __syncwarp();
+    for (int t = lane; t < nq * lm; t += 32) {
+      const int q = t / lm;
+      if (T.staged[q] > 0) P.st_idx[(size_t)c0 * lm + t] = T.idx[q][t - q * lm];
     }
     __syncwarp();
   }
@@ -627,7 +604,6 @@ __global__ void __launch_bounds__(32 * kWarps, QR ? 4 : 6) gfd_lsq(GfdParams P) 
     if (act) {
 #pragma unroll
       for (int k = 0; k < 9; ++k) X[k * lm + lane] = weight * y[k];
-      P.st_dist[(size_t)i0 * lm + lane] = dist;
     }
     // ---- rows of A1, A2 and the density rhs (solver.cpp:116-172) ----
     const double lap = act ? (weight * y[3] + weight * y[4]) + weight * y[5] : 0.0;
@@ -713,24 +689,24 @@ __global__ void potential_rhs_dirichlet(const double *__restrict__ rho, const do
 
 // -------------------------------------------------------------- differentiate
 
-// gradient / Hessian of phi: y = X (phi_j - phi_i) c_field (solver.cpp:315-358), one warp per cell
-__global__ void __launch_bounds__(256) differentiate_kernel(int m, int lm, int nc_nv,
-                                                            const int *__restrict__ st_idx,
-                                                            const double *__restrict__ gx,
-                                                            const double *__restrict__ phi,
-                                                            const double *__restrict__ h,
+// gradient / Hessian of phi: y = X (phi_j - phi_i) c_field (solver.cpp:315-358), one warp
+// per cell.  X is stored by the least squares: rebuilding its columns here from a stored
+// Cholesky factor (360 B per cell instead of 1,224) was measured slower, since the
+// rows' weights and the per-lane solves cost more than the bytes they save.
+__global__ void __launch_bounds__(256) differentiate_kernel(GfdParams P, const double *__restrict__ phi,
                                                             double c_field, double *deriv) {
   const int lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
-  for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < m; i += gridDim.x * wpb) {
+  const int lm = P.lm;
+  for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < P.m; i += gridDim.x * wpb) {
     const double p4 = phi[i];
     double r = 0.0;
     if (lane < lm) {
-      const int k = st_idx[(size_t)i * lm + lane];
-      const double p1 = k < nc_nv ? phi[k] : 0.0;
+      const int k = P.st_idx[(size_t)i * lm + lane];
+      const double p1 = k < P.nc_nv ? phi[k] : 0.0;
       r = (p1 - p4) * c_field;
     }
-    const double *X = gx + (size_t)i * 9 * lm;
+    const double *X = P.gx + (size_t)i * 9 * lm;
     double out = 0.0;
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
@@ -738,10 +714,44 @@ __global__ void __launch_bounds__(256) differentiate_kernel(int m, int lm, int n
       if (lane == k) out = t;
     }
     if (lane < 9) {
-      const double hi = h[i];
+      const double hi = P.ch[i];
       deriv[(size_t)i * 9 + lane] = lane < 3 ? out / hi : out / hi / hi;
     }
   }
+}
+
+// the stencil distances |x_mj - x_i| (solver.cpp:567-569), as the least squares compute them
+__global__ void stencil_dist_kernel(GfdParams P, double *__restrict__ dist) {
+  const long long total = (long long)P.m * P.lm;
+  for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < total;
+       f += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(f / P.lm);
+    double wx, wy, wz;
+    offset_of(P, P.st_idx[f], i, wx, wy, wz);
+    dist[f] = sqrt(sq3(wx, wy, wz));
+  }
+}
+
+// the geometry, stencil and operator fields of GfdParams for context c
+GfdParams gfd_params(apc_context *c) {
+  GfdParams P{};
+  const int M = c->nc + c->nv;
+  P.m = M;
+  P.lm = c->lm;
+  P.bc = c->cfg.bc;
+  P.nc_nv = M;
+  P.sort_cap = std::min(kListCap, 10 * c->lm);
+  for (int d = 0; d < 3; ++d) {
+    P.L[d] = c->cfg.box[2 * d + 1] - c->cfg.box[2 * d];
+    P.halfL[d] = c->cfg.bc == 1 ? 0.5 * P.L[d] : 1e308;
+  }
+  for (int k = 0; k < 9; ++k) P.rot[k] = c->rot[k];
+  P.e4 = std::exp(-4.0);
+  P.inv_1me4 = 1.0 / (1.0 - P.e4);
+  P.cx = c->cx; P.cy = c->cy; P.cz = c->cz; P.ch = c->ch;
+  P.count = c->ccount; P.type = c->ctype; P.nb24 = c->nb24; P.nnb = c->nnb;
+  P.st_idx = c->st_idx; P.gx = c->gfd_x;
+  return P;
 }
 
 }  // namespace
@@ -757,7 +767,6 @@ int apc_gfd_assemble(apc_context *c, double c_dens, int (*during)(apc_context *)
   // a hierarchy built beside an earlier density solve belongs to the old operator
   apc_mg_clear_prebuilt(c);
   APC_TRY(apc_ensure(c, &c->st_idx, mc * lm, nullptr));
-  APC_TRY(apc_ensure(c, &c->st_dist, mc * lm, nullptr));
   APC_TRY(apc_ensure(c, &c->gfd_x, mc * 9 * lm, nullptr));
   c->ell_w = lm + 1;
   if ((size_t)c->m_cap < mc) {
@@ -774,27 +783,13 @@ int apc_gfd_assemble(apc_context *c, double c_dens, int (*during)(apc_context *)
   APC_TRY(apc_ensure(c, &c->deriv, ld * 9, nullptr));
   APC_CUDA_TRY(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->s));
   APC_CUDA_TRY(c, cudaMemsetAsync(c->bcrhs, 0, sizeof(double) * M, c->s));
-  GfdParams P;
-  P.m = M;
-  P.lm = lm;
-  P.bc = c->cfg.bc;
-  P.nc_nv = M;
-  P.sort_cap = std::min(kListCap, 10 * lm);
-  for (int d = 0; d < 3; ++d) {
-    P.L[d] = c->cfg.box[2 * d + 1] - c->cfg.box[2 * d];
-    P.halfL[d] = c->cfg.bc == 1 ? 0.5 * P.L[d] : 1e308;
-  }
-  for (int k = 0; k < 9; ++k) P.rot[k] = c->rot[k];
-  P.e4 = std::exp(-4.0);
-  P.inv_1me4 = 1.0 / (1.0 - P.e4);
+  GfdParams P = gfd_params(c);
   P.c_dens = c_dens;
-  P.cx = c->cx; P.cy = c->cy; P.cz = c->cz; P.ch = c->ch;
-  P.count = c->ccount; P.type = c->ctype; P.nb24 = c->nb24; P.nnb = c->nnb;
-  P.st_idx = c->st_idx; P.st_dist = c->st_dist; P.gx = c->gfd_x;
   P.ell_col = c->ell_col; P.a1 = c->a1; P.a2 = c->a2; P.rhs = c->rhs;
   P.ld = ld;
   P.err = c->d_err;
-  const int sblocks = std::max(1, std::min((M + kSearchWarps - 1) / kSearchWarps, apc_sm_count(c) * 32));
+  const int sblocks =
+      std::max(1, std::min((M + kSearchWarps * kChunk - 1) / (kSearchWarps * kChunk), apc_sm_count(c) * 6));
   APC_TRY(apc_ensure(c, &c->gfd_scr_d, (size_t)sblocks * kSearchWarps * kListCap, nullptr));
   APC_TRY(apc_ensure(c, &c->gfd_scr_i, (size_t)sblocks * kSearchWarps * kListCap, nullptr));
   P.scr_d = c->gfd_scr_d;
@@ -855,9 +850,20 @@ int apc_potential_rhs(apc_context *c, double c_pot) {
 int apc_differentiate(apc_context *c, double c_field) {
   const int M = c->nc + c->nv;
   const int G = std::max(1, std::min((M + 7) / 8, apc_sm_count(c) * 16));
-  differentiate_kernel<<<G, 256, 0, c->s>>>(M, c->lm, M, c->st_idx, c->gfd_x, c->potential, c->ch,
-                                            c_field, c->deriv);
+  differentiate_kernel<<<G, 256, 0, c->s>>>(gfd_params(c), c->potential, c_field, c->deriv);
   apc_count_launch(c);
   APC_CUDA_TRY(c, cudaGetLastError());
+  return APC_OK;
+}
+
+int apc_gfd_stencil_dist(apc_context *c) {
+  const int M = c->nc + c->nv;
+  APC_TRY(apc_ensure(c, &c->st_dist, (size_t)M * c->lm + 1, nullptr));
+  const long long total = (long long)M * c->lm;
+  const int G = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, apc_sm_count(c) * 6));
+  stencil_dist_kernel<<<G, 256, 0, c->s>>>(gfd_params(c), c->st_dist);
+  apc_count_launch(c);
+  APC_CUDA_TRY(c, cudaGetLastError());
+  APC_CUDA_TRY(c, cudaStreamSynchronize(c->s));
   return APC_OK;
 }

@@ -792,6 +792,34 @@ static void run_gmres(int n, const int *rp, const int *ci, const double *v, cons
  * (182-218), Solve_Potential (220-293), Differentiate (295-362).  Returns 0, or the
  * negative code of the neighbour search / a positive LAPACK info where the reference
  * calls exit(). */
+/* Solver::Differentiate (solver.cpp:295-362) of a given potential: per cell the search
+ * and the weighted rows again, then the least-squares solve (dgels) for the differences
+ * (phi_j - phi_i) c_field; deriv9 gets the gradient / h and the Hessian / h^2.  Work
+ * buffers as in solve_all (b needs lm doubles here). */
+static int differentiate(apcor *o, const double *phi, double c_field, double *deriv9, int *neigh,
+                         double *distance, int nbuf, const double *A, double *B, double *b, double *w) {
+  const int lm = o->lm, ln = 9, M = o->nc + o->nv;
+  for (int i = 0; i < M; ++i) {
+    int s = search_octant(o, i, neigh, distance, nbuf, A);
+    if (s) return s;
+    gfd_rows(o, i, neigh, distance, B, w);
+    double p4 = phi[i];
+    for (int j = 0; j < lm; ++j) {
+      int k = neigh[j];
+      double p1 = k < M ? phi[k] : 0.0;
+      b[j] = w[j] * (p1 - p4) * c_field;
+    }
+    int info = oracle_dgels_rowmajor(lm, ln, 1, B, ln, b, 1);
+    if (info > 0) return info;
+    double h = o->ch[i];
+    double *d = deriv9 + 9 * (size_t)i;
+    d[0] = b[0] / h; d[1] = b[1] / h; d[2] = b[2] / h;
+    d[3] = b[3] / h / h; d[4] = b[4] / h / h; d[5] = b[5] / h / h;
+    d[6] = b[6] / h / h; d[7] = b[7] / h / h; d[8] = b[8] / h / h;
+  }
+  return 0;
+}
+
 static int solve_all(apcor *o, double c_dens, double c_pot, double c_field) {
   const int lm = o->lm, ln = 9, M = o->nc + o->nv;
   double A[9];
@@ -868,24 +896,7 @@ static int solve_all(apcor *o, double c_dens, double c_pot, double c_field) {
     keep_matrix(1, M, rp2, ci2, v2);
   }
   /* Differentiate (solver.cpp:295-362) */
-  for (int i = 0; i < M; ++i) {
-    int s = search_octant(o, i, neigh, distance, nbuf, A);
-    if (s) { rc = s; goto fail; }
-    gfd_rows(o, i, neigh, distance, B, w);
-    double p4 = o->potential[i];
-    for (int j = 0; j < lm; ++j) {
-      int k = neigh[j];
-      double p1 = k < M ? o->potential[k] : 0.0;
-      b[j] = w[j] * (p1 - p4) * c_field;
-    }
-    int info = oracle_dgels_rowmajor(lm, ln, 1, B, ln, b, 1);
-    if (info > 0) { rc = info; goto fail; }
-    double h = o->ch[i];
-    double *d = o->deriv + 9 * (size_t)i;
-    d[0] = b[0] / h; d[1] = b[1] / h; d[2] = b[2] / h;
-    d[3] = b[3] / h / h; d[4] = b[4] / h / h; d[5] = b[5] / h / h;
-    d[6] = b[6] / h / h; d[7] = b[7] / h / h; d[8] = b[8] / h / h;
-  }
+  rc = differentiate(o, o->potential, c_field, o->deriv, neigh, distance, nbuf, A, B, b, w);
 fail:
   rm_free(&A1);
   rm_free(&A2);
@@ -998,6 +1009,22 @@ int apcor_solve(void *h, double c_dens, double c_pot, double c_field) {
   double t0 = wall();
   int rc = solve_all(o, c_dens, c_pot, c_field);
   o->t_solve += wall() - t0;
+  return rc;
+}
+
+int apcor_differentiate(void *h, const double *potential, double c_field, double *deriv9) {
+  apcor *o = (apcor *)h;
+  const int lm = o->lm;
+  double A[9];
+  rotation(A);
+  int nbuf = 16 * lm > 8 * 10 * lm ? 16 * lm : 8 * 10 * lm;
+  int *neigh = (int *)calloc((size_t)nbuf, sizeof(int));
+  double *distance = (double *)calloc((size_t)nbuf, sizeof(double));
+  double *B = (double *)malloc(sizeof(double) * lm * 9);
+  double *b = (double *)malloc(sizeof(double) * lm * lm);
+  double *w = (double *)malloc(sizeof(double) * lm);
+  int rc = differentiate(o, potential, c_field, deriv9, neigh, distance, nbuf, A, B, b, w);
+  free(neigh); free(distance); free(B); free(b); free(w);
   return rc;
 }
 

@@ -27,6 +27,9 @@ int apcor_get_keys(void *h, uint64_t *keys, int *index);
 int apcor_octree_levels(void *h, int *numnodes);
 int apcor_solve(void *h, double c_dens, double c_pot, double c_field);
 int apcor_get_fields(void *h, double *density, double *potential, double *deriv9);
+/* Solver::Differentiate (solver.cpp:295-362) of the given potential on the selected cells
+ * (after apcor_select); returns 0 or the search / least-squares failure code */
+int apcor_differentiate(void *h, const double *potential, double c_field, double *deriv9);
 int apcor_get_stencils(void *h, int *idx17, double *dist17);
 int apcor_solve_stats(int k, int *its, double *rnorm, int *reason, double *seconds);
 int apcor_solve_count(void);

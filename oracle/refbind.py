@@ -65,6 +65,7 @@ def _bind_common(lib, prefix):
         ("octree_levels", C.c_int, [C.c_void_p, _ip]),
         ("solve", C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
         ("get_fields", C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+        ("differentiate", C.c_int, [C.c_void_p, _dp, C.c_double, _dp]),
         ("solve_stats", C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
                                   C.POINTER(C.c_int), C.POINTER(C.c_double)]),
         ("solve_count", C.c_int, []),
@@ -165,6 +166,18 @@ class CpuPath:
         rho, phi, der = np.zeros(m), np.zeros(m), np.zeros(9 * m)
         self.f["get_fields"](self.h, rho, phi, der)
         return Fields(rho, phi, der.reshape(m, 9))
+
+    def differentiate(self, potential: np.ndarray, c_field: float = -1.0) -> np.ndarray:
+        """Solver::Differentiate (solver.cpp:295-362) of a given potential on the selected
+        cells (the oracle only)."""
+        if "differentiate" not in self.f:
+            raise NotImplementedError("differentiate: oracle only")
+        m = self.cells().m
+        d = np.zeros(9 * m)
+        rc = self.f["differentiate"](self.h, np.ascontiguousarray(potential, dtype=np.float64), c_field, d)
+        if rc != 0:
+            raise RuntimeError(f"differentiate failed: {rc}")
+        return d.reshape(m, 9)
 
     def stencils(self) -> np.ndarray:
         """(M, lm) GFD neighbour indices of the last solve, in search order.  For the

@@ -16,10 +16,11 @@ Bars:
     order in which Build_Linear_System inserts row i of A1, solver.cpp:116-125);
   * matrices A1 and A2 (solver.cpp:116-171) - the same sparsity, every value within
     MATRIX_RTOL of the largest entry of its row;
-  * fields where the reference's GMRES(30) converges (ball32k, eds64) - density,
-    potential and the 9 derivatives within FIELD_RTOL (max norm relative to the field's
-    max) and accelerations within ACC_RMS (RMS relative) on the FP64 path, accelerations
-    within MIXED_ACC_RMS on the mixed path.  Two solutions that both meet rtol 1e-10
+  * fields where the reference's GMRES(30) converges (ball32k, eds64) - density and
+    potential within FIELD_RTOL (max norm relative to the field's max), the 9 derivatives
+    within DERIV_RTOL, and accelerations within ACC_RMS (RMS relative) on the FP64 path,
+    accelerations within MIXED_ACC_RMS on the mixed path; the differentiation alone, the
+    reference's least squares applied to the GPU's potential, within DIFF_RTOL.  Two solutions that both meet rtol 1e-10
     differ by up to cond(D^-1 A) 1e-10: at 20-33k cells the reference's own GMRES, run
     with its sums in another order (threaded), moves the potential by 1.9e-9 and the
     derivatives by 1.5e-8, so these bars sit above that spread, and the sharp check is
@@ -43,6 +44,17 @@ from apcloud.controller import for_config  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 FIELD_RTOL = 1e-7
+# The derivatives carry the potential's spread between two converged solves, amplified
+# about 30x by the second differences: at ball32k step 10 two builds whose matrices differ
+# in the last ulp of some entries stop GMRES at other iterates, with the potential 1.4e-9
+# and 3.5e-9 from the reference's and the derivatives 4.4e-8 and 1.1e-7.  The bar allows
+# the potential's FIELD_RTOL spread at a tenth of that amplification; DIFF_RTOL below
+# holds the differentiation itself sharply.
+DERIV_RTOL = 1e-6
+# the GPU's derivatives against the reference's least squares (the oracle's
+# Solver::Differentiate) applied to the GPU's own potential: no solver spread, only the
+# Cholesky-versus-Householder rounding of the operator X
+DIFF_RTOL = 1e-10
 ACC_RMS = 1e-7
 MATRIX_RTOL = 1e-12
 MIXED_ACC_RMS = 1e-6
@@ -165,7 +177,15 @@ def _compare_converged_step(cfg, state, ref, t, m_ref, acc_ref):
     for name in ("density", "potential", "deriv"):
         e = _rel(getattr(fg, name), getattr(fr, name))
         report[name] = e
-        assert e <= FIELD_RTOL, (name, e)
+        assert e <= (DERIV_RTOL if name == "deriv" else FIELD_RTOL), (name, e)
+    # the differentiation alone, free of the two solves' spread: the reference's least
+    # squares (the oracle's Solver::Differentiate) applied to the GPU's own potential
+    o = refbind.CpuPath("oracle", parts, cfg.depth, cfg.gfd_c, cfg.lm)
+    assert o.select() == m_ref
+    d_o = o.differentiate(fg.potential, k["c_field"])
+    o.close()
+    report["deriv_of_gpu_potential"] = _rel(fg.deriv, d_o)
+    assert report["deriv_of_gpu_potential"] <= DIFF_RTOL, report["deriv_of_gpu_potential"]
     gp.move_velocity(cfg.delta_a, k["c_vel"])
     report["fp64_acc_rms"] = _acc_rms(gp.particles()[6:9], acc_ref)
     assert report["fp64_acc_rms"] <= ACC_RMS
