@@ -520,21 +520,24 @@ __global__ void __launch_bounds__(32 * kWarps, QR ? 4 : 6) gfd_lsq(GfdParams P) 
       continue;
     }
     if (!QR) {
-      // lane j: y = G^-1 b_j by the two triangular solves
+      // lane j: y = G^-1 b_j by the two triangular solves.  The factor is read where it is
+      // used (volatile): hoisting its 45 broadcast loads ahead of the dependent chain of
+      // multiply-adds gains nothing and made the kernel spill its registers.
       double t9[9];
+      const volatile double *VL = S.L, *VI = S.inv;
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
         double t = b[k];
 #pragma unroll
-        for (int j = 0; j < k; ++j) t -= S.L[k * 9 + j] * t9[j];
-        t9[k] = t * S.inv[k];
+        for (int j = 0; j < k; ++j) t -= VL[k * 9 + j] * t9[j];
+        t9[k] = t * VI[k];
       }
 #pragma unroll
       for (int k = 8; k >= 0; --k) {
         double t = t9[k];
 #pragma unroll
-        for (int j = k + 1; j < 9; ++j) t -= S.L[j * 9 + k] * y[j];
-        y[k] = t * S.inv[k];
+        for (int j = k + 1; j < 9; ++j) t -= VL[j * 9 + k] * y[j];
+        y[k] = t * VI[k];
       }
     } else {
     // ---- Householder QR, one row per lane ----
