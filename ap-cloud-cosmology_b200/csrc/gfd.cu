@@ -56,6 +56,7 @@ struct GfdParams {
   double *scr_d;  // per search warp: kListCap sort keys and indices (lists over 32)
   int *scr_i;
   int *qr_list, *qr_count;  // cells for the Householder pass
+  int *chunk_next;          // the search's next unclaimed cell (zeroed before its launch)
   int *ell_col;
   double *a1, *a2, *rhs;
   size_t ld;  // ELL leading dimension (row capacity)
@@ -270,7 +271,13 @@ __global__ void __launch_bounds__(32 * kSearchWarps, 8) gfd_search(GfdParams P) 
   SortStage &T = stage[w];
   const int lm = P.lm;
   const int gw = blockIdx.x * kSearchWarps + w;
-  for (int c0 = gw * kChunk; c0 < P.m; c0 += gridDim.x * kSearchWarps * kChunk) {
+  // chunks are claimed from a counter: late in a run the cost per cell varies widely along
+  // the Morton order, and a fixed assignment left warps with runs of costly cells
+  for (;;) {
+    int c0 = 0;
+    if (lane == 0) c0 = atomicAdd(P.chunk_next, kChunk);
+    c0 = __shfl_sync(0xffffffffu, c0, 0);
+    if (c0 >= P.m) break;
     const int nq = min(kChunk, P.m - c0);
     // the next cell's Neigh24 row is loaded while the current cell is searched
     int cnt_next = P.nnb[c0];
@@ -389,8 +396,10 @@ __global__ void __launch_bounds__(32 * kSearchWarps, 8) gfd_search(GfdParams P) 
         __syncwarp();
       }
       if (l <= 32) {
+        int e = lane, m = i0;
+        double d2 = 0.0;
         if (lane < l) {
-          int b = 0, e = lane;
+          int b = 0;
 #pragma unroll
           for (int o = 0; o < 8; ++o) {
             if (b == o && e >= nn[o]) {
@@ -398,33 +407,46 @@ __global__ void __launch_bounds__(32 * kSearchWarps, 8) gfd_search(GfdParams P) 
               b = o + 1;
             }
           }
-          const int m = S.bidx[b][e];
+          m = S.bidx[b][e];
           double wx, wy, wz;
           offset_of(P, m, i0, wx, wy, wz);
-          T.key[q][lane] = sq3(wx, wy, wz);
+          d2 = sq3(wx, wy, wz);
+          T.key[q][lane] = d2;
           T.idx[q][lane] = m;
         }
         if (lane == 0) T.staged[q] = l;
       } else {
-        // a longer list: lane 0 sorts it now, in this warp's slice of a global scratch list
-        if (lane == 0) {
-          double *ldist = P.scr_d + (size_t)gw * kListCap;
-          int *lidx = P.scr_i + (size_t)gw * kListCap;
-          int k = 0;
-          for (int b = 0; b < 8; ++b) {
-            for (int e = 0; e < nn[b]; ++e) {
-              const int m = S.bidx[b][e];
-              double wx, wy, wz;
-              offset_of(P, m, i0, wx, wy, wz);
-              ldist[k] = sq3(wx, wy, wz);
-              lidx[k] = m;
-              ++k;
+        // a longer list: the warp writes it in bucket order to this warp's slice of a global
+        // scratch list, 32 entries at a time; lane 0 sorts it now
+        double *ldist = P.scr_d + (size_t)gw * kListCap;
+        int *lidx = P.scr_i + (size_t)gw * kListCap;
+        int pre[9];
+        pre[0] = 0;
+#pragma unroll
+        for (int o = 0; o < 8; ++o) pre[o + 1] = pre[o] + nn[o];
+        for (int p = lane; p < l; p += 32) {
+          int b = 0, base = 0;
+#pragma unroll
+          for (int o = 1; o < 8; ++o)
+            if (p >= pre[o]) {
+              b = o;
+              base = pre[o];
             }
-          }
+          const int m = S.bidx[b][p - base];
+          double wx, wy, wz;
+          offset_of(P, m, i0, wx, wy, wz);
+          ldist[p] = sq3(wx, wy, wz);
+          lidx[p] = m;
+        }
+        __threadfence_block();
+        __syncwarp();
+        if (lane == 0) {
           reference_sort(ldist, lidx, T.nn[q], l, lm);
-          for (int k2 = 0; k2 < lm; ++k2) P.st_idx[(size_t)i0 * lm + k2] = lidx[k2];
           T.staged[q] = 0;
         }
+        __threadfence_block();
+        __syncwarp();
+        if (lane < lm) P.st_idx[(size_t)i0 * lm + lane] = lidx[lane];
       }
       __syncwarp();
     }
@@ -801,7 +823,9 @@ int apc_gfd_assemble(apc_context *c, double c_dens, int (*during)(apc_context *)
   APC_TRY(apc_ensure(c, &c->gfd_qr, (size_t)M + 1, nullptr));
   P.qr_list = c->gfd_qr;
   P.qr_count = c->counters + 112;
+  P.chunk_next = c->counters + 114;
   const int blocks = std::max(1, std::min((M + kWarps - 1) / kWarps, apc_sm_count(c) * 16));
+  APC_CUDA_TRY(c, cudaMemsetAsync(P.chunk_next, 0, sizeof(int), c->s));
   APC_CUDA_TRY(c, cudaEventRecord(c->gev[0], c->s));
   gfd_search<<<sblocks, 32 * kSearchWarps, 0, c->s>>>(P);
   const size_t lsq_bytes = sizeof(double) * lsq_doubles(lm) * kWarps;

@@ -138,3 +138,4 @@ def test_sort_tail_gives_the_reference_stencil(seed):
         rd, rn = reference_tail(d2, idx, nn)
         kd, kn = kernel_tail(d2, idx, nn, 17)
         assert kn[:17] == rn[:17] and kd[:17] == rd[:17], (d2, idx, nn)
+
