@@ -467,7 +467,7 @@ __global__ void __launch_bounds__(32 * kSearchWarps, 8) gfd_search(GfdParams P) 
 // queued.  QR = true: the queued cells by Householder QR.  The two instantiations keep
 // their register budgets apart, so the fast path runs at higher occupancy.
 template <bool QR>
-__global__ void __launch_bounds__(32 * kWarps, QR ? 4 : 6) gfd_lsq(GfdParams P) {
+__global__ void __launch_bounds__(32 * kWarps, QR ? 4 : 7) gfd_lsq(GfdParams P) {
   extern __shared__ __align__(16) double lsq_smem[];  // kWarps slices of lsq_doubles(lm)
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int lm = P.lm;
