@@ -690,19 +690,33 @@ __global__ void mass_partials(const double *__restrict__ rho, const double *__re
   }
 }
 
-// rhs = (rho - mean_volume_weighted(rho)) * c_pot (solver.cpp:244-259)
-__global__ void potential_rhs_kernel(const double *__restrict__ rho, int m, const double *partial,
-                                     int nparts, double c_pot, double *rhs) {
-  __shared__ double mean;
-  if (threadIdx.x == 0) {
-    double a = 0.0, b = 0.0;
-    for (int k = 0; k < nparts; ++k) {
-      a += partial[2 * k];
-      b += partial[2 * k + 1];
-    }
-    mean = a / b;
+// the volume-weighted mean density sum(rho h^3) / sum(h^3) (solver.cpp:244-251) from the
+// blocks' partial sums, by one block in a fixed tree order (one thread summing them in
+// sequence, in every block of the next kernel, took longer than the kernel's own work)
+__global__ void mass_mean(const double *__restrict__ partial, int nparts, double *mean) {
+  __shared__ double s1[256], s2[256];
+  double a = 0.0, b = 0.0;
+  for (int k = threadIdx.x; k < nparts; k += blockDim.x) {
+    a += partial[2 * k];
+    b += partial[2 * k + 1];
   }
+  s1[threadIdx.x] = a;
+  s2[threadIdx.x] = b;
   __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      s1[threadIdx.x] += s1[threadIdx.x + o];
+      s2[threadIdx.x] += s2[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *mean = s1[0] / s2[0];
+}
+
+// rhs = (rho - mean_volume_weighted(rho)) * c_pot (solver.cpp:244-259)
+__global__ void potential_rhs_kernel(const double *__restrict__ rho, int m, const double *__restrict__ mean_p,
+                                     double c_pot, double *rhs) {
+  const double mean = *mean_p;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
     rhs[i] = (rho[i] - mean) * c_pot;
 }
@@ -718,13 +732,16 @@ __global__ void potential_rhs_dirichlet(const double *__restrict__ rho, const do
 // gradient / Hessian of phi: y = X (phi_j - phi_i) c_field (solver.cpp:315-358), one warp
 // per cell.  X is stored by the least squares: rebuilding its columns here from a stored
 // Cholesky factor (360 B per cell instead of 1,224) was measured slower, since the
-// rows' weights and the per-lane solves cost more than the bytes they save.
-__global__ void __launch_bounds__(256) differentiate_kernel(GfdParams P, const double *__restrict__ phi,
-                                                            double c_field, double *deriv) {
-  const int lane = threadIdx.x & 31;
-  const int wpb = blockDim.x >> 5;
+// rows' weights and the per-lane solves cost more than the bytes they save.  Lane j forms
+// the products X_kj (phi_j - phi_i) c_field in shared memory; lane k < 9 then sums row k in
+// stencil order (one short chain instead of nine five-level shuffle trees).
+constexpr int kDiffWarps = 8;
+__global__ void __launch_bounds__(32 * kDiffWarps) differentiate_kernel(GfdParams P, const double *__restrict__ phi,
+                                                                       double c_field, double *deriv) {
+  __shared__ double prod[kDiffWarps][9][33];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int lm = P.lm;
-  for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < P.m; i += gridDim.x * wpb) {
+  for (int i = blockIdx.x * kDiffWarps + w; i < P.m; i += gridDim.x * kDiffWarps) {
     const double p4 = phi[i];
     double r = 0.0;
     if (lane < lm) {
@@ -733,16 +750,18 @@ __global__ void __launch_bounds__(256) differentiate_kernel(GfdParams P, const d
       r = (p1 - p4) * c_field;
     }
     const double *X = P.gx + (size_t)i * 9 * lm;
-    double out = 0.0;
+    if (lane < lm) {
 #pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      const double t = warp_sum(lane < lm ? X[k * lm + lane] * r : 0.0);
-      if (lane == k) out = t;
+      for (int k = 0; k < 9; ++k) prod[w][k][lane] = X[k * lm + lane] * r;
     }
+    __syncwarp();
     if (lane < 9) {
+      double t = 0.0;
+      for (int j = 0; j < lm; ++j) t += prod[w][lane][j];
       const double hi = P.ch[i];
-      deriv[(size_t)i * 9 + lane] = lane < 3 ? out / hi : out / hi / hi;
+      deriv[(size_t)i * 9 + lane] = lane < 3 ? t / hi : t / hi / hi;
     }
+    __syncwarp();
   }
 }
 
@@ -865,8 +884,9 @@ int apc_potential_rhs(apc_context *c, double c_pot) {
   if (c->cfg.bc == 1) {
     APC_TRY(apc_ensure(c, &c->reduce_buf, (size_t)2 * G + 2, nullptr));
     mass_partials<<<G, 256, 0, c->s>>>(c->density, c->ch, M, c->reduce_buf);
-    potential_rhs_kernel<<<G, 256, 0, c->s>>>(c->density, M, c->reduce_buf, G, c_pot, c->rhs);
-    apc_count_launch(c, 2);
+    mass_mean<<<1, 256, 0, c->s>>>(c->reduce_buf, G, c->reduce_buf + 2 * G);
+    potential_rhs_kernel<<<G, 256, 0, c->s>>>(c->density, M, c->reduce_buf + 2 * G, c_pot, c->rhs);
+    apc_count_launch(c, 3);
   } else {
     potential_rhs_dirichlet<<<G, 256, 0, c->s>>>(c->density, c->bcrhs, M, c_pot, c->rhs);
     apc_count_launch(c);
@@ -877,8 +897,8 @@ int apc_potential_rhs(apc_context *c, double c_pot) {
 
 int apc_differentiate(apc_context *c, double c_field) {
   const int M = c->nc + c->nv;
-  const int G = std::max(1, std::min((M + 7) / 8, apc_sm_count(c) * 16));
-  differentiate_kernel<<<G, 256, 0, c->s>>>(gfd_params(c), c->potential, c_field, c->deriv);
+  const int G = std::max(1, std::min((M + kDiffWarps - 1) / kDiffWarps, apc_sm_count(c) * 16));
+  differentiate_kernel<<<G, 32 * kDiffWarps, 0, c->s>>>(gfd_params(c), c->potential, c_field, c->deriv);
   apc_count_launch(c);
   APC_CUDA_TRY(c, cudaGetLastError());
   return APC_OK;

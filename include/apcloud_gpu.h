@@ -193,7 +193,10 @@ int apc_get_keys(apc_context *ctx, uint64_t *keys, int *index);
 int apc_get_octree_levels(apc_context *ctx, int *numnodes);
 /* Density, Potential and p_x..p_yz (9 per cell, in that order) of cells 0..nc+nv-1. */
 int apc_get_fields(apc_context *ctx, double *density, double *potential, double *deriv9);
-/* GFD stencil of each cell: lm neighbour indices and distances, in search order. */
+/* GFD stencil of each cell: lm neighbour indices and distances, in search order (either
+ * pointer may be NULL).  The distances are not kept by the step: asking for them computes
+ * them from the indices on the device, as the least squares do, and needs a device buffer
+ * of lm doubles per cell. */
 int apc_get_stencils(apc_context *ctx, int *idx, double *dist);
 int apc_get_solve_stats(apc_context *ctx, apc_solve_stats *stats);
 /* Matrix A1 (which = 0) or A2 (which = 1) in CSR, columns sorted per row.  Call with
