@@ -456,8 +456,8 @@ def run_ours(args) -> dict:
                 "traffic": (traffic_per_cell * cells) if traffic_per_cell else None,
                 "algorithmic_bytes_per_launch": gfd_bytes, "bytes_per_cell": GFD_BYTES_PER_CELL,
                 "cells": cells, "ms_per_launch": gfd_ms,
-                "note": "issue bound (the exact per-cell quicksort and the FP64 least squares); the HBM "
-                        "fraction is low by nature of the kernels"}
+                "note": "latency- and issue-bound (the exact per-cell neighbour search and sort, the FP64 "
+                        "least squares); the HBM fraction is low by nature of the kernels"}
     # ---- roofline of the potential solve (one graph, or one persistent kernel, per step): its
     #      algorithmic bytes from the library's model (apc_profile.mg_bytes) over its CUDA-event
     #      time ----
