@@ -193,3 +193,21 @@ def test_gmres_petsc_semantics(oracle_lib):
     lib.oracle_gmres_csr(n, rp.ctypes.data, ci.ctypes.data, vals.ctypes.data, b.ctypes.data, x.ctypes.data,
                          C.byref(p2))
     assert p2.reason == -3 and p2.its == 7
+
+
+@pytest.mark.parametrize("path", CASES, ids=[os.path.basename(c)[:-4] for c in CASES])
+def test_oracle_differentiation_of_a_given_potential(oracle_lib, path):
+    """The oracle's Solver::Differentiate applied to a given potential (the checker behind
+    the GPU's full-size differentiation test): on the reference's own potential it gives the
+    reference's derivatives (golden) to the bit, and on the oracle's potential its solve's
+    derivatives to the bit."""
+    g = np.load(path)
+    r = refbind.CpuPath("oracle", _parts(g), int(g["depth"]), float(g["gfd_c"]), int(g["lm"]))
+    r.set_gmres(int(g["restart"]), float(g["rtol"]))
+    r.select()
+    d_ref = r.differentiate(g["potential"], -1.0)
+    assert np.array_equal(d_ref.reshape(-1), g["deriv"].reshape(-1))
+    r.solve(float(g["c_dens"]), float(g["c_pot"]), -1.0)
+    f = r.fields()
+    assert np.array_equal(r.differentiate(f.potential, -1.0), f.deriv)
+    r.close()
